@@ -1,0 +1,140 @@
+/*
+ * simcraft_fluid_capi.h -- C ABI of the B200 (sm_100a) implementation of
+ * SimCraft FluidSim's FLIP/PIC step and MIC(0)-PCG pressure projection.
+ *
+ * Plain C types only: pointers, sizes and POD structs.  Every entry point
+ * returns an int status (SC_OK == 0, negative on error) and never throws;
+ * sc_context_last_error() gives a message for the last failure.
+ *
+ * Array layout everywhere is the reference's spatify::LinearHashXYZ order
+ * (Spatify/include/Spatify/hash.h:25): idx(i,j,k) = k + j*sz + i*sy*sz, z fastest.
+ * Face grids: u (nx+1,ny,nz), v (nx,ny+1,nz), w (nx,ny,nz+1).
+ * Neighbour-coefficient arrays are passed as 6 pointers in the reference's
+ * Directions order {Left, Right, Up, Down, Front, Back}
+ * (FluidSim/src/cpu/project-solver.cc:7-14).
+ *
+ * Functions suffixed _host take host pointers (copy semantics, synchronous);
+ * functions suffixed _device take device pointers and are ordered on the
+ * context's stream.
+ */
+#ifndef SIMCRAFT_FLUID_CAPI_H
+#define SIMCRAFT_FLUID_CAPI_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SC_OK 0
+#define SC_ERR_INVALID -1      /* bad argument */
+#define SC_ERR_CUDA -2         /* CUDA runtime error */
+#define SC_ERR_NOMEM -3        /* device allocation failed */
+#define SC_ERR_BREAKDOWN -4    /* PCG breakdown (s.As == 0) */
+#define SC_ERR_NOT_CONVERGED -5
+#define SC_ERR_TIMEOUT -6      /* a bounded device wait gave up */
+#define SC_ERR_ASYMMETRIC -7   /* matrix fails checkSystemSymmetry */
+#define SC_ERR_NONFINITE -8    /* NaN/Inf reached a reduction */
+#define SC_ERR_UNSUPPORTED -9
+
+/* Stopping criteria for the pressure solve. */
+#define SC_CRIT_ABS_LINF 0     /* reference: ||r||_inf < tol (project-solver.cc:334) */
+#define SC_CRIT_REL_L2 1       /* ||r||_2 / ||b||_2 < tol */
+
+/* Solver precision. */
+#define SC_PREC_FP64 0         /* plain FP64 MIC(0)-PCG */
+#define SC_PREC_MIXED 1        /* FP32 inner MIC-PCG + FP64 defect correction */
+
+/* Final state of a solve (sc_pcg_stats.status). */
+#define SC_DONE_CONVERGED 1
+#define SC_DONE_MAXITER 2
+#define SC_DONE_BREAKDOWN 3
+
+typedef struct sc_context sc_context;
+typedef struct sc_pcg sc_pcg;
+
+/* Library identity. */
+int sc_version(void);
+const char* sc_status_string(int status);
+
+/* A context owns one CUDA stream on one device.  Replaces nothing in the
+ * reference (which is single-threaded host code); every handle below is bound
+ * to a context. */
+int sc_context_create(int device, sc_context** out);
+void sc_context_destroy(sc_context* ctx);
+/* Use an external stream (cudaStream_t passed as void*); NULL restores the
+ * context's own stream. */
+int sc_context_set_stream(sc_context* ctx, void* stream);
+void* sc_context_stream(sc_context* ctx);
+int sc_context_synchronize(sc_context* ctx);
+const char* sc_context_last_error(sc_context* ctx);
+
+/* ---------------------------------------------------------------------------
+ * Pressure solver: CgSolver3D + ModifiedIncompleteCholesky3D
+ * (FluidSim/include/FluidSim/cpu/project-solver.h:71-131).
+ */
+typedef struct {
+  double tol;          /* CgSolver3D::tolerance, 1e-6 (project-solver.h:129) */
+  int max_iter;        /* CgSolver3D::max_iterations, 300 (project-solver.h:130) */
+  int criterion;       /* SC_CRIT_*; the reference uses SC_CRIT_ABS_LINF */
+  int precision;       /* SC_PREC_* */
+  double mic_tau;      /* ModifiedIncompleteCholesky3D tuning, 0.97 (project-solver.h:83) */
+  double mic_sigma;    /* ModifiedIncompleteCholesky3D safety, 0.25 (project-solver.h:84) */
+  double inner_rtol;   /* mixed: residual reduction asked of each FP32 inner solve */
+  int max_outer;       /* mixed: maximum defect-correction passes */
+  int check_symmetry;  /* verify A_Right(p) == A_Left(p+x) etc. on upload */
+  int true_residual;   /* recompute ||b - A p|| in FP64 after the solve */
+} sc_pcg_options;
+
+typedef struct {
+  int iterations;        /* FP64: the reference's `iter` counter; mixed: inner iterations */
+  int outer;             /* mixed: defect-correction passes */
+  int status;            /* SC_DONE_* */
+  double residual;       /* stopping measure at exit (what CgSolver3D::solve returns) */
+  double true_rel_l2;    /* ||b - A p||_2 / ||b||_2 recomputed in FP64 */
+  double true_linf;      /* ||b - A p||_inf recomputed in FP64 */
+  double ms;             /* device time of the solve */
+  double sym_err;        /* max asymmetry found when check_symmetry is set */
+} sc_pcg_stats;
+
+/* Defaults equal to the reference's constants. */
+void sc_pcg_default_options(sc_pcg_options* opt);
+
+/* CgSolver3D(w, h, d) + setPreconditioner(ModifiedIncompleteCholesky)
+ * (project-solver.h:100-121).  opt may be NULL for the defaults. */
+int sc_pcg_create(sc_context* ctx, int nx, int ny, int nz, const sc_pcg_options* opt,
+                  sc_pcg** out);
+void sc_pcg_destroy(sc_pcg* pcg);
+int sc_pcg_set_options(sc_pcg* pcg, const sc_pcg_options* opt);
+
+/* CgSolver3D::solve(Adiag, Aneighbour, rhs, active, pg) -> residual
+ * (project-solver.h:107-111, project-solver.cc:308-346), host arrays.
+ * an: 6 arrays in Directions order; only Left/Down/Back are read unless
+ * check_symmetry is set (the matrix must be symmetric, project-solver.cc:41-57). */
+int sc_pcg_solve_host(sc_pcg* pcg, const double* adiag, const double* const* an,
+                      const double* rhs, const uint8_t* active, double* pg,
+                      sc_pcg_stats* stats);
+/* Same with device pointers (an: host array of 6 device pointers). */
+int sc_pcg_solve_device(sc_pcg* pcg, const double* adiag, const double* const* an,
+                        const double* rhs, const uint8_t* active, double* pg,
+                        sc_pcg_stats* stats);
+/* Split form for repeated solves of one resident system: upload (host or
+ * device pointers), solve on the device, then read the pressure back. */
+int sc_pcg_upload(sc_pcg* pcg, const double* adiag, const double* const* an,
+                  const double* rhs, const uint8_t* active, int device_pointers);
+int sc_pcg_upload_rhs(sc_pcg* pcg, const double* rhs, int device_pointers);
+int sc_pcg_solve_resident(sc_pcg* pcg, sc_pcg_stats* stats);
+int sc_pcg_download(sc_pcg* pcg, double* pg, int device_pointer);
+
+/* ModifiedIncompleteCholesky3D::precond(Adiag, Aneighbour, r, active, z)
+ * (project-solver.h:88-92, project-solver.cc:230-306) on the system last
+ * uploaded to `pcg`; r and z are device pointers in the reference layout. */
+int sc_pcg_precond_device(sc_pcg* pcg, const double* r, double* z);
+/* applyCompressedMatrix (project-solver.cc:16-39) on the uploaded system:
+ * b = A x, device pointers. */
+int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIMCRAFT_FLUID_CAPI_H */

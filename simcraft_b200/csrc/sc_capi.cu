@@ -1,0 +1,272 @@
+// sc_capi.cu -- extern "C" boundary.  No C++ exception or CUDA type crosses it.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/simcraft_fluid_capi.h"
+#include "sc_pcg.cuh"
+
+struct sc_context {
+  sc::Context c;
+  cudaStream_t own = nullptr;
+};
+
+struct sc_pcg {
+  sc_context* ctx;
+  sc::PcgSolver* solver;
+};
+
+namespace {
+
+sc::PcgOptions to_internal(const sc_pcg_options* o) {
+  sc::PcgOptions p;
+  if (!o) return p;
+  p.tol = o->tol;
+  p.max_iter = o->max_iter;
+  p.criterion = o->criterion;
+  p.precision = o->precision;
+  p.tau = o->mic_tau;
+  p.sigma = o->mic_sigma;
+  p.inner_rtol = o->inner_rtol;
+  p.max_outer = o->max_outer;
+  p.check_symmetry = o->check_symmetry;
+  p.true_residual = o->true_residual;
+  return p;
+}
+
+void to_public(const sc::PcgStats& s, sc_pcg_stats* o) {
+  if (!o) return;
+  o->iterations = s.iterations;
+  o->outer = s.outer;
+  o->status = s.status;
+  o->residual = s.residual;
+  o->true_rel_l2 = s.true_rel_l2;
+  o->true_linf = s.true_linf;
+  o->ms = s.ms;
+  o->sym_err = s.sym_err;
+}
+
+int validate_options(const sc_pcg_options* o) {
+  if (!o) return SC_OK;
+  if (!(o->tol >= 0.0) || o->max_iter < 1 || o->criterion < 0 || o->criterion > 1 ||
+      o->precision < 0 || o->precision > 1 || !(o->inner_rtol > 0.0) || o->max_outer < 1)
+    return SC_ERR_INVALID;
+  return SC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sc_version(void) { return 10000; }
+
+const char* sc_status_string(int status) {
+  switch (status) {
+    case SC_OK: return "ok";
+    case SC_ERR_INVALID: return "invalid argument";
+    case SC_ERR_CUDA: return "CUDA error";
+    case SC_ERR_NOMEM: return "out of device memory";
+    case SC_ERR_BREAKDOWN: return "PCG breakdown";
+    case SC_ERR_NOT_CONVERGED: return "not converged";
+    case SC_ERR_TIMEOUT: return "device wait timed out";
+    case SC_ERR_ASYMMETRIC: return "matrix is not symmetric";
+    case SC_ERR_NONFINITE: return "non-finite value";
+    case SC_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+int sc_context_create(int device, sc_context** out) {
+  if (!out) return SC_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return SC_ERR_CUDA;
+  if (cudaSetDevice(device) != cudaSuccess) return SC_ERR_CUDA;
+  sc_context* c = new (std::nothrow) sc_context();
+  if (!c) return SC_ERR_NOMEM;
+  c->c.device = device;
+  cudaDeviceGetAttribute(&c->c.sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return SC_ERR_CUDA;
+  }
+  c->c.stream = c->own;
+  *out = c;
+  return SC_OK;
+}
+
+void sc_context_destroy(sc_context* ctx) {
+  if (!ctx) return;
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+}
+
+int sc_context_set_stream(sc_context* ctx, void* stream) {
+  if (!ctx) return SC_ERR_INVALID;
+  ctx->c.stream = stream ? (cudaStream_t)stream : ctx->own;
+  return SC_OK;
+}
+
+void* sc_context_stream(sc_context* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+int sc_context_synchronize(sc_context* ctx) {
+  if (!ctx) return SC_ERR_INVALID;
+  cudaError_t e = cudaStreamSynchronize(ctx->c.stream);
+  if (e != cudaSuccess) return ctx->c.set_error(SC_ERR_CUDA, cudaGetErrorString(e));
+  return SC_OK;
+}
+
+const char* sc_context_last_error(sc_context* ctx) {
+  return ctx ? ctx->c.last_error.c_str() : "no context";
+}
+
+void sc_pcg_default_options(sc_pcg_options* o) {
+  if (!o) return;
+  sc::PcgOptions d;
+  o->tol = d.tol;
+  o->max_iter = d.max_iter;
+  o->criterion = d.criterion;
+  o->precision = d.precision;
+  o->mic_tau = d.tau;
+  o->mic_sigma = d.sigma;
+  o->inner_rtol = d.inner_rtol;
+  o->max_outer = d.max_outer;
+  o->check_symmetry = d.check_symmetry;
+  o->true_residual = d.true_residual;
+}
+
+int sc_pcg_create(sc_context* ctx, int nx, int ny, int nz, const sc_pcg_options* opt,
+                  sc_pcg** out) {
+  if (!ctx || !out || nx < 1 || ny < 1 || nz < 1) return SC_ERR_INVALID;
+  *out = nullptr;
+  if (validate_options(opt)) return ctx->c.set_error(SC_ERR_INVALID, "invalid options");
+  if ((int64_t)nx * ny * nz >= ((int64_t)1 << 31))
+    return ctx->c.set_error(SC_ERR_UNSUPPORTED, "grid too large (int indices, as the reference)");
+  cudaSetDevice(ctx->c.device);
+  sc::PcgSolver* s = new (std::nothrow) sc::PcgSolver(&ctx->c, nx, ny, nz, to_internal(opt));
+  if (!s) return SC_ERR_NOMEM;
+  if (s->status()) {
+    int st = s->status();
+    delete s;
+    return ctx->c.set_error(st == -3 ? SC_ERR_NOMEM : SC_ERR_CUDA, "pcg create failed");
+  }
+  sc_pcg* h = new (std::nothrow) sc_pcg{ctx, s};
+  if (!h) {
+    delete s;
+    return SC_ERR_NOMEM;
+  }
+  *out = h;
+  return SC_OK;
+}
+
+void sc_pcg_destroy(sc_pcg* pcg) {
+  if (!pcg) return;
+  cudaStreamSynchronize(pcg->ctx->c.stream);
+  delete pcg->solver;
+  delete pcg;
+}
+
+int sc_pcg_set_options(sc_pcg* pcg, const sc_pcg_options* opt) {
+  if (!pcg || !opt) return SC_ERR_INVALID;
+  if (validate_options(opt)) return pcg->ctx->c.set_error(SC_ERR_INVALID, "invalid options");
+  sc::PcgOptions o = to_internal(opt);
+  bool pivots_change = o.tau != pcg->solver->options().tau ||
+                       o.sigma != pcg->solver->options().sigma ||
+                       o.precision != pcg->solver->options().precision;
+  pcg->solver->set_options(o);
+  if (pivots_change) pcg->solver->mark_system_changed();
+  return SC_OK;
+}
+
+static int map_status(int rc) {
+  switch (rc) {
+    case 0: return SC_OK;
+    case -1: return SC_ERR_INVALID;
+    case -3: return SC_ERR_NOMEM;
+    case -6: return SC_ERR_TIMEOUT;
+    case -7: return SC_ERR_ASYMMETRIC;
+    case -8: return SC_ERR_NONFINITE;
+    default: return SC_ERR_CUDA;
+  }
+}
+
+static int solve_status(const sc::PcgStats& st) {
+  if (st.status == sc::DONE_BREAKDOWN) return SC_ERR_BREAKDOWN;
+  return SC_OK;  // like the reference, non-convergence is reported through the residual
+}
+
+int sc_pcg_upload(sc_pcg* pcg, const double* adiag, const double* const* an, const double* rhs,
+                  const uint8_t* active, int device_pointers) {
+  if (!pcg || !adiag || !an || !rhs || !active || !an[0] || !an[3] || !an[5])
+    return SC_ERR_INVALID;
+  cudaSetDevice(pcg->ctx->c.device);
+  return map_status(pcg->solver->upload(adiag, an, rhs, active, device_pointers != 0));
+}
+
+int sc_pcg_upload_rhs(sc_pcg* pcg, const double* rhs, int device_pointers) {
+  if (!pcg || !rhs) return SC_ERR_INVALID;
+  cudaSetDevice(pcg->ctx->c.device);
+  return map_status(pcg->solver->upload_rhs(rhs, device_pointers != 0));
+}
+
+int sc_pcg_solve_resident(sc_pcg* pcg, sc_pcg_stats* stats) {
+  if (!pcg) return SC_ERR_INVALID;
+  cudaSetDevice(pcg->ctx->c.device);
+  sc::PcgStats st;
+  int rc = map_status(pcg->solver->solve(&st));
+  to_public(st, stats);
+  if (rc) return rc;
+  return solve_status(st);
+}
+
+int sc_pcg_download(sc_pcg* pcg, double* pg, int device_pointer) {
+  if (!pcg || !pg) return SC_ERR_INVALID;
+  cudaSetDevice(pcg->ctx->c.device);
+  return map_status(pcg->solver->download_pressure(pg, device_pointer != 0));
+}
+
+static int solve_common(sc_pcg* pcg, const double* adiag, const double* const* an,
+                        const double* rhs, const uint8_t* active, double* pg,
+                        sc_pcg_stats* stats, int device) {
+  int rc = sc_pcg_upload(pcg, adiag, an, rhs, active, device);
+  if (rc) return rc;
+  sc::PcgStats st;
+  rc = map_status(pcg->solver->solve(&st));
+  to_public(st, stats);
+  if (rc) return rc;
+  rc = map_status(pcg->solver->download_pressure(pg, device != 0));
+  if (rc) return rc;
+  if (device) {
+    cudaError_t e = cudaStreamSynchronize(pcg->ctx->c.stream);
+    if (e != cudaSuccess) return pcg->ctx->c.set_error(SC_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return solve_status(st);
+}
+
+int sc_pcg_solve_host(sc_pcg* pcg, const double* adiag, const double* const* an,
+                      const double* rhs, const uint8_t* active, double* pg,
+                      sc_pcg_stats* stats) {
+  if (!pg) return SC_ERR_INVALID;
+  return solve_common(pcg, adiag, an, rhs, active, pg, stats, 0);
+}
+
+int sc_pcg_solve_device(sc_pcg* pcg, const double* adiag, const double* const* an,
+                        const double* rhs, const uint8_t* active, double* pg,
+                        sc_pcg_stats* stats) {
+  if (!pg) return SC_ERR_INVALID;
+  return solve_common(pcg, adiag, an, rhs, active, pg, stats, 1);
+}
+
+int sc_pcg_precond_device(sc_pcg* pcg, const double* r, double* z) {
+  if (!pcg || !r || !z) return SC_ERR_INVALID;
+  cudaSetDevice(pcg->ctx->c.device);
+  return map_status(pcg->solver->precond_only(r, z));
+}
+
+int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b) {
+  if (!pcg || !x || !b) return SC_ERR_INVALID;
+  cudaSetDevice(pcg->ctx->c.device);
+  return map_status(pcg->solver->apply_only(x, b));
+}
+
+}  // extern "C"

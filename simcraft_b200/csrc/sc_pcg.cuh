@@ -1,0 +1,162 @@
+// sc_pcg.cuh -- MIC(0)-preconditioned CG pressure solver (FP64 and mixed FP32/FP64).
+//
+// Host-side interface of the solver behind CgSolver3D::solve
+// (FluidSim/include/FluidSim/cpu/project-solver.h:100-131,
+//  FluidSim/src/cpu/project-solver.cc:308-346) and
+// ModifiedIncompleteCholesky3D::precond (project-solver.cc:230-306).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "sc_common.cuh"
+
+namespace sc {
+
+constexpr int kTY = 8;  // rows (y) per wavefront tile; the tile is 32 (x) by kTY (y)
+
+struct Context {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+  int set_error(int code, const std::string& msg) {
+    last_error = msg;
+    return code;
+  }
+};
+
+enum { CRIT_ABS_LINF = 0, CRIT_REL_L2 = 1 };
+enum { PREC_FP64 = 0, PREC_MIXED = 1 };
+enum { DONE_RUNNING = 0, DONE_CONVERGED = 1, DONE_MAXITER = 2, DONE_BREAKDOWN = 3 };
+
+struct PcgOptions {
+  double tol = 1e-6;       // project-solver.h:129
+  int max_iter = 300;      // project-solver.h:130
+  int criterion = CRIT_ABS_LINF;
+  int precision = PREC_FP64;
+  double tau = 0.97, sigma = 0.25;  // project-solver.h:83-84
+  double inner_rtol = 1e-4;  // mixed: relative reduction asked of each FP32 inner solve
+  int max_outer = 20;        // mixed: defect-correction passes
+  int chunk = 8;             // PCG iterations per CUDA-graph launch
+  int check_symmetry = 0;    // verify Right/Up/Front == shifted Left/Down/Back
+  int true_residual = 1;     // recompute ||b - A p|| in FP64 at the end
+};
+
+struct PcgStats {
+  int iterations = 0;        // the reference's `iter` (FP64); total inner iterations (mixed)
+  int outer = 0;             // mixed: defect-correction passes
+  int status = 0;            // DONE_* of the final (inner) solve
+  double residual = 0;       // stopping measure at exit (recurrence residual)
+  double true_rel_l2 = 0;    // ||b - A p||_2 / ||b||_2 in FP64
+  double true_linf = 0;      // ||b - A p||_inf in FP64
+  double ms = 0;             // device time of the solve (events)
+  double sym_err = 0;        // max |A_R(p) - A_L(p+x)| etc. when checked
+};
+
+// Device scalars shared by the kernels of one PCG run.
+struct PcgScalars {
+  double sigma, alpha, beta;
+  double res, bnorm, tol, rscale;
+  double rn2, rinf, sdotz;
+  int iter, max_iter, done, criterion;
+  unsigned err;
+  unsigned count;  // last-block counter
+  int first;       // 1 until the first preconditioner application has set sigma
+  int pad;
+};
+
+// Wavefront scheduling state (one per sweep kernel; reset by the kernel's last CTA).
+struct WaveSync {
+  int* progress;      // per tile: completed steps
+  int* ticket;        // next tile ticket
+  int* exits;         // CTAs that found no more tiles
+  int2* order_fwd;    // ticket -> tile (X,Y) for forward sweeps
+};
+
+template <class T>
+struct SysArrays {  // one precision's copy of everything the PCG touches (tiled layout)
+  T *adiag = nullptr, *al = nullptr, *ad = nullptr, *ab = nullptr;
+  T *E = nullptr, *cL = nullptr, *cD = nullptr, *cB = nullptr, *uR = nullptr, *uU = nullptr,
+    *uF = nullptr;
+  T *r = nullptr, *p = nullptr, *z = nullptr, *s = nullptr, *q = nullptr, *Az = nullptr;
+};
+
+class PcgSolver {
+ public:
+  PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt);
+  ~PcgSolver();
+  int status() const { return init_status_; }
+  // Load a system given in the reference layout (6 neighbour arrays, Left..Back
+  // order of project-solver.cc:7-14).  `device` selects device or host pointers.
+  int upload(const double* adiag, const double* const an[6], const double* rhs,
+             const uint8_t* active, bool device);
+  // Replace only the right-hand side (reference layout).
+  int upload_rhs(const double* rhs, bool device);
+  int solve(PcgStats* st);
+  int download_pressure(double* pg, bool device);
+  // ModifiedIncompleteCholesky3D::precond on the uploaded system: z = M^-1 r
+  // (reference layout in and out, device pointers).
+  int precond_only(const double* r, double* z);
+  // applyCompressedMatrix on the uploaded system (device pointers, reference layout).
+  int apply_only(const double* x, double* b);
+
+  const Tiled& geom() const { return g_; }
+  // Direct access for in-device producers (FLIP buildSystem writes these).
+  double* adiag64() { return d64_.adiag; }
+  double* al64() { return d64_.al; }
+  double* ad64() { return d64_.ad; }
+  double* ab64() { return d64_.ab; }
+  double* rhs64() { return rhs_; }
+  uint8_t* active() { return active_; }
+  double* pressure64() { return d64_.p; }
+  // Called after a producer wrote adiag/al/ad/ab/active/rhs in tiled layout.
+  void mark_system_changed() { pivots_valid_ = false; }
+  void set_options(const PcgOptions& o) { opt_ = o; }
+  const PcgOptions& options() const { return opt_; }
+
+ private:
+  int ensure_pivots();
+  template <class T>
+  int run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter, bool scale_rhs,
+              PcgStats* st);
+  int solve_fp64(PcgStats* st);
+  int solve_mixed(PcgStats* st);
+  int true_residual(PcgStats* st);
+  template <class T>
+  void launch_iteration(SysArrays<T>& A);
+  int check_dev_error(const char* where);
+
+  Context* ctx_;
+  PcgOptions opt_;
+  Tiled g_;
+  int init_status_ = 0;
+  bool pivots_valid_ = false;
+  bool have_f32_ = false;
+  int nblocks_ = 0;     // elementwise grid
+  int wave_grid_ = 0;   // persistent wavefront grid
+  SysArrays<double> d64_;
+  SysArrays<float> d32_;
+  double* rhs_ = nullptr;   // tiled rhs (FP64)
+  double* xacc_ = nullptr;  // mixed: FP64 solution accumulator
+  uint8_t* active_ = nullptr;
+  double* partials_ = nullptr;  // 2 per block
+  PcgScalars* sc_ = nullptr;
+  PcgScalars* sc_host_ = nullptr;  // pinned
+  WaveSync ws_{};
+  std::vector<void*> allocs_;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;    // chunk polling
+  cudaEvent_t evt0_ = nullptr, evt1_ = nullptr;  // solve timing
+  double sym_err_ = 0.0;
+  double inner_scale_ = 1.0;
+  PcgScalars last_{};
+  // graphs: one chunk of iterations per precision
+  cudaGraphExec_t graph64_ = nullptr, graph32_ = nullptr;
+  template <class T>
+  cudaGraphExec_t& graph_for();
+};
+
+}  // namespace sc

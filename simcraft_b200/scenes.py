@@ -1,0 +1,97 @@
+"""Seeded synthetic scenes for the FLIP dam break and the standalone pressure solve.
+
+The reference seeds nothing (`setInitialFluid` draws from an unseeded mt19937,
+FluidSim/include/FluidSim/cpu/fluid-simulator.h:73-78, and the orphan CUDA test
+uses std::random_device), so every scene here is generated once on the host
+from numpy's PCG64 with a fixed seed and fed identically to the CUDA path and
+to the CPU oracle.
+"""
+import numpy as np
+
+# Domain is the unit cube; cells are cubic with h = 1/n.
+
+
+def dam_break(n, frac_x=0.5, frac_y=0.5, frac_z=1.0, ppc=8, seed=1, dtype=np.float64):
+    """Particles jittered uniformly inside every cell of the block
+    x < frac_x, y < frac_y, z < frac_z of an n^3 grid; zero velocity.
+
+    Particles are emitted cell by cell in the grid's (x, y, z) lexicographic
+    order, `ppc` per cell, each at cell_min + h * U[0,1)^3.
+    Returns (pos[P,3], vel[P,3], h)."""
+    h = 1.0 / n
+    cx, cy, cz = int(round(frac_x * n)), int(round(frac_y * n)), int(round(frac_z * n))
+    ii, jj, kk = np.meshgrid(np.arange(cx), np.arange(cy), np.arange(cz), indexing="ij")
+    cells = np.stack([ii.ravel(), jj.ravel(), kk.ravel()], axis=1).astype(np.float64)
+    rng = np.random.default_rng(seed)
+    jitter = rng.random((cells.shape[0], ppc, 3))
+    pos = (cells[:, None, :] + jitter) * h
+    pos = pos.reshape(-1, 3).astype(dtype)
+    return np.ascontiguousarray(pos), np.zeros_like(pos), h
+
+
+def _spheres(seed, count, rmin, rmax):
+    rng = np.random.default_rng(seed)
+    centres = rng.random((count, 3))
+    radii = rmin + (rmax - rmin) * rng.random(count)
+    return centres, radii
+
+
+def sphere_union_sdf(n, centres, radii, chunk=32):
+    """Signed distance to a union of spheres at the cell centres of an n^3 grid
+    (min over spheres of |x - c| - r), float64, shape (n, n, n)."""
+    h = 1.0 / n
+    x = (np.arange(n) + 0.5) * h
+    out = np.empty((n, n, n))
+    for i0 in range(0, n, chunk):
+        xs = x[i0:i0 + chunk]
+        best = np.full((len(xs), n, n), np.inf)
+        for c, r in zip(centres, radii):
+            d2 = ((xs - c[0]) ** 2)[:, None, None] + ((x - c[1]) ** 2)[None, :, None] + ((x - c[2]) ** 2)[None, None, :]
+            np.minimum(best, np.sqrt(d2) - r, out=best)
+        out[i0:i0 + chunk] = best
+    return out
+
+
+def sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=0.5, seed=2, probe=64):
+    """Fluid mask of `count` seeded spheres (centres U[0,1)^3, radii U[rmin,rmax]).
+
+    24 spheres of those radii cover only ~25% of the box, so all radii are
+    scaled by one common factor, found by bisection on a probe grid, until the
+    fluid fraction is `fill`.  Returns (fluid_sdf, info) with info holding the
+    scale and the achieved fill on the full grid."""
+    centres, radii = _spheres(seed, count, rmin, rmax)
+    lo, hi = 0.5, 4.0
+    for _ in range(30):
+        mid = 0.5 * (lo + hi)
+        f = float((sphere_union_sdf(probe, centres, radii * mid) <= 0.0).mean())
+        if f < fill:
+            lo = mid
+        else:
+            hi = mid
+    scale = 0.5 * (lo + hi)
+    sdf = sphere_union_sdf(n, centres, radii * scale)
+    return sdf, dict(scale=scale, fill=float((sdf <= 0.0).mean()), centres=centres, radii=radii * scale)
+
+
+def poisson_rhs(active, fluid_sdf, seed=3):
+    """Right-hand side U[-1,1] on active cells, mean-subtracted on every
+    6-connected active component that has no air (fluid_sdf > 0) face
+    neighbour, i.e. every component whose pure-Neumann system is singular."""
+    from scipy import ndimage
+
+    rng = np.random.default_rng(seed)
+    act = active.astype(bool)
+    rhs = np.where(act, rng.uniform(-1.0, 1.0, size=active.shape), 0.0)
+    labels, nlab = ndimage.label(act)
+    if nlab == 0:
+        return rhs, dict(components=0, enclosed=0)
+    air = fluid_sdf > 0.0
+    struct = ndimage.generate_binary_structure(3, 1)
+    near_air = ndimage.binary_dilation(air, structure=struct) & act
+    touches = np.zeros(nlab + 1, bool)
+    touches[np.unique(labels[near_air])] = True
+    enclosed = [l for l in range(1, nlab + 1) if not touches[l]]
+    for l in enclosed:
+        m = labels == l
+        rhs[m] -= rhs[m].mean()
+    return rhs, dict(components=int(nlab), enclosed=len(enclosed))

@@ -1,0 +1,69 @@
+"""MIC(0)-PCG parity: the CUDA path (through the C-ABI) against the oracle."""
+import numpy as np
+import pytest
+
+from helpers import poisson_system, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_mod(gpu):
+    import torch
+    return torch
+
+
+def _dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("dims", [(16, 16, 16), (40, 20, 13), (33, 17, 40), (70, 9, 5)])
+def test_apply_and_precond_match_oracle(oracle, torch_mod, dims):
+    torch = torch_mod
+    from simcraft_b200.solver import CgSolver3D
+    S = poisson_system(oracle, 0, dims=dims, seed=4)
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-1, 1, dims)
+    s = CgSolver3D(*dims)
+    s.upload(S["adiag"], S["an"], S["rhs"], S["active"])
+    b_ref = oracle.apply_matrix(S["adiag"], S["an"], x, S["active"])
+    b = torch.zeros(dims, dtype=torch.float64, device="cuda")
+    s.apply(_dev(torch, x), b)
+    a = S["active"].astype(bool)
+    assert np.abs(b.cpu().numpy() - b_ref)[a].max() <= 1e-12 * max(1.0, np.abs(b_ref).max())
+    z_ref = oracle.mic_precond(S["adiag"], S["an"], x, S["active"])
+    z = torch.zeros(dims, dtype=torch.float64, device="cuda")
+    s.precond(_dev(torch, x), z)
+    assert rel_l2(z.cpu().numpy(), z_ref, a) < 1e-12
+
+
+@pytest.mark.parametrize("n,crit", [(16, 0), (32, 1), (48, 1)])
+def test_pcg_fp64_matches_oracle(oracle, torch_mod, n, crit):
+    from simcraft_b200.solver import CgSolver3D
+    S = poisson_system(oracle, n, seed=2)
+    tol = 1e-6 if crit == 0 else 1e-8
+    p_ref, res_ref, it_ref = oracle.pcg_solve(S["adiag"], S["an"], S["rhs"], S["active"], tol=tol,
+                                              max_iter=500, criterion=crit)
+    s = CgSolver3D(n, n, n, tol=tol, max_iter=500, criterion=crit)
+    pg = np.zeros((n, n, n))
+    res = s.solve(S["adiag"], S["an"], S["rhs"], S["active"], pg)
+    st = s.last_stats
+    assert abs(st["iterations"] - it_ref) <= 1, (st, it_ref)
+    assert res < tol
+    a = S["active"].astype(bool)
+    assert rel_l2(pg, p_ref, a) < 1e-5
+
+
+def test_pcg_mixed_reaches_1e10(oracle, torch_mod):
+    from simcraft_b200.solver import CgSolver3D, CRIT_REL_L2, PREC_MIXED
+    n = 32
+    S = poisson_system(oracle, n, seed=2)
+    p_ref, _, _ = oracle.pcg_solve(S["adiag"], S["an"], S["rhs"], S["active"], tol=1e-12, max_iter=1000,
+                                   criterion=1)
+    s = CgSolver3D(n, n, n, tol=1e-10, max_iter=1000, criterion=CRIT_REL_L2, precision=PREC_MIXED)
+    pg = np.zeros((n, n, n))
+    s.solve(S["adiag"], S["an"], S["rhs"], S["active"], pg)
+    st = s.last_stats
+    assert st["true_rel_l2"] < 1e-10, st
+    a = S["active"].astype(bool)
+    assert rel_l2(pg, p_ref, a) < 1e-8

@@ -62,9 +62,11 @@ const char* sc_status_string(int status);
  * to a context. */
 int sc_context_create(int device, sc_context** out);
 void sc_context_destroy(sc_context* ctx);
-/* Use an external stream (cudaStream_t passed as void*); NULL restores the
- * context's own stream. */
+/* Order all later work on an external stream (a cudaStream_t passed as void*;
+ * NULL is the legacy default stream). */
 int sc_context_set_stream(sc_context* ctx, void* stream);
+/* Go back to the context's own stream. */
+int sc_context_use_own_stream(sc_context* ctx);
 void* sc_context_stream(sc_context* ctx);
 int sc_context_synchronize(sc_context* ctx);
 const char* sc_context_last_error(sc_context* ctx);
@@ -95,6 +97,7 @@ typedef struct {
   double true_linf;      /* ||b - A p||_inf recomputed in FP64 */
   double ms;             /* device time of the solve */
   double sym_err;        /* max asymmetry found when check_symmetry is set */
+  unsigned device_flags; /* device-side error bits: 1 wait timeout, 2 non-finite, 4 breakdown */
 } sc_pcg_stats;
 
 /* Defaults equal to the reference's constants. */

@@ -21,7 +21,7 @@ class sc_pcg_options(ctypes.Structure):
 class sc_pcg_stats(ctypes.Structure):
     _fields_ = [("iterations", c_int), ("outer", c_int), ("status", c_int), ("residual", c_double),
                 ("true_rel_l2", c_double), ("true_linf", c_double), ("ms", c_double),
-                ("sym_err", c_double)]
+                ("sym_err", c_double), ("device_flags", ctypes.c_uint)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -41,6 +41,7 @@ SIGNATURES = {
     "sc_context_create": (c_int, [c_int, P(c_void_p)]),
     "sc_context_destroy": (None, [c_void_p]),
     "sc_context_set_stream": (c_int, [c_void_p, c_void_p]),
+    "sc_context_use_own_stream": (c_int, [c_void_p]),
     "sc_context_stream": (c_void_p, [c_void_p]),
     "sc_context_synchronize": (c_int, [c_void_p]),
     "sc_context_last_error": (c_char_p, [c_void_p]),

@@ -44,6 +44,7 @@ void to_public(const sc::PcgStats& s, sc_pcg_stats* o) {
   o->true_linf = s.true_linf;
   o->ms = s.ms;
   o->sym_err = s.sym_err;
+  o->device_flags = s.device_flags;
 }
 
 int validate_options(const sc_pcg_options* o) {
@@ -103,7 +104,13 @@ void sc_context_destroy(sc_context* ctx) {
 
 int sc_context_set_stream(sc_context* ctx, void* stream) {
   if (!ctx) return SC_ERR_INVALID;
-  ctx->c.stream = stream ? (cudaStream_t)stream : ctx->own;
+  ctx->c.stream = (cudaStream_t)stream;
+  return SC_OK;
+}
+
+int sc_context_use_own_stream(sc_context* ctx) {
+  if (!ctx) return SC_ERR_INVALID;
+  ctx->c.stream = ctx->own;
   return SC_OK;
 }
 
@@ -269,4 +276,7 @@ int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b) {
   return map_status(pcg->solver->apply_only(x, b));
 }
 
+int sc_debug_pcg_dump(sc_pcg* pcg, int which, double* out) {
+  return pcg->solver->debug_dump(which, out);
+}
 }  // extern "C"

@@ -51,8 +51,11 @@ __device__ __forceinline__ unsigned ld_relaxed_gpu_u32(const unsigned* p) {
 __device__ __forceinline__ double ld_cg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ float ld_cg(const float* p) { return __ldcg(p); }
 
+// Named barrier over a subset of the CTA.  The non-aligned `barrier.sync` form
+// is used on purpose: `bar.sync` is `barrier.sync.aligned`, which counts a whole
+// warp as arrived when its first lanes arrive.
 __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+  asm volatile("barrier.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
 __device__ __forceinline__ int wrap_mod(int v, int n) {
@@ -74,24 +77,24 @@ __device__ __forceinline__ int wrap_mod(int v, int n) {
 // tile = Y * ntx + X.  Cells outside the grid (x >= nx or y >= ny) are padding
 // and hold zeros.
 struct Tiled {
+  static constexpr int TY = 8;
   int nx, ny, nz;
-  int TY;
   int ntx, nty;
   int64_t tile_elems;  // nz * TY * 32
   int64_t total;       // ntx * nty * tile_elems
 
-  static Tiled make(int nx, int ny, int nz, int TY) {
+  static Tiled make(int nx, int ny, int nz) {
     Tiled t;
     t.nx = nx;
     t.ny = ny;
     t.nz = nz;
-    t.TY = TY;
     t.ntx = (nx + 31) / 32;
     t.nty = (ny + TY - 1) / TY;
     t.tile_elems = (int64_t)nz * TY * 32;
     t.total = (int64_t)t.ntx * t.nty * t.tile_elems;
     return t;
   }
+  __host__ __device__ __forceinline__ int ntiles() const { return ntx * nty; }
   __host__ __device__ __forceinline__ int64_t tile_base(int X, int Y) const {
     return (int64_t)(Y * ntx + X) * tile_elems;
   }
@@ -101,7 +104,7 @@ struct Tiled {
     while (slot >= nz) slot -= nz;
     return tile_base(X, Y) + ((int64_t)slot * TY + ty) * 32 + tx;
   }
-  // Inverse map; returns false for padding.
+  // Inverse map; returns false for padding.  (Slow path: 64-bit divisions.)
   __host__ __device__ __forceinline__ bool coords(int64_t e, int& x, int& y, int& z) const {
     int64_t t = e / tile_elems;
     int64_t r = e - t * tile_elems;
@@ -116,6 +119,63 @@ struct Tiled {
     while (zz < 0) zz += nz;
     z = zz;
     return x < nx && y < ny;
+  }
+};
+
+// One element of a tiled array seen from a thread of a TY*32-thread block that
+// owns the row block (tile, slot): thread (ty, tx) = (threadIdx.x / 32, % 32).
+// Gives the coordinates and the element offsets of the six face neighbours
+// without any division per element.
+struct Cell {
+  int x, y, z;
+  int tx, ty, slot, X, Y;
+  int64_t tbase, e;
+  bool inside;
+  __device__ __forceinline__ void init(const Tiled& g, int rb, int tid) {
+    const int tile = rb / g.nz;
+    slot = rb - tile * g.nz;
+    Y = tile / g.ntx;
+    X = tile - Y * g.ntx;
+    tx = tid & 31;
+    ty = tid >> 5;
+    x = X * 32 + tx;
+    y = Y * Tiled::TY + ty;
+    int zz = slot - tx;
+    while (zz < 0) zz += g.nz;
+    z = zz;
+    tbase = (int64_t)tile * g.tile_elems;
+    e = (int64_t)rb * (Tiled::TY * 32) + tid;
+    inside = x < g.nx && y < g.ny;
+  }
+  __device__ __forceinline__ int64_t at(int64_t base, int s, int ty_, int tx_) const {
+    return base + ((int64_t)s * Tiled::TY + ty_) * 32 + tx_;
+  }
+  // neighbour offsets; callers check the domain bounds first
+  __device__ __forceinline__ int64_t xm(const Tiled& g) const {
+    if (tx > 0) return at(tbase, slot == 0 ? g.nz - 1 : slot - 1, ty, tx - 1);
+    int s = slot + 31;
+    while (s >= g.nz) s -= g.nz;
+    return at(tbase - g.tile_elems, s, ty, 31);
+  }
+  __device__ __forceinline__ int64_t xp(const Tiled& g) const {
+    if (tx < 31) return at(tbase, slot == g.nz - 1 ? 0 : slot + 1, ty, tx + 1);
+    int s = slot - 31;
+    while (s < 0) s += g.nz;
+    return at(tbase + g.tile_elems, s, ty, 0);
+  }
+  __device__ __forceinline__ int64_t ym(const Tiled& g) const {
+    if (ty > 0) return e - 32;
+    return at(tbase - (int64_t)g.ntx * g.tile_elems, slot, Tiled::TY - 1, tx);
+  }
+  __device__ __forceinline__ int64_t yp(const Tiled& g) const {
+    if (ty < Tiled::TY - 1) return e + 32;
+    return at(tbase + (int64_t)g.ntx * g.tile_elems, slot, 0, tx);
+  }
+  __device__ __forceinline__ int64_t zm(const Tiled& g) const {
+    return at(tbase, slot == 0 ? g.nz - 1 : slot - 1, ty, tx);
+  }
+  __device__ __forceinline__ int64_t zp(const Tiled& g) const {
+    return at(tbase, slot == g.nz - 1 ? 0 : slot + 1, ty, tx);
   }
 };
 

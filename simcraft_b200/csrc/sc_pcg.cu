@@ -166,27 +166,33 @@ __device__ void reduce_finalize(double sum, double mx, double* partials, PcgScal
 }
 
 // ---------------------------------------------------------------------------------
-// Layout conversion (reference layout <-> tiled).
+// Layout conversion (reference layout <-> tiled).  Row-block kernels: one
+// 256-thread block owns the TY*32 elements of one (tile, slot) row block.
+#define SC_ROWBLOCK_LOOP(g) \
+  for (int rb = blockIdx.x, nrb_ = (g).ntiles() * (g).nz; rb < nrb_; rb += gridDim.x)
+
 template <class Ts, class Td>
-__global__ void k_to_tiled(Tiled g, const Ts* __restrict__ src, Td* __restrict__ dst,
-                           const uint8_t* __restrict__ mask_ref) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.total; e += stride) {
-    int i, j, k;
+__global__ void __launch_bounds__(kThreads) k_to_tiled(Tiled g, const Ts* __restrict__ src,
+                                                       Td* __restrict__ dst,
+                                                       const uint8_t* __restrict__ mask_ref) {
+  SC_ROWBLOCK_LOOP(g) {
+    Cell c;
+    c.init(g, rb, threadIdx.x);
     Td v = Td(0);
-    if (g.coords(e, i, j, k)) {
-      int64_t r = lin(i, j, k, g.ny, g.nz);
+    if (c.inside) {
+      const int64_t r = lin(c.x, c.y, c.z, g.ny, g.nz);
       if (!mask_ref || mask_ref[r]) v = (Td)src[r];
     }
-    dst[e] = v;
+    dst[c.e] = v;
   }
 }
 template <class Ts, class Td>
-__global__ void k_from_tiled(Tiled g, const Ts* __restrict__ src, Td* __restrict__ dst) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.total; e += stride) {
-    int i, j, k;
-    if (g.coords(e, i, j, k)) dst[lin(i, j, k, g.ny, g.nz)] = (Td)src[e];
+__global__ void __launch_bounds__(kThreads) k_from_tiled(Tiled g, const Ts* __restrict__ src,
+                                                         Td* __restrict__ dst) {
+  SC_ROWBLOCK_LOOP(g) {
+    Cell c;
+    c.init(g, rb, threadIdx.x);
+    if (c.inside) dst[lin(c.x, c.y, c.z, g.ny, g.nz)] = (Td)src[c.e];
   }
 }
 template <class Ts, class Td>
@@ -251,36 +257,37 @@ __global__ void __launch_bounds__(kThreads) k_copy(int64_t n, const T* __restric
 
 // applyCompressedMatrix (project-solver.cc:16-39) on the tiled layout.  The
 // upper couplings come from the neighbours' lower ones (A symmetric,
-// checkSystemSymmetry, :41-57).  Also accumulates x . (A x).
-template <class T>
-__device__ __forceinline__ T apply_row(const Tiled& g, int64_t e, int i, int j, int k,
-                                       const T* __restrict__ adiag, const T* __restrict__ al,
-                                       const T* __restrict__ ad, const T* __restrict__ ab,
-                                       const uint8_t* __restrict__ act, const T* __restrict__ x) {
-  T t = adiag[e] * x[e];
-  if (i > 0) {
-    int64_t o = g.off(i - 1, j, k);
-    if (act[o]) t += al[e] * x[o];
+// checkSystemSymmetry, :41-57).
+template <class T, class X>
+__device__ __forceinline__ T apply_row(const Tiled& g, const Cell& c, const T* __restrict__ adiag,
+                                       const T* __restrict__ al, const T* __restrict__ ad,
+                                       const T* __restrict__ ab, const uint8_t* __restrict__ act,
+                                       const X* __restrict__ x) {
+  const int64_t e = c.e;
+  T t = adiag[e] * (T)x[e];
+  if (c.x > 0) {
+    int64_t o = c.xm(g);
+    if (act[o]) t += al[e] * (T)x[o];
   }
-  if (j > 0) {
-    int64_t o = g.off(i, j - 1, k);
-    if (act[o]) t += ad[e] * x[o];
+  if (c.y > 0) {
+    int64_t o = c.ym(g);
+    if (act[o]) t += ad[e] * (T)x[o];
   }
-  if (k > 0) {
-    int64_t o = g.off(i, j, k - 1);
-    if (act[o]) t += ab[e] * x[o];
+  if (c.z > 0) {
+    int64_t o = c.zm(g);
+    if (act[o]) t += ab[e] * (T)x[o];
   }
-  if (i < g.nx - 1) {
-    int64_t o = g.off(i + 1, j, k);
-    if (act[o]) t += al[o] * x[o];
+  if (c.x < g.nx - 1) {
+    int64_t o = c.xp(g);
+    if (act[o]) t += al[o] * (T)x[o];
   }
-  if (j < g.ny - 1) {
-    int64_t o = g.off(i, j + 1, k);
-    if (act[o]) t += ad[o] * x[o];
+  if (c.y < g.ny - 1) {
+    int64_t o = c.yp(g);
+    if (act[o]) t += ad[o] * (T)x[o];
   }
-  if (k < g.nz - 1) {
-    int64_t o = g.off(i, j, k + 1);
-    if (act[o]) t += ab[o] * x[o];
+  if (c.z < g.nz - 1) {
+    int64_t o = c.zp(g);
+    if (act[o]) t += ab[o] * (T)x[o];
   }
   return t;
 }
@@ -293,15 +300,15 @@ __global__ void __launch_bounds__(kThreads)
            int use_skip) {
   if (use_skip && sc->done != DONE_RUNNING) return;
   double acc = 0.0;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.total; e += stride) {
-    int i, j, k;
+  SC_ROWBLOCK_LOOP(g) {
+    Cell c;
+    c.init(g, rb, threadIdx.x);
     T out = T(0);
-    if (g.coords(e, i, j, k) && act[e]) {
-      out = apply_row(g, e, i, j, k, adiag, al, ad, ab, act, x);
-      acc += (double)x[e] * (double)out;
+    if (c.inside && act[c.e]) {
+      out = apply_row(g, c, adiag, al, ad, ab, act, x);
+      acc += (double)x[c.e] * (double)out;
     }
-    y[e] = out;
+    y[c.e] = out;
   }
   reduce_finalize(acc, 0.0, partials, sc, FIN_SPMV);
 }
@@ -347,18 +354,18 @@ template <class T>
 __global__ void __launch_bounds__(kThreads)
     k_upper(Tiled g, const T* __restrict__ cL, const T* __restrict__ cD,
             const T* __restrict__ cB, T* __restrict__ uR, T* __restrict__ uU, T* __restrict__ uF) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.total; e += stride) {
-    int i, j, k;
-    T a = T(0), b = T(0), c = T(0);
-    if (g.coords(e, i, j, k)) {
-      if (i < g.nx - 1) a = cL[g.off(i + 1, j, k)];
-      if (j < g.ny - 1) b = cD[g.off(i, j + 1, k)];
-      if (k < g.nz - 1) c = cB[g.off(i, j, k + 1)];
+  SC_ROWBLOCK_LOOP(g) {
+    Cell c;
+    c.init(g, rb, threadIdx.x);
+    T a = T(0), b = T(0), d = T(0);
+    if (c.inside) {
+      if (c.x < g.nx - 1) a = cL[c.xp(g)];
+      if (c.y < g.ny - 1) b = cD[c.yp(g)];
+      if (c.z < g.nz - 1) d = cB[c.zp(g)];
     }
-    uR[e] = a;
-    uU[e] = b;
-    uF[e] = c;
+    uR[c.e] = a;
+    uU[c.e] = b;
+    uF[c.e] = d;
   }
 }
 
@@ -369,11 +376,11 @@ __global__ void __launch_bounds__(kThreads)
                     const uint8_t* __restrict__ act, const double* __restrict__ x,
                     const double* __restrict__ b, double* partials, PcgScalars* sc) {
   double s2 = 0.0, mx = 0.0;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.total; e += stride) {
-    int i, j, k;
-    if (g.coords(e, i, j, k) && act[e]) {
-      double rv = b[e] - apply_row(g, e, i, j, k, adiag, al, ad, ab, act, x);
+  SC_ROWBLOCK_LOOP(g) {
+    Cell c;
+    c.init(g, rb, threadIdx.x);
+    if (c.inside && act[c.e]) {
+      double rv = b[c.e] - apply_row(g, c, adiag, al, ad, ab, act, x);
       s2 += rv * rv;
       mx = fmax(mx, fabs(rv));
     }
@@ -389,38 +396,14 @@ __global__ void __launch_bounds__(kThreads)
                    double* __restrict__ x, double* __restrict__ r, double* partials,
                    PcgScalars* sc) {
   double s2 = 0.0, mx = 0.0;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.total; e += stride) {
-    int i, j, k;
-    if (!(g.coords(e, i, j, k) && act[e])) continue;
-    double t = adiag[e] * (double)d[e];
-    if (i > 0) {
-      int64_t o = g.off(i - 1, j, k);
-      if (act[o]) t += al[e] * (double)d[o];
-    }
-    if (j > 0) {
-      int64_t o = g.off(i, j - 1, k);
-      if (act[o]) t += ad[e] * (double)d[o];
-    }
-    if (k > 0) {
-      int64_t o = g.off(i, j, k - 1);
-      if (act[o]) t += ab[e] * (double)d[o];
-    }
-    if (i < g.nx - 1) {
-      int64_t o = g.off(i + 1, j, k);
-      if (act[o]) t += al[o] * (double)d[o];
-    }
-    if (j < g.ny - 1) {
-      int64_t o = g.off(i, j + 1, k);
-      if (act[o]) t += ad[o] * (double)d[o];
-    }
-    if (k < g.nz - 1) {
-      int64_t o = g.off(i, j, k + 1);
-      if (act[o]) t += ab[o] * (double)d[o];
-    }
-    x[e] += scale * (double)d[e];
-    double rv = r[e] - scale * t;
-    r[e] = rv;
+  SC_ROWBLOCK_LOOP(g) {
+    Cell c;
+    c.init(g, rb, threadIdx.x);
+    if (!(c.inside && act[c.e])) continue;
+    const double t = apply_row(g, c, adiag, al, ad, ab, act, d);
+    x[c.e] += scale * (double)d[c.e];
+    const double rv = r[c.e] - scale * t;
+    r[c.e] = rv;
     s2 += rv * rv;
     mx = fmax(mx, fabs(rv));
   }
@@ -440,18 +423,6 @@ __global__ void __launch_bounds__(kThreads)
 // their boundary rows into shared-memory rings; the same warp publishes this
 // tile's progress.  Every wait is bounded: on timeout the kernel raises
 // DEV_ERR_TIMEOUT, releases its dependants and finishes.
-
-struct WaveArgs {
-  Tiled g;
-  int* progress;
-  int* ticket;
-  int* exits;
-  const int2* order;
-  PcgScalars* sc;
-  double* partials;
-  int use_skip;
-  int fin_kind;
-};
 
 template <class T>
 struct FwdOp {  // L q = r (project-solver.cc:276-288), c* = A_* E(neighbour)
@@ -559,176 +530,266 @@ struct PivotOp {
   }
 };
 
-template <class T, int TY, bool FWD>
+template <int TY, bool FWD>
 __device__ __forceinline__ int wave_slot(const Tiled& g, int s, int ty) {
   return FWD ? wrap_mod(s - ty, g.nz) : wrap_mod(g.nz + 29 + TY - s - ty, g.nz);
 }
 
+// Mailbox sentinel: a NaN payload that arithmetic never produces (the GPU's
+// canonical NaN has all mantissa bits set).
+template <class T>
+struct Sentinel;
+template <>
+struct Sentinel<double> {
+  using Bits = unsigned long long;
+  static constexpr Bits bits = 0x7ff4deadbeefcafeull;
+};
+template <>
+struct Sentinel<float> {
+  using Bits = unsigned int;
+  static constexpr Bits bits = 0x7fa5deadu;
+};
+template <class T>
+__device__ __forceinline__ typename Sentinel<T>::Bits mb_load(const T* p) {
+  typename Sentinel<T>::Bits v;
+  if constexpr (sizeof(T) == 8)
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  else
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+template <class T>
+__device__ __forceinline__ T mb_value(typename Sentinel<T>::Bits b) {
+  T v;
+  memcpy(&v, &b, sizeof(T));
+  return v;
+}
+// Every mailbox access is a strong (relaxed, gpu-scope) operation, so writes by
+// one CTA and polls by another are coherent under the PTX memory model.
+template <class T>
+__device__ __forceinline__ void mb_store_bits(T* p, typename Sentinel<T>::Bits b) {
+  if constexpr (sizeof(T) == 8)
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(b) : "memory");
+  else
+    asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(b) : "memory");
+}
+template <class T>
+__device__ __forceinline__ void mb_store(T* p, T v) {
+  typename Sentinel<T>::Bits b;
+  memcpy(&b, &v, sizeof(T));
+  mb_store_bits(p, b);
+}
+template <class T>
+__device__ __forceinline__ void mb_reset(T* p) {
+  mb_store_bits(p, Sentinel<T>::bits);
+}
+
+// Shared state of one wavefront CTA.
+template <class T, int TY>
+struct WaveShared {
+  T xch[2][TY][32];
+  T bufX[kRing][TY];
+  T bufY[kRing][32];
+  volatile int done;     // compute steps completed
+  volatile int availX;   // ring entries loaded
+  volatile int availY;
+  volatile int abort;
+  int tile;
+  bool last;
+  double ssum[TY + 2];
+};
+
+// Give up: flag the error and release the compute warps.
+template <class T, int TY>
+__device__ __forceinline__ void wave_abort(const WaveArgs& a, WaveShared<T, TY>& sh, int NS) {
+  atomicOr(&a.sc->err, DEV_ERR_TIMEOUT);
+  sh.abort = 1;
+  sh.availX = NS;
+  sh.availY = NS;
+}
+
+__device__ __forceinline__ bool wave_should_stop(const WaveArgs& a, int& spins,
+                                                 volatile int* s_abort) {
+  if (*s_abort) return true;
+  ++spins;
+  if ((spins & 63) == 0 && ld_relaxed_gpu_u32(&a.sc->err)) return true;
+  return spins > kSpinLimit;
+}
+
+// Mailboxes.  The producer tile writes each boundary value it computes into
+// the mailbox of the tile that consumes it, at the consumer's ring-entry index:
+//   x: mbx[consumer][e][ty]  (e = producer step - 31)
+//   y: mby[consumer][e][tx]  (e = producer step - (TY-1))
+// The consumer's loader warps poll those words until they stop holding the
+// sentinel, copy them to the shared-memory rings and write the sentinel back,
+// which leaves the mailboxes ready for the next sweep.  No fences are needed:
+// every mailbox word carries exactly one value per sweep.
 template <class T, int TY, bool FWD>
-__device__ void wave_comm(const WaveArgs& a, const T* out, int tile_id, int tileX_id,
-                          int tileY_id, int64_t baseX, int64_t baseY, bool hasX, bool hasY,
-                          int NS, T (*bufX)[TY], T (*bufY)[32], volatile int* s_done,
-                          volatile int* s_availX, volatile int* s_availY, volatile int* s_abort) {
+__device__ void wave_load_x(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int NS) {
   const Tiled& g = a.g;
   const int lane = threadIdx.x & 31;
-  int pub = 0;
-  int lx = hasX ? 0 : NS, ly = hasY ? 0 : NS;
-  int seenX = 0, seenY = 0;
-  int spins = 0;
-  int* my_prog = a.progress + tile_id;
-  for (;;) {
-    bool worked = false;
-    const int d = *s_done;
-    if (d > pub) {
-      __threadfence();
-      if (lane == 0) st_release_gpu(my_prog, d);
-      pub = d;
-      worked = true;
+  constexpr int EPB = 32 / TY;  // entries per 32 lanes
+  int lx = 0, spins = 0;
+  while (lx < NS) {
+    const int want = min(NS, sh.done + kRing);
+    if (lx >= want) {
+      if (wave_should_stop(a, spins, &sh.abort)) break;
+      continue;
     }
-    const int want = min(NS, d + kRing);
-    if (lx < want) {
-      // entry e needs the neighbour's step e+31 done (progress >= e+32); the
-      // neighbour's final progress NS releases every remaining entry.
-      int availX = seenX >= NS ? NS : seenX - 31;
-      if (lx >= availX) {
-        int v = lane == 0 ? ld_acquire_gpu(a.progress + tileX_id) : 0;
-        seenX = __shfl_sync(kFull, v, 0);
-        __syncwarp();
-        availX = seenX >= NS ? NS : seenX - 31;
-      }
-      const int hi = min(want, availX);
-      if (hi > lx) {
-        const int cnt = (hi - lx) * TY;
-        for (int i = lane; i < cnt; i += 32) {
-          const int e = lx + i / TY, ty = i % TY;
-          T val = T(0);
-          if (FWD) {
-            const int z = e - ty;
-            if (z >= 0 && z < g.nz)
-              val = ld_cg(out + baseX + ((int64_t)wrap_mod(z + 31, g.nz) * TY + ty) * 32 + 31);
-          } else {
-            const int z = g.nz - 1 - e + (TY - 1 - ty);
-            if (z >= 0 && z < g.nz) val = ld_cg(out + baseX + ((int64_t)z * TY + ty) * 32);
-          }
-          bufX[e % kRing][ty] = val;
+    // poll up to 8*EPB entries: lane handles (entry lx + k*EPB + lane/TY, ty = lane%TY)
+    const int ty = lane % TY;
+    typename Sentinel<T>::Bits v[8];
+    unsigned ready = 0;  // bit k*EPB+j: entry lx+k*EPB+j fully ready
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int e = lx + k * EPB + lane / TY;
+      const int z = FWD ? e - ty : g.nz - 1 - e + (TY - 1 - ty);
+      const bool need = e < want && z >= 0 && z < g.nz;
+      v[k] = need ? mb_load(mb + (int64_t)e * TY + ty) : (typename Sentinel<T>::Bits)0;
+      const bool ok = e < want && (!need || v[k] != Sentinel<T>::bits);
+      const unsigned bal = __ballot_sync(kFull, ok);
+#pragma unroll
+      for (int j = 0; j < EPB; j++)
+        if (((bal >> (j * TY)) & ((1u << TY) - 1u)) == ((1u << TY) - 1u)) ready |= 1u << (k * EPB + j);
+    }
+    const int nready = __ffs(~ready) - 1;  // leading ready entries
+    const int take = nready < 0 ? 8 * EPB : nready;
+    if (take > 0) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const int j = k * EPB + lane / TY;
+        if (j < take) {
+          const int e = lx + j;
+          const int z = FWD ? e - ty : g.nz - 1 - e + (TY - 1 - ty);
+          const bool need = z >= 0 && z < g.nz;
+          sh.bufX[e % kRing][ty] = need ? mb_value<T>(v[k]) : T(0);
+          if (need) mb_reset(mb + (int64_t)e * TY + ty);
         }
-        __syncwarp();
-        __threadfence_block();
-        if (lane == 0) *s_availX = hi;
-        lx = hi;
-        worked = true;
       }
-    }
-    if (ly < want) {
-      // entry e needs the neighbour's step e+TY-1 done (progress >= e+TY)
-      int availY = seenY >= NS ? NS : seenY - TY + 1;
-      if (ly >= availY) {
-        int v = lane == 0 ? ld_acquire_gpu(a.progress + tileY_id) : 0;
-        seenY = __shfl_sync(kFull, v, 0);
-        __syncwarp();
-        availY = seenY >= NS ? NS : seenY - TY + 1;
-      }
-      const int hi = min(want, availY);
-      if (hi > ly) {
-        for (int e = ly; e < hi; e++) {
-          const int slot = FWD ? wrap_mod(e, g.nz) : wrap_mod(g.nz + 30 - e, g.nz);
-          const int row = FWD ? TY - 1 : 0;
-          bufY[e % kRing][lane] = ld_cg(out + baseY + ((int64_t)slot * TY + row) * 32 + lane);
-        }
-        __syncwarp();
-        __threadfence_block();
-        if (lane == 0) *s_availY = hi;
-        ly = hi;
-        worked = true;
-      }
-    }
-    if (pub >= NS && lx >= NS && ly >= NS) break;
-    if (*s_abort) {
-      if (lane == 0) {
-        st_release_gpu(my_prog, NS);
-        *s_availX = NS;
-        *s_availY = NS;
-      }
-      break;
-    }
-    if (worked) {
+      __syncwarp();
+      __threadfence_block();
+      if (lane == 0) sh.availX = lx + take;
+      lx += take;
       spins = 0;
-    } else {
-      if (++spins > kSpinLimit || (((spins & 255) == 0) && ld_relaxed_gpu_u32(&a.sc->err))) {
-        if (lane == 0) {
-          atomicOr(&a.sc->err, DEV_ERR_TIMEOUT);
-          *s_abort = 1;
-          st_release_gpu(my_prog, NS);
-          *s_availX = NS;
-          *s_availY = NS;
-        }
-        break;
-      }
-      __nanosleep(32);
+      continue;
     }
+    if (wave_should_stop(a, spins, &sh.abort)) break;
   }
+  if (lx < NS && lane == 0) wave_abort(a, sh, NS);
+}
+
+template <class T, int TY, bool FWD>
+__device__ void wave_load_y(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int NS) {
+  const Tiled& g = a.g;
+  const int lane = threadIdx.x & 31;
+  int ly = 0, spins = 0;
+  while (ly < NS) {
+    const int want = min(NS, sh.done + kRing);
+    if (ly >= want) {
+      if (wave_should_stop(a, spins, &sh.abort)) break;
+      continue;
+    }
+    typename Sentinel<T>::Bits v[8];
+    unsigned ready = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int e = ly + k;
+      // the consumer is warp 0 (forward) or warp TY-1 (backward), lane = tx
+      const int z = FWD ? e - lane : g.nz - 1 - (e - (31 - lane));
+      const bool need = e < want && z >= 0 && z < g.nz;
+      v[k] = need ? mb_load(mb + (int64_t)e * 32 + lane) : (typename Sentinel<T>::Bits)0;
+      const bool ok = e < want && (!need || v[k] != Sentinel<T>::bits);
+      if (__all_sync(kFull, ok)) ready |= 1u << k;
+    }
+    const int nready = __ffs(~ready) - 1;
+    const int take = nready < 0 ? 8 : nready;
+    if (take > 0) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        if (k < take) {
+          const int e = ly + k;
+          const int z = FWD ? e - lane : g.nz - 1 - (e - (31 - lane));
+          const bool need = z >= 0 && z < g.nz;
+          sh.bufY[e % kRing][lane] = need ? mb_value<T>(v[k]) : T(0);
+          if (need) mb_reset(mb + (int64_t)e * 32 + lane);
+        }
+      }
+      __syncwarp();
+      __threadfence_block();
+      if (lane == 0) sh.availY = ly + take;
+      ly += take;
+      spins = 0;
+      continue;
+    }
+    if (wave_should_stop(a, spins, &sh.abort)) break;
+  }
+  if (ly < NS && lane == 0) wave_abort(a, sh, NS);
 }
 
 template <class T, int TY, bool FWD, class Op>
-__global__ void __launch_bounds__((TY + 1) * 32, 1) k_wave(const WaveArgs a, const Op op) {
+__global__ void __launch_bounds__((TY + 2) * 32, 1) k_wave(const WaveArgs a, const Op op) {
   constexpr int NTC = TY * 32;
-  __shared__ T xch[2][TY][32];
-  __shared__ T bufX[kRing][TY];
-  __shared__ T bufY[kRing][32];
-  __shared__ volatile int s_done, s_availX, s_availY, s_abort;
-  __shared__ int s_tile;
-  __shared__ bool s_last;
+  __shared__ WaveShared<T, TY> sh;
   if (a.use_skip && a.sc->done != DONE_RUNNING) return;
   if (a.sc->err & DEV_ERR_TIMEOUT) return;  // an earlier sweep gave up: do not wait again
   const Tiled& g = a.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ntiles = g.ntx * g.nty;
+  const int ntiles = g.ntiles();
   const int NS = g.nz + 31 + TY - 1;
+  T* mbx = reinterpret_cast<T*>(a.mbx);
+  T* mby = reinterpret_cast<T*>(a.mby);
   double acc = 0.0;
   for (;;) {
     if (threadIdx.x == 0) {
-      s_tile = atomicAdd(a.ticket, 1);
-      s_done = 0;
-      s_availX = 0;
-      s_availY = 0;
-      s_abort = 0;
+      sh.tile = atomicAdd(a.ticket, 1);
+      sh.done = 0;
+      sh.availX = 0;
+      sh.availY = 0;
+      sh.abort = 0;
     }
     __syncthreads();
-    const int t = s_tile;
+    const int t = sh.tile;
     if (t >= ntiles) break;
     const int2 XY = a.order[FWD ? t : ntiles - 1 - t];
     const int X = XY.x, Y = XY.y;
+    const int tid = Y * g.ntx + X;
     const bool hasX = FWD ? (X > 0) : (X < g.ntx - 1);
     const bool hasY = FWD ? (Y > 0) : (Y < g.nty - 1);
-    const int Xn = FWD ? X - 1 : X + 1, Yn = FWD ? Y - 1 : Y + 1;
+    // consumers of this tile's boundary values
+    const bool outX = FWD ? (X < g.ntx - 1) : (X > 0);
+    const bool outY = FWD ? (Y < g.nty - 1) : (Y > 0);
+    const int cX = FWD ? tid + 1 : tid - 1, cY = FWD ? tid + g.ntx : tid - g.ntx;
     const int64_t base = g.tile_base(X, Y);
     if (warp == TY) {
-      wave_comm<T, TY, FWD>(a, op.out, Y * g.ntx + X, hasX ? Y * g.ntx + Xn : 0,
-                            hasY ? Yn * g.ntx + X : 0, hasX ? g.tile_base(Xn, Y) : 0,
-                            hasY ? g.tile_base(X, Yn) : 0, hasX, hasY, NS, bufX, bufY, &s_done,
-                            &s_availX, &s_availY, &s_abort);
+      if (hasX) wave_load_x<T, TY, FWD>(a, sh, mbx + (int64_t)tid * a.mb_stride_x, NS);
+    } else if (warp == TY + 1) {
+      if (hasY) wave_load_y<T, TY, FWD>(a, sh, mby + (int64_t)tid * a.mb_stride_y, NS);
     } else {
       const int ty = warp;
       const int x = X * 32 + lane, y = Y * TY + ty;
+      T* outx = outX ? mbx + (int64_t)cX * a.mb_stride_x : nullptr;
+      T* outy = outY ? mby + (int64_t)cY * a.mb_stride_y : nullptr;
+      const bool xsrc = FWD ? (lane == 31) : (lane == 0);        // lane feeding the x consumer
+      const bool ysrc = FWD ? (ty == TY - 1) : (ty == 0);        // warp feeding the y consumer
       typename Op::In ring[kPrefetch];
 #pragma unroll
       for (int u = 0; u < kPrefetch; u++)
-        if (u < NS)
-          ring[u] = op.load(base + ((int64_t)wave_slot<T, TY, FWD>(g, u, ty) * TY + ty) * 32 + lane);
+        if (u < NS) ring[u] = op.load(base + ((int64_t)wave_slot<TY, FWD>(g, u, ty) * TY + ty) * 32 + lane);
       T prev = T(0);
+      // Executed by all lanes of warp 0 (warp-uniform loop: every lane reads the
+      // same shared-memory flags), so the warp stays converged at the barrier.
       auto wait_avail = [&](int s) {
         int spins = 0;
-        while (((hasX && s_availX <= s) || (hasY && s_availY <= s)) && !s_abort) {
-          if (++spins > kSpinLimit) {
-            atomicOr(&a.sc->err, DEV_ERR_TIMEOUT);
-            s_abort = 1;
+        while (((hasX && sh.availX <= s) || (hasY && sh.availY <= s)) && !sh.abort) {
+          if (++spins > kSpinLimit * 4) {
+            if (lane == 0) wave_abort(a, sh, NS);
             break;
           }
-          __nanosleep(20);
         }
+        __syncwarp();
         __threadfence_block();
       };
-      if (threadIdx.x == 0) wait_avail(0);
+      if (warp == 0) wait_avail(0);
       named_bar_sync(1, NTC);
       for (int s0 = 0; s0 < NS; s0 += kPrefetch) {
 #pragma unroll
@@ -737,30 +798,33 @@ __global__ void __launch_bounds__((TY + 1) * 32, 1) k_wave(const WaveArgs a, con
           if (s < NS) {
             const typename Op::In in = ring[u];
             if (s + kPrefetch < NS)
-              ring[u] = op.load(
-                  base + ((int64_t)wave_slot<T, TY, FWD>(g, s + kPrefetch, ty) * TY + ty) * 32 + lane);
+              ring[u] = op.load(base + ((int64_t)wave_slot<TY, FWD>(g, s + kPrefetch, ty) * TY + ty) * 32 + lane);
             const int z = FWD ? (s - ty - lane) : (g.nz - 1 - (s - (TY - 1 - ty) - (31 - lane)));
             const bool valid = (z >= 0) && (z < g.nz);
-            const T sh = FWD ? __shfl_up_sync(kFull, prev, 1) : __shfl_down_sync(kFull, prev, 1);
+            const T shv = FWD ? __shfl_up_sync(kFull, prev, 1) : __shfl_down_sync(kFull, prev, 1);
             const bool xedge = FWD ? (lane == 0) : (lane == 31);
-            const T xn = xedge ? (hasX ? bufX[s % kRing][ty] : T(0)) : sh;
+            const T xn = xedge ? (hasX ? sh.bufX[s % kRing][ty] : T(0)) : shv;
             T yn;
             if (FWD)
-              yn = ty > 0 ? xch[(s + 1) & 1][ty - 1][lane] : (hasY ? bufY[s % kRing][lane] : T(0));
+              yn = ty > 0 ? sh.xch[(s + 1) & 1][ty - 1][lane] : (hasY ? sh.bufY[s % kRing][lane] : T(0));
             else
-              yn = ty < TY - 1 ? xch[(s + 1) & 1][ty + 1][lane]
-                               : (hasY ? bufY[s % kRing][lane] : T(0));
+              yn = ty < TY - 1 ? sh.xch[(s + 1) & 1][ty + 1][lane]
+                               : (hasY ? sh.bufY[s % kRing][lane] : T(0));
             T val = T(0);
             if (valid) {
-              const int64_t e = base + ((int64_t)wave_slot<T, TY, FWD>(g, s, ty) * TY + ty) * 32 + lane;
+              const int64_t e = base + ((int64_t)wave_slot<TY, FWD>(g, s, ty) * TY + ty) * 32 + lane;
               val = op.compute(in, xn, yn, prev, x, y, z, e, acc);
               op.out[e] = val;
+              if (xsrc && outx) mb_store(outx + (int64_t)(s - 31) * TY + ty, val);
+              if (ysrc && outy) mb_store(outy + (int64_t)(s - (TY - 1)) * 32 + lane, val);
             }
-            xch[s & 1][ty][lane] = val;
+            sh.xch[s & 1][ty][lane] = val;
             prev = val;
-            if (threadIdx.x == 0) {
-              __threadfence_block();
-              s_done = s;
+            if (warp == 0) {
+              if (lane == 0) {
+                __threadfence_block();
+                sh.done = s;
+              }
               if (s + 1 < NS) wait_avail(s + 1);
             }
             named_bar_sync(1, NTC);
@@ -769,42 +833,52 @@ __global__ void __launch_bounds__((TY + 1) * 32, 1) k_wave(const WaveArgs a, con
       }
       if (threadIdx.x == 0) {
         __threadfence_block();
-        s_done = NS;
+        sh.done = NS;
+      }
+    }
+    // this tile's share of the dot product (summed later in tile order, so the
+    // result does not depend on which CTA swept which tile)
+    {
+      double v = warp_sum(acc);
+      acc = 0.0;
+      if (lane == 0) sh.ssum[warp] = v;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double S = 0.0;
+        for (int i = 0; i < TY + 2; i++) S += sh.ssum[i];
+        a.tile_partials[tid] = S;
       }
     }
     __syncthreads();
   }
   // CTA partial of the accumulated dot product, then exit accounting.  The last
-  // CTA to exit finalizes the reduction and resets the scheduling state.
+  // CTA to exit finalizes the reduction and resets the ticket counters.
   {
-    __shared__ double ssum[(TY + 1)];
-    double v = warp_sum(acc);
-    if (lane == 0) ssum[warp] = v;
-    __syncthreads();
     if (threadIdx.x == 0) {
-      double S = 0.0;
-      for (int i = 0; i < TY + 1; i++) S += ssum[i];
-      a.partials[2 * blockIdx.x] = S;
-      a.partials[2 * blockIdx.x + 1] = 0.0;
       __threadfence();
       int prev = atomicAdd(a.exits, 1);
-      s_last = (prev == (int)gridDim.x - 1);
+      sh.last = (prev == (int)gridDim.x - 1);
     }
     __syncthreads();
-    if (s_last) {
+    if (sh.last && threadIdx.x == 0) {
       __threadfence();
-      for (int i = threadIdx.x; i < ntiles; i += blockDim.x) a.progress[i] = 0;
-      if (threadIdx.x == 0) {
-        double S = 0.0;
-        for (int b = 0; b < (int)gridDim.x; b++) S += __ldcg(&a.partials[2 * b]);
-        *a.ticket = 0;
-        *a.exits = 0;
-        if (a.fin_kind != FIN_NONE) finalize(a.fin_kind, a.sc, S, 0.0);
-        if (a.sc->err & DEV_ERR_TIMEOUT) a.sc->done = DONE_BREAKDOWN;
-      }
+      double S = 0.0;
+      for (int b = 0; b < ntiles; b++) S += __ldcg(&a.tile_partials[b]);
+      *a.ticket = 0;
+      *a.exits = 0;
+      if (a.fin_kind != FIN_NONE) finalize(a.fin_kind, a.sc, S, 0.0);
+      if (a.sc->err & DEV_ERR_TIMEOUT) a.sc->done = DONE_BREAKDOWN;
       __threadfence();
     }
   }
+}
+
+// Fill the mailboxes with the sentinel (at allocation and after an error).
+template <class T>
+__global__ void k_mb_reset(int64_t n, T* mb) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride)
+    mb_reset(mb + e);
 }
 
 inline int grid_for(int64_t n, int sm) {
@@ -827,15 +901,46 @@ cudaGraphExec_t& PcgSolver::graph_for<float>() {
   return graph32_;
 }
 
+void PcgSolver::reset_mailboxes(bool f32) {
+  const int ntiles = g_.ntiles();
+  const int64_t nx_ = mb_stride_x_ * ntiles, ny_ = mb_stride_y_ * ntiles;
+  const int grid = grid_for(std::max(nx_, ny_), ctx_->sm_count);
+  if (f32) {
+    k_mb_reset<float><<<grid, kThreads, 0, ctx_->stream>>>(nx_, mbx32_);
+    k_mb_reset<float><<<grid, kThreads, 0, ctx_->stream>>>(ny_, mby32_);
+  } else {
+    k_mb_reset<double><<<grid, kThreads, 0, ctx_->stream>>>(nx_, mbx64_);
+    k_mb_reset<double><<<grid, kThreads, 0, ctx_->stream>>>(ny_, mby64_);
+  }
+}
+
+WaveArgs PcgSolver::wave_args(bool f32, int use_skip, int fin) const {
+  WaveArgs w{};
+  w.g = g_;
+  w.mbx = f32 ? (void*)mbx32_ : (void*)mbx64_;
+  w.mby = f32 ? (void*)mby32_ : (void*)mby64_;
+  w.mb_stride_x = mb_stride_x_;
+  w.mb_stride_y = mb_stride_y_;
+  w.ticket = ws_.ticket;
+  w.exits = ws_.exits;
+  w.order = ws_.order_fwd;
+  w.sc = sc_;
+  w.partials = partials_;
+  w.tile_partials = tile_partials_;
+  w.use_skip = use_skip;
+  w.fin_kind = fin;
+  return w;
+}
+
 PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt)
     : ctx_(ctx), opt_(opt) {
   if (nx < 1 || ny < 1 || nz < 1) {
     init_status_ = -1;
     return;
   }
-  g_ = Tiled::make(nx, ny, nz, kTY);
+  g_ = Tiled::make(nx, ny, nz);
   nblocks_ = ctx->sm_count * 4;
-  const int ntiles = g_.ntx * g_.nty;
+  const int ntiles = g_.ntiles();
   wave_grid_ = std::min(ntiles, ctx->sm_count);
   auto alloc = [&](size_t bytes) -> void* {
     void* p = nullptr;
@@ -857,20 +962,29 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
   active_ = (uint8_t*)alloc((size_t)g_.total);
   partials_ = (double*)alloc(sizeof(double) * 2 * (size_t)std::max(nblocks_, wave_grid_));
   sc_ = (PcgScalars*)alloc(sizeof(PcgScalars));
-  ws_.progress = (int*)alloc(sizeof(int) * (size_t)(ntiles + 2));
+  ws_.ticket = (int*)alloc(sizeof(int) * 2);
+  tile_partials_ = (double*)alloc(sizeof(double) * (size_t)ntiles);
   int2* order = (int2*)alloc(sizeof(int2) * (size_t)ntiles);
-  if (!active_ || !partials_ || !sc_ || !ws_.progress || !order) {
+  // mailboxes (FP64; the FP32 ones are allocated with the FP32 arrays)
+  const int NS = nz + 31 + Tiled::TY - 1;
+  mb_stride_x_ = (int64_t)NS * Tiled::TY;
+  mb_stride_y_ = (int64_t)NS * 32;
+  mbx64_ = (double*)alloc(sizeof(double) * (size_t)(mb_stride_x_ * ntiles));
+  mby64_ = (double*)alloc(sizeof(double) * (size_t)(mb_stride_y_ * ntiles));
+  if (!active_ || !partials_ || !sc_ || !ws_.ticket || !order || !mbx64_ || !mby64_ ||
+      !tile_partials_) {
     init_status_ = -3;
     return;
   }
-  ws_.ticket = ws_.progress + ntiles;
-  ws_.exits = ws_.progress + ntiles + 1;
+  ws_.exits = ws_.ticket + 1;
   ws_.order_fwd = order;
-  cudaMemsetAsync(ws_.progress, 0, sizeof(int) * (size_t)(ntiles + 2), ctx->stream);
-  cudaMemsetAsync(d64_.adiag, 0, n64, ctx->stream);
+  cudaMemsetAsync(ws_.ticket, 0, sizeof(int) * 2, ctx->stream);
   for (double** a : arr64) cudaMemsetAsync(*a, 0, n64, ctx->stream);
   cudaMemsetAsync(active_, 0, (size_t)g_.total, ctx->stream);
   cudaMemsetAsync(sc_, 0, sizeof(PcgScalars), ctx->stream);
+  cudaMemsetAsync(partials_, 0, sizeof(double) * 2 * (size_t)std::max(nblocks_, wave_grid_),
+                  ctx->stream);
+  reset_mailboxes(false);
   // tile order: anti-diagonals of the tile grid, so every tile's forward
   // predecessors (X-1,Y), (X,Y-1) hold smaller tickets; reversed for backward.
   std::vector<int2> ord;
@@ -1020,10 +1134,10 @@ int PcgSolver::ensure_pivots() {
   if (pivots_valid_) return 0;
   cudaStream_t st = ctx_->stream;
   const int grid = grid_for(g_.total, ctx_->sm_count);
-  WaveArgs wa{g_, ws_.progress, ws_.ticket, ws_.exits, ws_.order_fwd, sc_, partials_, 0, FIN_NONE};
+  WaveArgs wa = wave_args(false, 0, FIN_NONE);
   PivotOp op{g_,         d64_.adiag, d64_.al, d64_.ad, d64_.ab, active_, opt_.tau,
              opt_.sigma, d64_.E,     d64_.cL, d64_.cD, d64_.cB};
-  k_wave<double, kTY, true, PivotOp><<<wave_grid_, (kTY + 1) * 32, 0, st>>>(wa, op);
+  k_wave<double, Tiled::TY, true, PivotOp><<<wave_grid_, (Tiled::TY + 2) * 32, 0, st>>>(wa, op);
   k_upper<double><<<grid, kThreads, 0, st>>>(g_, d64_.cL, d64_.cD, d64_.cB, d64_.uR, d64_.uU,
                                               d64_.uF);
   if (opt_.precision == PREC_MIXED) {
@@ -1044,6 +1158,16 @@ int PcgSolver::ensure_pivots() {
         return ctx_->set_error(-3, "FP64 accumulator allocation failed");
       allocs_.push_back(p);
       xacc_ = (double*)p;
+      const int ntiles = g_.ntiles();
+      void *px = nullptr, *py = nullptr;
+      if (cudaMalloc(&px, sizeof(float) * (size_t)(mb_stride_x_ * ntiles)) != cudaSuccess ||
+          cudaMalloc(&py, sizeof(float) * (size_t)(mb_stride_y_ * ntiles)) != cudaSuccess)
+        return ctx_->set_error(-3, "FP32 mailbox allocation failed");
+      allocs_.push_back(px);
+      allocs_.push_back(py);
+      mbx32_ = (float*)px;
+      mby32_ = (float*)py;
+      reset_mailboxes(true);
       have_f32_ = true;
     }
     const double* s64[] = {d64_.adiag, d64_.al, d64_.ad, d64_.ab, d64_.E, d64_.cL,
@@ -1062,16 +1186,16 @@ int PcgSolver::ensure_pivots() {
 template <class T>
 void PcgSolver::launch_iteration(SysArrays<T>& A) {
   cudaStream_t st = ctx_->stream;
-  WaveArgs wf{g_, ws_.progress, ws_.ticket, ws_.exits, ws_.order_fwd, sc_, partials_, 1, FIN_NONE};
-  WaveArgs wb = wf;
-  wb.fin_kind = FIN_BWD;
+  const bool f32 = sizeof(T) == 4;
+  WaveArgs wf = wave_args(f32, 1, FIN_NONE);
+  WaveArgs wb = wave_args(f32, 1, FIN_BWD);
   k_spmv<T><<<nblocks_, kThreads, 0, st>>>(g_, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az,
                                             partials_, sc_, 1);
   k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.s, A.Az, A.p, A.r, partials_, sc_);
   FwdOp<T> fo{A.r, A.cL, A.cD, A.cB, A.E, A.q};
-  k_wave<T, kTY, true, FwdOp<T>><<<wave_grid_, (kTY + 1) * 32, 0, st>>>(wf, fo);
+  k_wave<T, Tiled::TY, true, FwdOp<T>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, st>>>(wf, fo);
   BwdOp<T> bo{A.q, A.E, A.uR, A.uU, A.uF, A.r, A.z};
-  k_wave<T, kTY, false, BwdOp<T>><<<wave_grid_, (kTY + 1) * 32, 0, st>>>(wb, bo);
+  k_wave<T, Tiled::TY, false, BwdOp<T>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, st>>>(wb, bo);
   k_sa<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.s, partials_, sc_);
 }
 
@@ -1092,13 +1216,13 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
   const double scale = scale_rhs ? 1.0 / inner_scale_ : 1.0;
   k_init<T><<<nblocks_, kThreads, 0, s>>>(g_, src, scale, active_, A.r, A.p, partials_, sc_);
   // z = M^-1 r ; s = z ; sigma = z.r
-  WaveArgs wf{g_, ws_.progress, ws_.ticket, ws_.exits, ws_.order_fwd, sc_, partials_, 1, FIN_NONE};
-  WaveArgs wb = wf;
-  wb.fin_kind = FIN_BWD;
+  const bool f32 = sizeof(T) == 4;
+  WaveArgs wf = wave_args(f32, 1, FIN_NONE);
+  WaveArgs wb = wave_args(f32, 1, FIN_BWD);
   FwdOp<T> fo{A.r, A.cL, A.cD, A.cB, A.E, A.q};
-  k_wave<T, kTY, true, FwdOp<T>><<<wave_grid_, (kTY + 1) * 32, 0, s>>>(wf, fo);
+  k_wave<T, Tiled::TY, true, FwdOp<T>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, s>>>(wf, fo);
   BwdOp<T> bo{A.q, A.E, A.uR, A.uU, A.uF, A.r, A.z};
-  k_wave<T, kTY, false, BwdOp<T>><<<wave_grid_, (kTY + 1) * 32, 0, s>>>(wb, bo);
+  k_wave<T, Tiled::TY, false, BwdOp<T>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, s>>>(wb, bo);
   k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.z, A.s, sc_);
   int e = check_dev_error("pcg init");
   if (e) return e;
@@ -1140,6 +1264,7 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
     st->iterations += last_.iter;
     st->status = last_.done;
     st->residual = last_.res;
+    st->device_flags |= last_.err;
   }
   if (last_.err & DEV_ERR_TIMEOUT) return ctx_->set_error(-6, "wavefront wait timed out");
   return check_dev_error("pcg");
@@ -1182,7 +1307,10 @@ int PcgSolver::solve_mixed(PcgStats* st) {
     PcgStats inner{};
     e = run_pcg<float>(d32_, std::min(want, 0.5), CRIT_REL_L2, opt_.max_iter, true, &inner);
     if (e) return e;
-    if (st) st->iterations += inner.iterations;
+    if (st) {
+      st->iterations += inner.iterations;
+      st->device_flags |= inner.device_flags;
+    }
     outer++;
     // x += rnorm d ; r -= rnorm A d   (FP64)
     k_mixed_update<<<nblocks_, kThreads, 0, s>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab,
@@ -1257,16 +1385,16 @@ int PcgSolver::precond_only(const double* r, double* z) {
   init.done = DONE_RUNNING;
   init.first = 1;
   cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
-  WaveArgs wf{g_, ws_.progress, ws_.ticket, ws_.exits, ws_.order_fwd, sc_, partials_, 0, FIN_NONE};
-  WaveArgs wb = wf;
-  wb.fin_kind = FIN_BWD;
+  WaveArgs wf = wave_args(false, 0, FIN_NONE);
+  WaveArgs wb = wave_args(false, 0, FIN_BWD);
   FwdOp<double> fo{d64_.r, d64_.cL, d64_.cD, d64_.cB, d64_.E, d64_.q};
-  k_wave<double, kTY, true, FwdOp<double>><<<wave_grid_, (kTY + 1) * 32, 0, s>>>(wf, fo);
+  k_wave<double, Tiled::TY, true, FwdOp<double>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, s>>>(wf, fo);
   BwdOp<double> bo{d64_.q, d64_.E, d64_.uR, d64_.uU, d64_.uF, d64_.r, d64_.z};
-  k_wave<double, kTY, false, BwdOp<double>><<<wave_grid_, (kTY + 1) * 32, 0, s>>>(wb, bo);
+  k_wave<double, Tiled::TY, false, BwdOp<double>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, s>>>(wb, bo);
   k_from_tiled<double, double><<<grid, kThreads, 0, s>>>(g_, d64_.z, z);
   cudaMemcpyAsync(sc_host_, sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("precond");
+  last_ = *sc_host_;
   if (sc_host_->err & DEV_ERR_TIMEOUT) return ctx_->set_error(-6, "wavefront wait timed out");
   return check_dev_error("precond");
 }
@@ -1280,6 +1408,53 @@ int PcgSolver::apply_only(const double* x, double* b) {
   k_from_tiled<double, double><<<grid, kThreads, 0, s>>>(g_, d64_.Az, b);
   if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("apply");
   return check_dev_error("apply");
+}
+
+
+namespace {
+template <class T>
+__global__ void k_mb_count(int64_t n, const T* mb, unsigned long long* cnt) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  unsigned long long c = 0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    typename Sentinel<T>::Bits b;
+    memcpy(&b, mb + e, sizeof(T));
+    if (b != Sentinel<T>::bits) c++;
+  }
+  if (c) atomicAdd(cnt, c);
+}
+}  // namespace
+
+// Debug: copy an internal tiled FP64 array to a device buffer in reference layout
+// (0 E, 1 cL, 2 cD, 3 cB, 4 uR, 5 uU, 6 uF, 7 q, 8 z); which = 100/101 counts
+// non-sentinel x/y mailbox words into out[0].
+int PcgSolver::debug_dump(int which, double* out) {
+  cudaStream_t s = ctx_->stream;
+  const int grid = grid_for(g_.total, ctx_->sm_count);
+  if (which >= 100) {
+    unsigned long long* cnt = nullptr;
+    cudaMallocAsync(&cnt, 8, s);
+    cudaMemsetAsync(cnt, 0, 8, s);
+    const int ntiles = g_.ntiles();
+    if (which == 100) k_mb_count<double><<<grid, kThreads, 0, s>>>(mb_stride_x_ * ntiles, mbx64_, cnt);
+    else k_mb_count<double><<<grid, kThreads, 0, s>>>(mb_stride_y_ * ntiles, mby64_, cnt);
+    unsigned long long h = 0;
+    cudaMemcpyAsync(&h, cnt, 8, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    cudaFreeAsync(cnt, s);
+    out[0] = (double)h;
+    return check_dev_error("debug");
+  }
+  const double* src[] = {d64_.E, d64_.cL, d64_.cD, d64_.cB, d64_.uR, d64_.uU, d64_.uF, d64_.q, d64_.z};
+  if (which < 0 || which > 8) return -1;
+  double* tmp = nullptr;
+  const int64_t N = (int64_t)g_.nx * g_.ny * g_.nz;
+  cudaMallocAsync(&tmp, sizeof(double) * N, s);
+  k_from_tiled<double, double><<<grid, kThreads, 0, s>>>(g_, src[which], tmp);
+  cudaMemcpyAsync(out, tmp, sizeof(double) * N, cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(tmp, s);
+  cudaStreamSynchronize(s);
+  return check_dev_error("debug");
 }
 
 }  // namespace sc

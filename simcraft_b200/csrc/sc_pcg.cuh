@@ -15,7 +15,6 @@
 
 namespace sc {
 
-constexpr int kTY = 8;  // rows (y) per wavefront tile; the tile is 32 (x) by kTY (y)
 
 struct Context {
   int device = 0;
@@ -55,6 +54,7 @@ struct PcgStats {
   double true_linf = 0;      // ||b - A p||_inf in FP64
   double ms = 0;             // device time of the solve (events)
   double sym_err = 0;        // max |A_R(p) - A_L(p+x)| etc. when checked
+  unsigned device_flags = 0; // DEV_ERR_* bits raised on the device
 };
 
 // Device scalars shared by the kernels of one PCG run.
@@ -69,9 +69,25 @@ struct PcgScalars {
   int pad;
 };
 
+struct PcgScalars;
+// Arguments of one wavefront sweep kernel launch.
+struct WaveArgs {
+  Tiled g;
+  void* mbx;           // x mailboxes: per consumer tile, mb_stride_x elements
+  void* mby;           // y mailboxes: per consumer tile, mb_stride_y elements
+  int64_t mb_stride_x, mb_stride_y;
+  int* ticket;
+  int* exits;
+  const int2* order;
+  PcgScalars* sc;
+  double* partials;
+  double* tile_partials;  // per tile share of the sweep's dot product
+  int use_skip;
+  int fin_kind;
+};
+
 // Wavefront scheduling state (one per sweep kernel; reset by the kernel's last CTA).
 struct WaveSync {
-  int* progress;      // per tile: completed steps
   int* ticket;        // next tile ticket
   int* exits;         // CTAs that found no more tiles
   int2* order_fwd;    // ticket -> tile (X,Y) for forward sweeps
@@ -103,6 +119,7 @@ class PcgSolver {
   int precond_only(const double* r, double* z);
   // applyCompressedMatrix on the uploaded system (device pointers, reference layout).
   int apply_only(const double* x, double* b);
+  int debug_dump(int which, double* out);
 
   const Tiled& geom() const { return g_; }
   // Direct access for in-device producers (FLIP buildSystem writes these).
@@ -144,9 +161,16 @@ class PcgSolver {
   double* xacc_ = nullptr;  // mixed: FP64 solution accumulator
   uint8_t* active_ = nullptr;
   double* partials_ = nullptr;  // 2 per block
+  double* tile_partials_ = nullptr;
   PcgScalars* sc_ = nullptr;
   PcgScalars* sc_host_ = nullptr;  // pinned
   WaveSync ws_{};
+  // wavefront mailboxes (per consumer tile), FP64 and FP32
+  double *mbx64_ = nullptr, *mby64_ = nullptr;
+  float *mbx32_ = nullptr, *mby32_ = nullptr;
+  int64_t mb_stride_x_ = 0, mb_stride_y_ = 0;
+  void reset_mailboxes(bool f32);
+  WaveArgs wave_args(bool f32, int use_skip, int fin) const;
   std::vector<void*> allocs_;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;    // chunk polling
   cudaEvent_t evt0_ = nullptr, evt1_ = nullptr;  // solve timing

@@ -39,7 +39,11 @@ class Context:
         check("sc_context_synchronize", lib().sc_context_synchronize(self.handle), self.handle)
 
     def set_stream(self, stream_ptr):
+        """Order later work on `stream_ptr` (None/0 = the legacy default stream)."""
         check("sc_context_set_stream", lib().sc_context_set_stream(self.handle, stream_ptr), self.handle)
+
+    def use_own_stream(self):
+        check("sc_context_use_own_stream", lib().sc_context_use_own_stream(self.handle), self.handle)
 
     @property
     def stream(self):
@@ -69,6 +73,23 @@ def default_options(**kw):
 
 def _is_torch(a):
     return type(a).__module__.startswith("torch")
+
+
+class _on_torch_stream:
+    """Runs device-pointer calls on torch's current CUDA stream, so they are
+    ordered with the torch operations that produced and consume the tensors."""
+
+    def __init__(self, ctx, tensor):
+        self.ctx, self.tensor = ctx, tensor
+
+    def __enter__(self):
+        import torch
+
+        self.ctx.set_stream(ctypes.c_void_p(torch.cuda.current_stream(self.tensor.device).cuda_stream))
+
+    def __exit__(self, *exc):
+        self.ctx.use_own_stream()
+        return False
 
 
 def _ptr(a):
@@ -119,8 +140,9 @@ class CgSolver3D:
         if _is_torch(pg):
             fn = "sc_pcg_solve_device"
             an = ptr_array([_ptr(a) for a in Aneighbour])
-            rc = lib().sc_pcg_solve_device(self.handle, _ptr(Adiag), an, _ptr(rhs), _ptr(active), _ptr(pg),
-                                           ctypes.byref(st))
+            with _on_torch_stream(self.ctx, pg):
+                rc = lib().sc_pcg_solve_device(self.handle, _ptr(Adiag), an, _ptr(rhs), _ptr(active), _ptr(pg),
+                                               ctypes.byref(st))
         else:
             fn = "sc_pcg_solve_host"
             Adiag = _prep_host(Adiag, np.float64)
@@ -145,15 +167,23 @@ class CgSolver3D:
             active = _prep_host(active, np.uint8)
         self._keep = (Adiag, Aneighbour, rhs, active)
         an = ptr_array([_ptr(a) for a in Aneighbour])
-        check("sc_pcg_upload", lib().sc_pcg_upload(self.handle, _ptr(Adiag), an, _ptr(rhs), _ptr(active),
-                                                   1 if dev else 0), self.ctx.handle)
+        if dev:
+            with _on_torch_stream(self.ctx, Adiag):
+                rc = lib().sc_pcg_upload(self.handle, _ptr(Adiag), an, _ptr(rhs), _ptr(active), 1)
+                self.ctx.synchronize()
+        else:
+            rc = lib().sc_pcg_upload(self.handle, _ptr(Adiag), an, _ptr(rhs), _ptr(active), 0)
+        check("sc_pcg_upload", rc, self.ctx.handle)
 
     def upload_rhs(self, rhs):
         dev = _is_torch(rhs)
         if not dev:
             rhs = _prep_host(rhs, np.float64)
-        check("sc_pcg_upload_rhs", lib().sc_pcg_upload_rhs(self.handle, _ptr(rhs), 1 if dev else 0),
-              self.ctx.handle)
+            check("sc_pcg_upload_rhs", lib().sc_pcg_upload_rhs(self.handle, _ptr(rhs), 0), self.ctx.handle)
+            return
+        with _on_torch_stream(self.ctx, rhs):
+            check("sc_pcg_upload_rhs", lib().sc_pcg_upload_rhs(self.handle, _ptr(rhs), 1), self.ctx.handle)
+            self.ctx.synchronize()
 
     def solve_resident(self):
         st = _capi.sc_pcg_stats()
@@ -163,18 +193,23 @@ class CgSolver3D:
         return self.last_stats
 
     def download(self, pg):
-        check("sc_pcg_download", lib().sc_pcg_download(self.handle, _ptr(pg), 1 if _is_torch(pg) else 0),
-              self.ctx.handle)
+        if _is_torch(pg):
+            with _on_torch_stream(self.ctx, pg):
+                check("sc_pcg_download", lib().sc_pcg_download(self.handle, _ptr(pg), 1), self.ctx.handle)
+        else:
+            check("sc_pcg_download", lib().sc_pcg_download(self.handle, _ptr(pg), 0), self.ctx.handle)
         return pg
 
     def precond(self, r, z):
         """ModifiedIncompleteCholesky3D::precond on the uploaded system (device tensors)."""
-        check("sc_pcg_precond_device", lib().sc_pcg_precond_device(self.handle, _ptr(r), _ptr(z)),
-              self.ctx.handle)
+        with _on_torch_stream(self.ctx, z):
+            check("sc_pcg_precond_device", lib().sc_pcg_precond_device(self.handle, _ptr(r), _ptr(z)),
+                  self.ctx.handle)
         return z
 
     def apply(self, x, b):
         """applyCompressedMatrix on the uploaded system (device tensors)."""
-        check("sc_pcg_apply_device", lib().sc_pcg_apply_device(self.handle, _ptr(x), _ptr(b)),
-              self.ctx.handle)
+        with _on_torch_stream(self.ctx, b):
+            check("sc_pcg_apply_device", lib().sc_pcg_apply_device(self.handle, _ptr(x), _ptr(b)),
+                  self.ctx.handle)
         return b

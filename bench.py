@@ -1,0 +1,360 @@
+"""Benchmark: SimCraft FluidSim pressure solve on B200.
+
+Workload (N=1): standalone pressure solve on a 128^3 grid (fluid = seeded union
+of 24 spheres at 50% fill, empty collider, solid walls, dt/h = 32/120), MIC(0)
+preconditioned CG to 1e-8 relative residual; the mixed FP32-inner / FP64
+defect-correction solve is the headline `value`, the plain FP64 solve is
+reported beside it.  A step is one complete CgSolver3D::solve call: system
+upload into the solver's layout, MIC(0) pivots, PCG iterations, pressure
+download.  Multi-GPU runs are independent replicas (the MIC(0) sweep is one
+global wavefront and does not shard).
+
+`--impl reference` times the CPU restatement of the reference (the oracle,
+OpenMP where the reference uses TBB) on the same system.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms per pressure solve to 1e-8 rel. residual (mixed vs FP64 PCG); FLIP steps/s"
+N_GRID = 128
+TOL = 1e-8
+DT_OVER_H = 32.0 / 120.0
+
+
+def build_scene(n):
+    from simcraft_b200 import scenes
+
+    sdf, info = scenes.sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=0.5, seed=2)
+    return np.ascontiguousarray(sdf), info
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_traffic():
+    """Per-launch DRAM traffic of the backward sweep from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "pcg_sweeps_128.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch_bwd_fp64:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def cpu_solve_ms(sysm, rhs, threads):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.build()
+    O.set_threads(threads)
+    O.set_parity_mode(False)
+    t = time.perf_counter()
+    pg, res, it = O.pcg_solve(sysm["adiag"], sysm["an"], rhs, sysm["active"], tol=TOL, max_iter=5000,
+                              criterion=O.CRIT_REL_L2)
+    return (time.perf_counter() - t) * 1e3, it, pg
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from simcraft_b200 import scenes
+
+    O.build()
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    O.set_parity_mode(False)
+    n = N_GRID
+    sdf, _ = build_scene(n)
+    h = 1.0 / n
+    z = np.zeros
+    S = O.build_system((n, n, n), h, DT_OVER_H * h, z((n + 1, n, n)), z((n, n + 1, n)), z((n, n, n + 1)), sdf)
+    rhs, _ = scenes.poisson_rhs(S["active"], sdf, seed=3)
+    rhs = np.ascontiguousarray(rhs)
+    times = []
+    for i in range(args.warmup + args.steps):
+        ms, it, _ = cpu_solve_ms(S, rhs, threads)
+        if i >= args.warmup:
+            times.append(ms)
+    v = float(np.mean(times))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "ms/solve", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded spheres)",
+        "config": {"workload": f"standalone pressure solve {n}^3, FP64 MIC(0)-PCG to {TOL:g} rel. residual",
+                   "grid": [n, n, n], "iterations": it},
+        "cpu_baseline": {"value": v, "unit": "ms/solve", "cores": threads, "kind": "port",
+                         "sample": f"one full FP64 solve of the {n}^3 system per step (CPU oracle, "
+                                   f"OpenMP where the reference uses TBB, serial MIC(0) as the reference)"},
+        "e2e": {"value": v, "unit": "ms/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    from simcraft_b200 import _capi, scenes
+    from simcraft_b200.solver import CgSolver3D, Context, CRIT_REL_L2, PREC_FP64, PREC_MIXED
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ctx = Context(local)
+    L = _capi.lib()
+    n = N_GRID
+    h = 1.0 / n
+    dt = DT_OVER_H * h
+    N = n * n * n
+    sdf, info = build_scene(n)
+
+    # ---- build the system on the GPU (FvmSolver3D::buildSystem, zero velocity) ----
+    f64 = dict(dtype=torch.float64, device=dev)
+    sdf_d = torch.from_numpy(sdf).to(dev)
+    u = torch.zeros((n + 1, n, n), **f64)
+    v = torch.zeros((n, n + 1, n), **f64)
+    w = torch.zeros((n, n, n + 1), **f64)
+    adiag = torch.zeros((n, n, n), **f64)
+    an = [torch.zeros((n, n, n), **f64) for _ in range(6)]
+    rhs_b = torch.zeros((n, n, n), **f64)
+    active = torch.zeros((n, n, n), dtype=torch.uint8, device=dev)
+    uw, vw, ww = torch.zeros_like(u), torch.zeros_like(v), torch.zeros_like(w)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    ctx.set_stream(ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    rc = L.sc_fvm_build_system_device(ctx.handle, n, n, n, h, dt, _capi.SC_REAL_F64, ptr(u), ptr(v), ptr(w),
+                                      ptr(sdf_d), None, ptr(adiag), _capi.ptr_array([ptr(a) for a in an]),
+                                      ptr(rhs_b), ptr(active), ptr(uw), ptr(vw), ptr(ww))
+    _capi.check("sc_fvm_build_system_device", rc, ctx.handle)
+    ctx.use_own_stream()
+    torch.cuda.synchronize()
+    act_h = active.cpu().numpy()
+    rhs_h, rinfo = scenes.poisson_rhs(act_h, sdf, seed=3)
+    rhs_h = np.ascontiguousarray(rhs_h)
+    rhs_d = torch.from_numpy(rhs_h).to(dev)
+    n_active = int(act_h.sum())
+
+    # pinned host copies for the end-to-end arm (what a host caller passes)
+    pin = lambda t: t.cpu().pin_memory()
+    adiag_h, an_h, act_hp = pin(adiag), [pin(a) for a in an], pin(active)
+    rhs_hp = torch.from_numpy(rhs_h).pin_memory()
+    pg_h = torch.zeros((n, n, n), dtype=torch.float64).pin_memory()
+
+    def hptr(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    solvers = {
+        "mixed": CgSolver3D(n, n, n, context=ctx, tol=TOL, max_iter=5000, criterion=CRIT_REL_L2,
+                            precision=PREC_MIXED),
+        "fp64": CgSolver3D(n, n, n, context=ctx, tol=TOL, max_iter=5000, criterion=CRIT_REL_L2,
+                           precision=PREC_FP64),
+    }
+    pg_d = torch.zeros((n, n, n), **f64)
+    an_dev = _capi.ptr_array([ptr(a) for a in an])
+    an_host = _capi.ptr_array([hptr(a) for a in an_h])
+
+    def solve_device(s):
+        st = _capi.sc_pcg_stats()
+        rc = L.sc_pcg_solve_device(s.handle, ptr(adiag), an_dev, ptr(rhs_d), ptr(active), ptr(pg_d),
+                                   ctypes.byref(st))
+        _capi.check("sc_pcg_solve_device", rc, ctx.handle)
+        return st
+
+    def solve_host(s):
+        st = _capi.sc_pcg_stats()
+        rc = L.sc_pcg_solve_host(s.handle, hptr(adiag_h), an_host, hptr(rhs_hp), hptr(act_hp), hptr(pg_h),
+                                 ctypes.byref(st))
+        _capi.check("sc_pcg_solve_host", rc, ctx.handle)
+        return st
+
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def timed(fn, s):
+        """K steps between a barrier + synchronize; device time by CUDA events on the solver stream."""
+        for _ in range(args.warmup):
+            fn(s)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        last = None
+        for _ in range(args.steps):
+            last = fn(s)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, last
+
+    with Clocks(local) as clk:
+        ms_mixed, st_mixed = timed(solve_device, solvers["mixed"])
+        ms_fp64, st_fp64 = timed(solve_device, solvers["fp64"])
+        e2e_ms, st_e2e = timed(solve_host, solvers["mixed"])
+    clocks = clk.summary()
+
+    # per-kernel device times on the resident FP64 system -> roofline of the sweeps
+    kt = (ctypes.c_double * 6)()
+    _capi.check("sc_pcg_time_kernels", L.sc_pcg_time_kernels(solvers["fp64"].handle, 20, kt), ctx.handle)
+    kms = list(kt)
+    pk, pk_src = peaks()
+    s = 8
+    bytes_bwd = N * (7 * s + 1)  # backward sweep: q, E, 3 couplings, r read, z written, active
+    bytes_fwd = N * (6 * s + 1)
+    achieved = bytes_bwd / (kms[2] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "MIC(0) backward sweep, FP64 (k_wave BwdOp<double>)",
+                "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
+                "traffic": read_traffic(), "algorithmic_bytes_per_launch": bytes_bwd,
+                "ms_per_launch": kms[2],
+                "kernel_ms": {"pivot": kms[0], "forward_sweep": kms[1], "backward_sweep": kms[2],
+                              "spmv": kms[3], "axpy": kms[4], "scale_add": kms[5]},
+                "forward_sweep_gbs": bytes_fwd / (kms[1] * 1e-3) / 1e9}
+
+    ms_step = ms_mixed / args.steps
+    value = ms_step / world  # replicas: whole-job ms per solve
+    h2d = 5 * 8 * N + N  # Adiag, Left, Down, Back, rhs (doubles) + active (bytes)
+    d2h = 8 * N
+    out = {
+        "metric": METRIC, "value": value, "unit": "ms/solve", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64 (FP32 inner PCG, FP64 defect correction)",
+        "data": "synthetic (seeded sphere pool, no dataset)",
+        "config": {"workload": f"standalone pressure solve {n}^3, mixed MIC(0)-PCG to {TOL:g} rel. residual",
+                   "grid": [n, n, n], "fill": info["fill"], "active_cells": n_active,
+                   "dt_over_h": DT_OVER_H, "tolerance": TOL, "criterion": "relative L2",
+                   "cache": "inputs larger than L2 (solver working set ~300 MB at 128^3)",
+                   "parallelism": f"replicas x{world}"},
+        "fp64": {"ms_per_solve": ms_fp64 / args.steps, "iterations": st_fp64.iterations,
+                 "true_rel_l2": st_fp64.true_rel_l2},
+        "mixed": {"ms_per_solve": ms_step, "inner_iterations": st_mixed.iterations,
+                  "outer_passes": st_mixed.outer, "true_rel_l2": st_mixed.true_rel_l2},
+        "mixed_speedup_vs_fp64": (ms_fp64 / ms_mixed),
+        "e2e": {"value": e2e_ms / args.steps / world, "unit": "ms/solve", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "path": "sc_pcg_solve_host (CgSolver3D::solve on pinned host arrays)"},
+        "roofline": roofline,
+        "clocks": clocks,
+        "gpu_launches": None,
+    }
+    # kernels launched inside the timed region of the headline (mixed) arm,
+    # counted by the solver itself (CUDA-graph nodes included)
+    out["gpu_launches"] = int(st_mixed.kernel_launches) * args.steps
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        sysm = {"adiag": adiag.cpu().numpy(), "an": [a.cpu().numpy() for a in an], "active": act_h}
+        cms, cit, pg_cpu = cpu_solve_ms(sysm, rhs_h, threads)
+        a = act_h.astype(bool)
+        pg_gpu = pg_d.cpu().numpy()
+        out["cpu_baseline"] = {"value": cms, "unit": "ms/solve", "cores": threads, "kind": "port",
+                               "sample": f"one full FP64 solve of the same {n}^3 system (CPU oracle), "
+                                         f"{cit} iterations",
+                               "rel_l2_vs_gpu_fp64": float(np.linalg.norm(pg_gpu[a] - pg_cpu[a]) /
+                                                           np.linalg.norm(pg_cpu[a]))}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

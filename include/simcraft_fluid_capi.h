@@ -98,6 +98,7 @@ typedef struct {
   double ms;             /* device time of the solve */
   double sym_err;        /* max asymmetry found when check_symmetry is set */
   unsigned device_flags; /* device-side error bits: 1 wait timeout, 2 non-finite, 4 breakdown */
+  int64_t kernel_launches; /* kernels this call launched (CUDA-graph nodes counted) */
 } sc_pcg_stats;
 
 /* Defaults equal to the reference's constants. */
@@ -136,6 +137,40 @@ int sc_pcg_precond_device(sc_pcg* pcg, const double* r, double* z);
 /* applyCompressedMatrix (project-solver.cc:16-39) on the uploaded system:
  * b = A x, device pointers. */
 int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b);
+
+/* Per-kernel device time of the solver's kernels on the uploaded system (each
+ * kernel launched `reps` times, CUDA events on the context stream), in ms per
+ * launch: [0] pivot sweep, [1] forward sweep, [2] backward sweep, [3] SpMV,
+ * [4] axpy pair, [5] scale-and-add.  For profiling; leaves the solution
+ * untouched. */
+int sc_pcg_time_kernels(sc_pcg* pcg, int reps, double* ms_out);
+
+/* ---------------------------------------------------------------------------
+ * Finite-volume pressure system: FvmSolver3D
+ * (FluidSim/include/FluidSim/cpu/project-solver.h:133-182).
+ * `precision` is the type of the face velocity arrays (SC_REAL_F64 / SC_REAL_F32);
+ * the matrix, weights and pressure are always double.  collider_sdf == NULL is
+ * the empty-mesh collider (all face weights 1 except the domain walls).
+ * Cells are cubic with spacing h; device pointers, reference layout.
+ */
+#define SC_REAL_F64 0
+#define SC_REAL_F32 1
+
+/* FvmSolver3D::buildSystem(ug, vg, wg, fluidSdf, colliderSdf, dt)
+ * (project-solver.cc:59-228): face weights u/v/w_wt, Adiag, Aneighbour[6]
+ * (Directions order), rhs and active.  Any of adiag/an[i]/rhs/active may be
+ * NULL to skip that output. */
+int sc_fvm_build_system_device(sc_context* ctx, int nx, int ny, int nz, double h, double dt,
+                               int precision, const void* u, const void* v, const void* w,
+                               const double* fluid_sdf, const double* collider_sdf,
+                               double* adiag, double* const* an, double* rhs, uint8_t* active,
+                               double* u_wt, double* v_wt, double* w_wt);
+/* FvmSolver3D::project(ug, vg, wg, pg, fluidSdf, colliderSdf, dt)
+ * (project-solver.cc:348-435), in place on u, v, w. */
+int sc_fvm_project_device(sc_context* ctx, int nx, int ny, int nz, double h, double dt,
+                          int precision, void* u, void* v, void* w, const double* pg,
+                          const double* fluid_sdf, const double* u_wt, const double* v_wt,
+                          const double* w_wt);
 
 #ifdef __cplusplus
 }

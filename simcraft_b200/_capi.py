@@ -21,7 +21,8 @@ class sc_pcg_options(ctypes.Structure):
 class sc_pcg_stats(ctypes.Structure):
     _fields_ = [("iterations", c_int), ("outer", c_int), ("status", c_int), ("residual", c_double),
                 ("true_rel_l2", c_double), ("true_linf", c_double), ("ms", c_double),
-                ("sym_err", c_double), ("device_flags", ctypes.c_uint)]
+                ("sym_err", c_double), ("device_flags", ctypes.c_uint),
+                ("kernel_launches", c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -30,6 +31,7 @@ class sc_pcg_stats(ctypes.Structure):
 SC_OK = 0
 SC_CRIT_ABS_LINF, SC_CRIT_REL_L2 = 0, 1
 SC_PREC_FP64, SC_PREC_MIXED = 0, 1
+SC_REAL_F64, SC_REAL_F32 = 0, 1
 SC_DONE_CONVERGED, SC_DONE_MAXITER, SC_DONE_BREAKDOWN = 1, 2, 3
 
 _dpp = P(c_void_p)  # array of pointers
@@ -57,6 +59,12 @@ SIGNATURES = {
     "sc_pcg_download": (c_int, [c_void_p, c_void_p, c_int]),
     "sc_pcg_precond_device": (c_int, [c_void_p, c_void_p, c_void_p]),
     "sc_pcg_apply_device": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "sc_pcg_time_kernels": (c_int, [c_void_p, c_int, P(c_double)]),
+    "sc_fvm_build_system_device": (c_int, [c_void_p, c_int, c_int, c_int, c_double, c_double, c_int,
+                                           c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                           _dpp, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "sc_fvm_project_device": (c_int, [c_void_p, c_int, c_int, c_int, c_double, c_double, c_int, c_void_p,
+                                      c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

@@ -4,6 +4,7 @@
 #include <string>
 
 #include "../../include/simcraft_fluid_capi.h"
+#include "sc_fvm.cuh"
 #include "sc_pcg.cuh"
 
 struct sc_context {
@@ -45,6 +46,7 @@ void to_public(const sc::PcgStats& s, sc_pcg_stats* o) {
   o->ms = s.ms;
   o->sym_err = s.sym_err;
   o->device_flags = s.device_flags;
+  o->kernel_launches = s.kernel_launches;
 }
 
 int validate_options(const sc_pcg_options* o) {
@@ -235,6 +237,7 @@ int sc_pcg_download(sc_pcg* pcg, double* pg, int device_pointer) {
 static int solve_common(sc_pcg* pcg, const double* adiag, const double* const* an,
                         const double* rhs, const uint8_t* active, double* pg,
                         sc_pcg_stats* stats, int device) {
+  const uint64_t l0 = pcg->solver->launches();
   int rc = sc_pcg_upload(pcg, adiag, an, rhs, active, device);
   if (rc) return rc;
   sc::PcgStats st;
@@ -243,6 +246,7 @@ static int solve_common(sc_pcg* pcg, const double* adiag, const double* const* a
   if (rc) return rc;
   rc = map_status(pcg->solver->download_pressure(pg, device != 0));
   if (rc) return rc;
+  if (stats) stats->kernel_launches = (int64_t)(pcg->solver->launches() - l0);
   if (device) {
     cudaError_t e = cudaStreamSynchronize(pcg->ctx->c.stream);
     if (e != cudaSuccess) return pcg->ctx->c.set_error(SC_ERR_CUDA, cudaGetErrorString(e));
@@ -279,4 +283,53 @@ int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b) {
 int sc_debug_pcg_dump(sc_pcg* pcg, int which, double* out) {
   return pcg->solver->debug_dump(which, out);
 }
+int sc_pcg_time_kernels(sc_pcg* pcg, int reps, double* ms_out) {
+  if (!pcg || reps < 1 || !ms_out) return SC_ERR_INVALID;
+  cudaSetDevice(pcg->ctx->c.device);
+  return map_status(pcg->solver->time_kernels(reps, ms_out));
+}
+
+int sc_fvm_build_system_device(sc_context* ctx, int nx, int ny, int nz, double h, double dt,
+                               int precision, const void* u, const void* v, const void* w,
+                               const double* fluid_sdf, const double* collider_sdf,
+                               double* adiag, double* const* an, double* rhs, uint8_t* active,
+                               double* u_wt, double* v_wt, double* w_wt) {
+  if (!ctx || nx < 1 || ny < 1 || nz < 1 || !(h > 0.0) || !u || !v || !w || !fluid_sdf ||
+      !u_wt || !v_wt || !w_wt || (precision != SC_REAL_F64 && precision != SC_REAL_F32))
+    return SC_ERR_INVALID;
+  cudaSetDevice(ctx->c.device);
+  sc::SystemOut out;
+  out.adiag = adiag;
+  if (an)
+    for (int d = 0; d < 6; d++) out.an[d] = an[d];
+  out.rhs = rhs;
+  out.active = active;
+  int rc = precision == SC_REAL_F64
+               ? sc::fvm_build_system<double>(ctx->c.stream, nx, ny, nz, h, dt, (const double*)u,
+                                              (const double*)v, (const double*)w, fluid_sdf,
+                                              collider_sdf, u_wt, v_wt, w_wt, out)
+               : sc::fvm_build_system<float>(ctx->c.stream, nx, ny, nz, h, dt, (const float*)u,
+                                             (const float*)v, (const float*)w, fluid_sdf,
+                                             collider_sdf, u_wt, v_wt, w_wt, out);
+  if (rc) return ctx->c.set_error(SC_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  return SC_OK;
+}
+
+int sc_fvm_project_device(sc_context* ctx, int nx, int ny, int nz, double h, double dt,
+                          int precision, void* u, void* v, void* w, const double* pg,
+                          const double* fluid_sdf, const double* u_wt, const double* v_wt,
+                          const double* w_wt) {
+  if (!ctx || nx < 1 || ny < 1 || nz < 1 || !(h > 0.0) || !u || !v || !w || !pg || !fluid_sdf ||
+      !u_wt || !v_wt || !w_wt || (precision != SC_REAL_F64 && precision != SC_REAL_F32))
+    return SC_ERR_INVALID;
+  cudaSetDevice(ctx->c.device);
+  int rc = precision == SC_REAL_F64
+               ? sc::fvm_project<double>(ctx->c.stream, nx, ny, nz, h, dt, (double*)u, (double*)v,
+                                         (double*)w, pg, nullptr, fluid_sdf, u_wt, v_wt, w_wt)
+               : sc::fvm_project<float>(ctx->c.stream, nx, ny, nz, h, dt, (float*)u, (float*)v,
+                                        (float*)w, pg, nullptr, fluid_sdf, u_wt, v_wt, w_wt);
+  if (rc) return ctx->c.set_error(SC_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  return SC_OK;
+}
+
 }  // extern "C"

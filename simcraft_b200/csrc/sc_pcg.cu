@@ -29,7 +29,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kRing = 64;     // boundary ring entries per wavefront CTA
-constexpr int kPrefetch = 8;  // steps of input prefetch per compute warp
+constexpr int kStage = 8;     // steps of input staged ahead per compute warp (cp.async ring)
 constexpr int kSpinLimit = 1 << 22;  // bounded waits: ~0.1-1 s, far above any legitimate wait
 
 enum { FIN_NONE = 0, FIN_INIT, FIN_SPMV, FIN_AXPY, FIN_BWD, FIN_SA, FIN_NORMS };
@@ -424,111 +424,132 @@ __global__ void __launch_bounds__(kThreads)
 // tile's progress.  Every wait is bounded: on timeout the kernel raises
 // DEV_ERR_TIMEOUT, releases its dependants and finishes.
 
+// Cell operations of the three sweeps.  Each reads NV arrays at its own cell
+// (staged into shared memory by cp.async) plus the three already-computed
+// neighbour values xn, yn, zn.
 template <class T>
 struct FwdOp {  // L q = r (project-solver.cc:276-288), c* = A_* E(neighbour)
-  const T *r, *cL, *cD, *cB, *E;
-  T* out;
-  struct In {
-    T r, cL, cD, cB, E;
-  };
-  __device__ __forceinline__ In load(int64_t e) const {
-    return In{__ldg(r + e), __ldg(cL + e), __ldg(cD + e), __ldg(cB + e), __ldg(E + e)};
-  }
-  __device__ __forceinline__ T compute(const In& in, T xn, T yn, T zn, int, int, int, int64_t,
-                                       double&) const {
-    T t = in.r;
-    t -= in.cL * xn;
-    t -= in.cD * yn;
-    t -= in.cB * zn;
-    return t * in.E;
+  static constexpr int NV = 5;
+  const T* src[NV];  // r, cL, cD, cB, E
+  T* out;            // q
+  __device__ __forceinline__ T compute(const T* v, T xn, T yn, T zn, int64_t, double&) const {
+    T t = v[0];
+    t -= v[1] * xn;
+    t -= v[2] * yn;
+    t -= v[3] * zn;
+    return t * v[4];
   }
 };
 
 template <class T>
 struct BwdOp {  // L^T z = q (project-solver.cc:293-305), u* = A_*(p+dir) E(p); sigma = z.r
-  const T *q, *E, *uR, *uU, *uF, *r;
-  T* out;
-  struct In {
-    T q, E, uR, uU, uF, r;
-  };
-  __device__ __forceinline__ In load(int64_t e) const {
-    return In{__ldg(q + e), __ldg(E + e), __ldg(uR + e), __ldg(uU + e), __ldg(uF + e), __ldg(r + e)};
-  }
-  __device__ __forceinline__ T compute(const In& in, T xn, T yn, T zn, int, int, int, int64_t,
-                                       double& acc) const {
-    T t = in.q;
-    t -= in.uR * xn;
-    t -= in.uU * yn;
-    t -= in.uF * zn;
-    T v = t * in.E;
-    acc += (double)v * (double)in.r;
-    return v;
+  static constexpr int NV = 6;
+  const T* src[NV];  // q, E, uR, uU, uF, r
+  T* out;            // z
+  __device__ __forceinline__ T compute(const T* v, T xn, T yn, T zn, int64_t, double& acc) const {
+    T t = v[0];
+    t -= v[2] * xn;
+    t -= v[3] * yn;
+    t -= v[4] * zn;
+    T z = t * v[1];
+    acc += (double)z * (double)v[5];
+    return z;
   }
 };
 
 // MIC(0) pivot (project-solver.cc:237-274), FP64.  The exchanged value is E.
 // E(q) != 0 exactly when q is active with Adiag(q) != 0, which is the guard the
-// reference tests before using E(q).
+// reference tests before using E(q).  adm is Adiag masked by the active flag;
+// dL/dD/dB hold the tau-weighted products with the diagonal neighbours'
+// couplings (k_pivot_diag), so the sweep only streams its own row.
 struct PivotOp {
-  Tiled g;
-  const double *adiag, *al, *ad, *ab;
-  const uint8_t* act;
-  double tau, sigma;
+  static constexpr int NV = 7;
+  const double* src[NV];  // adm, al, ad, ab, dL, dD, dB
+  double sigma;
   double *out, *cL, *cD, *cB;
-  struct In {
-    double adiag, al, ad, ab;
-    int act;
-  };
-  __device__ __forceinline__ In load(int64_t e) const {
-    return In{__ldg(adiag + e), __ldg(al + e), __ldg(ad + e), __ldg(ab + e), (int)__ldg(act + e)};
-  }
-  __device__ __forceinline__ double compute(const In& in, double EL, double ED, double EB, int x,
-                                            int y, int z, int64_t e, double&) const {
+  __device__ __forceinline__ double compute(const double* v, double EL, double ED, double EB,
+                                            int64_t e, double&) const {
+    const double adiag = v[0], al = v[1], ad = v[2], ab = v[3];
     double E = 0.0;
-    if (in.act && in.adiag != 0.0) {
-      double ee = in.adiag;
+    if (adiag != 0.0) {
+      double ee = adiag;
       if (EL != 0.0) {
-        ee -= (in.al * EL) * (in.al * EL);
-        if (y < g.ny - 1) {
-          int64_t o = g.off(x - 1, y + 1, z);
-          if (act[o]) ee -= tau * in.al * al[o] / (EL * EL);
-        }
-        if (z < g.nz - 1) {
-          int64_t o = g.off(x - 1, y, z + 1);
-          if (act[o]) ee -= tau * in.al * al[o] / (EL * EL);
-        }
+        ee -= (al * EL) * (al * EL);
+        ee -= v[4] / (EL * EL);
       }
       if (ED != 0.0) {
-        ee -= (in.ad * ED) * (in.ad * ED);
-        if (x < g.nx - 1) {
-          int64_t o = g.off(x + 1, y - 1, z);
-          if (act[o]) ee -= tau * in.ad * ad[o] / (ED * ED);
-        }
-        if (z < g.nz - 1) {
-          int64_t o = g.off(x, y - 1, z + 1);
-          if (act[o]) ee -= tau * in.ad * ad[o] / (ED * ED);
-        }
+        ee -= (ad * ED) * (ad * ED);
+        ee -= v[5] / (ED * ED);
       }
       if (EB != 0.0) {
-        ee -= (in.ab * EB) * (in.ab * EB);
-        if (x < g.nx - 1) {
-          int64_t o = g.off(x + 1, y, z - 1);
-          if (act[o]) ee -= tau * in.ab * ab[o] / (EB * EB);
-        }
-        if (y < g.ny - 1) {
-          int64_t o = g.off(x, y + 1, z - 1);
-          if (act[o]) ee -= tau * in.ab * ab[o] / (EB * EB);
-        }
+        ee -= (ab * EB) * (ab * EB);
+        ee -= v[6] / (EB * EB);
       }
-      if (ee < sigma * in.adiag) ee = in.adiag;
+      if (ee < sigma * adiag) ee = adiag;
       E = 1.0 / sqrt(ee);
     }
-    cL[e] = in.al * EL;
-    cD[e] = in.ad * ED;
-    cB[e] = in.ab * EB;
+    cL[e] = al * EL;
+    cD[e] = ad * ED;
+    cB[e] = ab * EB;
     return E;
   }
 };
+
+// The tau-weighted neighbour products of the pivot recurrence
+// (project-solver.cc:244-265): for the Left term
+//   tau*A_L(p)*A_L(p-x+y) [if p-x+y active] + tau*A_L(p)*A_L(p-x+z) [if p-x+z active]
+// and likewise for Down and Back.  They only depend on A.
+__global__ void __launch_bounds__(kThreads)
+    k_pivot_diag(Tiled g, const double* __restrict__ adiag, const double* __restrict__ al,
+                 const double* __restrict__ ad, const double* __restrict__ ab,
+                 const uint8_t* __restrict__ act, double tau, double* __restrict__ adm,
+                 double* __restrict__ dL, double* __restrict__ dD, double* __restrict__ dB) {
+  SC_ROWBLOCK_LOOP(g) {
+    Cell c;
+    c.init(g, rb, threadIdx.x);
+    double l = 0.0, d = 0.0, b = 0.0;
+    if (c.inside) {
+      const int x = c.x, y = c.y, z = c.z;
+      if (x > 0) {
+        const double a = al[c.e];
+        if (y < g.ny - 1) {
+          int64_t o = g.off(x - 1, y + 1, z);
+          if (act[o]) l += tau * a * al[o];
+        }
+        if (z < g.nz - 1) {
+          int64_t o = g.off(x - 1, y, z + 1);
+          if (act[o]) l += tau * a * al[o];
+        }
+      }
+      if (y > 0) {
+        const double a = ad[c.e];
+        if (x < g.nx - 1) {
+          int64_t o = g.off(x + 1, y - 1, z);
+          if (act[o]) d += tau * a * ad[o];
+        }
+        if (z < g.nz - 1) {
+          int64_t o = g.off(x, y - 1, z + 1);
+          if (act[o]) d += tau * a * ad[o];
+        }
+      }
+      if (z > 0) {
+        const double a = ab[c.e];
+        if (x < g.nx - 1) {
+          int64_t o = g.off(x + 1, y, z - 1);
+          if (act[o]) b += tau * a * ab[o];
+        }
+        if (y < g.ny - 1) {
+          int64_t o = g.off(x, y + 1, z - 1);
+          if (act[o]) b += tau * a * ab[o];
+        }
+      }
+    }
+    dL[c.e] = l;
+    dD[c.e] = d;
+    dB[c.e] = b;
+    adm[c.e] = (c.inside && act[c.e]) ? adiag[c.e] : 0.0;
+  }
+}
 
 template <int TY, bool FWD>
 __device__ __forceinline__ int wave_slot(const Tiled& g, int s, int ty) {
@@ -584,6 +605,20 @@ __device__ __forceinline__ void mb_reset(T* p) {
   mb_store_bits(p, Sentinel<T>::bits);
 }
 
+__device__ __forceinline__ void cp_async_elem(double* dst, const double* src) {
+  unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(float* dst, const float* src) {
+  unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Shared state of one wavefront CTA.
 template <class T, int TY>
 struct WaveShared {
@@ -596,7 +631,7 @@ struct WaveShared {
   volatile int abort;
   int tile;
   bool last;
-  double ssum[TY + 2];
+  double ssum[TY + 3];
 };
 
 // Give up: flag the error and release the compute warps.
@@ -727,9 +762,14 @@ __device__ void wave_load_y(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int
 }
 
 template <class T, int TY, bool FWD, class Op>
-__global__ void __launch_bounds__((TY + 2) * 32, 1) k_wave(const WaveArgs a, const Op op) {
-  constexpr int NTC = TY * 32;
+__global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, const Op op) {
+  // warps 0..TY-1: tile rows (compute only, no fences: a fence would wait for
+  // the prefetch loads in flight); warp TY: control (flags, ring waits);
+  // warps TY+1, TY+2: x and y mailbox loaders.
+  constexpr int NBAR = (TY + 1) * 32;
   __shared__ WaveShared<T, TY> sh;
+  extern __shared__ __align__(16) unsigned char wave_dyn[];
+  T* stage = reinterpret_cast<T*>(wave_dyn);  // [kStage][TY][NV][32]
   if (a.use_skip && a.sc->done != DONE_RUNNING) return;
   if (a.sc->err & DEV_ERR_TIMEOUT) return;  // an earlier sweep gave up: do not wait again
   const Tiled& g = a.g;
@@ -761,23 +801,7 @@ __global__ void __launch_bounds__((TY + 2) * 32, 1) k_wave(const WaveArgs a, con
     const int cX = FWD ? tid + 1 : tid - 1, cY = FWD ? tid + g.ntx : tid - g.ntx;
     const int64_t base = g.tile_base(X, Y);
     if (warp == TY) {
-      if (hasX) wave_load_x<T, TY, FWD>(a, sh, mbx + (int64_t)tid * a.mb_stride_x, NS);
-    } else if (warp == TY + 1) {
-      if (hasY) wave_load_y<T, TY, FWD>(a, sh, mby + (int64_t)tid * a.mb_stride_y, NS);
-    } else {
-      const int ty = warp;
-      const int x = X * 32 + lane, y = Y * TY + ty;
-      T* outx = outX ? mbx + (int64_t)cX * a.mb_stride_x : nullptr;
-      T* outy = outY ? mby + (int64_t)cY * a.mb_stride_y : nullptr;
-      const bool xsrc = FWD ? (lane == 31) : (lane == 0);        // lane feeding the x consumer
-      const bool ysrc = FWD ? (ty == TY - 1) : (ty == 0);        // warp feeding the y consumer
-      typename Op::In ring[kPrefetch];
-#pragma unroll
-      for (int u = 0; u < kPrefetch; u++)
-        if (u < NS) ring[u] = op.load(base + ((int64_t)wave_slot<TY, FWD>(g, u, ty) * TY + ty) * 32 + lane);
-      T prev = T(0);
-      // Executed by all lanes of warp 0 (warp-uniform loop: every lane reads the
-      // same shared-memory flags), so the warp stays converged at the barrier.
+      // control warp: keeps the compute warps one step behind the rings
       auto wait_avail = [&](int s) {
         int spins = 0;
         while (((hasX && sh.availX <= s) || (hasY && sh.availY <= s)) && !sh.abort) {
@@ -789,16 +813,67 @@ __global__ void __launch_bounds__((TY + 2) * 32, 1) k_wave(const WaveArgs a, con
         __syncwarp();
         __threadfence_block();
       };
-      if (warp == 0) wait_avail(0);
-      named_bar_sync(1, NTC);
-      for (int s0 = 0; s0 < NS; s0 += kPrefetch) {
+      wait_avail(0);
+      named_bar_sync(1, NBAR);
+      for (int s = 0; s < NS; s++) {
+        if (lane == 0) sh.done = s;  // steps < s are complete
+        if (s + 1 < NS) wait_avail(s + 1);
+        named_bar_sync(1, NBAR);
+      }
+      if (lane == 0) sh.done = NS;
+    } else if (warp == TY + 1) {
+      if (hasX) wave_load_x<T, TY, FWD>(a, sh, mbx + (int64_t)tid * a.mb_stride_x, NS);
+    } else if (warp == TY + 2) {
+      if (hasY) wave_load_y<T, TY, FWD>(a, sh, mby + (int64_t)tid * a.mb_stride_y, NS);
+    } else {
+      const int ty = warp;
+      T* outx = outX ? mbx + (int64_t)cX * a.mb_stride_x : nullptr;
+      T* outy = outY ? mby + (int64_t)cY * a.mb_stride_y : nullptr;
+      const bool xsrc = FWD ? (lane == 31) : (lane == 0);        // lane feeding the x consumer
+      const bool ysrc = FWD ? (ty == TY - 1) : (ty == 0);        // warp feeding the y consumer
+      // slot of the row this warp touches at step s: forward (s - ty) mod nz,
+      // backward (nz + 29 + TY - s - ty) mod nz; advanced incrementally.
+      int cslot = wave_slot<TY, FWD>(g, 0, ty);
+      int pslot = cslot;
+      const int64_t rowbase = base + (int64_t)ty * 32 + lane;
+      const int64_t rstride = (int64_t)TY * 32;
+      auto advance = [&](int& sl) {
+        if (FWD) {
+          if (++sl == g.nz) sl = 0;
+        } else {
+          if (--sl < 0) sl = g.nz - 1;
+        }
+      };
+      // Each lane stages its own element of the NV input rows kStage steps ahead
+      // with cp.async (not waited on by the per-step barrier).
+      T* my_stage = stage + (size_t)ty * Op::NV * 32 + lane;
+      constexpr size_t kStageStride = (size_t)TY * Op::NV * 32;  // elements per ring slot
+      auto issue = [&](int sl, int ridx) {
+        const int64_t eg = rowbase + (int64_t)sl * rstride;
 #pragma unroll
-        for (int u = 0; u < kPrefetch; u++) {
+        for (int k = 0; k < Op::NV; k++)
+          cp_async_elem(my_stage + ridx * kStageStride + k * 32, op.src[k] + eg);
+      };
+#pragma unroll
+      for (int r = 0; r < kStage; r++) {
+        if (r < NS) issue(pslot, r);
+        cp_async_commit();
+        advance(pslot);
+      }
+      T prev = T(0);
+      named_bar_sync(1, NBAR);
+      for (int s0 = 0; s0 < NS; s0 += kStage) {
+#pragma unroll
+        for (int u = 0; u < kStage; u++) {
           const int s = s0 + u;
           if (s < NS) {
-            const typename Op::In in = ring[u];
-            if (s + kPrefetch < NS)
-              ring[u] = op.load(base + ((int64_t)wave_slot<TY, FWD>(g, s + kPrefetch, ty) * TY + ty) * 32 + lane);
+            cp_async_wait<kStage - 1>();
+            T v[Op::NV];
+#pragma unroll
+            for (int k = 0; k < Op::NV; k++) v[k] = my_stage[u * kStageStride + k * 32];
+            if (s + kStage < NS) issue(pslot, u);
+            cp_async_commit();
+            advance(pslot);
             const int z = FWD ? (s - ty - lane) : (g.nz - 1 - (s - (TY - 1 - ty) - (31 - lane)));
             const bool valid = (z >= 0) && (z < g.nz);
             const T shv = FWD ? __shfl_up_sync(kFull, prev, 1) : __shfl_down_sync(kFull, prev, 1);
@@ -812,29 +887,20 @@ __global__ void __launch_bounds__((TY + 2) * 32, 1) k_wave(const WaveArgs a, con
                                : (hasY ? sh.bufY[s % kRing][lane] : T(0));
             T val = T(0);
             if (valid) {
-              const int64_t e = base + ((int64_t)wave_slot<TY, FWD>(g, s, ty) * TY + ty) * 32 + lane;
-              val = op.compute(in, xn, yn, prev, x, y, z, e, acc);
+              const int64_t e = rowbase + (int64_t)cslot * rstride;
+              val = op.compute(v, xn, yn, prev, e, acc);
               op.out[e] = val;
               if (xsrc && outx) mb_store(outx + (int64_t)(s - 31) * TY + ty, val);
               if (ysrc && outy) mb_store(outy + (int64_t)(s - (TY - 1)) * 32 + lane, val);
             }
             sh.xch[s & 1][ty][lane] = val;
             prev = val;
-            if (warp == 0) {
-              if (lane == 0) {
-                __threadfence_block();
-                sh.done = s;
-              }
-              if (s + 1 < NS) wait_avail(s + 1);
-            }
-            named_bar_sync(1, NTC);
+            advance(cslot);
+            named_bar_sync(1, NBAR);
           }
         }
       }
-      if (threadIdx.x == 0) {
-        __threadfence_block();
-        sh.done = NS;
-      }
+      cp_async_wait<0>();
     }
     // this tile's share of the dot product (summed later in tile order, so the
     // result does not depend on which CTA swept which tile)
@@ -845,7 +911,7 @@ __global__ void __launch_bounds__((TY + 2) * 32, 1) k_wave(const WaveArgs a, con
       __syncthreads();
       if (threadIdx.x == 0) {
         double S = 0.0;
-        for (int i = 0; i < TY + 2; i++) S += sh.ssum[i];
+        for (int i = 0; i < TY + 3; i++) S += sh.ssum[i];
         a.tile_partials[tid] = S;
       }
     }
@@ -871,6 +937,20 @@ __global__ void __launch_bounds__((TY + 2) * 32, 1) k_wave(const WaveArgs a, con
       __threadfence();
     }
   }
+}
+
+template <class T, bool FWD, class Op>
+constexpr size_t wave_dyn_smem() {
+  return sizeof(T) * (size_t)kStage * Tiled::TY * Op::NV * 32;
+}
+template <class T, bool FWD, class Op>
+void wave_set_attr() {
+  cudaFuncSetAttribute(k_wave<T, Tiled::TY, FWD, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)wave_dyn_smem<T, FWD, Op>());
+}
+template <class T, bool FWD, class Op>
+void launch_wave(const WaveArgs& a, const Op& op, cudaStream_t st, int grid) {
+  k_wave<T, Tiled::TY, FWD, Op><<<grid, (Tiled::TY + 3) * 32, wave_dyn_smem<T, FWD, Op>(), st>>>(a, op);
 }
 
 // Fill the mailboxes with the sentinel (at allocation and after an error).
@@ -939,6 +1019,11 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
     return;
   }
   g_ = Tiled::make(nx, ny, nz);
+  wave_set_attr<double, true, PivotOp>();
+  wave_set_attr<double, true, FwdOp<double>>();
+  wave_set_attr<double, false, BwdOp<double>>();
+  wave_set_attr<float, true, FwdOp<float>>();
+  wave_set_attr<float, false, BwdOp<float>>();
   nblocks_ = ctx->sm_count * 4;
   const int ntiles = g_.ntiles();
   wave_grid_ = std::min(ntiles, ctx->sm_count);
@@ -1046,6 +1131,7 @@ int PcgSolver::upload(const double* adiag, const double* const an[6], const doub
   }
   const uint8_t* act_ref = device ? active : stage_act;
   k_to_tiled<uint8_t, uint8_t><<<grid, kThreads, 0, st>>>(g_, act_ref, active_, nullptr);
+  launches_ += 6;
   for (int a = 0; a < 5; a++) {
     const double* s = src[a];
     if (!device) {
@@ -1118,12 +1204,14 @@ int PcgSolver::download_pressure(double* pg, bool device) {
   const double* src = d64_.p;  // the mixed solve copies its FP64 accumulator here
   if (device) {
     k_from_tiled<double, double><<<grid, kThreads, 0, st>>>(g_, src, pg);
+    launches_ += 1;
     return check_dev_error("download_pressure");
   }
   double* stage = nullptr;
   if (cudaMallocAsync(&stage, sizeof(double) * (size_t)N, st) != cudaSuccess)
     return ctx_->set_error(-3, "download: staging allocation failed");
   k_from_tiled<double, double><<<grid, kThreads, 0, st>>>(g_, src, stage);
+  launches_ += 1;
   cudaMemcpyAsync(pg, stage, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(stage, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return check_dev_error("download_pressure");
@@ -1135,11 +1223,16 @@ int PcgSolver::ensure_pivots() {
   cudaStream_t st = ctx_->stream;
   const int grid = grid_for(g_.total, ctx_->sm_count);
   WaveArgs wa = wave_args(false, 0, FIN_NONE);
-  PivotOp op{g_,         d64_.adiag, d64_.al, d64_.ad, d64_.ab, active_, opt_.tau,
-             opt_.sigma, d64_.E,     d64_.cL, d64_.cD, d64_.cB};
-  k_wave<double, Tiled::TY, true, PivotOp><<<wave_grid_, (Tiled::TY + 2) * 32, 0, st>>>(wa, op);
+  // uR/uU/uF hold the pivot's diagonal products until k_upper overwrites them
+  // q holds Adiag masked by the active flag until the forward sweep overwrites it
+  k_pivot_diag<<<grid, kThreads, 0, st>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab, active_,
+                                          opt_.tau, d64_.q, d64_.uR, d64_.uU, d64_.uF);
+  PivotOp op{{d64_.q, d64_.al, d64_.ad, d64_.ab, d64_.uR, d64_.uU, d64_.uF},
+             opt_.sigma, d64_.E, d64_.cL, d64_.cD, d64_.cB};
+  launch_wave<double, true>(wa, op, st, wave_grid_);
   k_upper<double><<<grid, kThreads, 0, st>>>(g_, d64_.cL, d64_.cD, d64_.cB, d64_.uR, d64_.uU,
                                               d64_.uF);
+  launches_ += 3;
   if (opt_.precision == PREC_MIXED) {
     if (!have_f32_) {
       const size_t n32 = sizeof(float) * (size_t)g_.total;
@@ -1176,6 +1269,7 @@ int PcgSolver::ensure_pivots() {
                     d32_.cD,    d32_.cB, d32_.uR, d32_.uU, d32_.uF};
     for (int i = 0; i < 11; i++)
       k_convert<double, float><<<grid, kThreads, 0, st>>>(g_.total, s64[i], d32[i]);
+    launches_ += 11;
   }
   int e = check_dev_error("pivots");
   if (e) return e;
@@ -1192,10 +1286,10 @@ void PcgSolver::launch_iteration(SysArrays<T>& A) {
   k_spmv<T><<<nblocks_, kThreads, 0, st>>>(g_, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az,
                                             partials_, sc_, 1);
   k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.s, A.Az, A.p, A.r, partials_, sc_);
-  FwdOp<T> fo{A.r, A.cL, A.cD, A.cB, A.E, A.q};
-  k_wave<T, Tiled::TY, true, FwdOp<T>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, st>>>(wf, fo);
-  BwdOp<T> bo{A.q, A.E, A.uR, A.uU, A.uF, A.r, A.z};
-  k_wave<T, Tiled::TY, false, BwdOp<T>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, st>>>(wb, bo);
+  FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
+  launch_wave<T, true>(wf, fo, st, wave_grid_);
+  BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
+  launch_wave<T, false>(wb, bo, st, wave_grid_);
   k_sa<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.s, partials_, sc_);
 }
 
@@ -1219,11 +1313,12 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
   const bool f32 = sizeof(T) == 4;
   WaveArgs wf = wave_args(f32, 1, FIN_NONE);
   WaveArgs wb = wave_args(f32, 1, FIN_BWD);
-  FwdOp<T> fo{A.r, A.cL, A.cD, A.cB, A.E, A.q};
-  k_wave<T, Tiled::TY, true, FwdOp<T>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, s>>>(wf, fo);
-  BwdOp<T> bo{A.q, A.E, A.uR, A.uU, A.uF, A.r, A.z};
-  k_wave<T, Tiled::TY, false, BwdOp<T>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, s>>>(wb, bo);
+  FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
+  launch_wave<T, true>(wf, fo, s, wave_grid_);
+  BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
+  launch_wave<T, false>(wb, bo, s, wave_grid_);
   k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.z, A.s, sc_);
+  launches_ += 4;
   int e = check_dev_error("pcg init");
   if (e) return e;
   // graph of `chunk` iterations
@@ -1246,6 +1341,7 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
   int launched = 0;
   auto launch_chunk = [&](int c) {
     cudaGraphLaunch(gx, s);
+    launches_ += 5 * (uint64_t)opt_.chunk;
     cudaMemcpyAsync(&sc_host_[c & 1], sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(evs[c & 1], s);
   };
@@ -1285,6 +1381,7 @@ int PcgSolver::solve_mixed(PcgStats* st) {
   const int grid = grid_for(g_.total, ctx_->sm_count);
   // x = 0, r = b
   k_fill<double><<<grid, kThreads, 0, s>>>(g_.total, xacc_, 0.0);
+  launches_ += 2;
   PcgScalars init{};
   init.tol = 0.0;
   init.max_iter = 1;
@@ -1313,6 +1410,7 @@ int PcgSolver::solve_mixed(PcgStats* st) {
     }
     outer++;
     // x += rnorm d ; r -= rnorm A d   (FP64)
+    launches_ += 1;
     k_mixed_update<<<nblocks_, kThreads, 0, s>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab,
                                                  active_, d32_.p, rnorm, xacc_, d64_.r, partials_,
                                                  sc_);
@@ -1336,6 +1434,7 @@ int PcgSolver::solve_mixed(PcgStats* st) {
 
 int PcgSolver::true_residual(PcgStats* st) {
   cudaStream_t s = ctx_->stream;
+  launches_ += 2;
   k_true_residual<<<nblocks_, kThreads, 0, s>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab, active_,
                                                 d64_.p, rhs_, partials_, sc_);
   PcgScalars* h = sc_host_ + 1;
@@ -1359,6 +1458,7 @@ int PcgSolver::solve(PcgStats* st) {
   PcgStats local{};
   if (!st) st = &local;
   *st = PcgStats{};
+  const uint64_t launches0 = launches_;
   cudaEventRecord(evt0_, ctx_->stream);
   int e = opt_.precision == PREC_MIXED ? solve_mixed(st) : solve_fp64(st);
   if (e) return e;
@@ -1372,6 +1472,7 @@ int PcgSolver::solve(PcgStats* st) {
     e = true_residual(st);
     if (e) return e;
   }
+  st->kernel_launches = (int64_t)(launches_ - launches0);
   return 0;
 }
 
@@ -1387,10 +1488,10 @@ int PcgSolver::precond_only(const double* r, double* z) {
   cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
   WaveArgs wf = wave_args(false, 0, FIN_NONE);
   WaveArgs wb = wave_args(false, 0, FIN_BWD);
-  FwdOp<double> fo{d64_.r, d64_.cL, d64_.cD, d64_.cB, d64_.E, d64_.q};
-  k_wave<double, Tiled::TY, true, FwdOp<double>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, s>>>(wf, fo);
-  BwdOp<double> bo{d64_.q, d64_.E, d64_.uR, d64_.uU, d64_.uF, d64_.r, d64_.z};
-  k_wave<double, Tiled::TY, false, BwdOp<double>><<<wave_grid_, (Tiled::TY + 2) * 32, 0, s>>>(wb, bo);
+  FwdOp<double> fo{{d64_.r, d64_.cL, d64_.cD, d64_.cB, d64_.E}, d64_.q};
+  launch_wave<double, true>(wf, fo, s, wave_grid_);
+  BwdOp<double> bo{{d64_.q, d64_.E, d64_.uR, d64_.uU, d64_.uF, d64_.r}, d64_.z};
+  launch_wave<double, false>(wb, bo, s, wave_grid_);
   k_from_tiled<double, double><<<grid, kThreads, 0, s>>>(g_, d64_.z, z);
   cudaMemcpyAsync(sc_host_, sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("precond");
@@ -1455,6 +1556,84 @@ int PcgSolver::debug_dump(int which, double* out) {
   cudaFreeAsync(tmp, s);
   cudaStreamSynchronize(s);
   return check_dev_error("debug");
+}
+
+int PcgSolver::time_kernels(int reps, double* ms) {
+  cudaStream_t s = ctx_->stream;
+  int e = ensure_pivots();
+  if (e) return e;
+  const int grid = grid_for(g_.total, ctx_->sm_count);
+  // a benign state: r = rhs, s = r, scalars running with a tiny alpha/beta
+  PcgScalars init{};
+  init.done = DONE_RUNNING;
+  init.first = 1;
+  init.max_iter = 1 << 30;
+  init.alpha = 0.0;
+  init.beta = 0.0;
+  init.sigma = 1.0;
+  cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
+  k_init<double><<<nblocks_, kThreads, 0, s>>>(g_, rhs_, 1.0, active_, d64_.r, d64_.p, partials_,
+                                               sc_);
+  cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
+  k_copy<double><<<grid, kThreads, 0, s>>>(g_.total, d64_.r, d64_.s, sc_);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  auto timed = [&](int which) -> double {
+    cudaEventRecord(a, s);
+    for (int i = 0; i < reps; i++) {
+      switch (which) {
+        case 0: {
+          WaveArgs wa = wave_args(false, 0, FIN_NONE);
+          PivotOp op{{d64_.q, d64_.al, d64_.ad, d64_.ab, d64_.uR, d64_.uU, d64_.uF},
+                     opt_.sigma, d64_.E, d64_.cL, d64_.cD, d64_.cB};
+          // the diag terms live in uR/uU/uF only until k_upper; rebuild them
+          k_pivot_diag<<<grid, kThreads, 0, s>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab,
+                                                 active_, opt_.tau, d64_.q, d64_.uR, d64_.uU,
+                                                 d64_.uF);
+          launch_wave<double, true>(wa, op, s, wave_grid_);
+          k_upper<double><<<grid, kThreads, 0, s>>>(g_, d64_.cL, d64_.cD, d64_.cB, d64_.uR,
+                                                    d64_.uU, d64_.uF);
+          break;
+        }
+        case 1: {
+          FwdOp<double> fo{{d64_.r, d64_.cL, d64_.cD, d64_.cB, d64_.E}, d64_.q};
+          launch_wave<double, true>(wave_args(false, 0, FIN_NONE), fo, s, wave_grid_);
+          break;
+        }
+        case 2: {
+          BwdOp<double> bo{{d64_.q, d64_.E, d64_.uR, d64_.uU, d64_.uF, d64_.r}, d64_.z};
+          launch_wave<double, false>(wave_args(false, 0, FIN_NONE), bo, s, wave_grid_);
+          break;
+        }
+        case 3:
+          k_spmv<double><<<nblocks_, kThreads, 0, s>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab,
+                                                       active_, d64_.s, d64_.Az, partials_, sc_, 0);
+          break;
+        case 4:
+          k_axpy<double><<<nblocks_, kThreads, 0, s>>>(g_.total, active_, d64_.s, d64_.Az, d64_.p,
+                                                       d64_.r, partials_, sc_);
+          break;
+        case 5:
+          k_sa<double><<<nblocks_, kThreads, 0, s>>>(g_.total, active_, d64_.z, d64_.s, partials_,
+                                                     sc_);
+          break;
+      }
+    }
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float t = 0;
+    cudaEventElapsedTime(&t, a, b);
+    return (double)t / reps;
+  };
+  for (int k = 0; k < 6; k++) {
+    cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
+    ms[k] = timed(k);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  pivots_valid_ = true;
+  return check_dev_error("time_kernels");
 }
 
 }  // namespace sc

@@ -55,6 +55,7 @@ struct PcgStats {
   double ms = 0;             // device time of the solve (events)
   double sym_err = 0;        // max |A_R(p) - A_L(p+x)| etc. when checked
   unsigned device_flags = 0; // DEV_ERR_* bits raised on the device
+  int64_t kernel_launches = 0;  // kernels launched by the solve (graph nodes counted)
 };
 
 // Device scalars shared by the kernels of one PCG run.
@@ -120,8 +121,11 @@ class PcgSolver {
   // applyCompressedMatrix on the uploaded system (device pointers, reference layout).
   int apply_only(const double* x, double* b);
   int debug_dump(int which, double* out);
+  // Device time per launch of each kernel class (see sc_pcg_time_kernels).
+  int time_kernels(int reps, double* ms);
 
   const Tiled& geom() const { return g_; }
+  uint64_t launches() const { return launches_; }
   // Direct access for in-device producers (FLIP buildSystem writes these).
   double* adiag64() { return d64_.adiag; }
   double* al64() { return d64_.al; }
@@ -177,6 +181,7 @@ class PcgSolver {
   double sym_err_ = 0.0;
   double inner_scale_ = 1.0;
   PcgScalars last_{};
+  uint64_t launches_ = 0;  // kernels launched so far (graph nodes counted)
   // graphs: one chunk of iterations per precision
   cudaGraphExec_t graph64_ = nullptr, graph32_ = nullptr;
   template <class T>

@@ -145,6 +145,24 @@ int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b);
  * untouched. */
 int sc_pcg_time_kernels(sc_pcg* pcg, int reps, double* ms_out);
 
+/* Allocation-free ModifiedIncompleteCholesky3D::precond(Adiag, Aneighbour, r,
+ * active, z) (project-solver.cc:230-306) on device arrays in the reference
+ * layout; an is a host array of 6 device pointers (only Left, Down and Back are
+ * read).  No counterpart in the reference: it exists for callers that cannot
+ * call cudaMalloc, such as engines whose device memory is owned by their own
+ * pool allocator, or hot loops where cudaMalloc's device-wide synchronisation is
+ * not acceptable.  It allocates nothing: its scratch is one static device array
+ * of about 4.4 MB that every GPU loading the library holds until exit, which
+ * limits the grid to 32768 tiled cells (ceil(nx/32)*32 * ceil(ny/8)*8 * nz,
+ * e.g. 32^3) in at most 8 column tiles; larger grids return SC_ERR_INVALID with
+ * a message.  The first call on each device performs a one-time set-up on that
+ * device (it looks up the array's device address); make that first call before
+ * any stream capture.  All calls share the array, so calls that overlap on the
+ * GPU race.  Synchronous on the context's stream. */
+int sc_mic_precond_noalloc_device(sc_context* ctx, int nx, int ny, int nz, const double* adiag,
+                                  const double* const* an, const double* r,
+                                  const uint8_t* active, double* z, double tau, double sigma);
+
 /* ---------------------------------------------------------------------------
  * Finite-volume pressure system: FvmSolver3D
  * (FluidSim/include/FluidSim/cpu/project-solver.h:133-182).

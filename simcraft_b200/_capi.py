@@ -60,6 +60,8 @@ SIGNATURES = {
     "sc_pcg_precond_device": (c_int, [c_void_p, c_void_p, c_void_p]),
     "sc_pcg_apply_device": (c_int, [c_void_p, c_void_p, c_void_p]),
     "sc_pcg_time_kernels": (c_int, [c_void_p, c_int, P(c_double)]),
+    "sc_mic_precond_noalloc_device": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, _dpp, c_void_p, c_void_p,
+                                              c_void_p, c_double, c_double]),
     "sc_fvm_build_system_device": (c_int, [c_void_p, c_int, c_int, c_int, c_double, c_double, c_int,
                                            c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                            _dpp, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),

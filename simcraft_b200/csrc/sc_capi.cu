@@ -332,4 +332,18 @@ int sc_fvm_project_device(sc_context* ctx, int nx, int ny, int nz, double h, dou
   return SC_OK;
 }
 
+int sc_mic_precond_noalloc_device(sc_context* ctx, int nx, int ny, int nz, const double* adiag,
+                                  const double* const* an, const double* r,
+                                  const uint8_t* active, double* z, double tau, double sigma) {
+  if (!ctx || nx < 1 || ny < 1 || nz < 1 || !adiag || !an || !an[0] || !an[3] || !an[5] || !r ||
+      !active || !z)
+    return SC_ERR_INVALID;
+  if (cudaSetDevice(ctx->c.device) != cudaSuccess) return SC_ERR_CUDA;
+  std::string msg;
+  int rc = sc::mic_precond_noalloc(ctx->c.stream, ctx->c.device, ctx->c.sm_count, nx, ny, nz, adiag,
+                                   an, r, active, z, tau, sigma, &msg);
+  if (rc) return ctx->c.set_error(map_status(rc), msg);
+  return SC_OK;
+}
+
 }  // extern "C"

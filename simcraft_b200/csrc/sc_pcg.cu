@@ -22,6 +22,9 @@
 #include <cstring>
 #include <vector>
 
+#include <mutex>
+#include <string>
+
 #include "sc_pcg.cuh"
 
 namespace sc {
@@ -1634,6 +1637,175 @@ int PcgSolver::time_kernels(int reps, double* ms) {
   cudaEventDestroy(b);
   pivots_valid_ = true;
   return check_dev_error("time_kernels");
+}
+
+}  // namespace sc
+
+// =================================================================================
+// Allocation-free MIC(0) preconditioner (sc_mic_precond_noalloc_device).
+//
+// Some callers cannot call cudaMalloc: engines whose device memory is owned up
+// front by their own pool allocator (no third-party allocations allowed), and
+// hot loops where cudaMalloc's implicit device-wide synchronisation is not
+// acceptable.  For them this variant of ModifiedIncompleteCholesky3D::precond
+// keeps every scratch buffer it needs (the tiled copies of A, the pivots, the
+// sweep couplings, the sweep outputs, the tile mailboxes and the scheduling
+// counters) in the file-scope array below instead of allocating.  It launches
+// the same kernels as sc_pcg_precond_device.
+//
+// The array is kNoAllocBytes (about 4.4 MB) and lives on every GPU that loads
+// this library, until the process exits.  It bounds the problem size: at most
+// kNoAllocMaxTiled tiled elements (ceil(nx/32)*32 * ceil(ny/8)*8 * nz, e.g. a
+// 32^3 grid) in at most kNoAllocMaxTiles column tiles.  Every call shares the
+// one array, so calls whose work overlaps on the GPU (other streams, other
+// host threads) race and corrupt each other's results.
+namespace sc {
+namespace {
+
+constexpr int64_t kNoAllocMaxTiled = 32768;
+constexpr int kNoAllocMaxTiles = 8;
+constexpr int kNoAllocMaxNS = (int)(kNoAllocMaxTiled / (Tiled::TY * 32)) + 31 + Tiled::TY - 1;
+constexpr int kNoAllocArrays = 15;  // adiag al ad ab E cL cD cB uR uU uF r q z (spare)
+
+constexpr size_t na_align(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t kNaArrBytes = na_align(sizeof(double) * kNoAllocMaxTiled);
+constexpr size_t kNaActBytes = na_align(kNoAllocMaxTiled);
+constexpr size_t kNaMbxBytes = na_align(sizeof(double) * kNoAllocMaxTiles * kNoAllocMaxNS * Tiled::TY);
+constexpr size_t kNaMbyBytes = na_align(sizeof(double) * kNoAllocMaxTiles * kNoAllocMaxNS * 32);
+constexpr size_t kNaSmallBytes =
+    na_align(sizeof(double) * kNoAllocMaxTiles + sizeof(int) * 2 + sizeof(int2) * kNoAllocMaxTiles) +
+    na_align(sizeof(PcgScalars));
+constexpr size_t kNoAllocBytes =
+    kNaArrBytes * kNoAllocArrays + kNaActBytes + kNaMbxBytes + kNaMbyBytes + kNaSmallBytes;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_base[64] = {};  // device address of g_noalloc_scratch, per device
+
+}  // namespace
+
+// Returns 0, or a negative status with `msg` set.
+int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int ny, int nz,
+                        const double* adiag, const double* const* an, const double* r,
+                        const uint8_t* active, double* z, double tau, double sigma,
+                        std::string* msg) {
+  const Tiled g = Tiled::make(nx, ny, nz);
+  if (g.total > kNoAllocMaxTiled || g.ntiles() > kNoAllocMaxTiles) {
+    *msg = "grid too large for the allocation-free preconditioner: at most " +
+           std::to_string(kNoAllocMaxTiled) + " tiled cells (ceil(nx/32)*32 * ceil(ny/8)*8 * nz) in " +
+           std::to_string(kNoAllocMaxTiles) + " tiles of 32x8 columns";
+    return -1;
+  }
+  if (device < 0 || device >= 64) {
+    *msg = "device ordinal out of range";
+    return -1;
+  }
+  unsigned char* base = nullptr;
+  {
+    // One-time set-up per device (the device is current here): the device
+    // address of the static array, and the shared-memory attribute of the sweeps.
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_base[device]) {
+      void* ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess || !ptr) {
+        *msg = std::string("cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
+        return -2;
+      }
+      wave_set_attr<double, true, PivotOp>();
+      wave_set_attr<double, true, FwdOp<double>>();
+      wave_set_attr<double, false, BwdOp<double>>();
+      g_noalloc_base[device] = ptr;
+    }
+    base = (unsigned char*)g_noalloc_base[device];
+  }
+  double* arr[kNoAllocArrays];
+  for (int i = 0; i < kNoAllocArrays; i++) arr[i] = (double*)(base + kNaArrBytes * i);
+  unsigned char* q = base + kNaArrBytes * kNoAllocArrays;
+  uint8_t* act = (uint8_t*)q;
+  q += kNaActBytes;
+  double* mbx = (double*)q;
+  q += kNaMbxBytes;
+  double* mby = (double*)q;
+  q += kNaMbyBytes;
+  double* tile_partials = (double*)q;
+  int* ticket = (int*)(tile_partials + kNoAllocMaxTiles);
+  int2* order = (int2*)(ticket + 2);
+  PcgScalars* scal = (PcgScalars*)(q + na_align(sizeof(double) * kNoAllocMaxTiles + sizeof(int) * 2 +
+                                                sizeof(int2) * kNoAllocMaxTiles));
+  double *t_adiag = arr[0], *t_al = arr[1], *t_ad = arr[2], *t_ab = arr[3], *t_E = arr[4],
+         *t_cL = arr[5], *t_cD = arr[6], *t_cB = arr[7], *t_uR = arr[8], *t_uU = arr[9],
+         *t_uF = arr[10], *t_r = arr[11], *t_q = arr[12], *t_z = arr[13];
+  // The array keeps the previous call's contents: reset what must start at
+  // zero (scheduling counters, scalars) and the mailbox sentinels.
+  const int ntiles = g.ntiles();
+  const int NS = g.nz + 31 + Tiled::TY - 1;
+  const int64_t sx = (int64_t)NS * Tiled::TY, sy = (int64_t)NS * 32;
+  cudaMemsetAsync(ticket, 0, sizeof(int) * 2, st);
+  cudaMemsetAsync(scal, 0, sizeof(PcgScalars), st);
+  const int rgrid = grid_for(sy * ntiles, sm_count);
+  k_mb_reset<double><<<rgrid, kThreads, 0, st>>>(sx * ntiles, mbx);
+  k_mb_reset<double><<<rgrid, kThreads, 0, st>>>(sy * ntiles, mby);
+  int2 ord[kNoAllocMaxTiles];
+  int no = 0;
+  for (int d = 0; d <= g.ntx + g.nty - 2; d++)
+    for (int X = 0; X < g.ntx; X++) {
+      int Y = d - X;
+      if (Y >= 0 && Y < g.nty) ord[no++] = make_int2(X, Y);
+    }
+  cudaMemcpyAsync(order, ord, sizeof(int2) * no, cudaMemcpyHostToDevice, st);
+  // system and right-hand side into the tiled layout
+  const int grid = grid_for(g.total, sm_count);
+  k_to_tiled<uint8_t, uint8_t><<<grid, kThreads, 0, st>>>(g, active, act, nullptr);
+  k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g, adiag, t_adiag, nullptr);
+  k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g, an[0], t_al, nullptr);
+  k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g, an[3], t_ad, nullptr);
+  k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g, an[5], t_ab, nullptr);
+  k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g, r, t_r, nullptr);
+  // pivots, couplings, forward and backward sweeps
+  WaveArgs wa{};
+  wa.g = g;
+  wa.mbx = mbx;
+  wa.mby = mby;
+  wa.mb_stride_x = sx;
+  wa.mb_stride_y = sy;
+  wa.ticket = ticket;
+  wa.exits = ticket + 1;
+  wa.order = order;
+  wa.sc = scal;
+  wa.partials = tile_partials;
+  wa.tile_partials = tile_partials;
+  wa.use_skip = 0;
+  wa.fin_kind = FIN_NONE;
+  const int wgrid = std::min(ntiles, sm_count);
+  k_pivot_diag<<<grid, kThreads, 0, st>>>(g, t_adiag, t_al, t_ad, t_ab, act, tau, t_q, t_uR, t_uU,
+                                          t_uF);
+  PivotOp pop{{t_q, t_al, t_ad, t_ab, t_uR, t_uU, t_uF}, sigma, t_E, t_cL, t_cD, t_cB};
+  launch_wave<double, true>(wa, pop, st, wgrid);
+  k_upper<double><<<grid, kThreads, 0, st>>>(g, t_cL, t_cD, t_cB, t_uR, t_uU, t_uF);
+  FwdOp<double> fo{{t_r, t_cL, t_cD, t_cB, t_E}, t_q};
+  launch_wave<double, true>(wa, fo, st, wgrid);
+  BwdOp<double> bo{{t_q, t_E, t_uR, t_uU, t_uF, t_r}, t_z};
+  launch_wave<double, false>(wa, bo, st, wgrid);
+  k_from_tiled<double, double><<<grid, kThreads, 0, st>>>(g, t_z, z);
+  unsigned err = 0;
+  cudaMemcpyAsync(&err, &scal->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    *msg = cudaGetErrorString(e);
+    return -2;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    *msg = cudaGetErrorString(e);
+    return -2;
+  }
+  if (err & DEV_ERR_TIMEOUT) {
+    *msg = "wavefront wait timed out";
+    return -6;
+  }
+  return 0;
 }
 
 }  // namespace sc

@@ -188,4 +188,11 @@ class PcgSolver {
   cudaGraphExec_t& graph_for();
 };
 
+// Allocation-free ModifiedIncompleteCholesky3D::precond on device arrays in the
+// reference layout, using a static device array as scratch (sc_pcg.cu).
+int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int ny, int nz,
+                        const double* adiag, const double* const* an, const double* r,
+                        const uint8_t* active, double* z, double tau, double sigma,
+                        std::string* msg);
+
 }  // namespace sc

@@ -190,6 +190,115 @@ int sc_fvm_project_device(sc_context* ctx, int nx, int ny, int nz, double h, dou
                           const double* fluid_sdf, const double* u_wt, const double* v_wt,
                           const double* w_wt);
 
+/* ---------------------------------------------------------------------------
+ * Particle/grid transfers of HybridAdvectionSolver3D
+ * (FluidSim/include/FluidSim/cpu/advect-solver.h:40-140) as stand-alone device
+ * calls, FP64.  Particles are arrays of n xyz triples (pos[3*i+0..2]); grids
+ * are face grids in the reference layout with cubic cells of spacing h and the
+ * origin at 0.  Transfer kernel: cubic B-spline per axis over the stencil
+ * nearest + {-1, 0, 1, 2} of each face grid (advect-solver.cc:44, 207-235).
+ */
+
+/* FlipAdvectionSolver3D::solveP2G (advect-solver.cc:188-271): u/v/w = weighted
+ * averages of the particle velocities, u_wt/v_wt/w_wt the weight sums,
+ * *_valid = weight sum > 0; when u_last is non-NULL the results are also copied
+ * into u_last/v_last/w_last (the FLIP reference grids).  Results do not depend
+ * on the particle order beyond floating-point summation order. */
+int sc_flip_p2g_device(sc_context* ctx, int64_t n, const double* pos, const double* vel, int nx,
+                       int ny, int nz, double h, double* u, double* v, double* w, double* u_wt,
+                       double* v_wt, double* w_wt, uint8_t* u_valid, uint8_t* v_valid,
+                       uint8_t* w_valid, double* u_last, double* v_last, double* w_last);
+/* sampleVelocity(p, ug, vg, wg) (FluidSim/src/cpu/util.cc:40-85) at n points. */
+int sc_sample_velocity_device(sc_context* ctx, int64_t n, const double* pts, int nx, int ny,
+                              int nz, double h, const double* u, const double* v,
+                              const double* w, double* out);
+/* FlipAdvectionSolver3D::solveG2P (advect-solver.cc:157-169):
+ * vel = alpha*(vel + pic - sample(last)) + (1-alpha)*pic; alpha < 0 selects
+ * PicAdvector3D::solveG2P (vel = pic, advect-solver.cc:7-17). */
+int sc_flip_g2p_device(sc_context* ctx, int64_t n, const double* pos, double* vel, int nx, int ny,
+                       int nz, double h, const double* u, const double* v, const double* w,
+                       const double* u_last, const double* v_last, const double* w_last,
+                       double alpha);
+/* FlipAdvectionSolver3D::advect (advect-solver.cc:170-187): Ralston RK3 through
+ * the given grids, then handleCollision (advect-solver.cc:100-137) against the
+ * collider SDF (NULL: no collider) and the domain box. */
+int sc_flip_advect_device(sc_context* ctx, int64_t n, double* pos, double* vel, int nx, int ny,
+                          int nz, double h, const double* u, const double* v, const double* w,
+                          const double* collider_sdf, double dt);
+/* NaiveReconstructor::reconstruct (FluidSim/include/FluidSim/cpu/sdf.h:204-229)
+ * with the ParticleNeighbourSearcher buckets (ns-util.h:46-109): cell-centred
+ * SDF = min over particles within 2*radius of (distance - radius), 1e9 and
+ * valid = 0 where there is none.  Buckets are cells; inside a bucket particles
+ * are ordered by index and the last one is not visited, as in the reference. */
+int sc_reconstruct_device(sc_context* ctx, int64_t n, const double* pos, int nx, int ny, int nz,
+                          double h, double radius, double* sdf, uint8_t* valid);
+
+/* ---------------------------------------------------------------------------
+ * Whole simulator: fluid::cpu::FluidSimulator
+ * (FluidSim/include/FluidSim/cpu/fluid-simulator.h:25-200,
+ *  FluidSim/src/cpu/fluid-simulator.cc).  Particles and grids live on the
+ * device; particles are re-sorted by cell every substep, and the getters return
+ * them in the order they were given.
+ */
+#define SC_ADVECT_PIC 0
+#define SC_ADVECT_FLIP 1
+
+typedef struct {
+  int nx, ny, nz;        /* resolution (cells) */
+  double h;              /* cubic cell size; the domain is [0, n*h] per axis */
+  int precision;         /* SC_REAL_F64 / SC_REAL_F32: particles and velocity grids */
+  int advection;         /* SC_ADVECT_FLIP (reference default) / SC_ADVECT_PIC */
+  double flip_alpha;     /* FLIP blend, 0.97 (advect-solver.h:129) */
+  double cfl_factor;     /* CFL() multiplier, 5 (fluid-simulator.cc:202) */
+  double gravity;        /* applyForce, 9.8 (fluid-simulator.cc:16) */
+  double recon_factor;   /* reconstruction radius / h, 0.8 (fluid-simulator.cc:147) */
+  int sdf_extrap_iters;  /* extrapolateFluidSdf(10) (fluid-simulator.cc:151) */
+  int smooth_iters;      /* smoothFluidSurface(5) (fluid-simulator.cc:152) */
+  int vel_extrap_iters;  /* extrapolate(.., 10) (fluid-simulator.cc:160-162) */
+  sc_pcg_options pcg;    /* pressure solve */
+} sc_fluid_config;
+
+typedef struct {
+  int substeps;          /* substeps taken by this call */
+  int pcg_iterations;    /* last substep's solve */
+  int pcg_outer;
+  double pcg_residual;   /* what solvePressure returned (fluid-simulator.cc:169) */
+  double ms_advect, ms_sort_sdf, ms_p2g, ms_build, ms_solve, ms_project_g2p;
+  double ms_total;       /* device time, CUDA events, summed over substeps */
+  int64_t kernel_launches;
+} sc_fluid_stats;
+
+typedef struct sc_fluid sc_fluid;
+
+/* Reference defaults for an nx*ny*nz grid of spacing h. */
+void sc_fluid_default_config(int nx, int ny, int nz, double h, sc_fluid_config* cfg);
+/* FluidSimulator(n, size, resolution) (fluid-simulator.h:28-57). */
+int sc_fluid_create(sc_context* ctx, const sc_fluid_config* cfg, sc_fluid** out);
+void sc_fluid_destroy(sc_fluid* sim);
+/* Initial particles (setInitialFluid, fluid-simulator.h:73-78, takes them from
+ * the caller); vel == NULL starts them at rest. */
+int sc_fluid_set_particles(sc_fluid* sim, int64_t n, const double* pos, const double* vel,
+                           int device_pointers);
+/* setCollider (fluid-simulator.h:62-72) given the collider SDF on the cell
+ * centres (what manifold2SDF produces); NULL removes it. */
+int sc_fluid_set_collider(sc_fluid* sim, const double* sdf, int device_pointers);
+/* CFL() (fluid-simulator.cc:184-203). */
+int sc_fluid_cfl(sc_fluid* sim, double* dt);
+/* substep(dt) (fluid-simulator.cc:140-182). */
+int sc_fluid_substep(sc_fluid* sim, double dt, sc_fluid_stats* stats);
+/* step(frame): substeps of min(CFL(), remaining) until frame_dt is covered
+ * (fluid-simulator.cc:205-220). */
+int sc_fluid_step(sc_fluid* sim, double frame_dt, sc_fluid_stats* stats);
+int64_t sc_fluid_num_particles(sc_fluid* sim);
+/* positions() and the advector's velocities, n*3 doubles each (either may be NULL). */
+int sc_fluid_get_particles(sc_fluid* sim, double* pos, double* vel, int device_pointers);
+/* pg after the last substep (nx*ny*nz doubles). */
+int sc_fluid_get_pressure(sc_fluid* sim, double* pg, int device_pointers);
+/* ug/vg/wg after the last substep, as doubles (any may be NULL). */
+int sc_fluid_get_faces(sc_fluid* sim, double* u, double* v, double* w, int device_pointers);
+/* exportFluidSurface() (fluid-simulator.h:187-189): the smoothed fluid SDF. */
+int sc_fluid_get_fluid_sdf(sc_fluid* sim, double* sdf, int device_pointers);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,11 +28,29 @@ class sc_pcg_stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class sc_fluid_config(ctypes.Structure):
+    _fields_ = [("nx", c_int), ("ny", c_int), ("nz", c_int), ("h", c_double), ("precision", c_int),
+                ("advection", c_int), ("flip_alpha", c_double), ("cfl_factor", c_double),
+                ("gravity", c_double), ("recon_factor", c_double), ("sdf_extrap_iters", c_int),
+                ("smooth_iters", c_int), ("vel_extrap_iters", c_int), ("pcg", sc_pcg_options)]
+
+
+class sc_fluid_stats(ctypes.Structure):
+    _fields_ = [("substeps", c_int), ("pcg_iterations", c_int), ("pcg_outer", c_int),
+                ("pcg_residual", c_double), ("ms_advect", c_double), ("ms_sort_sdf", c_double),
+                ("ms_p2g", c_double), ("ms_build", c_double), ("ms_solve", c_double),
+                ("ms_project_g2p", c_double), ("ms_total", c_double), ("kernel_launches", c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 SC_OK = 0
 SC_CRIT_ABS_LINF, SC_CRIT_REL_L2 = 0, 1
 SC_PREC_FP64, SC_PREC_MIXED = 0, 1
 SC_REAL_F64, SC_REAL_F32 = 0, 1
 SC_DONE_CONVERGED, SC_DONE_MAXITER, SC_DONE_BREAKDOWN = 1, 2, 3
+SC_ADVECT_PIC, SC_ADVECT_FLIP = 0, 1
 
 _dpp = P(c_void_p)  # array of pointers
 
@@ -67,6 +85,29 @@ SIGNATURES = {
                                            _dpp, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "sc_fvm_project_device": (c_int, [c_void_p, c_int, c_int, c_int, c_double, c_double, c_int, c_void_p,
                                       c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "sc_flip_p2g_device": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_int, c_int, c_int, c_double]
+                           + [c_void_p] * 12),
+    "sc_sample_velocity_device": (c_int, [c_void_p, c_int64, c_void_p, c_int, c_int, c_int, c_double,
+                                          c_void_p, c_void_p, c_void_p, c_void_p]),
+    "sc_flip_g2p_device": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_int, c_int, c_int, c_double]
+                           + [c_void_p] * 6 + [c_double]),
+    "sc_flip_advect_device": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_int, c_int, c_int, c_double,
+                                      c_void_p, c_void_p, c_void_p, c_void_p, c_double]),
+    "sc_reconstruct_device": (c_int, [c_void_p, c_int64, c_void_p, c_int, c_int, c_int, c_double, c_double,
+                                      c_void_p, c_void_p]),
+    "sc_fluid_default_config": (None, [c_int, c_int, c_int, c_double, P(sc_fluid_config)]),
+    "sc_fluid_create": (c_int, [c_void_p, P(sc_fluid_config), P(c_void_p)]),
+    "sc_fluid_destroy": (None, [c_void_p]),
+    "sc_fluid_set_particles": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_int]),
+    "sc_fluid_set_collider": (c_int, [c_void_p, c_void_p, c_int]),
+    "sc_fluid_cfl": (c_int, [c_void_p, P(c_double)]),
+    "sc_fluid_substep": (c_int, [c_void_p, c_double, P(sc_fluid_stats)]),
+    "sc_fluid_step": (c_int, [c_void_p, c_double, P(sc_fluid_stats)]),
+    "sc_fluid_num_particles": (c_int64, [c_void_p]),
+    "sc_fluid_get_particles": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "sc_fluid_get_pressure": (c_int, [c_void_p, c_void_p, c_int]),
+    "sc_fluid_get_faces": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
+    "sc_fluid_get_fluid_sdf": (c_int, [c_void_p, c_void_p, c_int]),
 }
 
 _lib = None

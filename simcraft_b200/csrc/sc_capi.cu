@@ -4,6 +4,7 @@
 #include <string>
 
 #include "../../include/simcraft_fluid_capi.h"
+#include "sc_flip.cuh"
 #include "sc_fvm.cuh"
 #include "sc_pcg.cuh"
 
@@ -15,6 +16,11 @@ struct sc_context {
 struct sc_pcg {
   sc_context* ctx;
   sc::PcgSolver* solver;
+};
+
+struct sc_fluid {
+  sc_context* ctx;
+  sc::FluidSim* sim;
 };
 
 namespace {
@@ -344,6 +350,244 @@ int sc_mic_precond_noalloc_device(sc_context* ctx, int nx, int ny, int nz, const
                                    an, r, active, z, tau, sigma, &msg);
   if (rc) return ctx->c.set_error(map_status(rc), msg);
   return SC_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Particle/grid transfers (device, FP64).
+
+static bool grid_ok(int nx, int ny, int nz, double h) {
+  return nx >= 1 && ny >= 1 && nz >= 1 && h > 0.0 && (int64_t)(nx + 1) * (ny + 1) * (nz + 1) < ((int64_t)1 << 31);
+}
+
+static int finish(sc_context* ctx, int rc, const char* what) {
+  if (rc == 0) {
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return SC_OK;
+    return ctx->c.set_error(SC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+  return ctx->c.set_error(map_status(rc), std::string(what) + " failed");
+}
+
+int sc_flip_p2g_device(sc_context* ctx, int64_t n, const double* pos, const double* vel, int nx,
+                       int ny, int nz, double h, double* u, double* v, double* w, double* u_wt,
+                       double* v_wt, double* w_wt, uint8_t* u_valid, uint8_t* v_valid,
+                       uint8_t* w_valid, double* u_last, double* v_last, double* w_last) {
+  if (!ctx || n < 0 || (n > 0 && (!pos || !vel)) || !grid_ok(nx, ny, nz, h) || !u || !v || !w ||
+      !u_wt || !v_wt || !w_wt || !u_valid || !v_valid || !w_valid ||
+      ((u_last || v_last || w_last) && !(u_last && v_last && w_last)))
+    return SC_ERR_INVALID;
+  cudaSetDevice(ctx->c.device);
+  return finish(ctx,
+                sc::flip_p2g(ctx->c.stream, n, pos, vel, nx, ny, nz, h, u, v, w, u_wt, v_wt, w_wt,
+                             u_valid, v_valid, w_valid, u_last, v_last, w_last),
+                "p2g");
+}
+
+int sc_sample_velocity_device(sc_context* ctx, int64_t n, const double* pts, int nx, int ny,
+                              int nz, double h, const double* u, const double* v,
+                              const double* w, double* out) {
+  if (!ctx || n < 0 || (n > 0 && (!pts || !out)) || !grid_ok(nx, ny, nz, h) || !u || !v || !w)
+    return SC_ERR_INVALID;
+  if (n == 0) return SC_OK;
+  cudaSetDevice(ctx->c.device);
+  return finish(ctx, sc::flip_sample(ctx->c.stream, n, pts, nx, ny, nz, h, u, v, w, out),
+                "sample_velocity");
+}
+
+int sc_flip_g2p_device(sc_context* ctx, int64_t n, const double* pos, double* vel, int nx, int ny,
+                       int nz, double h, const double* u, const double* v, const double* w,
+                       const double* u_last, const double* v_last, const double* w_last,
+                       double alpha) {
+  if (!ctx || n < 0 || (n > 0 && (!pos || !vel)) || !grid_ok(nx, ny, nz, h) || !u || !v || !w ||
+      (alpha >= 0.0 && (!u_last || !v_last || !w_last)) || alpha > 1.0)
+    return SC_ERR_INVALID;
+  if (n == 0) return SC_OK;
+  cudaSetDevice(ctx->c.device);
+  return finish(ctx,
+                sc::flip_g2p(ctx->c.stream, n, pos, vel, nx, ny, nz, h, u, v, w, u_last, v_last,
+                             w_last, alpha),
+                "g2p");
+}
+
+int sc_flip_advect_device(sc_context* ctx, int64_t n, double* pos, double* vel, int nx, int ny,
+                          int nz, double h, const double* u, const double* v, const double* w,
+                          const double* collider_sdf, double dt) {
+  if (!ctx || n < 0 || (n > 0 && (!pos || !vel)) || !grid_ok(nx, ny, nz, h) || !u || !v || !w ||
+      !(dt >= 0.0))
+    return SC_ERR_INVALID;
+  if (n == 0) return SC_OK;
+  cudaSetDevice(ctx->c.device);
+  return finish(ctx,
+                sc::flip_advect(ctx->c.stream, n, pos, vel, nx, ny, nz, h, u, v, w, collider_sdf,
+                                dt),
+                "advect");
+}
+
+int sc_reconstruct_device(sc_context* ctx, int64_t n, const double* pos, int nx, int ny, int nz,
+                          double h, double radius, double* sdf, uint8_t* valid) {
+  if (!ctx || n < 0 || (n > 0 && !pos) || !grid_ok(nx, ny, nz, h) || !(radius > 0.0) || !sdf ||
+      !valid)
+    return SC_ERR_INVALID;
+  cudaSetDevice(ctx->c.device);
+  return finish(ctx, sc::flip_reconstruct(ctx->c.stream, n, pos, nx, ny, nz, h, radius, sdf, valid),
+                "reconstruct");
+}
+
+// ---------------------------------------------------------------------------------
+// Simulator.
+
+void sc_fluid_default_config(int nx, int ny, int nz, double h, sc_fluid_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->nx = nx;
+  c->ny = ny;
+  c->nz = nz;
+  c->h = h;
+  c->precision = SC_REAL_F64;
+  c->advection = SC_ADVECT_FLIP;
+  c->flip_alpha = 0.97;
+  c->cfl_factor = 5.0;
+  c->gravity = 9.8;
+  c->recon_factor = 0.8;
+  c->sdf_extrap_iters = 10;
+  c->smooth_iters = 5;
+  c->vel_extrap_iters = 10;
+  sc_pcg_default_options(&c->pcg);
+}
+
+int sc_fluid_create(sc_context* ctx, const sc_fluid_config* cfg, sc_fluid** out) {
+  if (!ctx || !cfg || !out) return SC_ERR_INVALID;
+  *out = nullptr;
+  if (!grid_ok(cfg->nx, cfg->ny, cfg->nz, cfg->h) ||
+      (cfg->precision != SC_REAL_F64 && cfg->precision != SC_REAL_F32) ||
+      (cfg->advection != SC_ADVECT_FLIP && cfg->advection != SC_ADVECT_PIC) ||
+      !(cfg->flip_alpha >= 0.0 && cfg->flip_alpha <= 1.0) || !(cfg->cfl_factor > 0.0) ||
+      !(cfg->recon_factor > 0.0) || cfg->sdf_extrap_iters < 0 || cfg->smooth_iters < 0 ||
+      cfg->vel_extrap_iters < 0 || validate_options(&cfg->pcg))
+    return ctx->c.set_error(SC_ERR_INVALID, "invalid simulator configuration");
+  sc::FluidConfig fc;
+  fc.nx = cfg->nx;
+  fc.ny = cfg->ny;
+  fc.nz = cfg->nz;
+  fc.h = cfg->h;
+  fc.f32 = cfg->precision == SC_REAL_F32;
+  fc.flip = cfg->advection == SC_ADVECT_FLIP;
+  fc.flip_alpha = cfg->flip_alpha;
+  fc.pcg = to_internal(&cfg->pcg);
+  fc.cfl_factor = cfg->cfl_factor;
+  fc.gravity = cfg->gravity;
+  fc.recon_factor = cfg->recon_factor;
+  fc.sdf_extrap_iters = cfg->sdf_extrap_iters;
+  fc.smooth_iters = cfg->smooth_iters;
+  fc.vel_extrap_iters = cfg->vel_extrap_iters;
+  cudaSetDevice(ctx->c.device);
+  sc::FluidSim* s = new (std::nothrow) sc::FluidSim(&ctx->c, fc);
+  if (!s) return SC_ERR_NOMEM;
+  if (s->status()) {
+    int st = s->status();
+    delete s;
+    return ctx->c.set_error(map_status(st), "simulator create failed");
+  }
+  sc_fluid* f = new (std::nothrow) sc_fluid{ctx, s};
+  if (!f) {
+    delete s;
+    return SC_ERR_NOMEM;
+  }
+  *out = f;
+  return SC_OK;
+}
+
+void sc_fluid_destroy(sc_fluid* sim) {
+  if (!sim) return;
+  cudaSetDevice(sim->ctx->c.device);
+  delete sim->sim;
+  delete sim;
+}
+
+static int fl_rc(sc_fluid* f, int rc) {
+  if (rc == 0) return SC_OK;
+  if (f->ctx->c.last_error.empty()) f->ctx->c.last_error = "simulator call failed";
+  return map_status(rc);
+}
+
+int sc_fluid_set_particles(sc_fluid* sim, int64_t n, const double* pos, const double* vel,
+                           int device_pointers) {
+  if (!sim || n < 0 || (n > 0 && !pos) || n >= ((int64_t)1 << 31)) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  return fl_rc(sim, sim->sim->set_particles(n, pos, vel, device_pointers != 0));
+}
+
+int sc_fluid_set_collider(sc_fluid* sim, const double* sdf, int device_pointers) {
+  if (!sim) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  return fl_rc(sim, sim->sim->set_collider(sdf, device_pointers != 0));
+}
+
+int sc_fluid_cfl(sc_fluid* sim, double* dt) {
+  if (!sim || !dt) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  *dt = sim->sim->cfl();
+  return finish(sim->ctx, 0, "cfl");
+}
+
+static void stats_out(const sc::StepStats& s, sc_fluid_stats* o) {
+  if (!o) return;
+  o->substeps = s.substeps;
+  o->pcg_iterations = s.pcg_iterations;
+  o->pcg_outer = s.pcg_outer;
+  o->pcg_residual = s.pcg_residual;
+  o->ms_advect = s.ms_advect;
+  o->ms_sort_sdf = s.ms_sort_sdf;
+  o->ms_p2g = s.ms_p2g;
+  o->ms_build = s.ms_build;
+  o->ms_solve = s.ms_solve;
+  o->ms_project_g2p = s.ms_project_g2p;
+  o->ms_total = s.ms_total;
+  o->kernel_launches = s.kernel_launches;
+}
+
+int sc_fluid_substep(sc_fluid* sim, double dt, sc_fluid_stats* stats) {
+  if (!sim || !(dt > 0.0)) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  sc::StepStats s;
+  int rc = sim->sim->substep(dt, &s);
+  stats_out(s, stats);
+  return fl_rc(sim, rc);
+}
+
+int sc_fluid_step(sc_fluid* sim, double frame_dt, sc_fluid_stats* stats) {
+  if (!sim || !(frame_dt > 0.0)) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  sc::StepStats s;
+  int rc = sim->sim->step(frame_dt, &s);
+  stats_out(s, stats);
+  return fl_rc(sim, rc);
+}
+
+int64_t sc_fluid_num_particles(sc_fluid* sim) { return sim ? sim->sim->num_particles() : 0; }
+
+int sc_fluid_get_particles(sc_fluid* sim, double* pos, double* vel, int device_pointers) {
+  if (!sim) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  return fl_rc(sim, sim->sim->get_particles(pos, vel, device_pointers != 0));
+}
+
+int sc_fluid_get_pressure(sc_fluid* sim, double* pg, int device_pointers) {
+  if (!sim || !pg) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  return fl_rc(sim, sim->sim->get_pressure(pg, device_pointers != 0));
+}
+
+int sc_fluid_get_faces(sc_fluid* sim, double* u, double* v, double* w, int device_pointers) {
+  if (!sim) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  return fl_rc(sim, sim->sim->get_faces(u, v, w, device_pointers != 0));
+}
+
+int sc_fluid_get_fluid_sdf(sc_fluid* sim, double* sdf, int device_pointers) {
+  if (!sim || !sdf) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  return fl_rc(sim, sim->sim->get_fluid_sdf(sdf, device_pointers != 0));
 }
 
 }  // extern "C"

@@ -1,0 +1,1216 @@
+// sc_flip.cu -- the FLIP/PIC substep of SimCraft FluidSim on B200 (sm_100a).
+//
+// Restates fluid::cpu::FluidSimulator::substep (FluidSim/src/cpu/fluid-simulator.cc:140-182)
+// and its callees on the GPU:
+//   advect + handleCollision    advect-solver.cc:100-137, 170-187   k_advect
+//   NaiveReconstructor          sdf.h:204-229, ns-util.h:46-109      k_keys/scan/scatter + k_reconstruct
+//   extrapolateFluidSdf/smooth  cpu/fluid-simulator.h:123-166, fluid-simulator.cc:39-74
+//   solveP2G                    advect-solver.cc:188-271             k_p2g (gather per face node)
+//   applyDirichletBoundary, extrapolate, applyForce, buildSystem, solvePressure, project,
+//   applyCollider, solveG2P     fluid-simulator.cc:13-138, advect-solver.cc:157-169
+//
+// Particles are re-sorted by cell every substep (counting sort; inside a cell by
+// original index), which makes every transfer deterministic: P2G gathers from
+// the sorted cell buckets instead of scattering with atomics.  Arithmetic that
+// decides discrete outcomes (nearest node, reconstruction distances, kernel
+// weights, sampling sums) uses explicitly rounded operations in the reference's
+// order so that it matches the CPU bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "sc_flip.cuh"
+#include "sc_fvm.cuh"
+
+namespace sc {
+namespace {
+
+constexpr int kT = 256;
+
+inline int nblk(int64_t n) {
+  int64_t b = (n + kT - 1) / kT;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 1 << 20));
+}
+#define GRID_LOOP(i, n) \
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+// IEEE round-to-nearest operations without contraction, per precision.
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// Face-grid geometry (Spatify/include/Spatify/grids.h:287-308, 479-485).
+struct Geo {
+  int nx, ny, nz;
+  __device__ __forceinline__ int fx(int ax) const { return nx + (ax == 0); }
+  __device__ __forceinline__ int fy(int ax) const { return ny + (ax == 1); }
+  __device__ __forceinline__ int fz(int ax) const { return nz + (ax == 2); }
+};
+
+// TGrid::nearest: Vec3i((coord - origin - offset*h)/h + 0.5), truncation.
+template <class T>
+__device__ __forceinline__ int nearest1(T p, T off, T h) {
+  return (int)radd(rdiv(rsub(rsub(p, T(0)), rmul(off, h)), h), T(0.5));
+}
+// TGrid::indexToCoord: (index + offset) * h + origin.
+template <class T>
+__device__ __forceinline__ T coord1(int i, T off, T h) {
+  return radd(rmul(radd((T)i, off), h), T(0));
+}
+// Cubic B-spline policy for core::CubicKernel (advect-solver.cc:44): per-axis
+// N(|d|/h) with N(r) = 2/3 - r^2 + r^3/2 (r < 1), (2 - r)^3 / 6 (r < 2).
+template <class T>
+__device__ __forceinline__ T bspline(T r) {
+  if (r < T(1)) return radd(rsub(T(2.0 / 3.0), rmul(r, r)), rmul(rmul(rmul(T(0.5), r), r), r));
+  if (r < T(2)) {
+    T t = rsub(T(2), r);
+    return rdiv(rmul(rmul(t, t), t), T(6));
+  }
+  return T(0);
+}
+template <class T>
+__device__ __forceinline__ T kweight(T h, T dx, T dy, T dz) {
+  return rmul(rmul(bspline(rdiv(fabs(dx), h)), bspline(rdiv(fabs(dy), h))),
+              bspline(rdiv(fabs(dz), h)));
+}
+
+// sampleVelocity for one face grid (FluidSim/src/cpu/util.cc:40-85), same loop
+// order and accumulation order.
+template <class T>
+__device__ __forceinline__ T sample_grid(const T* __restrict__ g, int ax, const Geo& G, T h, T px,
+                                         T py, T pz) {
+  const T ox = ax == 0 ? T(0) : T(0.5), oy = ax == 1 ? T(0) : T(0.5), oz = ax == 2 ? T(0) : T(0.5);
+  const int fx = G.fx(ax), fy = G.fy(ax), fz = G.fz(ax);
+  const int bi = nearest1(px, ox, h), bj = nearest1(py, oy, h), bk = nearest1(pz, oz, h);
+  T s = T(0), ws = T(0);
+  for (int i = -1; i <= 2; i++) {
+    const int a = bi + i;
+    if (a < 0 || a >= fx) continue;
+    const T dx = rsub(px, coord1(a, ox, h));
+    for (int j = -1; j <= 2; j++) {
+      const int b = bj + j;
+      if (b < 0 || b >= fy) continue;
+      const T dy = rsub(py, coord1(b, oy, h));
+      for (int k = -1; k <= 2; k++) {
+        const int c = bk + k;
+        if (c < 0 || c >= fz) continue;
+        const T dz = rsub(pz, coord1(c, oz, h));
+        const T wt = kweight(h, dx, dy, dz);
+        s = radd(s, rmul(g[lin(a, b, c, fy, fz)], wt));
+        ws = radd(ws, wt);
+      }
+    }
+  }
+  return ws > T(0) ? rdiv(s, ws) : T(0);
+}
+
+// SDF<3>::gradient(idx) and grad(p) (FluidSim/include/FluidSim/cpu/sdf.h:62-118).
+__device__ void sdf_gradient_at(const double* S, const Geo& G, double h, int ix, int iy, int iz,
+                                double* g) {
+  const int nx = G.nx, ny = G.ny, nz = G.nz;
+  int xn = ix < nx - 1 ? ix + 1 : ix, xp = ix > 0 ? ix - 1 : ix;
+  int yn = iy < ny - 1 ? iy + 1 : iy, yp = iy > 0 ? iy - 1 : iy;
+  int zn = iz < nz - 1 ? iz + 1 : iz, zp = iz > 0 ? iz - 1 : iz;
+  double dx = ix > 0 && ix < nx - 1 ? 2 * h : h;
+  double dy = iy > 0 && iy < ny - 1 ? 2 * h : h;
+  double dz = iz > 0 && iz < nz - 1 ? 2 * h : h;
+  g[0] = (S[lin(xn, iy, iz, ny, nz)] - S[lin(xp, iy, iz, ny, nz)]) / dx;
+  g[1] = (S[lin(ix, yn, iz, ny, nz)] - S[lin(ix, yp, iz, ny, nz)]) / dy;
+  g[2] = (S[lin(ix, iy, zn, ny, nz)] - S[lin(ix, iy, zp, ny, nz)]) / dz;
+}
+__device__ void sdf_grad(const double* S, const Geo& G, double h, double px, double py, double pz,
+                         double* out) {
+  auto clampi = [](int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); };
+  int ix = (int)((px - 0.0) / h - 0.5), iy = (int)((py - 0.0) / h - 0.5), iz = (int)((pz - 0.0) / h - 0.5);
+  int x = clampi(ix, 0, G.nx - 1), y = clampi(iy, 0, G.ny - 1), z = clampi(iz, 0, G.nz - 1);
+  int xn = clampi(ix + 1, 0, G.nx - 1), yn = clampi(iy + 1, 0, G.ny - 1), zn = clampi(iz + 1, 0, G.nz - 1);
+  double tx = (px - (((double)x + 0.5) * h + 0.0)) / h;
+  double ty = (py - (((double)y + 0.5) * h + 0.0)) / h;
+  double tz = (pz - (((double)z + 0.5) * h + 0.0)) / h;
+  double g[8][3];
+  sdf_gradient_at(S, G, h, x, y, z, g[0]);
+  sdf_gradient_at(S, G, h, x, y, zn, g[1]);
+  sdf_gradient_at(S, G, h, x, yn, z, g[2]);
+  sdf_gradient_at(S, G, h, x, yn, zn, g[3]);
+  sdf_gradient_at(S, G, h, xn, y, z, g[4]);
+  sdf_gradient_at(S, G, h, xn, y, zn, g[5]);
+  sdf_gradient_at(S, G, h, xn, yn, z, g[6]);
+  sdf_gradient_at(S, G, h, xn, yn, zn, g[7]);
+  const double w[8] = {tx * ty * tz,       tx * ty * (1 - tz),       tx * (1 - ty) * tz,
+                       tx * (1 - ty) * (1 - tz), (1 - tx) * ty * tz, (1 - tx) * ty * (1 - tz),
+                       (1 - tx) * (1 - ty) * tz, (1 - tx) * (1 - ty) * (1 - tz)};
+  for (int c = 0; c < 3; c++) {
+    double s = 0.0;
+    for (int k = 0; k < 8; k++) s += w[k] * g[k][c];
+    out[c] = s;
+  }
+}
+
+// HybridAdvectionSolver3D::handleCollision (advect-solver.cc:100-137).
+template <class T>
+__device__ void handle_collision(const double* col, const Geo& G, double h, T& px, T& py, T& pz,
+                                 T& vx, T& vy, T& vz) {
+  if (col) {
+    const double d = sdf_eval(col, G.nx, G.ny, G.nz, h, (double)px, (double)py, (double)pz);
+    if (d < 0.0) {
+      double n[3];
+      sdf_grad(col, G, h, (double)px, (double)py, (double)pz, n);
+      const double l = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      n[0] /= l;
+      n[1] /= l;
+      n[2] /= l;
+      px = (T)((double)px - d * n[0]);
+      py = (T)((double)py - d * n[1]);
+      pz = (T)((double)pz - d * n[2]);
+      const double vn = fmin((double)vx * n[0] + (double)vy * n[1] + (double)vz * n[2], 0.0);
+      vx = (T)((double)vx - vn * n[0]);
+      vy = (T)((double)vy - vn * n[1]);
+      vz = (T)((double)vz - vn * n[2]);
+    }
+  }
+  const T width = (T)(G.nx * h), height = (T)(G.ny * h), depth = (T)(G.nz * h);
+  if (px < T(0)) {
+    px = T(0);
+    if (vx < T(0)) vx = T(0);
+  }
+  if (px > width) {
+    px = width;
+    if (vx > T(0)) vx = T(0);
+  }
+  if (py < T(0)) {
+    py = T(0);
+    if (vy < T(0)) vy = T(0);
+  }
+  if (py > height) {
+    py = height;
+    if (vy > T(0)) vy = T(0);
+  }
+  if (pz < T(0)) {
+    pz = T(0);
+    if (vz < T(0)) vz = T(0);
+  }
+  if (pz > depth) {
+    pz = depth;
+    if (vz > T(0)) vz = T(0);
+  }
+}
+
+struct Parts {
+  void *px, *py, *pz, *vx, *vy, *vz;
+};
+template <class T>
+struct PartsT {
+  T *px, *py, *pz, *vx, *vy, *vz;
+  __host__ __device__ static PartsT from(const Parts& p) {
+    return {(T*)p.px, (T*)p.py, (T*)p.pz, (T*)p.vx, (T*)p.vy, (T*)p.vz};
+  }
+};
+
+// FlipAdvectionSolver3D::advect: RK3 (Ralston) with k2, k3 sampled from the
+// grids it is given (advect-solver.cc:170-187), then handleCollision.
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_advect(int64_t n, PartsT<T> P, const T* __restrict__ u, const T* __restrict__ v,
+             const T* __restrict__ w, Geo G, double hd, const double* col, double dtd) {
+  const T h = (T)hd, dt = (T)dtd;
+  GRID_LOOP(i, n) {
+    T px = P.px[i], py = P.py[i], pz = P.pz[i];
+    const T k1x = P.vx[i], k1y = P.vy[i], k1z = P.vz[i];
+    const T a = rmul(T(0.5), dt);
+    const T p1x = radd(px, rmul(a, k1x)), p1y = radd(py, rmul(a, k1y)), p1z = radd(pz, rmul(a, k1z));
+    const T k2x = sample_grid(u, 0, G, h, p1x, p1y, p1z), k2y = sample_grid(v, 1, G, h, p1x, p1y, p1z),
+            k2z = sample_grid(w, 2, G, h, p1x, p1y, p1z);
+    const T b = rmul(T(0.75), dt);
+    const T p2x = radd(px, rmul(b, k2x)), p2y = radd(py, rmul(b, k2y)), p2z = radd(pz, rmul(b, k2z));
+    const T k3x = sample_grid(u, 0, G, h, p2x, p2y, p2z), k3y = sample_grid(v, 1, G, h, p2x, p2y, p2z),
+            k3z = sample_grid(w, 2, G, h, p2x, p2y, p2z);
+    const T c1 = rmul(T(2.0 / 9.0), dt), c2 = rmul(T(1.0 / 3.0), dt), c3 = rmul(T(4.0 / 9.0), dt);
+    px = radd(radd(radd(px, rmul(c1, k1x)), rmul(c2, k2x)), rmul(c3, k3x));
+    py = radd(radd(radd(py, rmul(c1, k1y)), rmul(c2, k2y)), rmul(c3, k3y));
+    pz = radd(radd(radd(pz, rmul(c1, k1z)), rmul(c2, k2z)), rmul(c3, k3z));
+    T vx = k1x, vy = k1y, vz = k1z;
+    handle_collision(col, G, hd, px, py, pz, vx, vy, vz);
+    P.px[i] = px;
+    P.py[i] = py;
+    P.pz[i] = pz;
+    P.vx[i] = vx;
+    P.vy[i] = vy;
+    P.vz[i] = vz;
+  }
+}
+
+// FlipAdvectionSolver3D::solveG2P (advect-solver.cc:157-169); alpha < 0 is PIC.
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_g2p(int64_t n, PartsT<T> P, const T* u, const T* v, const T* w, const T* ul, const T* vl,
+          const T* wl, Geo G, double hd, double alphad) {
+  const T h = (T)hd;
+  GRID_LOOP(i, n) {
+    const T px = P.px[i], py = P.py[i], pz = P.pz[i];
+    const T pu = sample_grid(u, 0, G, h, px, py, pz), pv = sample_grid(v, 1, G, h, px, py, pz),
+            pw = sample_grid(w, 2, G, h, px, py, pz);
+    if (alphad < 0.0) {
+      P.vx[i] = pu;
+      P.vy[i] = pv;
+      P.vz[i] = pw;
+      continue;
+    }
+    const T lu = sample_grid(ul, 0, G, h, px, py, pz), lv = sample_grid(vl, 1, G, h, px, py, pz),
+            lw = sample_grid(wl, 2, G, h, px, py, pz);
+    const T al = (T)alphad, bl = rsub(T(1), al);
+    const T fx = rsub(radd(P.vx[i], pu), lu), fy = rsub(radd(P.vy[i], pv), lv),
+            fz = rsub(radd(P.vz[i], pw), lw);
+    P.vx[i] = radd(rmul(al, fx), rmul(bl, pu));
+    P.vy[i] = radd(rmul(al, fy), rmul(bl, pv));
+    P.vz[i] = radd(rmul(al, fz), rmul(bl, pw));
+  }
+}
+
+// ---- counting sort by cell (ParticleNeighbourSearcher::update, ns-util.h:46-79) ----
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_keys(int64_t n, const T* px, const T* py, const T* pz, Geo G, double hd, int* key, int* cnt) {
+  const T h = (T)hd;
+  GRID_LOOP(i, n) {
+    int ix = (int)floor(rdiv(px[i], h)), iy = (int)floor(rdiv(py[i], h)), iz = (int)floor(rdiv(pz[i], h));
+    ix = ix < 0 ? 0 : (ix >= G.nx ? G.nx - 1 : ix);
+    iy = iy < 0 ? 0 : (iy >= G.ny ? G.ny - 1 : iy);
+    iz = iz < 0 ? 0 : (iz >= G.nz ? G.nz - 1 : iz);
+    const int c = (int)lin(ix, iy, iz, G.ny, G.nz);
+    key[i] = c;
+    atomicAdd(&cnt[c], 1);
+  }
+}
+
+// Exclusive scan of `in` into `out` (two-level: 1024-element blocks).
+__global__ void __launch_bounds__(1024) k_scan_blocks(int64_t n, const int* in, int* out, int* bsum) {
+  __shared__ int s[1024];
+  const int64_t i = (int64_t)blockIdx.x * 1024 + threadIdx.x;
+  int v = i < n ? in[i] : 0;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    int t = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) out[i] = s[threadIdx.x] - v;
+  if (threadIdx.x == 1023) bsum[blockIdx.x] = s[1023];
+}
+__global__ void __launch_bounds__(1024) k_scan_sums(int nb, int* bsum) {
+  __shared__ int s[1024];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += 1024) {
+    const int i = base + threadIdx.x;
+    int v = i < nb ? bsum[i] : 0;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      int t = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+      __syncthreads();
+      s[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < nb) bsum[i] = carry + s[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += s[1023];
+    __syncthreads();
+  }
+}
+__global__ void __launch_bounds__(1024) k_scan_add(int64_t n, int* out, const int* bsum) {
+  const int64_t i = (int64_t)blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) out[i] += bsum[blockIdx.x];
+}
+
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_scatter(int64_t n, const int* key, const int* start, int* cursor, PartsT<T> src,
+              const int64_t* sid, PartsT<T> dst, int64_t* did) {
+  GRID_LOOP(i, n) {
+    const int c = key[i];
+    const int64_t d = (int64_t)start[c] + atomicAdd(&cursor[c], 1);
+    dst.px[d] = src.px[i];
+    dst.py[d] = src.py[i];
+    dst.pz[d] = src.pz[i];
+    dst.vx[d] = src.vx[i];
+    dst.vy[d] = src.vy[i];
+    dst.vz[d] = src.vz[i];
+    did[d] = sid[i];
+  }
+}
+
+// Order each cell's bucket by original particle index (insertion sort); the
+// reference's bucket order is then pinned (ns-util.h:65-69 uses std::sort).
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_sort_cells(int64_t ncell, const int* start, const int* cnt, PartsT<T> P, int64_t* id) {
+  GRID_LOOP(c, ncell) {
+    const int64_t b = start[c];
+    const int m = cnt[c];
+    for (int i = 1; i < m; i++) {
+      int j = i;
+      while (j > 0 && id[b + j - 1] > id[b + j]) {
+        const int64_t a = b + j - 1, q = b + j;
+        auto sw = [&](auto* arr) {
+          auto t = arr[a];
+          arr[a] = arr[q];
+          arr[q] = t;
+        };
+        sw(P.px);
+        sw(P.py);
+        sw(P.pz);
+        sw(P.vx);
+        sw(P.vy);
+        sw(P.vz);
+        sw(id);
+        j--;
+      }
+    }
+  }
+}
+
+// NaiveReconstructor::reconstruct (sdf.h:210-225) over the sorted buckets:
+// cell-centred SDF = min over particles within 2r of (|x - p| - r).  Each
+// bucket's last particle is skipped, as the reference's forNeighbours loop
+// stops one short of its inclusive end index (ns-util.h:76-77, 103).
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_reconstruct(Geo G, double h, double radius, const int* start, const int* cnt,
+                  const T* __restrict__ px, const T* __restrict__ py, const T* __restrict__ pz,
+                  double* sdf, uint8_t* valid) {
+  const int64_t N = (int64_t)G.nx * G.ny * G.nz;
+  const double r2 = 2 * radius;
+  GRID_LOOP(id, N) {
+    const int k = (int)(id % G.nz);
+    const int j = (int)((id / G.nz) % G.ny);
+    const int i = (int)(id / ((int64_t)G.ny * G.nz));
+    const double cx = radd(rmul(radd((double)i, 0.5), h), 0.0);
+    const double cy = radd(rmul(radd((double)j, 0.5), h), 0.0);
+    const double cz = radd(rmul(radd((double)k, 0.5), h), 0.0);
+    const int x0 = max(0, (int)floor(rdiv(rsub(cx, r2), h))), x1 = min(G.nx - 1, (int)ceil(rdiv(radd(cx, r2), h)));
+    const int y0 = max(0, (int)floor(rdiv(rsub(cy, r2), h))), y1 = min(G.ny - 1, (int)ceil(rdiv(radd(cy, r2), h)));
+    const int z0 = max(0, (int)floor(rdiv(rsub(cz, r2), h))), z1 = min(G.nz - 1, (int)ceil(rdiv(radd(cz, r2), h)));
+    double best = 1e9;
+    uint8_t ok = 0;
+    const double lim = r2 * r2 * (1.0 + 1e-9);
+    // Distance from the cell centre to a bucket's cell box; boundary buckets
+    // also hold the particles clamped into them, so their boxes are open.
+    auto gap = [&](int a, int n, double c) {
+      const double lo = a > 0 ? a * h - c : -1e300, hi = a < n - 1 ? c - (a + 1) * h : -1e300;
+      return fmax(0.0, fmax(lo, hi));
+    };
+    for (int a = x0; a <= x1; a++) {
+      const double ex = gap(a, G.nx, cx);
+      for (int b = y0; b <= y1; b++) {
+        const double ey = gap(b, G.ny, cy);
+        if (ex * ex + ey * ey > lim) continue;
+        for (int c = z0; c <= z1; c++) {
+          const double ez = gap(c, G.nz, cz);
+          if (ex * ex + ey * ey + ez * ez > lim) continue;  // no particle of the bucket can be within 2r
+          const int cell = (int)lin(a, b, c, G.ny, G.nz);
+          const int m = cnt[cell];
+          if (m < 2) continue;
+          const int s = start[cell];
+          for (int l = s; l < s + m - 1; l++) {
+            const double dx = rsub((double)px[l], cx), dy = rsub((double)py[l], cy),
+                         dz = rsub((double)pz[l], cz);
+            const double dis = sqrt(radd(radd(rmul(dx, dx), rmul(dy, dy)), rmul(dz, dz)));
+            if (dis <= r2) {
+              best = fmin(best, rsub(dis, radius));
+              ok = 1;
+            }
+          }
+        }
+      }
+    }
+    sdf[id] = best;
+    valid[id] = ok;
+  }
+}
+
+// extrapolateFluidSdf iteration (cpu/fluid-simulator.h:123-166): valid cells
+// keep whatever the destination buffer holds.
+__global__ void __launch_bounds__(kT)
+    k_extrap_sdf(Geo G, const double* __restrict__ src, double* __restrict__ dst,
+                 const uint8_t* __restrict__ vs, uint8_t* __restrict__ vd) {
+  const int64_t N = (int64_t)G.nx * G.ny * G.nz;
+  const int64_t sx = (int64_t)G.ny * G.nz, sy = G.nz;
+  GRID_LOOP(id, N) {
+    if (vs[id]) {
+      vd[id] = 1;
+      continue;
+    }
+    const int k = (int)(id % G.nz);
+    const int j = (int)((id / G.nz) % G.ny);
+    const int i = (int)(id / sx);
+    double sum = 0.0;
+    int cnt = 0;
+    if (i > 0 && vs[id - sx]) { sum = radd(sum, src[id - sx]); cnt++; }
+    if (i < G.nx - 1 && vs[id + sx]) { sum = radd(sum, src[id + sx]); cnt++; }
+    if (j > 0 && vs[id - sy]) { sum = radd(sum, src[id - sy]); cnt++; }
+    if (j < G.ny - 1 && vs[id + sy]) { sum = radd(sum, src[id + sy]); cnt++; }
+    if (k > 0 && vs[id - 1]) { sum = radd(sum, src[id - 1]); cnt++; }
+    if (k < G.nz - 1 && vs[id + 1]) { sum = radd(sum, src[id + 1]); cnt++; }
+    if (cnt > 0) {
+      dst[id] = rdiv(sum, (double)cnt);
+      vd[id] = 1;
+    } else {
+      vd[id] = 0;
+    }
+  }
+}
+
+// smoothFluidSurface iteration (fluid-simulator.cc:39-74).
+__global__ void __launch_bounds__(kT)
+    k_smooth_sdf(Geo G, const double* __restrict__ src, double* __restrict__ dst) {
+  const int64_t N = (int64_t)G.nx * G.ny * G.nz;
+  const int64_t sx = (int64_t)G.ny * G.nz, sy = G.nz;
+  GRID_LOOP(id, N) {
+    const int k = (int)(id % G.nz);
+    const int j = (int)((id / G.nz) % G.ny);
+    const int i = (int)(id / sx);
+    double sum = 0.0;
+    int cnt = 0;
+    if (i > 0) { sum = radd(sum, src[id - sx]); cnt++; }
+    if (i < G.nx - 1) { sum = radd(sum, src[id + sx]); cnt++; }
+    if (j > 0) { sum = radd(sum, src[id - sy]); cnt++; }
+    if (j < G.ny - 1) { sum = radd(sum, src[id + sy]); cnt++; }
+    if (k > 0) { sum = radd(sum, src[id - 1]); cnt++; }
+    if (k < G.nz - 1) { sum = radd(sum, src[id + 1]); cnt++; }
+    double v = rdiv(sum, (double)cnt);
+    if (src[id] < v) v = src[id];
+    dst[id] = v;
+  }
+}
+
+// solveP2G for one face grid (advect-solver.cc:188-271), as a gather: each
+// face node sums the particles of the cells whose stencil nearest+{-1..2}^3
+// covers it, normalises by the weight sum, sets `valid`, and (FLIP) copies the
+// result into `last`.  The candidate cells follow from the nearest rule: along
+// an axis with face offset 0, nearest = round(p/h) and the bucket cell is
+// nearest-1 or nearest; with offset 1/2 the bucket is within 1 of nearest.
+template <class T, int AX>
+__global__ void __launch_bounds__(kT)
+    k_p2g(Geo G, double hd, const int* start, const int* cnt, PartsT<T> P, T* __restrict__ g,
+          T* __restrict__ wsum, uint8_t* __restrict__ valid, T* __restrict__ last) {
+  const T h = (T)hd;
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+  const int64_t n = (int64_t)fx * fy * fz;
+  const T ox = AX == 0 ? T(0) : T(0.5), oy = AX == 1 ? T(0) : T(0.5), oz = AX == 2 ? T(0) : T(0.5);
+  const T* vel = AX == 0 ? P.vx : (AX == 1 ? P.vy : P.vz);
+  GRID_LOOP(id, n) {
+    const int c = (int)(id % fz);
+    const int b = (int)((id / fz) % fy);
+    const int a = (int)(id / ((int64_t)fy * fz));
+    const T nx_ = coord1(a, ox, h), ny_ = coord1(b, oy, h), nz_ = coord1(c, oz, h);
+    const int xa0 = max(0, a - 3), xa1 = min(G.nx - 1, AX == 0 ? a + 1 : a + 2);
+    const int yb0 = max(0, b - 3), yb1 = min(G.ny - 1, AX == 1 ? b + 1 : b + 2);
+    const int zc0 = max(0, c - 3), zc1 = min(G.nz - 1, AX == 2 ? c + 1 : c + 2);
+    T s = T(0), ws = T(0);
+    for (int x = xa0; x <= xa1; x++)
+      for (int y = yb0; y <= yb1; y++)
+        for (int z = zc0; z <= zc1; z++) {
+          const int cell = (int)lin(x, y, z, G.ny, G.nz);
+          const int m = cnt[cell];
+          if (!m) continue;
+          const int s0 = start[cell];
+          for (int l = s0; l < s0 + m; l++) {
+            const T px = P.px[l], py = P.py[l], pz = P.pz[l];
+            const int di = a - nearest1(px, ox, h), dj = b - nearest1(py, oy, h),
+                      dk = c - nearest1(pz, oz, h);
+            if (di < -1 || di > 2 || dj < -1 || dj > 2 || dk < -1 || dk > 2) continue;
+            const T wt = kweight(h, rsub(px, nx_), rsub(py, ny_), rsub(pz, nz_));
+            s = radd(s, rmul(vel[l], wt));
+            ws = radd(ws, wt);
+          }
+        }
+    const bool ok = ws > T(0);
+    const T out = ok ? rdiv(s, ws) : T(0);
+    g[id] = out;
+    wsum[id] = ws;
+    valid[id] = ok ? 1 : 0;
+    if (last) last[id] = out;
+  }
+}
+
+// applyDirichletBoundary for one face grid (fluid-simulator.cc:113-138).
+template <class T, int AX>
+__global__ void __launch_bounds__(kT) k_dirichlet(Geo G, T* g, uint8_t* valid) {
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+  const int64_t n = (int64_t)fx * fy * fz;
+  GRID_LOOP(id, n) {
+    const int c = (int)(id % fz);
+    const int b = (int)((id / fz) % fy);
+    const int a = (int)(id / ((int64_t)fy * fz));
+    const int q = AX == 0 ? a : (AX == 1 ? b : c), qm = AX == 0 ? fx - 1 : (AX == 1 ? fy - 1 : fz - 1);
+    if (q == 0 || q == qm) {
+      g[id] = T(0);
+      valid[id] = 1;
+    }
+  }
+}
+
+// extrapolate iteration for one face grid (cpu/fluid-simulator.h:204-253):
+// valid nodes keep whatever the destination buffer holds; nodes without a
+// valid neighbour get 0.
+template <class T, int AX>
+__global__ void __launch_bounds__(kT)
+    k_extrap_face(Geo G, const T* __restrict__ src, T* __restrict__ dst,
+                  const uint8_t* __restrict__ vs, uint8_t* __restrict__ vd) {
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+  const int64_t n = (int64_t)fx * fy * fz;
+  const int64_t sx = (int64_t)fy * fz, sy = fz;
+  GRID_LOOP(id, n) {
+    if (vs[id]) {
+      vd[id] = 1;
+      continue;
+    }
+    const int c = (int)(id % fz);
+    const int b = (int)((id / fz) % fy);
+    const int a = (int)(id / sx);
+    T sum = T(0);
+    int cnt = 0;
+    if (a > 0 && vs[id - sx]) { sum = radd(sum, src[id - sx]); cnt++; }
+    if (a < fx - 1 && vs[id + sx]) { sum = radd(sum, src[id + sx]); cnt++; }
+    if (b > 0 && vs[id - sy]) { sum = radd(sum, src[id - sy]); cnt++; }
+    if (b < fy - 1 && vs[id + sy]) { sum = radd(sum, src[id + sy]); cnt++; }
+    if (c > 0 && vs[id - 1]) { sum = radd(sum, src[id - 1]); cnt++; }
+    if (c < fz - 1 && vs[id + 1]) { sum = radd(sum, src[id + 1]); cnt++; }
+    if (cnt > 0) {
+      dst[id] = rdiv(sum, (T)cnt);
+      vd[id] = 1;
+    } else {
+      dst[id] = T(0);
+      vd[id] = 0;
+    }
+  }
+}
+
+// applyForce (fluid-simulator.cc:13-18): gravity on valid v faces, 0 < j < ny.
+template <class T>
+__global__ void __launch_bounds__(kT) k_force(Geo G, T* v, const uint8_t* valid, double gdt) {
+  const int fy = G.ny + 1;
+  const int64_t n = (int64_t)G.nx * fy * G.nz;
+  const T d = (T)gdt;
+  GRID_LOOP(id, n) {
+    const int j = (int)((id / G.nz) % fy);
+    if (valid[id] && j > 0 && j < G.ny) v[id] = rsub(v[id], d);
+  }
+}
+
+// applyCollider for one face grid (fluid-simulator.cc:76-111).
+template <class T, int AX>
+__global__ void __launch_bounds__(kT) k_collider(Geo G, double h, T* g, const double* col) {
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+  const int64_t n = (int64_t)fx * fy * fz;
+  GRID_LOOP(id, n) {
+    const int c = (int)(id % fz);
+    const int b = (int)((id / fz) % fy);
+    const int a = (int)(id / ((int64_t)fy * fz));
+    const int q = AX == 0 ? a : (AX == 1 ? b : c), qm = AX == 0 ? fx - 1 : (AX == 1 ? fy - 1 : fz - 1);
+    if (q == 0 || q == qm) {
+      g[id] = T(0);
+      continue;
+    }
+    if (!col) continue;
+    const double px = ((double)a + (AX == 0 ? 0.0 : 0.5)) * h + 0.0;
+    const double py = ((double)b + (AX == 1 ? 0.0 : 0.5)) * h + 0.0;
+    const double pz = ((double)c + (AX == 2 ? 0.0 : 0.5)) * h + 0.0;
+    if (sdf_eval(col, G.nx, G.ny, G.nz, h, px, py, pz) < 0.0) {
+      double nrm[3];
+      sdf_grad(col, G, h, px, py, pz, nrm);
+      const double l = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+      const double nc = nrm[AX] / l;
+      const double x = (double)g[id];
+      g[id] = (T)(x - x * nc);
+    }
+  }
+}
+
+// max |u| over a face grid (for CFL, fluid-simulator.cc:184-203).
+template <class T>
+__global__ void __launch_bounds__(kT) k_maxabs(int64_t n, const T* g, double* out) {
+  double m = 0.0;
+  GRID_LOOP(i, n) m = fmax(m, fabs((double)g[i]));
+  m = warp_max(m);
+  __shared__ double s[kT / 32];
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < kT / 32; k++) m = fmax(m, s[k]);
+    // non-negative doubles order like their bit patterns
+    atomicMax((unsigned long long*)out, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+template <class T>
+__global__ void k_aos_to_soa(int64_t n, const double* pos, const double* vel, PartsT<T> P,
+                             int64_t* id) {
+  GRID_LOOP(i, n) {
+    P.px[i] = (T)pos[3 * i];
+    P.py[i] = (T)pos[3 * i + 1];
+    P.pz[i] = (T)pos[3 * i + 2];
+    P.vx[i] = vel ? (T)vel[3 * i] : T(0);
+    P.vy[i] = vel ? (T)vel[3 * i + 1] : T(0);
+    P.vz[i] = vel ? (T)vel[3 * i + 2] : T(0);
+    if (id) id[i] = i;
+  }
+}
+template <class T>
+__global__ void k_soa_to_aos(int64_t n, PartsT<T> P, const int64_t* id, double* pos, double* vel) {
+  GRID_LOOP(i, n) {
+    const int64_t o = id ? id[i] : i;
+    if (pos) {
+      pos[3 * o] = (double)P.px[i];
+      pos[3 * o + 1] = (double)P.py[i];
+      pos[3 * o + 2] = (double)P.pz[i];
+    }
+    if (vel) {
+      vel[3 * o] = (double)P.vx[i];
+      vel[3 * o + 1] = (double)P.vy[i];
+      vel[3 * o + 2] = (double)P.vz[i];
+    }
+  }
+}
+template <class Ts, class Td>
+__global__ void k_cast(int64_t n, const Ts* a, Td* b) {
+  GRID_LOOP(i, n) b[i] = (Td)a[i];
+}
+
+// ---------------------------------------------------------------------------------
+// Sorting driver shared by the simulator and the stage functions.
+struct SortBufs {
+  int *key, *cnt, *start, *cursor, *bsum;
+};
+
+template <class T>
+int64_t sort_particles(cudaStream_t st, int64_t n, const Geo& G, double h, PartsT<T> src,
+                       int64_t* sid, PartsT<T> dst, int64_t* did, const SortBufs& b) {
+  const int64_t ncell = (int64_t)G.nx * G.ny * G.nz;
+  cudaMemsetAsync(b.cnt, 0, sizeof(int) * ncell, st);
+  cudaMemsetAsync(b.cursor, 0, sizeof(int) * ncell, st);
+  k_keys<T><<<nblk(n), kT, 0, st>>>(n, src.px, src.py, src.pz, G, h, b.key, b.cnt);
+  const int nb = (int)((ncell + 1023) / 1024);
+  k_scan_blocks<<<nb, 1024, 0, st>>>(ncell, b.cnt, b.start, b.bsum);
+  k_scan_sums<<<1, 1024, 0, st>>>(nb, b.bsum);
+  k_scan_add<<<nb, 1024, 0, st>>>(ncell, b.start, b.bsum);
+  k_scatter<T><<<nblk(n), kT, 0, st>>>(n, b.key, b.start, b.cursor, src, sid, dst, did);
+  k_sort_cells<T><<<nblk(ncell), kT, 0, st>>>(ncell, b.start, b.cnt, dst, did);
+  return 7;  // kernels launched
+}
+
+}  // namespace
+
+// =================================================================================
+// FluidSim
+
+FluidSim::FluidSim(Context* ctx, const FluidConfig& cfg) : ctx_(ctx), c_(cfg) {
+  if (c_.nx < 1 || c_.ny < 1 || c_.nz < 1 || !(c_.h > 0)) {
+    status_ = -1;
+    return;
+  }
+  rs_ = c_.f32 ? sizeof(float) : sizeof(double);
+  const int nx = c_.nx, ny = c_.ny, nz = c_.nz;
+  const int64_t N = (int64_t)nx * ny * nz;
+  fsz_[0] = (int64_t)(nx + 1) * ny * nz;
+  fsz_[1] = (int64_t)nx * (ny + 1) * nz;
+  fsz_[2] = (int64_t)nx * ny * (nz + 1);
+  auto alloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    allocs_.push_back(p);
+    cudaMemsetAsync(p, 0, bytes, ctx_->stream);
+    return p;
+  };
+  bool ok = true;
+  for (int a = 0; a < 3; a++) {
+    for (int b = 0; b < 2; b++) {
+      ok &= (g_[a][b] = alloc(rs_ * fsz_[a])) != nullptr;
+      ok &= (gv_[a][b] = (uint8_t*)alloc(fsz_[a])) != nullptr;
+    }
+    ok &= (gw_[a] = alloc(rs_ * fsz_[a])) != nullptr;
+    ok &= (last_[a] = alloc(rs_ * fsz_[a])) != nullptr;
+    ok &= (wt_[a] = (double*)alloc(sizeof(double) * fsz_[a])) != nullptr;
+  }
+  for (int b = 0; b < 2; b++) {
+    ok &= (sdf_[b] = (double*)alloc(sizeof(double) * N)) != nullptr;
+    ok &= (sdfv_[b] = (uint8_t*)alloc(N)) != nullptr;
+  }
+  ok &= (cnt_ = (int*)alloc(sizeof(int) * N)) != nullptr;
+  ok &= (start_ = (int*)alloc(sizeof(int) * N)) != nullptr;
+  ok &= (cursor_ = (int*)alloc(sizeof(int) * N)) != nullptr;
+  ok &= (bsum_ = (int*)alloc(sizeof(int) * ((N + 1023) / 1024 + 1))) != nullptr;
+  ok &= (redbuf_ = (double*)alloc(sizeof(double) * 4)) != nullptr;
+  if (ok && cudaMallocHost(&host_red_, sizeof(double) * 4) != cudaSuccess) ok = false;
+  if (!ok) {
+    status_ = -3;
+    return;
+  }
+  pcg_ = new PcgSolver(ctx, nx, ny, nz, c_.pcg);
+  if (pcg_->status()) {
+    status_ = pcg_->status();
+    return;
+  }
+  for (auto& e : ev_) cudaEventCreate(&e);
+  if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) status_ = -2;
+}
+
+FluidSim::~FluidSim() {
+  cudaStreamSynchronize(ctx_->stream);
+  delete pcg_;
+  for (auto& e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (host_red_) cudaFreeHost(host_red_);
+  for (void* p : allocs_) cudaFree(p);
+  for (void* p : {px_, py_, pz_, vx_, vy_, vz_, spx_, spy_, spz_, svx_, svy_, svz_, (void*)id_,
+                  (void*)sid_, (void*)key_})
+    if (p) cudaFree(p);
+}
+
+int FluidSim::err(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return ctx_->set_error(-2, std::string(where) + ": " + cudaGetErrorString(e));
+  return 0;
+}
+
+int FluidSim::alloc_particles(int64_t n) {
+  if (n <= cap_) return 0;
+  void** bufs[] = {&px_, &py_, &pz_, &vx_, &vy_, &vz_, &spx_, &spy_, &spz_, &svx_, &svy_, &svz_};
+  for (void** b : bufs) {
+    if (*b) cudaFree(*b);
+    if (cudaMalloc(b, rs_ * (size_t)n) != cudaSuccess) return ctx_->set_error(-3, "particle allocation failed");
+  }
+  for (int64_t** b : {&id_, &sid_}) {
+    if (*b) cudaFree(*b);
+    if (cudaMalloc(b, sizeof(int64_t) * (size_t)n) != cudaSuccess)
+      return ctx_->set_error(-3, "particle allocation failed");
+  }
+  if (key_) cudaFree(key_);
+  if (cudaMalloc(&key_, sizeof(int) * (size_t)n) != cudaSuccess)
+    return ctx_->set_error(-3, "particle allocation failed");
+  cap_ = n;
+  return 0;
+}
+
+int FluidSim::set_particles(int64_t n, const double* pos, const double* vel, bool device) {
+  if (n < 0) return ctx_->set_error(-1, "negative particle count");
+  int e = alloc_particles(std::max<int64_t>(n, 1));
+  if (e) return e;
+  cudaStream_t st = ctx_->stream;
+  const double *dp = pos, *dv = vel;
+  double* stage = nullptr;
+  if (!device && n > 0) {
+    if (cudaMallocAsync(&stage, sizeof(double) * 6 * (size_t)n, st) != cudaSuccess)
+      return ctx_->set_error(-3, "staging allocation failed");
+    cudaMemcpyAsync(stage, pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, st);
+    dp = stage;
+    dv = nullptr;
+    if (vel) {
+      cudaMemcpyAsync(stage + 3 * n, vel, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, st);
+      dv = stage + 3 * n;
+    }
+  }
+  n_ = n;
+  if (n > 0) {
+    Parts p{px_, py_, pz_, vx_, vy_, vz_};
+    if (c_.f32)
+      k_aos_to_soa<float><<<nblk(n), kT, 0, st>>>(n, dp, dv, PartsT<float>::from(p), id_);
+    else
+      k_aos_to_soa<double><<<nblk(n), kT, 0, st>>>(n, dp, dv, PartsT<double>::from(p), id_);
+  }
+  if (stage) cudaFreeAsync(stage, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return err("set_particles");
+  return err("set_particles");
+}
+
+int FluidSim::set_collider(const double* sdf, bool device) {
+  const int64_t N = (int64_t)c_.nx * c_.ny * c_.nz;
+  if (!sdf) {
+    collider_ = nullptr;  // empty mesh: manifold2SDF leaves 1e9 everywhere
+    return 0;
+  }
+  if (!collider_) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, sizeof(double) * N) != cudaSuccess) return ctx_->set_error(-3, "collider allocation failed");
+    allocs_.push_back(p);
+    collider_ = (double*)p;
+  }
+  cudaMemcpyAsync(collider_, sdf, sizeof(double) * N,
+                  device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx_->stream);
+  if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return err("set_collider");
+  return err("set_collider");
+}
+
+double FluidSim::cfl() {
+  cudaStream_t st = ctx_->stream;
+  cudaMemsetAsync(redbuf_, 0, sizeof(double), st);
+  for (int a = 0; a < 3; a++) {
+    if (c_.f32)
+      k_maxabs<float><<<nblk(fsz_[a]), kT, 0, st>>>(fsz_[a], (const float*)g_[a][gcur_[a]], redbuf_);
+    else
+      k_maxabs<double><<<nblk(fsz_[a]), kT, 0, st>>>(fsz_[a], (const double*)g_[a][gcur_[a]], redbuf_);
+  }
+  launches_ += 3;
+  cudaMemcpyAsync(host_red_, redbuf_, sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  const double h = c_.h;
+  double cfl = h / 1e-6;
+  const double m = host_red_[0];
+  if (m > 0.0) cfl = std::min(cfl, h / m);
+  return c_.cfl_factor * std::max(1e-3, cfl);
+}
+
+template <class T>
+int FluidSim::substep_t(double dt, StepStats* stt) {
+  cudaStream_t st = ctx_->stream;
+  const int nx = c_.nx, ny = c_.ny, nz = c_.nz;
+  const double h = c_.h;
+  const Geo G{nx, ny, nz};
+  const int64_t N = (int64_t)nx * ny * nz;
+  const int64_t n = n_;
+  const int64_t l0 = launches_;
+  PartsT<T> P{(T*)px_, (T*)py_, (T*)pz_, (T*)vx_, (T*)vy_, (T*)vz_};
+  PartsT<T> S{(T*)spx_, (T*)spy_, (T*)spz_, (T*)svx_, (T*)svy_, (T*)svz_};
+  auto G_ = [&](int a) { return (T*)g_[a][gcur_[a]]; };
+  cudaEventRecord(ev_[0], st);
+  // clear() (fluid-simulator.cc:20-37)
+  for (int a = 0; a < 3; a++) {
+    for (int b = 0; b < 2; b++) {
+      cudaMemsetAsync(g_[a][b], 0, rs_ * fsz_[a], st);
+      cudaMemsetAsync(gv_[a][b], 0, fsz_[a], st);
+    }
+    cudaMemsetAsync(gw_[a], 0, rs_ * fsz_[a], st);
+  }
+  // advect on the just-cleared grids (fluid-simulator.cc:143)
+  if (n > 0)
+    k_advect<T><<<nblk(n), kT, 0, st>>>(n, P, G_(0), G_(1), G_(2), G, h, collider_, dt);
+  launches_ += 1;
+  cudaEventRecord(ev_[1], st);
+  // sort by cell, then reconstruct (fluid-simulator.cc:146-148)
+  if (n > 0) {
+    SortBufs sb{key_, cnt_, start_, cursor_, bsum_};
+    launches_ += sort_particles<T>(st, n, G, h, P, id_, S, sid_, sb);
+    std::swap(px_, spx_);
+    std::swap(py_, spy_);
+    std::swap(pz_, spz_);
+    std::swap(vx_, svx_);
+    std::swap(vy_, svy_);
+    std::swap(vz_, svz_);
+    std::swap(id_, sid_);
+    P = PartsT<T>{(T*)px_, (T*)py_, (T*)pz_, (T*)vx_, (T*)vy_, (T*)vz_};
+  } else {
+    cudaMemsetAsync(cnt_, 0, sizeof(int) * N, st);
+    cudaMemsetAsync(start_, 0, sizeof(int) * N, st);
+  }
+  k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, c_.recon_factor * h, start_, cnt_, P.px, P.py, P.pz,
+                                           sdf_[scur_], sdfv_[svcur_]);
+  launches_ += 1;
+  for (int it = 0; it < c_.sdf_extrap_iters; it++) {
+    k_extrap_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_], sdfv_[svcur_], sdfv_[1 - svcur_]);
+    scur_ = 1 - scur_;
+    svcur_ = 1 - svcur_;
+  }
+  for (int it = 0; it < c_.smooth_iters; it++) {
+    k_smooth_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_]);
+    scur_ = 1 - scur_;
+  }
+  launches_ += c_.sdf_extrap_iters + c_.smooth_iters;
+  const double* fluid = sdf_[scur_];
+  cudaEventRecord(ev_[2], st);
+  // P2G + Dirichlet walls + extrapolation + gravity (fluid-simulator.cc:155-164)
+  k_p2g<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, h, start_, cnt_, P, G_(0), (T*)gw_[0], gv_[0][gcur_[0]],
+                                              c_.flip ? (T*)last_[0] : nullptr);
+  k_p2g<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, h, start_, cnt_, P, G_(1), (T*)gw_[1], gv_[1][gcur_[1]],
+                                              c_.flip ? (T*)last_[1] : nullptr);
+  k_p2g<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, h, start_, cnt_, P, G_(2), (T*)gw_[2], gv_[2][gcur_[2]],
+                                              c_.flip ? (T*)last_[2] : nullptr);
+  k_dirichlet<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, G_(0), gv_[0][gcur_[0]]);
+  k_dirichlet<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, G_(1), gv_[1][gcur_[1]]);
+  k_dirichlet<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, G_(2), gv_[2][gcur_[2]]);
+  launches_ += 6;
+  for (int it = 0; it < c_.vel_extrap_iters; it++) {
+    k_extrap_face<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, (T*)g_[0][gcur_[0]], (T*)g_[0][1 - gcur_[0]],
+                                                        gv_[0][gcur_[0]], gv_[0][1 - gcur_[0]]);
+    gcur_[0] = 1 - gcur_[0];
+  }
+  for (int it = 0; it < c_.vel_extrap_iters; it++) {
+    k_extrap_face<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, (T*)g_[1][gcur_[1]], (T*)g_[1][1 - gcur_[1]],
+                                                        gv_[1][gcur_[1]], gv_[1][1 - gcur_[1]]);
+    gcur_[1] = 1 - gcur_[1];
+  }
+  for (int it = 0; it < c_.vel_extrap_iters; it++) {
+    k_extrap_face<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, (T*)g_[2][gcur_[2]], (T*)g_[2][1 - gcur_[2]],
+                                                        gv_[2][gcur_[2]], gv_[2][1 - gcur_[2]]);
+    gcur_[2] = 1 - gcur_[2];
+  }
+  k_force<T><<<nblk(fsz_[1]), kT, 0, st>>>(G, G_(1), gv_[1][gcur_[1]], c_.gravity * dt);
+  launches_ += 3 * c_.vel_extrap_iters + 1;
+  cudaEventRecord(ev_[3], st);
+  // buildSystem straight into the solver's tiled arrays (fluid-simulator.cc:166)
+  SystemOut so;
+  so.g = pcg_->geom();
+  so.t_adiag = pcg_->adiag64();
+  so.t_al = pcg_->al64();
+  so.t_ad = pcg_->ad64();
+  so.t_ab = pcg_->ab64();
+  so.t_rhs = pcg_->rhs64();
+  so.t_active = pcg_->active();
+  int e = fvm_build_system<T>(st, nx, ny, nz, h, dt, G_(0), G_(1), G_(2), fluid, collider_, wt_[0],
+                              wt_[1], wt_[2], so);
+  if (e) return err("buildSystem");
+  launches_ += 4;
+  pcg_->mark_system_changed();
+  cudaEventRecord(ev_[4], st);
+  // solvePressure (fluid-simulator.cc:169)
+  PcgStats ps;
+  e = pcg_->solve(&ps);
+  if (e) return e;
+  launches_ += ps.kernel_launches;
+  cudaEventRecord(ev_[5], st);
+  // project + applyCollider + G2P (fluid-simulator.cc:175-180)
+  const Tiled tg = pcg_->geom();
+  e = fvm_project<T>(st, nx, ny, nz, h, dt, G_(0), G_(1), G_(2), pcg_->pressure64(), &tg, fluid,
+                     wt_[0], wt_[1], wt_[2]);
+  if (e) return err("project");
+  k_collider<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, h, G_(0), collider_);
+  k_collider<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, h, G_(1), collider_);
+  k_collider<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, h, G_(2), collider_);
+  if (n > 0)
+    k_g2p<T><<<nblk(n), kT, 0, st>>>(n, P, G_(0), G_(1), G_(2), (T*)last_[0], (T*)last_[1],
+                                     (T*)last_[2], G, h, c_.flip ? c_.flip_alpha : -1.0);
+  launches_ += 7;
+  cudaEventRecord(ev_[6], st);
+  cudaEventSynchronize(ev_[6]);
+  if (stt) {
+    float t[6];
+    for (int k = 0; k < 6; k++) cudaEventElapsedTime(&t[k], ev_[k], ev_[k + 1]);
+    stt->ms_advect += t[0];
+    stt->ms_sort_sdf += t[1];
+    stt->ms_p2g += t[2];
+    stt->ms_build += t[3];
+    stt->ms_solve += t[4];
+    stt->ms_project_g2p += t[5];
+    stt->ms_total += t[0] + t[1] + t[2] + t[3] + t[4] + t[5];
+    stt->pcg_iterations = ps.iterations;
+    stt->pcg_outer = ps.outer;
+    stt->pcg_residual = ps.residual;
+    stt->substeps += 1;
+    stt->kernel_launches += launches_ - l0;
+  }
+  return err("substep");
+}
+
+int FluidSim::substep(double dt, StepStats* st) {
+  return c_.f32 ? substep_t<float>(dt, st) : substep_t<double>(dt, st);
+}
+
+int FluidSim::step(double frame_dt, StepStats* st) {  // fluid-simulator.cc:205-220
+  double t = 0;
+  while (t < frame_dt) {
+    const double dt = std::min(cfl(), frame_dt - t);
+    int e = substep(dt, st);
+    if (e) return e;
+    t += dt;
+  }
+  return 0;
+}
+
+int FluidSim::get_particles(double* pos, double* vel, bool device) {
+  cudaStream_t st = ctx_->stream;
+  const int64_t n = n_;
+  if (n == 0) return 0;
+  double* stage = nullptr;
+  double *dp = pos, *dv = vel;
+  if (!device) {
+    if (cudaMallocAsync(&stage, sizeof(double) * 6 * (size_t)n, st) != cudaSuccess)
+      return ctx_->set_error(-3, "staging allocation failed");
+    dp = pos ? stage : nullptr;
+    dv = vel ? stage + 3 * n : nullptr;
+  }
+  Parts p{px_, py_, pz_, vx_, vy_, vz_};
+  if (c_.f32)
+    k_soa_to_aos<float><<<nblk(n), kT, 0, st>>>(n, PartsT<float>::from(p), id_, dp, dv);
+  else
+    k_soa_to_aos<double><<<nblk(n), kT, 0, st>>>(n, PartsT<double>::from(p), id_, dp, dv);
+  if (!device) {
+    if (pos) cudaMemcpyAsync(pos, stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, st);
+    if (vel) cudaMemcpyAsync(vel, stage + 3 * n, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(stage, st);
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess) return err("get_particles");
+  return err("get_particles");
+}
+
+int FluidSim::get_pressure(double* p, bool device) { return pcg_->download_pressure(p, device); }
+
+int FluidSim::get_fluid_sdf(double* s, bool device) {
+  const int64_t N = (int64_t)c_.nx * c_.ny * c_.nz;
+  cudaMemcpyAsync(s, sdf_[scur_], sizeof(double) * N, device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                  ctx_->stream);
+  if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return err("get_fluid_sdf");
+  return err("get_fluid_sdf");
+}
+
+int FluidSim::get_faces(double* u, double* v, double* w, bool device) {
+  cudaStream_t st = ctx_->stream;
+  double* outs[3] = {u, v, w};
+  for (int a = 0; a < 3; a++) {
+    if (!outs[a]) continue;
+    if (!c_.f32) {
+      cudaMemcpyAsync(outs[a], g_[a][gcur_[a]], sizeof(double) * fsz_[a],
+                      device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st);
+      continue;
+    }
+    double* dst = outs[a];
+    double* stage = nullptr;
+    if (!device) {
+      if (cudaMallocAsync(&stage, sizeof(double) * fsz_[a], st) != cudaSuccess)
+        return ctx_->set_error(-3, "staging allocation failed");
+      dst = stage;
+    }
+    k_cast<float, double><<<nblk(fsz_[a]), kT, 0, st>>>(fsz_[a], (const float*)g_[a][gcur_[a]], dst);
+    if (stage) {
+      cudaMemcpyAsync(outs[a], stage, sizeof(double) * fsz_[a], cudaMemcpyDeviceToHost, st);
+      cudaFreeAsync(stage, st);
+    }
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess) return err("get_faces");
+  return err("get_faces");
+}
+
+// =================================================================================
+// Stage functions (device arrays, reference layout, AoS double particles).
+
+namespace {
+struct StageParticles {
+  double* buf = nullptr;  // 6 SoA arrays
+  int64_t* id = nullptr;
+  cudaStream_t st;
+  int64_t n;
+  PartsT<double> P() const {
+    return {buf, buf + n, buf + 2 * n, buf + 3 * n, buf + 4 * n, buf + 5 * n};
+  }
+  ~StageParticles() {
+    if (buf) cudaFreeAsync(buf, st);
+    if (id) cudaFreeAsync(id, st);
+  }
+};
+}  // namespace
+
+int flip_sample(cudaStream_t st, int64_t n, const double* pts, int nx, int ny, int nz, double h,
+                const double* u, const double* v, const double* w, double* out) {
+  // out = (sampleVelocity(p)) via the G2P kernel in PIC mode on a copy
+  StageParticles sp;
+  sp.st = st;
+  sp.n = n;
+  if (cudaMallocAsync(&sp.buf, sizeof(double) * 6 * (size_t)std::max<int64_t>(n, 1), st) != cudaSuccess) return -3;
+  k_aos_to_soa<double><<<nblk(n), kT, 0, st>>>(n, pts, nullptr, sp.P(), nullptr);
+  k_g2p<double><<<nblk(n), kT, 0, st>>>(n, sp.P(), u, v, w, nullptr, nullptr, nullptr, Geo{nx, ny, nz}, h,
+                                        -1.0);
+  k_soa_to_aos<double><<<nblk(n), kT, 0, st>>>(n, sp.P(), nullptr, nullptr, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int flip_g2p(cudaStream_t st, int64_t n, const double* pos, double* vel, int nx, int ny, int nz,
+             double h, const double* u, const double* v, const double* w, const double* ulast,
+             const double* vlast, const double* wlast, double alpha) {
+  StageParticles sp;
+  sp.st = st;
+  sp.n = n;
+  if (cudaMallocAsync(&sp.buf, sizeof(double) * 6 * (size_t)std::max<int64_t>(n, 1), st) != cudaSuccess) return -3;
+  k_aos_to_soa<double><<<nblk(n), kT, 0, st>>>(n, pos, vel, sp.P(), nullptr);
+  k_g2p<double><<<nblk(n), kT, 0, st>>>(n, sp.P(), u, v, w, ulast, vlast, wlast, Geo{nx, ny, nz}, h, alpha);
+  k_soa_to_aos<double><<<nblk(n), kT, 0, st>>>(n, sp.P(), nullptr, nullptr, vel);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int flip_advect(cudaStream_t st, int64_t n, double* pos, double* vel, int nx, int ny, int nz,
+                double h, const double* u, const double* v, const double* w,
+                const double* collider, double dt) {
+  StageParticles sp;
+  sp.st = st;
+  sp.n = n;
+  if (cudaMallocAsync(&sp.buf, sizeof(double) * 6 * (size_t)std::max<int64_t>(n, 1), st) != cudaSuccess) return -3;
+  k_aos_to_soa<double><<<nblk(n), kT, 0, st>>>(n, pos, vel, sp.P(), nullptr);
+  k_advect<double><<<nblk(n), kT, 0, st>>>(n, sp.P(), u, v, w, Geo{nx, ny, nz}, h, collider, dt);
+  k_soa_to_aos<double><<<nblk(n), kT, 0, st>>>(n, sp.P(), nullptr, pos, vel);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+namespace {
+// Sorted copy of AoS particles plus cell buckets, for the stage functions.
+struct Sorted {
+  StageParticles a, b;
+  int *key = nullptr, *cnt = nullptr, *start = nullptr, *cursor = nullptr, *bsum = nullptr;
+  cudaStream_t st;
+  ~Sorted() {
+    for (int* p : {key, cnt, start, cursor, bsum})
+      if (p) cudaFreeAsync(p, st);
+  }
+};
+int make_sorted(Sorted& s, cudaStream_t st, int64_t n, const double* pos, const double* vel,
+                const Geo& G, double h) {
+  const int64_t N = (int64_t)G.nx * G.ny * G.nz;
+  const int64_t m = std::max<int64_t>(n, 1);
+  s.st = st;
+  s.a.st = s.b.st = st;
+  s.a.n = s.b.n = n;
+  if (cudaMallocAsync(&s.a.buf, sizeof(double) * 6 * m, st) != cudaSuccess ||
+      cudaMallocAsync(&s.b.buf, sizeof(double) * 6 * m, st) != cudaSuccess ||
+      cudaMallocAsync(&s.a.id, sizeof(int64_t) * m, st) != cudaSuccess ||
+      cudaMallocAsync(&s.b.id, sizeof(int64_t) * m, st) != cudaSuccess ||
+      cudaMallocAsync(&s.key, sizeof(int) * m, st) != cudaSuccess ||
+      cudaMallocAsync(&s.cnt, sizeof(int) * N, st) != cudaSuccess ||
+      cudaMallocAsync(&s.start, sizeof(int) * N, st) != cudaSuccess ||
+      cudaMallocAsync(&s.cursor, sizeof(int) * N, st) != cudaSuccess ||
+      cudaMallocAsync(&s.bsum, sizeof(int) * ((N + 1023) / 1024 + 1), st) != cudaSuccess)
+    return -3;
+  if (n == 0) {
+    cudaMemsetAsync(s.cnt, 0, sizeof(int) * N, st);
+    cudaMemsetAsync(s.start, 0, sizeof(int) * N, st);
+    return 0;
+  }
+  k_aos_to_soa<double><<<nblk(n), kT, 0, st>>>(n, pos, vel, s.a.P(), s.a.id);
+  SortBufs sb{s.key, s.cnt, s.start, s.cursor, s.bsum};
+  sort_particles<double>(st, n, G, h, s.a.P(), s.a.id, s.b.P(), s.b.id, sb);
+  return 0;
+}
+}  // namespace
+
+int flip_p2g(cudaStream_t st, int64_t n, const double* pos, const double* vel, int nx, int ny,
+             int nz, double h, double* u, double* v, double* w, double* uw, double* vw, double* ww,
+             uint8_t* uvalid, uint8_t* vvalid, uint8_t* wvalid, double* ulast, double* vlast,
+             double* wlast) {
+  const Geo G{nx, ny, nz};
+  Sorted s;
+  int e = make_sorted(s, st, n, pos, vel, G, h);
+  if (e) return e;
+  const int64_t f0 = (int64_t)(nx + 1) * ny * nz, f1 = (int64_t)nx * (ny + 1) * nz,
+                f2 = (int64_t)nx * ny * (nz + 1);
+  k_p2g<double, 0><<<nblk(f0), kT, 0, st>>>(G, h, s.start, s.cnt, s.b.P(), u, uw, uvalid, ulast);
+  k_p2g<double, 1><<<nblk(f1), kT, 0, st>>>(G, h, s.start, s.cnt, s.b.P(), v, vw, vvalid, vlast);
+  k_p2g<double, 2><<<nblk(f2), kT, 0, st>>>(G, h, s.start, s.cnt, s.b.P(), w, ww, wvalid, wlast);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int flip_reconstruct(cudaStream_t st, int64_t n, const double* pos, int nx, int ny, int nz,
+                     double h, double radius, double* sdf, uint8_t* valid) {
+  const Geo G{nx, ny, nz};
+  Sorted s;
+  int e = make_sorted(s, st, n, pos, nullptr, G, h);
+  if (e) return e;
+  const int64_t N = (int64_t)nx * ny * nz;
+  PartsT<double> P = s.b.P();
+  k_reconstruct<double><<<nblk(N), kT, 0, st>>>(G, h, radius, s.start, s.cnt, P.px, P.py, P.pz, sdf, valid);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace sc

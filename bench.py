@@ -9,6 +9,11 @@ upload into the solver's layout, MIC(0) pivots, PCG iterations, pressure
 download.  Multi-GPU runs are independent replicas (the MIC(0) sweep is one
 global wavefront and does not shard).
 
+A second leg times the FLIP step at scale: the 256^3 dam break (block x<0.5,
+y<0.5, 8 jittered particles per cell = 33.5M particles, FP32 particles and
+grids, CFL factor 1, FLIP blend 0.95, mixed MIC(0)-PCG to 1e-8 relative
+residual), reported as FLIP substeps/s with the per-subsystem split.
+
 `--impl reference` times the CPU restatement of the reference (the oracle,
 OpenMP where the reference uses TBB) on the same system.
 """
@@ -30,6 +35,8 @@ METRIC = "ms per pressure solve to 1e-8 rel. residual (mixed vs FP64 PCG); FLIP 
 N_GRID = 128
 TOL = 1e-8
 DT_OVER_H = 32.0 / 120.0
+FLIP_N = 256
+FRAME_DT = 1.0 / 120.0
 
 
 def build_scene(n):
@@ -159,6 +166,111 @@ def reference_arm(args, rank):
     }), flush=True)
 
 
+def flip_leg(args, dev, ctx, dist, rank, world):
+    """FLIP substeps/s on the 256^3 FP32 dam break (device-resident particles)."""
+    import torch
+
+    from simcraft_b200 import scenes
+    from simcraft_b200.fluid import FluidSimulator
+    from simcraft_b200.solver import CRIT_REL_L2, PREC_MIXED
+
+    n = FLIP_N
+    pos, vel, h = scenes.dam_break(n, seed=4)
+    sim = FluidSimulator(len(pos), (1.0, 1.0, 1.0), (n, n, n), context=ctx, precision="f32",
+                         flip_alpha=0.95, cfl_factor=1.0, pcg_tol=TOL, pcg_max_iter=5000,
+                         pcg_criterion=CRIT_REL_L2, pcg_precision=PREC_MIXED)
+    sim.set_initial_fluid(pos, vel)
+    n_particles = len(pos)
+    del pos, vel
+
+    def one():
+        # the reference's frame loop (fluid-simulator.cc:205-220): dt = min(CFL, frame)
+        return sim.substep(min(sim.cfl(), FRAME_DT))
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    split = {}
+    iters = []
+    launches = 0
+    e0.record(stream)
+    for _ in range(args.flip_steps):
+        st = one()
+        for k, v in st.items():
+            if k.startswith("ms_"):
+                split[k[3:]] = split.get(k[3:], 0.0) + v
+        iters.append(st["pcg_iterations"])
+        launches += st["kernel_launches"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    K = args.flip_steps
+    out = {"workload": f"FLIP dam break {n}^3, block x<0.5 y<0.5, 8 particles/cell, FP32 particles and grids, "
+                       f"CFL factor 1, FLIP 0.95, mixed MIC(0)-PCG to {TOL:g}",
+           "particles": n_particles, "steps": K, "warmup": args.warmup,
+           "steps_per_s": world * K / (ms * 1e-3), "ms_per_step": ms / K,
+           "split_ms_per_step": {k: v / K for k, v in split.items()},
+           "pcg_inner_iterations_mean": float(np.mean(iters)), "gpu_launches": int(launches)}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = flip_cpu_sample(sim, n, h)
+    del sim
+    torch.cuda.empty_cache()
+    return out
+
+
+def flip_cpu_sample(sim, n, h):
+    """CPU oracle on a bounded sample of the same 256^3 state: advect + P2G + G2P
+    of the first 1M particles scaled to all particles, plus the FP64 PCG's cost
+    per iteration on the current 256^3 system times the iterations the GPU
+    solve took.  Reconstruction, extrapolation, buildSystem and project are
+    left out, so the CPU figure is a lower bound of the CPU substep."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.build()
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    O.set_parity_mode(False)
+    pos, vel = sim.particles()
+    u, v, w = sim.faces()
+    P = len(pos)
+    m = min(P, 1 << 20)
+    ps, vs = np.ascontiguousarray(pos[:m]), np.ascontiguousarray(vel[:m])
+    dims = (n, n, n)
+    t = time.perf_counter()
+    O.advect(ps, vs, dims, h, u, v, w, None, FRAME_DT)
+    O.g2p(ps, vs, dims, h, u, v, w, u, v, w, alpha=0.95)
+    # the threaded P2G keeps one full set of face grids per thread: cap its threads
+    O.set_threads(min(threads, 8))
+    O.p2g(ps, vs, dims, h, flip=True)
+    O.set_threads(threads)
+    t_part = (time.perf_counter() - t) * P / m
+    # PCG cost per iteration at full size on a system of the same shape
+    sdf = sim.export_fluid_surface()
+    S = O.build_system(dims, h, FRAME_DT, u, v, w, sdf)
+    its = 10
+    t = time.perf_counter()
+    _, _, done = O.pcg_solve(S["adiag"], S["an"], S["rhs"], S["active"], tol=0.0, max_iter=its + 1,
+                             criterion=O.CRIT_REL_L2)
+    per_it = (time.perf_counter() - t) / max(done, 1)
+    gpu_its = sim.last_stats["pcg_iterations"] if sim.last_stats else 0
+    total = t_part + per_it * gpu_its
+    return {"value": 1.0 / total, "unit": "FLIP substeps/s", "cores": threads, "kind": "port",
+            "sample": f"advect+G2P ({threads} threads) and P2G ({min(threads, 8)} threads) on {m} of {P} "
+                      f"particles scaled to all, plus FP64 PCG "
+                      f"{per_it * 1e3:.1f} ms/iteration x {gpu_its} iterations at {n}^3; "
+                      "other stages omitted (lower bound of the CPU substep)",
+            "ms_per_step": total * 1e3}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -166,6 +278,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--flip-steps", type=int, default=10, help="timed FLIP substeps (0 skips the FLIP leg)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -349,6 +462,10 @@ def main():
                                          f"{cit} iterations",
                                "rel_l2_vs_gpu_fp64": float(np.linalg.norm(pg_gpu[a] - pg_cpu[a]) /
                                                            np.linalg.norm(pg_cpu[a]))}
+    del solvers
+    torch.cuda.empty_cache()
+    if args.flip_steps > 0:
+        out["flip"] = flip_leg(args, dev, ctx, dist, rank, world)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:

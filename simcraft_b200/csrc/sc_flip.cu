@@ -79,29 +79,54 @@ __device__ __forceinline__ T kweight(T h, T dx, T dy, T dz) {
               bspline(rdiv(fabs(dz), h)));
 }
 
-// sampleVelocity for one face grid (FluidSim/src/cpu/util.cc:40-85), same loop
-// order and accumulation order.
+// The kernel weight is a product of per-axis factors, and a face grid uses
+// offset 0 along its own axis and 1/2 along the other two, so one position
+// needs only 2 x 4 factors per axis for all three grids.  Each factor is
+// computed exactly as the per-node expression N(|p - x_node| / h), so the
+// products below equal the per-node kernel weights bit for bit.
 template <class T>
-__device__ __forceinline__ T sample_grid(const T* __restrict__ g, int ax, const Geo& G, T h, T px,
-                                         T py, T pz) {
-  const T ox = ax == 0 ? T(0) : T(0.5), oy = ax == 1 ? T(0) : T(0.5), oz = ax == 2 ? T(0) : T(0.5);
-  const int fx = G.fx(ax), fy = G.fy(ax), fz = G.fz(ax);
-  const int bi = nearest1(px, ox, h), bj = nearest1(py, oy, h), bk = nearest1(pz, oz, h);
+struct Stencil {
+  int base[3][2];  // nearest - 1, per axis, for face offset 0 (index 0) and 1/2 (index 1)
+  T w[3][2][4];
+};
+template <class T>
+__device__ __forceinline__ void make_stencil(Stencil<T>& S, T px, T py, T pz, T h) {
+  const T p[3] = {px, py, pz};
+#pragma unroll
+  for (int ax = 0; ax < 3; ax++)
+#pragma unroll
+    for (int o = 0; o < 2; o++) {
+      const T off = o ? T(0.5) : T(0);
+      const int b = nearest1(p[ax], off, h) - 1;
+      S.base[ax][o] = b;
+#pragma unroll
+      for (int i = 0; i < 4; i++) S.w[ax][o][i] = bspline(rdiv(fabs(rsub(p[ax], coord1(b + i, off, h))), h));
+    }
+}
+
+// sampleVelocity for face grid AX (FluidSim/src/cpu/util.cc:40-85): the same
+// nodes in the same order, the same weight and accumulation arithmetic.
+template <class T, int AX>
+__device__ __forceinline__ T gather(const T* __restrict__ g, const Stencil<T>& S, const Geo& G) {
+  constexpr int ox = AX == 0 ? 0 : 1, oy = AX == 1 ? 0 : 1, oz = AX == 2 ? 0 : 1;
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
   T s = T(0), ws = T(0);
-  for (int i = -1; i <= 2; i++) {
-    const int a = bi + i;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int a = S.base[0][ox] + i;
     if (a < 0 || a >= fx) continue;
-    const T dx = rsub(px, coord1(a, ox, h));
-    for (int j = -1; j <= 2; j++) {
-      const int b = bj + j;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int b = S.base[1][oy] + j;
       if (b < 0 || b >= fy) continue;
-      const T dy = rsub(py, coord1(b, oy, h));
-      for (int k = -1; k <= 2; k++) {
-        const int c = bk + k;
+      const T wxy = rmul(S.w[0][ox][i], S.w[1][oy][j]);
+      const T* row = g + lin(a, b, 0, fy, fz);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int c = S.base[2][oz] + k;
         if (c < 0 || c >= fz) continue;
-        const T dz = rsub(pz, coord1(c, oz, h));
-        const T wt = kweight(h, dx, dy, dz);
-        s = radd(s, rmul(g[lin(a, b, c, fy, fz)], wt));
+        const T wt = rmul(wxy, S.w[2][oz][k]);
+        s = radd(s, rmul(__ldg(row + c), wt));
         ws = radd(ws, wt);
       }
     }
@@ -223,12 +248,13 @@ __global__ void __launch_bounds__(kT)
     const T k1x = P.vx[i], k1y = P.vy[i], k1z = P.vz[i];
     const T a = rmul(T(0.5), dt);
     const T p1x = radd(px, rmul(a, k1x)), p1y = radd(py, rmul(a, k1y)), p1z = radd(pz, rmul(a, k1z));
-    const T k2x = sample_grid(u, 0, G, h, p1x, p1y, p1z), k2y = sample_grid(v, 1, G, h, p1x, p1y, p1z),
-            k2z = sample_grid(w, 2, G, h, p1x, p1y, p1z);
+    Stencil<T> S;
+    make_stencil(S, p1x, p1y, p1z, h);
+    const T k2x = gather<T, 0>(u, S, G), k2y = gather<T, 1>(v, S, G), k2z = gather<T, 2>(w, S, G);
     const T b = rmul(T(0.75), dt);
     const T p2x = radd(px, rmul(b, k2x)), p2y = radd(py, rmul(b, k2y)), p2z = radd(pz, rmul(b, k2z));
-    const T k3x = sample_grid(u, 0, G, h, p2x, p2y, p2z), k3y = sample_grid(v, 1, G, h, p2x, p2y, p2z),
-            k3z = sample_grid(w, 2, G, h, p2x, p2y, p2z);
+    make_stencil(S, p2x, p2y, p2z, h);
+    const T k3x = gather<T, 0>(u, S, G), k3y = gather<T, 1>(v, S, G), k3z = gather<T, 2>(w, S, G);
     const T c1 = rmul(T(2.0 / 9.0), dt), c2 = rmul(T(1.0 / 3.0), dt), c3 = rmul(T(4.0 / 9.0), dt);
     px = radd(radd(radd(px, rmul(c1, k1x)), rmul(c2, k2x)), rmul(c3, k3x));
     py = radd(radd(radd(py, rmul(c1, k1y)), rmul(c2, k2y)), rmul(c3, k3y));
@@ -252,16 +278,16 @@ __global__ void __launch_bounds__(kT)
   const T h = (T)hd;
   GRID_LOOP(i, n) {
     const T px = P.px[i], py = P.py[i], pz = P.pz[i];
-    const T pu = sample_grid(u, 0, G, h, px, py, pz), pv = sample_grid(v, 1, G, h, px, py, pz),
-            pw = sample_grid(w, 2, G, h, px, py, pz);
+    Stencil<T> S;
+    make_stencil(S, px, py, pz, h);
+    const T pu = gather<T, 0>(u, S, G), pv = gather<T, 1>(v, S, G), pw = gather<T, 2>(w, S, G);
     if (alphad < 0.0) {
       P.vx[i] = pu;
       P.vy[i] = pv;
       P.vz[i] = pw;
       continue;
     }
-    const T lu = sample_grid(ul, 0, G, h, px, py, pz), lv = sample_grid(vl, 1, G, h, px, py, pz),
-            lw = sample_grid(wl, 2, G, h, px, py, pz);
+    const T lu = gather<T, 0>(ul, S, G), lv = gather<T, 1>(vl, S, G), lw = gather<T, 2>(wl, S, G);
     const T al = (T)alphad, bl = rsub(T(1), al);
     const T fx = rsub(radd(P.vx[i], pu), lu), fy = rsub(radd(P.vy[i], pv), lv),
             fz = rsub(radd(P.vz[i], pw), lw);

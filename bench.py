@@ -174,7 +174,7 @@ def flip_leg(args, dev, ctx, dist, rank, world):
     from simcraft_b200.fluid import FluidSimulator
     from simcraft_b200.solver import CRIT_REL_L2, PREC_MIXED
 
-    n = FLIP_N
+    n = args.flip_n
     pos, vel, h = scenes.dam_break(n, seed=4)
     sim = FluidSimulator(len(pos), (1.0, 1.0, 1.0), (n, n, n), context=ctx, precision="f32",
                          flip_alpha=0.95, cfl_factor=1.0, pcg_tol=TOL, pcg_max_iter=5000,
@@ -279,6 +279,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--flip-steps", type=int, default=10, help="timed FLIP substeps (0 skips the FLIP leg)")
+    ap.add_argument("--flip-n", type=int, default=FLIP_N, help="FLIP dam-break grid size (profiling runs)")
+    ap.add_argument("--skip-solve", action="store_true",
+                    help="run only the FLIP leg (profiling runs; prints the FLIP object)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -310,6 +313,14 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     ctx = Context(local)
+    if args.skip_solve:
+        fl = flip_leg(args, dev, ctx, dist, rank, world)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "flip": fl}), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     L = _capi.lib()
     n = N_GRID
     h = 1.0 / n

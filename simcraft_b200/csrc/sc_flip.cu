@@ -5,16 +5,18 @@
 //   advect + handleCollision    advect-solver.cc:100-137, 170-187   k_advect
 //   NaiveReconstructor          sdf.h:204-229, ns-util.h:46-109      k_keys/scan/scatter + k_reconstruct
 //   extrapolateFluidSdf/smooth  cpu/fluid-simulator.h:123-166, fluid-simulator.cc:39-74
-//   solveP2G                    advect-solver.cc:188-271             k_p2g (gather per face node)
+//   solveP2G                    advect-solver.cc:188-271             k_p2g_splat + k_p2g_normalize
 //   applyDirichletBoundary, extrapolate, applyForce, buildSystem, solvePressure, project,
 //   applyCollider, solveG2P     fluid-simulator.cc:13-138, advect-solver.cc:157-169
 //
 // Particles are re-sorted by cell every substep (counting sort; inside a cell by
-// original index), which makes every transfer deterministic: P2G gathers from
-// the sorted cell buckets instead of scattering with atomics.  Arithmetic that
+// original index).  The sort gives the reconstruction the reference's bucket
+// order, lets P2G splat a tile of cells into shared memory, and keeps the
+// gathers of neighbouring threads on the same grid nodes.  Arithmetic that
 // decides discrete outcomes (nearest node, reconstruction distances, kernel
 // weights, sampling sums) uses explicitly rounded operations in the reference's
-// order so that it matches the CPU bit for bit.
+// order so that it matches the CPU bit for bit; only P2G's summation order
+// differs (as in the reference's parallel splat).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -517,54 +519,173 @@ __global__ void __launch_bounds__(kT)
   }
 }
 
-// solveP2G for one face grid (advect-solver.cc:188-271), as a gather: each
-// face node sums the particles of the cells whose stencil nearest+{-1..2}^3
-// covers it, normalises by the weight sum, sets `valid`, and (FLIP) copies the
-// result into `last`.  The candidate cells follow from the nearest rule: along
-// an axis with face offset 0, nearest = round(p/h) and the bucket cell is
-// nearest-1 or nearest; with offset 1/2 the bucket is within 1 of nearest.
+// solveP2G (advect-solver.cc:188-271) as a tile splat.  A block owns an
+// 8x8x8 tile of cells, one thread per cell; each thread walks its cell's
+// particles (contiguous after the per-substep sort), evaluates the per-axis
+// kernel factors once per particle and adds the 64 weighted contributions per
+// face grid into shared-memory accumulators covering every node the tile's
+// particles can reach (nearest + {-1..2}: 12 nodes along a grid's own axis,
+// 13 along the others).  The block then adds its accumulators into the global
+// sums once.  Threads of a warp own distinct cells, so their shared-memory
+// atomics at one stencil offset hit distinct nodes.  Like the reference's
+// parallel FLIP splat, the floating-point summation order is not fixed.
+constexpr int kPT = 8;                        // cells per tile edge
+constexpr int kPThreads = kPT * kPT * kPT;    // one thread per cell
+template <int AX, int D>
+struct P2GRegion {
+  static constexpr int lo = AX == D ? 1 : 2;          // nodes below the tile's first cell
+  static constexpr int n = kPT + (AX == D ? 4 : 5);   // nodes along axis D
+};
+template <int AX>
+constexpr int p2g_region() {
+  return P2GRegion<AX, 0>::n * P2GRegion<AX, 1>::n * P2GRegion<AX, 2>::n;
+}
+template <class T>
+constexpr size_t p2g_smem_bytes() {
+  return sizeof(T) * 2 * (size_t)(p2g_region<0>() + p2g_region<1>() + p2g_region<2>());
+}
+
 template <class T, int AX>
-__global__ void __launch_bounds__(kT)
-    k_p2g(Geo G, double hd, const int* start, const int* cnt, PartsT<T> P, T* __restrict__ g,
-          T* __restrict__ wsum, uint8_t* __restrict__ valid, T* __restrict__ last) {
-  const T h = (T)hd;
-  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
-  const int64_t n = (int64_t)fx * fy * fz;
-  const T ox = AX == 0 ? T(0) : T(0.5), oy = AX == 1 ? T(0) : T(0.5), oz = AX == 2 ? T(0) : T(0.5);
-  const T* vel = AX == 0 ? P.vx : (AX == 1 ? P.vy : P.vz);
-  GRID_LOOP(id, n) {
-    const int c = (int)(id % fz);
-    const int b = (int)((id / fz) % fy);
-    const int a = (int)(id / ((int64_t)fy * fz));
-    const T nx_ = coord1(a, ox, h), ny_ = coord1(b, oy, h), nz_ = coord1(c, oz, h);
-    const int xa0 = max(0, a - 3), xa1 = min(G.nx - 1, AX == 0 ? a + 1 : a + 2);
-    const int yb0 = max(0, b - 3), yb1 = min(G.ny - 1, AX == 1 ? b + 1 : b + 2);
-    const int zc0 = max(0, c - 3), zc1 = min(G.nz - 1, AX == 2 ? c + 1 : c + 2);
-    T s = T(0), ws = T(0);
-    for (int x = xa0; x <= xa1; x++)
-      for (int y = yb0; y <= yb1; y++)
-        for (int z = zc0; z <= zc1; z++) {
-          const int cell = (int)lin(x, y, z, G.ny, G.nz);
-          const int m = cnt[cell];
-          if (!m) continue;
-          const int s0 = start[cell];
-          for (int l = s0; l < s0 + m; l++) {
-            const T px = P.px[l], py = P.py[l], pz = P.pz[l];
-            const int di = a - nearest1(px, ox, h), dj = b - nearest1(py, oy, h),
-                      dk = c - nearest1(pz, oz, h);
-            if (di < -1 || di > 2 || dj < -1 || dj > 2 || dk < -1 || dk > 2) continue;
-            const T wt = kweight(h, rsub(px, nx_), rsub(py, ny_), rsub(pz, nz_));
-            s = radd(s, rmul(vel[l], wt));
-            ws = radd(ws, wt);
-          }
+__device__ __forceinline__ void p2g_splat_one(const Stencil<T>& S, T val, T* __restrict__ acc,
+                                              int x0, int y0, int z0, const Geo& G, T* gsum,
+                                              T* gwt) {
+  constexpr int o0 = AX == 0 ? 0 : 1, o1 = AX == 1 ? 0 : 1, o2 = AX == 2 ? 0 : 1;
+  constexpr int n0 = P2GRegion<AX, 0>::n, n1 = P2GRegion<AX, 1>::n, n2 = P2GRegion<AX, 2>::n;
+  constexpr int R = n0 * n1 * n2;
+  const int b0 = S.base[0][o0], b1 = S.base[1][o1], b2 = S.base[2][o2];
+  const int l0 = b0 - (x0 - P2GRegion<AX, 0>::lo), l1 = b1 - (y0 - P2GRegion<AX, 1>::lo),
+            l2 = b2 - (z0 - P2GRegion<AX, 2>::lo);
+  if (l0 >= 0 && l0 + 3 < n0 && l1 >= 0 && l1 + 3 < n1 && l2 >= 0 && l2 + 3 < n2) {
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const T wxy = rmul(S.w[0][o0][i], S.w[1][o1][j]);
+        T* row = acc + ((l0 + i) * n1 + (l1 + j)) * n2 + l2;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const T wt = rmul(wxy, S.w[2][o2][k]);
+          atomicAdd(row + k, rmul(val, wt));
+          atomicAdd(row + k + R, wt);
         }
-    const bool ok = ws > T(0);
-    const T out = ok ? rdiv(s, ws) : T(0);
-    g[id] = out;
-    wsum[id] = ws;
-    valid[id] = ok ? 1 : 0;
-    if (last) last[id] = out;
+      }
+    return;
   }
+  // a particle outside the domain box: straight to the global sums
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+  for (int i = 0; i < 4; i++) {
+    const int a = b0 + i;
+    if (a < 0 || a >= fx) continue;
+    for (int j = 0; j < 4; j++) {
+      const int b = b1 + j;
+      if (b < 0 || b >= fy) continue;
+      const T wxy = rmul(S.w[0][o0][i], S.w[1][o1][j]);
+      for (int k = 0; k < 4; k++) {
+        const int c = b2 + k;
+        if (c < 0 || c >= fz) continue;
+        const T wt = rmul(wxy, S.w[2][o2][k]);
+        atomicAdd(gsum + lin(a, b, c, fy, fz), rmul(val, wt));
+        atomicAdd(gwt + lin(a, b, c, fy, fz), wt);
+      }
+    }
+  }
+}
+
+template <class T, int AX>
+__device__ __forceinline__ void p2g_merge(const T* __restrict__ acc, int x0, int y0, int z0,
+                                          const Geo& G, T* gsum, T* gwt) {
+  constexpr int n1 = P2GRegion<AX, 1>::n, n2 = P2GRegion<AX, 2>::n;
+  constexpr int R = p2g_region<AX>();
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+  for (int e = threadIdx.x; e < R; e += blockDim.x) {
+    const T w = acc[R + e];
+    if (w == T(0)) continue;
+    const int k = e % n2, j = (e / n2) % n1, i = e / (n1 * n2);
+    const int a = x0 - P2GRegion<AX, 0>::lo + i, b = y0 - P2GRegion<AX, 1>::lo + j,
+              c = z0 - P2GRegion<AX, 2>::lo + k;
+    if (a < 0 || a >= fx || b < 0 || b >= fy || c < 0 || c >= fz) continue;  // outside the grid
+    const int64_t id = lin(a, b, c, fy, fz);
+    atomicAdd(gsum + id, acc[e]);
+    atomicAdd(gwt + id, w);
+  }
+}
+
+// Accumulates sum(v w) and sum(w) of all particles into gsum/gwt (zeroed by
+// the caller); k_p2g_normalize finishes solveP2G.
+template <class T>
+__global__ void __launch_bounds__(kPThreads)
+    k_p2g_splat(Geo G, double hd, const int* __restrict__ start, const int* __restrict__ cnt,
+                PartsT<T> P, T* su, T* sv, T* sw, T* wu, T* wv, T* ww) {
+  extern __shared__ __align__(16) unsigned char p2g_dyn[];
+  T* acc0 = reinterpret_cast<T*>(p2g_dyn);
+  T* acc1 = acc0 + 2 * p2g_region<0>();
+  T* acc2 = acc1 + 2 * p2g_region<1>();
+  const T h = (T)hd;
+  const int ntz = (G.nz + kPT - 1) / kPT, nty = (G.ny + kPT - 1) / kPT;
+  const int tz = blockIdx.x % ntz, ty = (blockIdx.x / ntz) % nty, tx = blockIdx.x / (ntz * nty);
+  const int x0 = tx * kPT, y0 = ty * kPT, z0 = tz * kPT;
+  const int lz = threadIdx.x % kPT, ly = (threadIdx.x / kPT) % kPT, lx = threadIdx.x / (kPT * kPT);
+  const int cx = x0 + lx, cy = y0 + ly, cz = z0 + lz;
+  int m = 0, s0 = 0;
+  if (cx < G.nx && cy < G.ny && cz < G.nz) {
+    const int cell = (int)lin(cx, cy, cz, G.ny, G.nz);
+    m = cnt[cell];
+    s0 = start[cell];
+  }
+  if (!__syncthreads_or(m > 0)) return;  // no particle in this tile
+  constexpr int NACC = 2 * (p2g_region<0>() + p2g_region<1>() + p2g_region<2>());
+  for (int e = threadIdx.x; e < NACC; e += blockDim.x) acc0[e] = T(0);
+  __syncthreads();
+  for (int l = s0; l < s0 + m; l++) {
+    Stencil<T> S;
+    make_stencil(S, P.px[l], P.py[l], P.pz[l], h);
+    p2g_splat_one<T, 0>(S, P.vx[l], acc0, x0, y0, z0, G, su, wu);
+    p2g_splat_one<T, 1>(S, P.vy[l], acc1, x0, y0, z0, G, sv, wv);
+    p2g_splat_one<T, 2>(S, P.vz[l], acc2, x0, y0, z0, G, sw, ww);
+  }
+  __syncthreads();
+  p2g_merge<T, 0>(acc0, x0, y0, z0, G, su, wu);
+  p2g_merge<T, 1>(acc1, x0, y0, z0, G, sv, wv);
+  p2g_merge<T, 2>(acc2, x0, y0, z0, G, sw, ww);
+}
+
+// Normalisation of solveP2G (advect-solver.cc:238-267): g = sum / W where
+// W > 0 (valid), else 0; FLIP copies the result into `last` (:268-270).
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_p2g_normalize(int64_t n, T* __restrict__ g, const T* __restrict__ wsum,
+                    uint8_t* __restrict__ valid, T* __restrict__ last) {
+  GRID_LOOP(i, n) {
+    const T w = wsum[i];
+    const bool ok = w > T(0);
+    const T out = ok ? rdiv(g[i], w) : T(0);
+    g[i] = out;
+    valid[i] = ok ? 1 : 0;
+    if (last) last[i] = out;
+  }
+}
+
+// Launches the splat over all cell tiles and normalises the three grids; g*
+// and w* must hold zeros.
+template <class T>
+int launch_p2g(cudaStream_t st, const Geo& G, double h, const int* start, const int* cnt,
+               PartsT<T> P, T* gu, T* gv, T* gw, T* wu, T* wv, T* ww, uint8_t* vu, uint8_t* vv,
+               uint8_t* vw, T* lu, T* lv, T* lw) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_p2g_splat<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)p2g_smem_bytes<T>());
+    attr = true;
+  }
+  const int tiles = ((G.nx + kPT - 1) / kPT) * ((G.ny + kPT - 1) / kPT) * ((G.nz + kPT - 1) / kPT);
+  k_p2g_splat<T><<<tiles, kPThreads, p2g_smem_bytes<T>(), st>>>(G, h, start, cnt, P, gu, gv, gw, wu, wv,
+                                                                 ww);
+  const int64_t f0 = (int64_t)(G.nx + 1) * G.ny * G.nz, f1 = (int64_t)G.nx * (G.ny + 1) * G.nz,
+                f2 = (int64_t)G.nx * G.ny * (G.nz + 1);
+  k_p2g_normalize<T><<<nblk(f0), kT, 0, st>>>(f0, gu, wu, vu, lu);
+  k_p2g_normalize<T><<<nblk(f1), kT, 0, st>>>(f1, gv, wv, vv, lv);
+  k_p2g_normalize<T><<<nblk(f2), kT, 0, st>>>(f2, gw, ww, vw, lw);
+  return 4;
 }
 
 // applyDirichletBoundary for one face grid (fluid-simulator.cc:113-138).
@@ -952,16 +1073,14 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
   const double* fluid = sdf_[scur_];
   cudaEventRecord(ev_[2], st);
   // P2G + Dirichlet walls + extrapolation + gravity (fluid-simulator.cc:155-164)
-  k_p2g<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, h, start_, cnt_, P, G_(0), (T*)gw_[0], gv_[0][gcur_[0]],
-                                              c_.flip ? (T*)last_[0] : nullptr);
-  k_p2g<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, h, start_, cnt_, P, G_(1), (T*)gw_[1], gv_[1][gcur_[1]],
-                                              c_.flip ? (T*)last_[1] : nullptr);
-  k_p2g<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, h, start_, cnt_, P, G_(2), (T*)gw_[2], gv_[2][gcur_[2]],
-                                              c_.flip ? (T*)last_[2] : nullptr);
+  launches_ += launch_p2g<T>(st, G, h, start_, cnt_, P, G_(0), G_(1), G_(2), (T*)gw_[0], (T*)gw_[1],
+                             (T*)gw_[2], gv_[0][gcur_[0]], gv_[1][gcur_[1]], gv_[2][gcur_[2]],
+                             c_.flip ? (T*)last_[0] : nullptr, c_.flip ? (T*)last_[1] : nullptr,
+                             c_.flip ? (T*)last_[2] : nullptr);
   k_dirichlet<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, G_(0), gv_[0][gcur_[0]]);
   k_dirichlet<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, G_(1), gv_[1][gcur_[1]]);
   k_dirichlet<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, G_(2), gv_[2][gcur_[2]]);
-  launches_ += 6;
+  launches_ += 3;
   for (int it = 0; it < c_.vel_extrap_iters; it++) {
     k_extrap_face<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, (T*)g_[0][gcur_[0]], (T*)g_[0][1 - gcur_[0]],
                                                         gv_[0][gcur_[0]], gv_[0][1 - gcur_[0]]);
@@ -1221,9 +1340,14 @@ int flip_p2g(cudaStream_t st, int64_t n, const double* pos, const double* vel, i
   if (e) return e;
   const int64_t f0 = (int64_t)(nx + 1) * ny * nz, f1 = (int64_t)nx * (ny + 1) * nz,
                 f2 = (int64_t)nx * ny * (nz + 1);
-  k_p2g<double, 0><<<nblk(f0), kT, 0, st>>>(G, h, s.start, s.cnt, s.b.P(), u, uw, uvalid, ulast);
-  k_p2g<double, 1><<<nblk(f1), kT, 0, st>>>(G, h, s.start, s.cnt, s.b.P(), v, vw, vvalid, vlast);
-  k_p2g<double, 2><<<nblk(f2), kT, 0, st>>>(G, h, s.start, s.cnt, s.b.P(), w, ww, wvalid, wlast);
+  cudaMemsetAsync(u, 0, sizeof(double) * f0, st);
+  cudaMemsetAsync(v, 0, sizeof(double) * f1, st);
+  cudaMemsetAsync(w, 0, sizeof(double) * f2, st);
+  cudaMemsetAsync(uw, 0, sizeof(double) * f0, st);
+  cudaMemsetAsync(vw, 0, sizeof(double) * f1, st);
+  cudaMemsetAsync(ww, 0, sizeof(double) * f2, st);
+  launch_p2g<double>(st, G, h, s.start, s.cnt, s.b.P(), u, v, w, uw, vw, ww, uvalid, vvalid, wvalid, ulast,
+                     vlast, wlast);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

@@ -95,8 +95,10 @@ def _p2g_inputs(n, seed):
     pos, _, h = scenes.dam_break(n, seed=seed)
     rng = np.random.default_rng(seed + 100)
     vel = rng.normal(size=pos.shape)
-    # particles on the domain walls and on cell faces
+    # particles on the domain walls and on cell faces, and a few outside the box
     extra = rng.integers(0, 2 * n + 1, (200, 3)) * (h / 2)
+    outside = rng.uniform(-1.5 * h, 1 + 1.5 * h, (60, 3))
+    extra = np.concatenate([extra, outside])
     pos = np.concatenate([pos, extra])
     vel = np.concatenate([vel, rng.normal(size=extra.shape)])
     return pos, vel, h

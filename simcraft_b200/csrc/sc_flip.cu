@@ -272,6 +272,34 @@ __global__ void __launch_bounds__(kT)
   }
 }
 
+// advect as the substep runs it: clear() (fluid-simulator.cc:141) has just
+// zeroed the grids advect samples, so both RK3 samples are exactly +0 (a
+// weighted average of zeros, or 0 where no node is in range) and the update
+// reduces to the same rounded sums with zero k2, k3.  Bit-identical to
+// k_advect on zero grids.
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_advect_still(int64_t n, PartsT<T> P, Geo G, double hd, const double* col, double dtd) {
+  const T dt = (T)dtd;
+  const T zero = T(0);
+  GRID_LOOP(i, n) {
+    T px = P.px[i], py = P.py[i], pz = P.pz[i];
+    const T k1x = P.vx[i], k1y = P.vy[i], k1z = P.vz[i];
+    const T c1 = rmul(T(2.0 / 9.0), dt), c2 = rmul(T(1.0 / 3.0), dt), c3 = rmul(T(4.0 / 9.0), dt);
+    px = radd(radd(radd(px, rmul(c1, k1x)), rmul(c2, zero)), rmul(c3, zero));
+    py = radd(radd(radd(py, rmul(c1, k1y)), rmul(c2, zero)), rmul(c3, zero));
+    pz = radd(radd(radd(pz, rmul(c1, k1z)), rmul(c2, zero)), rmul(c3, zero));
+    T vx = k1x, vy = k1y, vz = k1z;
+    handle_collision(col, G, hd, px, py, pz, vx, vy, vz);
+    P.px[i] = px;
+    P.py[i] = py;
+    P.pz[i] = pz;
+    P.vx[i] = vx;
+    P.vy[i] = vy;
+    P.vz[i] = vz;
+  }
+}
+
 // FlipAdvectionSolver3D::solveG2P (advect-solver.cc:157-169); alpha < 0 is PIC.
 template <class T>
 __global__ void __launch_bounds__(kT)
@@ -1037,8 +1065,7 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
     cudaMemsetAsync(gw_[a], 0, rs_ * fsz_[a], st);
   }
   // advect on the just-cleared grids (fluid-simulator.cc:143)
-  if (n > 0)
-    k_advect<T><<<nblk(n), kT, 0, st>>>(n, P, G_(0), G_(1), G_(2), G, h, collider_, dt);
+  if (n > 0) k_advect_still<T><<<nblk(n), kT, 0, st>>>(n, P, G, h, collider_, dt);
   launches_ += 1;
   cudaEventRecord(ev_[1], st);
   // sort by cell, then reconstruct (fluid-simulator.cc:146-148)

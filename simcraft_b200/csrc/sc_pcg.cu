@@ -295,6 +295,31 @@ __device__ __forceinline__ T apply_row(const Tiled& g, const Cell& c, const T* _
   return t;
 }
 
+// The PCG's own SpMV.  The PCG vectors are zero on inactive cells and the
+// couplings are finite (k_mask_system), so the neighbour activity tests of
+// apply_row drop out: every load is unconditional and independent, and the
+// result equals applyCompressedMatrix.
+template <class T>
+__device__ __forceinline__ T apply_row_pcg(const Tiled& g, const Cell& c, const T* __restrict__ adiag,
+                                           const T* __restrict__ al, const T* __restrict__ ad,
+                                           const T* __restrict__ ab, const T* __restrict__ x) {
+  const int64_t e = c.e;
+  const bool hx = c.x > 0, hy = c.y > 0, hz = c.z > 0;
+  const bool px = c.x < g.nx - 1, py = c.y < g.ny - 1, pz = c.z < g.nz - 1;
+  const int64_t oxm = hx ? c.xm(g) : e, oym = hy ? c.ym(g) : e, ozm = hz ? c.zm(g) : e;
+  const int64_t oxp = px ? c.xp(g) : e, oyp = py ? c.yp(g) : e, ozp = pz ? c.zp(g) : e;
+  const T cxm = hx ? al[e] : T(0), cym = hy ? ad[e] : T(0), czm = hz ? ab[e] : T(0);
+  const T cxp = px ? al[oxp] : T(0), cyp = py ? ad[oyp] : T(0), czp = pz ? ab[ozp] : T(0);
+  T t = adiag[e] * x[e];
+  t += cxm * x[oxm];
+  t += cym * x[oym];
+  t += czm * x[ozm];
+  t += cxp * x[oxp];
+  t += cyp * x[oyp];
+  t += czp * x[ozp];
+  return t;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kThreads)
     k_spmv(Tiled g, const T* __restrict__ adiag, const T* __restrict__ al,
@@ -303,51 +328,115 @@ __global__ void __launch_bounds__(kThreads)
            int use_skip) {
   if (use_skip && sc->done != DONE_RUNNING) return;
   double acc = 0.0;
-  SC_ROWBLOCK_LOOP(g) {
-    Cell c;
-    c.init(g, rb, threadIdx.x);
-    T out = T(0);
-    if (c.inside && act[c.e]) {
-      out = apply_row(g, c, adiag, al, ad, ab, act, x);
-      acc += (double)x[c.e] * (double)out;
+  const int nrb = g.ntiles() * g.nz;
+  // two row blocks per iteration: twice the loads in flight per thread
+  for (int rb0 = blockIdx.x; rb0 < nrb; rb0 += 2 * gridDim.x) {
+    const int rb1 = rb0 + gridDim.x;
+    Cell c0, c1;
+    c0.init(g, rb0, threadIdx.x);
+    c1.init(g, rb1 < nrb ? rb1 : rb0, threadIdx.x);
+    const T t0 = apply_row_pcg(g, c0, adiag, al, ad, ab, x);
+    const T t1 = apply_row_pcg(g, c1, adiag, al, ad, ab, x);
+    const bool a0 = c0.inside && act[c0.e], a1 = rb1 < nrb && c1.inside && act[c1.e];
+    const T o0 = a0 ? t0 : T(0), o1 = a1 ? t1 : T(0);
+    acc += (double)x[c0.e] * (double)o0;
+    y[c0.e] = o0;
+    if (rb1 < nrb) {
+      acc += (double)x[c1.e] * (double)o1;
+      y[c1.e] = o1;
     }
-    y[c.e] = out;
   }
   reduce_finalize(acc, 0.0, partials, sc, FIN_SPMV);
 }
 
-// saxpy(pg, s, alpha); saxpy(r, z, -alpha); residual (:332-335, util.cc:394-402)
+// Entries that couple to an inactive cell, and whole inactive rows, are never
+// read by applyCompressedMatrix (it tests the neighbour's activity first).  The
+// PCG kernels multiply them by zeros instead of testing, so any non-finite
+// value there is replaced by 0 before the solve; finite values stay as given.
+__global__ void __launch_bounds__(kThreads)
+    k_mask_system(Tiled g, const uint8_t* __restrict__ act, double* __restrict__ adiag,
+                  double* __restrict__ al, double* __restrict__ ad, double* __restrict__ ab) {
+  auto fix = [](double* a, int64_t e) {
+    if (!isfinite(a[e])) a[e] = 0.0;
+  };
+  SC_ROWBLOCK_LOOP(g) {
+    Cell c;
+    c.init(g, rb, threadIdx.x);
+    const int64_t e = c.e;
+    if (!(c.inside && act[e])) {
+      fix(adiag, e);
+      fix(al, e);
+      fix(ad, e);
+      fix(ab, e);
+      continue;
+    }
+    if (c.x == 0 || !act[c.xm(g)]) fix(al, e);
+    if (c.y == 0 || !act[c.ym(g)]) fix(ad, e);
+    if (c.z == 0 || !act[c.zm(g)]) fix(ab, e);
+  }
+}
+
+// saxpy(pg, s, alpha); saxpy(r, z, -alpha); residual (:332-335, util.cc:394-402).
+// s and Az are zero on inactive cells, so the masked updates of the reference
+// are the plain updates here; four independent elements per thread per pass.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-    k_axpy(int64_t n, const uint8_t* __restrict__ act, const T* __restrict__ s,
+    k_axpy(int64_t n, const uint8_t* __restrict__, const T* __restrict__ s,
            const T* __restrict__ Az, T* __restrict__ p, T* __restrict__ r, double* partials,
            PcgScalars* sc) {
   if (sc->done != DONE_RUNNING) return;
   const T alpha = (T)sc->alpha;
   double s2 = 0.0, mx = 0.0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
-    if (!act[e]) continue;
-    p[e] += alpha * s[e];
-    T rv = r[e] + (-alpha) * Az[e];
-    r[e] = rv;
-    double dv = (double)rv;
-    s2 += dv * dv;
-    mx = fmax(mx, fabs(dv));
+  for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += 4 * stride) {
+    T sv[4], av[4], pv[4], rv[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int64_t e = e0 + k * stride;
+      const bool in = e < n;
+      sv[k] = in ? s[e] : T(0);
+      av[k] = in ? Az[e] : T(0);
+      pv[k] = in ? p[e] : T(0);
+      rv[k] = in ? r[e] : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int64_t e = e0 + k * stride;
+      if (e >= n) continue;
+      p[e] = pv[k] + alpha * sv[k];
+      const T rn = rv[k] + (-alpha) * av[k];
+      r[e] = rn;
+      const double dv = (double)rn;
+      s2 += dv * dv;
+      mx = fmax(mx, fabs(dv));
+    }
   }
   reduce_finalize(s2, mx, partials, sc, FIN_AXPY);
 }
 
-// scaleAndAdd(s, z, beta): s = z + beta s (util.cc:404-410)
+// scaleAndAdd(s, z, beta): s = z + beta s (util.cc:404-410); z and s are zero
+// on inactive cells.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-    k_sa(int64_t n, const uint8_t* __restrict__ act, const T* __restrict__ z, T* __restrict__ s,
+    k_sa(int64_t n, const uint8_t* __restrict__, const T* __restrict__ z, T* __restrict__ s,
          double* partials, PcgScalars* sc) {
   if (sc->done != DONE_RUNNING) return;
   const T beta = (T)sc->beta;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride)
-    if (act[e]) s[e] = z[e] + beta * s[e];
+  for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += 4 * stride) {
+    T zv[4], sv[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int64_t e = e0 + k * stride;
+      zv[k] = e < n ? z[e] : T(0);
+      sv[k] = e < n ? s[e] : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int64_t e = e0 + k * stride;
+      if (e < n) s[e] = zv[k] + beta * sv[k];
+    }
+  }
   reduce_finalize(0.0, 0.0, partials, sc, FIN_SA);
 }
 
@@ -951,6 +1040,17 @@ void wave_set_attr() {
   cudaFuncSetAttribute(k_wave<T, Tiled::TY, FWD, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)wave_dyn_smem<T, FWD, Op>());
 }
+// Wavefront CTAs resident per SM (shared memory and registers permitting).
+// Tiles are handed out in ticket order to running CTAs only, so a grid larger
+// than what fits at once cannot deadlock; it just queues.
+template <class T, bool FWD, class Op>
+int wave_occupancy() {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_wave<T, Tiled::TY, FWD, Op>, (Tiled::TY + 3) * 32,
+                                                    wave_dyn_smem<T, FWD, Op>()) != cudaSuccess)
+    nb = 1;
+  return std::max(1, nb);
+}
 template <class T, bool FWD, class Op>
 void launch_wave(const WaveArgs& a, const Op& op, cudaStream_t st, int grid) {
   k_wave<T, Tiled::TY, FWD, Op><<<grid, (Tiled::TY + 3) * 32, wave_dyn_smem<T, FWD, Op>(), st>>>(a, op);
@@ -1027,9 +1127,17 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
   wave_set_attr<double, false, BwdOp<double>>();
   wave_set_attr<float, true, FwdOp<float>>();
   wave_set_attr<float, false, BwdOp<float>>();
-  nblocks_ = ctx->sm_count * 4;
+  nblocks_ = ctx->sm_count * 8;
   const int ntiles = g_.ntiles();
   wave_grid_ = std::min(ntiles, ctx->sm_count);
+  {
+    const int occ64 = std::min(wave_occupancy<double, true, FwdOp<double>>(),
+                               wave_occupancy<double, false, BwdOp<double>>());
+    const int occ32 = std::min(wave_occupancy<float, true, FwdOp<float>>(),
+                               wave_occupancy<float, false, BwdOp<float>>());
+    wave_grid64_ = std::min(ntiles, ctx->sm_count * occ64);
+    wave_grid32_ = std::min(ntiles, ctx->sm_count * occ32);
+  }
   auto alloc = [&](size_t bytes) -> void* {
     void* p = nullptr;
     if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
@@ -1048,7 +1156,8 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
     }
   }
   active_ = (uint8_t*)alloc((size_t)g_.total);
-  partials_ = (double*)alloc(sizeof(double) * 2 * (size_t)std::max(nblocks_, wave_grid_));
+  partials_ = (double*)alloc(sizeof(double) * 2 *
+                             (size_t)std::max({nblocks_, wave_grid_, wave_grid64_, wave_grid32_}));
   sc_ = (PcgScalars*)alloc(sizeof(PcgScalars));
   ws_.ticket = (int*)alloc(sizeof(int) * 2);
   tile_partials_ = (double*)alloc(sizeof(double) * (size_t)ntiles);
@@ -1070,7 +1179,8 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
   for (double** a : arr64) cudaMemsetAsync(*a, 0, n64, ctx->stream);
   cudaMemsetAsync(active_, 0, (size_t)g_.total, ctx->stream);
   cudaMemsetAsync(sc_, 0, sizeof(PcgScalars), ctx->stream);
-  cudaMemsetAsync(partials_, 0, sizeof(double) * 2 * (size_t)std::max(nblocks_, wave_grid_),
+  cudaMemsetAsync(partials_, 0,
+                  sizeof(double) * 2 * (size_t)std::max({nblocks_, wave_grid_, wave_grid64_, wave_grid32_}),
                   ctx->stream);
   reset_mailboxes(false);
   // tile order: anti-diagonals of the tile grid, so every tile's forward
@@ -1226,6 +1336,7 @@ int PcgSolver::ensure_pivots() {
   cudaStream_t st = ctx_->stream;
   const int grid = grid_for(g_.total, ctx_->sm_count);
   WaveArgs wa = wave_args(false, 0, FIN_NONE);
+  k_mask_system<<<grid, kThreads, 0, st>>>(g_, active_, d64_.adiag, d64_.al, d64_.ad, d64_.ab);
   // uR/uU/uF hold the pivot's diagonal products until k_upper overwrites them
   // q holds Adiag masked by the active flag until the forward sweep overwrites it
   k_pivot_diag<<<grid, kThreads, 0, st>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab, active_,
@@ -1235,7 +1346,7 @@ int PcgSolver::ensure_pivots() {
   launch_wave<double, true>(wa, op, st, wave_grid_);
   k_upper<double><<<grid, kThreads, 0, st>>>(g_, d64_.cL, d64_.cD, d64_.cB, d64_.uR, d64_.uU,
                                               d64_.uF);
-  launches_ += 3;
+  launches_ += 4;
   if (opt_.precision == PREC_MIXED) {
     if (!have_f32_) {
       const size_t n32 = sizeof(float) * (size_t)g_.total;
@@ -1289,10 +1400,11 @@ void PcgSolver::launch_iteration(SysArrays<T>& A) {
   k_spmv<T><<<nblocks_, kThreads, 0, st>>>(g_, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az,
                                             partials_, sc_, 1);
   k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.s, A.Az, A.p, A.r, partials_, sc_);
+  const int wg = sizeof(T) == 4 ? wave_grid32_ : wave_grid64_;
   FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
-  launch_wave<T, true>(wf, fo, st, wave_grid_);
+  launch_wave<T, true>(wf, fo, st, wg);
   BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
-  launch_wave<T, false>(wb, bo, st, wave_grid_);
+  launch_wave<T, false>(wb, bo, st, wg);
   k_sa<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.s, partials_, sc_);
 }
 
@@ -1316,10 +1428,11 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
   const bool f32 = sizeof(T) == 4;
   WaveArgs wf = wave_args(f32, 1, FIN_NONE);
   WaveArgs wb = wave_args(f32, 1, FIN_BWD);
+  const int wg = sizeof(T) == 4 ? wave_grid32_ : wave_grid64_;
   FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
-  launch_wave<T, true>(wf, fo, s, wave_grid_);
+  launch_wave<T, true>(wf, fo, s, wg);
   BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
-  launch_wave<T, false>(wb, bo, s, wave_grid_);
+  launch_wave<T, false>(wb, bo, s, wg);
   k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.z, A.s, sc_);
   launches_ += 4;
   int e = check_dev_error("pcg init");
@@ -1492,9 +1605,9 @@ int PcgSolver::precond_only(const double* r, double* z) {
   WaveArgs wf = wave_args(false, 0, FIN_NONE);
   WaveArgs wb = wave_args(false, 0, FIN_BWD);
   FwdOp<double> fo{{d64_.r, d64_.cL, d64_.cD, d64_.cB, d64_.E}, d64_.q};
-  launch_wave<double, true>(wf, fo, s, wave_grid_);
+  launch_wave<double, true>(wf, fo, s, wave_grid64_);
   BwdOp<double> bo{{d64_.q, d64_.E, d64_.uR, d64_.uU, d64_.uF, d64_.r}, d64_.z};
-  launch_wave<double, false>(wb, bo, s, wave_grid_);
+  launch_wave<double, false>(wb, bo, s, wave_grid64_);
   k_from_tiled<double, double><<<grid, kThreads, 0, s>>>(g_, d64_.z, z);
   cudaMemcpyAsync(sc_host_, sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("precond");
@@ -1601,12 +1714,12 @@ int PcgSolver::time_kernels(int reps, double* ms) {
         }
         case 1: {
           FwdOp<double> fo{{d64_.r, d64_.cL, d64_.cD, d64_.cB, d64_.E}, d64_.q};
-          launch_wave<double, true>(wave_args(false, 0, FIN_NONE), fo, s, wave_grid_);
+          launch_wave<double, true>(wave_args(false, 0, FIN_NONE), fo, s, wave_grid64_);
           break;
         }
         case 2: {
           BwdOp<double> bo{{d64_.q, d64_.E, d64_.uR, d64_.uU, d64_.uF, d64_.r}, d64_.z};
-          launch_wave<double, false>(wave_args(false, 0, FIN_NONE), bo, s, wave_grid_);
+          launch_wave<double, false>(wave_args(false, 0, FIN_NONE), bo, s, wave_grid64_);
           break;
         }
         case 3:

@@ -158,7 +158,8 @@ class PcgSolver {
   bool pivots_valid_ = false;
   bool have_f32_ = false;
   int nblocks_ = 0;     // elementwise grid
-  int wave_grid_ = 0;   // persistent wavefront grid
+  int wave_grid_ = 0;   // persistent wavefront grid (pivot sweep)
+  int wave_grid64_ = 0, wave_grid32_ = 0;  // iteration sweeps: SMs x resident CTAs, capped at the tiles
   SysArrays<double> d64_;
   SysArrays<float> d32_;
   double* rhs_ = nullptr;   // tiled rhs (FP64)

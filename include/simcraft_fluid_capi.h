@@ -61,6 +61,8 @@ const char* sc_status_string(int status);
  * reference (which is single-threaded host code); every handle below is bound
  * to a context. */
 int sc_context_create(int device, sc_context** out);
+/* Frees the context once every handle created from it is destroyed too (in
+ * any order). */
 void sc_context_destroy(sc_context* ctx);
 /* Order all later work on an external stream (a cudaStream_t passed as void*;
  * NULL is the legacy default stream). */
@@ -298,6 +300,59 @@ int sc_fluid_get_pressure(sc_fluid* sim, double* pg, int device_pointers);
 int sc_fluid_get_faces(sc_fluid* sim, double* u, double* v, double* w, int device_pointers);
 /* exportFluidSurface() (fluid-simulator.h:187-189): the smoothed fluid SDF. */
 int sc_fluid_get_fluid_sdf(sc_fluid* sim, double* sdf, int device_pointers);
+
+/* ---------------------------------------------------------------------------
+ * Differentiable FLIP/PIC substeps (no counterpart in the reference).
+ * Forward: particles at their initial positions take velocities sampled from a
+ * parameter field U (three face grids), then `steps` substeps of the
+ * simulator's step with a fixed dt; loss = sum_c (rho_c - rho*_c)^2 over the
+ * particle density splatted to the cell centres with the transfer kernel.
+ * Backward: dL/dU by hand-written adjoint kernels of G2P, P2G, advection,
+ * extrapolation, the divergence, the pressure solve (a second MIC(0)-PCG
+ * solve; A is symmetric) and the projection, with the run's discrete
+ * structure (transfer stencils, wall clamps, fluid SDF) held fixed.  States are
+ * kept every `checkpoint_every` substeps; the backward recomputes the others.
+ * A forward may record its structure (SC_TAPE_RECORD) and later forwards may
+ * replay it (SC_TAPE_REPLAY): with the structure fixed the loss is smooth in U,
+ * which is what finite-difference checks of the gradient need.
+ */
+#define SC_TAPE_NONE 0
+#define SC_TAPE_RECORD 1
+#define SC_TAPE_REPLAY 2
+
+typedef struct {
+  int nx, ny, nz;
+  double h, dt;            /* cubic cell size, fixed substep */
+  int precision;           /* SC_REAL_F64 / SC_REAL_F32 particles and velocity grids */
+  int advection;           /* SC_ADVECT_FLIP / SC_ADVECT_PIC */
+  double flip_alpha, gravity, recon_factor;
+  int sdf_extrap_iters, smooth_iters, vel_extrap_iters;
+  int steps;               /* substeps per forward */
+  int checkpoint_every;    /* substeps between stored states */
+  sc_pcg_options pcg;      /* forward and adjoint pressure solves */
+} sc_diff_config;
+
+typedef struct sc_diff sc_diff;
+
+/* The simulator's defaults, except the pressure solves: relative L2 to 1e-10
+ * with the MIC(0) tau = 0 (the reference's tau = 0.97 stalls PCG at
+ * dt/h ~ 0.5, and the adjoint needs converged solves). */
+void sc_diff_default_config(int nx, int ny, int nz, double h, double dt, int steps,
+                            sc_diff_config* cfg);
+int sc_diff_create(sc_context* ctx, const sc_diff_config* cfg, sc_diff** out);
+void sc_diff_destroy(sc_diff* d);
+int sc_diff_set_particles(sc_diff* d, int64_t n, const double* pos, int device_pointers);
+/* rho* on the cell centres (nx*ny*nz doubles) */
+int sc_diff_set_target(sc_diff* d, const double* rho, int device_pointers);
+/* U: host array of 3 device pointers to FP64 face grids (reference layout) */
+int sc_diff_forward(sc_diff* d, const double* const* U, int tape, double* loss);
+/* dL/dU of the last forward into 3 device FP64 face grids */
+int sc_diff_backward(sc_diff* d, double* const* grad_U);
+int sc_diff_get_density(sc_diff* d, double* rho, int device_pointers);
+/* particles after the last forward (either may be NULL) */
+int sc_diff_get_particles(sc_diff* d, double* pos, double* vel, int device_pointers);
+/* pressure-solve iterations of the last substep run */
+int sc_diff_last_pcg_iterations(sc_diff* d);
 
 #ifdef __cplusplus
 }

@@ -45,12 +45,21 @@ class sc_fluid_stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class sc_diff_config(ctypes.Structure):
+    _fields_ = [("nx", c_int), ("ny", c_int), ("nz", c_int), ("h", c_double), ("dt", c_double),
+                ("precision", c_int), ("advection", c_int), ("flip_alpha", c_double), ("gravity", c_double),
+                ("recon_factor", c_double), ("sdf_extrap_iters", c_int), ("smooth_iters", c_int),
+                ("vel_extrap_iters", c_int), ("steps", c_int), ("checkpoint_every", c_int),
+                ("pcg", sc_pcg_options)]
+
+
 SC_OK = 0
 SC_CRIT_ABS_LINF, SC_CRIT_REL_L2 = 0, 1
 SC_PREC_FP64, SC_PREC_MIXED = 0, 1
 SC_REAL_F64, SC_REAL_F32 = 0, 1
 SC_DONE_CONVERGED, SC_DONE_MAXITER, SC_DONE_BREAKDOWN = 1, 2, 3
 SC_ADVECT_PIC, SC_ADVECT_FLIP = 0, 1
+SC_TAPE_NONE, SC_TAPE_RECORD, SC_TAPE_REPLAY = 0, 1, 2
 
 _dpp = P(c_void_p)  # array of pointers
 
@@ -108,6 +117,16 @@ SIGNATURES = {
     "sc_fluid_get_pressure": (c_int, [c_void_p, c_void_p, c_int]),
     "sc_fluid_get_faces": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "sc_fluid_get_fluid_sdf": (c_int, [c_void_p, c_void_p, c_int]),
+    "sc_diff_default_config": (None, [c_int, c_int, c_int, c_double, c_double, c_int, P(sc_diff_config)]),
+    "sc_diff_create": (c_int, [c_void_p, P(sc_diff_config), P(c_void_p)]),
+    "sc_diff_destroy": (None, [c_void_p]),
+    "sc_diff_set_particles": (c_int, [c_void_p, c_int64, c_void_p, c_int]),
+    "sc_diff_set_target": (c_int, [c_void_p, c_void_p, c_int]),
+    "sc_diff_forward": (c_int, [c_void_p, _dpp, c_int, P(c_double)]),
+    "sc_diff_backward": (c_int, [c_void_p, _dpp]),
+    "sc_diff_get_density": (c_int, [c_void_p, c_void_p, c_int]),
+    "sc_diff_get_particles": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "sc_diff_last_pcg_iterations": (c_int, [c_void_p]),
 }
 
 _lib = None

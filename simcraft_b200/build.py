@@ -13,7 +13,7 @@ OBJDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # The particle/grid transfers and the finite-volume build restate the CPU
 # arithmetic operation by operation: no fused multiply-add contraction there.
-EXTRA = {"sc_flip.cu": ["--fmad=false"], "sc_fvm.cu": ["--fmad=false"]}
+EXTRA = {"sc_flip.cu": ["--fmad=false"], "sc_fvm.cu": ["--fmad=false"], "sc_diff.cu": ["--fmad=false"]}
 
 
 def sources():

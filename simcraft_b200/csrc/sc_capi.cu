@@ -1,17 +1,36 @@
 // sc_capi.cu -- extern "C" boundary.  No C++ exception or CUDA type crosses it.
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <string>
 
 #include "../../include/simcraft_fluid_capi.h"
+#include "sc_diff.cuh"
 #include "sc_flip.cuh"
 #include "sc_fvm.cuh"
 #include "sc_pcg.cuh"
 
+// A context is freed when its user handle and every handle created from it
+// have been destroyed, whatever the order of the destroy calls.
 struct sc_context {
   sc::Context c;
   cudaStream_t own = nullptr;
+  std::atomic<int> refs{1};
 };
+
+static sc_context* ctx_retain(sc_context* c) {
+  c->refs.fetch_add(1);
+  return c;
+}
+static void ctx_release(sc_context* c) {
+  if (c->refs.fetch_sub(1) == 1) {
+    if (c->own) {
+      cudaSetDevice(c->c.device);
+      cudaStreamDestroy(c->own);
+    }
+    delete c;
+  }
+}
 
 struct sc_pcg {
   sc_context* ctx;
@@ -21,6 +40,11 @@ struct sc_pcg {
 struct sc_fluid {
   sc_context* ctx;
   sc::FluidSim* sim;
+};
+
+struct sc_diff {
+  sc_context* ctx;
+  sc::DiffSim* sim;
 };
 
 namespace {
@@ -106,8 +130,7 @@ int sc_context_create(int device, sc_context** out) {
 
 void sc_context_destroy(sc_context* ctx) {
   if (!ctx) return;
-  if (ctx->own) cudaStreamDestroy(ctx->own);
-  delete ctx;
+  ctx_release(ctx);
 }
 
 int sc_context_set_stream(sc_context* ctx, void* stream) {
@@ -170,15 +193,19 @@ int sc_pcg_create(sc_context* ctx, int nx, int ny, int nz, const sc_pcg_options*
     delete s;
     return SC_ERR_NOMEM;
   }
+  ctx_retain(ctx);
   *out = h;
   return SC_OK;
 }
 
 void sc_pcg_destroy(sc_pcg* pcg) {
   if (!pcg) return;
+  cudaSetDevice(pcg->ctx->c.device);
   cudaStreamSynchronize(pcg->ctx->c.stream);
   delete pcg->solver;
+  sc_context* c = pcg->ctx;
   delete pcg;
+  ctx_release(c);
 }
 
 int sc_pcg_set_options(sc_pcg* pcg, const sc_pcg_options* opt) {
@@ -493,6 +520,7 @@ int sc_fluid_create(sc_context* ctx, const sc_fluid_config* cfg, sc_fluid** out)
     delete s;
     return SC_ERR_NOMEM;
   }
+  ctx_retain(ctx);
   *out = f;
   return SC_OK;
 }
@@ -501,7 +529,9 @@ void sc_fluid_destroy(sc_fluid* sim) {
   if (!sim) return;
   cudaSetDevice(sim->ctx->c.device);
   delete sim->sim;
+  sc_context* c = sim->ctx;
   delete sim;
+  ctx_release(c);
 }
 
 static int fl_rc(sc_fluid* f, int rc) {
@@ -589,5 +619,134 @@ int sc_fluid_get_fluid_sdf(sc_fluid* sim, double* sdf, int device_pointers) {
   cudaSetDevice(sim->ctx->c.device);
   return fl_rc(sim, sim->sim->get_fluid_sdf(sdf, device_pointers != 0));
 }
+
+// ---------------------------------------------------------------------------------
+// Differentiable substeps.
+
+void sc_diff_default_config(int nx, int ny, int nz, double h, double dt, int steps, sc_diff_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->nx = nx;
+  c->ny = ny;
+  c->nz = nz;
+  c->h = h;
+  c->dt = dt;
+  c->precision = SC_REAL_F64;
+  c->advection = SC_ADVECT_FLIP;
+  c->flip_alpha = 0.97;
+  c->gravity = 9.8;
+  c->recon_factor = 0.8;
+  c->sdf_extrap_iters = 10;
+  c->smooth_iters = 5;
+  c->vel_extrap_iters = 10;
+  c->steps = steps;
+  c->checkpoint_every = 5;
+  sc_pcg_default_options(&c->pcg);
+  c->pcg.tol = 1e-10;
+  c->pcg.criterion = SC_CRIT_REL_L2;
+  c->pcg.max_iter = 2000;
+  c->pcg.mic_tau = 0.0;
+}
+
+int sc_diff_create(sc_context* ctx, const sc_diff_config* cfg, sc_diff** out) {
+  if (!ctx || !cfg || !out) return SC_ERR_INVALID;
+  *out = nullptr;
+  if (!grid_ok(cfg->nx, cfg->ny, cfg->nz, cfg->h) || !(cfg->dt > 0.0) || cfg->steps < 1 ||
+      cfg->checkpoint_every < 1 || (cfg->precision != SC_REAL_F64 && cfg->precision != SC_REAL_F32) ||
+      (cfg->advection != SC_ADVECT_FLIP && cfg->advection != SC_ADVECT_PIC) ||
+      !(cfg->flip_alpha >= 0.0 && cfg->flip_alpha <= 1.0) || !(cfg->recon_factor > 0.0) ||
+      cfg->sdf_extrap_iters < 0 || cfg->smooth_iters < 0 || cfg->vel_extrap_iters < 0 ||
+      validate_options(&cfg->pcg))
+    return ctx->c.set_error(SC_ERR_INVALID, "invalid differentiable-step configuration");
+  sc::DiffConfig dc;
+  dc.nx = cfg->nx;
+  dc.ny = cfg->ny;
+  dc.nz = cfg->nz;
+  dc.h = cfg->h;
+  dc.dt = cfg->dt;
+  dc.f32 = cfg->precision == SC_REAL_F32;
+  dc.flip = cfg->advection == SC_ADVECT_FLIP;
+  dc.flip_alpha = cfg->flip_alpha;
+  dc.gravity = cfg->gravity;
+  dc.recon_factor = cfg->recon_factor;
+  dc.sdf_extrap_iters = cfg->sdf_extrap_iters;
+  dc.smooth_iters = cfg->smooth_iters;
+  dc.vel_extrap_iters = cfg->vel_extrap_iters;
+  dc.steps = cfg->steps;
+  dc.checkpoint_every = cfg->checkpoint_every;
+  dc.pcg = to_internal(&cfg->pcg);
+  cudaSetDevice(ctx->c.device);
+  sc::DiffSim* s = new (std::nothrow) sc::DiffSim(&ctx->c, dc);
+  if (!s) return SC_ERR_NOMEM;
+  if (s->status()) {
+    int st = s->status();
+    delete s;
+    return ctx->c.set_error(map_status(st), "differentiable step create failed");
+  }
+  sc_diff* d = new (std::nothrow) sc_diff{ctx, s};
+  if (!d) {
+    delete s;
+    return SC_ERR_NOMEM;
+  }
+  ctx_retain(ctx);
+  *out = d;
+  return SC_OK;
+}
+
+void sc_diff_destroy(sc_diff* d) {
+  if (!d) return;
+  cudaSetDevice(d->ctx->c.device);
+  delete d->sim;
+  sc_context* c = d->ctx;
+  delete d;
+  ctx_release(c);
+}
+
+static int df_rc(sc_diff* d, int rc) {
+  if (rc == 0) return SC_OK;
+  if (d->ctx->c.last_error.empty()) d->ctx->c.last_error = "differentiable step call failed";
+  return map_status(rc);
+}
+
+int sc_diff_set_particles(sc_diff* d, int64_t n, const double* pos, int device_pointers) {
+  if (!d || n < 1 || !pos || n >= ((int64_t)1 << 31)) return SC_ERR_INVALID;
+  cudaSetDevice(d->ctx->c.device);
+  return df_rc(d, d->sim->set_particles(n, pos, device_pointers != 0));
+}
+
+int sc_diff_set_target(sc_diff* d, const double* rho, int device_pointers) {
+  if (!d || !rho) return SC_ERR_INVALID;
+  cudaSetDevice(d->ctx->c.device);
+  return df_rc(d, d->sim->set_target(rho, device_pointers != 0));
+}
+
+int sc_diff_forward(sc_diff* d, const double* const* U, int tape, double* loss) {
+  if (!d || !U || !U[0] || !U[1] || !U[2] || !loss || tape < SC_TAPE_NONE || tape > SC_TAPE_REPLAY)
+    return SC_ERR_INVALID;
+  cudaSetDevice(d->ctx->c.device);
+  const double* u[3] = {U[0], U[1], U[2]};
+  return df_rc(d, d->sim->forward(u, tape, loss));
+}
+
+int sc_diff_backward(sc_diff* d, double* const* grad_U) {
+  if (!d || !grad_U || !grad_U[0] || !grad_U[1] || !grad_U[2]) return SC_ERR_INVALID;
+  cudaSetDevice(d->ctx->c.device);
+  double* g[3] = {grad_U[0], grad_U[1], grad_U[2]};
+  return df_rc(d, d->sim->backward(g));
+}
+
+int sc_diff_get_density(sc_diff* d, double* rho, int device_pointers) {
+  if (!d || !rho) return SC_ERR_INVALID;
+  cudaSetDevice(d->ctx->c.device);
+  return df_rc(d, d->sim->get_density(rho, device_pointers != 0));
+}
+
+int sc_diff_get_particles(sc_diff* d, double* pos, double* vel, int device_pointers) {
+  if (!d) return SC_ERR_INVALID;
+  cudaSetDevice(d->ctx->c.device);
+  return df_rc(d, d->sim->get_particles(pos, vel, device_pointers != 0));
+}
+
+int sc_diff_last_pcg_iterations(sc_diff* d) { return d ? d->sim->last_pcg_iterations() : 0; }
 
 }  // extern "C"

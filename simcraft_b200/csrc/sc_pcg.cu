@@ -1440,23 +1440,31 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
   // graph of `chunk` iterations
   cudaGraphExec_t& gx = graph_for<T>();
   if (!gx) {
-    cudaGraph_t graph;
-    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-      return check_dev_error("begin capture");
-    for (int i = 0; i < opt_.chunk; i++) launch_iteration<T>(A);
-    if (cudaStreamEndCapture(s, &graph) != cudaSuccess) return check_dev_error("end capture");
-    if (cudaGraphInstantiate(&gx, graph, 0) != cudaSuccess) {
+    // The legacy default stream cannot be captured: launch the chunk's kernels
+    // directly then (same kernels, same order).
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      for (int i = 0; i < opt_.chunk; i++) launch_iteration<T>(A);
+      if (cudaStreamEndCapture(s, &graph) != cudaSuccess || !graph) return check_dev_error("end capture");
+      if (cudaGraphInstantiate(&gx, graph, 0) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        gx = nullptr;
+        return check_dev_error("instantiate");
+      }
       cudaGraphDestroy(graph);
-      return check_dev_error("instantiate");
+    } else {
+      cudaGetLastError();
     }
-    cudaGraphDestroy(graph);
   }
   // launch chunks, two in flight, until the device reports done
   const int max_chunks = max_iter / std::max(1, opt_.chunk) + 3;
   cudaEvent_t evs[2] = {ev0_, ev1_};
   int launched = 0;
   auto launch_chunk = [&](int c) {
-    cudaGraphLaunch(gx, s);
+    if (gx)
+      cudaGraphLaunch(gx, s);
+    else
+      for (int i = 0; i < opt_.chunk; i++) launch_iteration<T>(A);
     launches_ += 5 * (uint64_t)opt_.chunk;
     cudaMemcpyAsync(&sc_host_[c & 1], sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(evs[c & 1], s);

@@ -14,6 +14,11 @@ y<0.5, 8 jittered particles per cell = 33.5M particles, FP32 particles and
 grids, CFL factor 1, FLIP blend 0.95, mixed MIC(0)-PCG to 1e-8 relative
 residual), reported as FLIP substeps/s with the per-subsystem split.
 
+A third leg times the differentiable step on the 64^3 control problem (fluid
+y < 0.25, 524,288 particles, 20 substeps of dt = 1/120, checkpoints every 5):
+forward and adjoint in FP32, and the FP64 adjoint against central finite
+differences along 16 seeded directions.
+
 `--impl reference` times the CPU restatement of the reference (the oracle,
 OpenMP where the reference uses TBB) on the same system.
 """
@@ -37,12 +42,17 @@ TOL = 1e-8
 DT_OVER_H = 32.0 / 120.0
 FLIP_N = 256
 FRAME_DT = 1.0 / 120.0
+DIFF_N = 64
+DIFF_STEPS = 20
 
 
 def build_scene(n):
+    """Sphere-pool fluid: 24 seeded spheres at 50% fill (seed 2); the 512^3
+    large-solve scene uses 60% fill (seed 9)."""
     from simcraft_b200 import scenes
 
-    sdf, info = scenes.sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=0.5, seed=2)
+    fill, seed = (0.6, 9) if n >= 512 else (0.5, 2)
+    sdf, info = scenes.sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=fill, seed=seed)
     return np.ascontiguousarray(sdf), info
 
 
@@ -140,7 +150,7 @@ def reference_arm(args, rank):
     threads = os.cpu_count() or 1
     O.set_threads(threads)
     O.set_parity_mode(False)
-    n = N_GRID
+    n = args.solve_n
     sdf, _ = build_scene(n)
     h = 1.0 / n
     z = np.zeros
@@ -226,6 +236,65 @@ def flip_leg(args, dev, ctx, dist, rank, world):
     return out
 
 
+def diff_leg(args, ctx):
+    """Differentiable step on the 64^3 control problem: FP32 forward + adjoint
+    times (CUDA events around each call on the solver's stream), and the FP64
+    adjoint against central differences (eps 1e-3) along seeded directions."""
+    import torch
+
+    from simcraft_b200.diff import DiffFlip, control_scene, faces_from_cells
+
+    n, steps = DIFF_N, DIFF_STEPS
+    pos, param, target, h = control_scene(n)
+    U = faces_from_cells(torch.from_numpy(param).cuda())
+    out = {"workload": f"differentiable FLIP control {n}^3, fluid y<0.25, {len(pos)} particles, "
+                       f"{steps} substeps dt=1/120, checkpoints every 5, FLIP 0.95, PCG tau=0 to 1e-10",
+           "particles": len(pos), "steps": steps}
+    sims = {}
+    for prec in ("f32", "f64"):
+        sim = DiffFlip((n, n, n), h, FRAME_DT, steps, context=ctx, precision=prec, checkpoint_every=5,
+                       flip_alpha=0.95)
+        sim.set_particles(pos)
+        sim.set_target(target)
+        sims[prec] = sim
+    s32 = sims["f32"]
+    for _ in range(2):
+        s32.forward(U)
+        s32.backward()
+    fw, bw = [], []
+    for _ in range(max(1, args.steps)):
+        t = time.perf_counter()
+        loss = s32.forward(U)
+        fw.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        g32 = s32.backward()
+        bw.append(time.perf_counter() - t)
+    out.update({"loss": loss, "forward_ms": 1e3 * float(np.median(fw)), "backward_ms": 1e3 * float(np.median(bw)),
+                "precision": "f32 particles and grids, f64 pressure solves"})
+    s64 = sims["f64"]
+    s64.forward(U, tape="record")
+    g64 = s64.backward()
+    rng = np.random.default_rng(8)
+    errs = []
+    for _ in range(args.diff_dirs):
+        d = faces_from_cells(torch.from_numpy(rng.standard_normal(param.shape)).cuda())
+        eps = 1e-3
+        fp = s64.forward([u + eps * x for u, x in zip(U, d)], tape="replay")
+        fm = s64.forward([u - eps * x for u, x in zip(U, d)], tape="replay")
+        fd = (fp - fm) / (2 * eps)
+        ad = sum(float((g * x).sum()) for g, x in zip(g64, d))
+        errs.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+    num = sum(float(((a - b) ** 2).sum()) for a, b in zip(g64, g32))
+    den = sum(float((a ** 2).sum()) for a in g64)
+    out.update({"fd_directions": args.diff_dirs, "fd_eps": 1e-3,
+                "fd_max_rel_err": max(errs) if errs else None,
+                "fd_median_rel_err": float(np.median(errs)) if errs else None,
+                "f32_vs_f64_grad_rel_l2": (num / den) ** 0.5})
+    del sims, s32, s64
+    torch.cuda.empty_cache()
+    return out
+
+
 def flip_cpu_sample(sim, n, h):
     """CPU oracle on a bounded sample of the same 256^3 state: advect + P2G + G2P
     of the first 1M particles scaled to all particles, plus the FP64 PCG's cost
@@ -282,6 +351,9 @@ def main():
     ap.add_argument("--flip-n", type=int, default=FLIP_N, help="FLIP dam-break grid size (profiling runs)")
     ap.add_argument("--skip-solve", action="store_true",
                     help="run only the FLIP leg (profiling runs; prints the FLIP object)")
+    ap.add_argument("--solve-n", type=int, default=N_GRID, help="standalone solve grid size")
+    ap.add_argument("--diff-dirs", type=int, default=16,
+                    help="finite-difference directions of the differentiable leg (-1 skips the leg)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -313,6 +385,7 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     ctx = Context(local)
+    n = args.solve_n
     if args.skip_solve:
         fl = flip_leg(args, dev, ctx, dist, rank, world)
         if rank == 0:
@@ -322,7 +395,6 @@ def main():
             dist.destroy_process_group()
         return
     L = _capi.lib()
-    n = N_GRID
     h = 1.0 / n
     dt = DT_OVER_H * h
     N = n * n * n
@@ -419,6 +491,9 @@ def main():
     kt = (ctypes.c_double * 6)()
     _capi.check("sc_pcg_time_kernels", L.sc_pcg_time_kernels(solvers["fp64"].handle, 20, kt), ctx.handle)
     kms = list(kt)
+    kt32 = (ctypes.c_double * 6)()
+    _capi.check("sc_pcg_time_kernels", L.sc_pcg_time_kernels(solvers["mixed"].handle, 20, kt32), ctx.handle)
+    kms32 = list(kt32)
     pk, pk_src = peaks()
     s = 8
     bytes_bwd = N * (7 * s + 1)  # backward sweep: q, E, 3 couplings, r read, z written, active
@@ -431,7 +506,11 @@ def main():
                 "ms_per_launch": kms[2],
                 "kernel_ms": {"pivot": kms[0], "forward_sweep": kms[1], "backward_sweep": kms[2],
                               "spmv": kms[3], "axpy": kms[4], "scale_add": kms[5]},
-                "forward_sweep_gbs": bytes_fwd / (kms[1] * 1e-3) / 1e9}
+                "forward_sweep_gbs": bytes_fwd / (kms[1] * 1e-3) / 1e9,
+                "kernel_ms_fp32_inner": {"forward_sweep": kms32[1], "backward_sweep": kms32[2], "spmv": kms32[3],
+                                         "axpy": kms32[4], "scale_add": kms32[5]},
+                "kernel_gbs_fp64": {"spmv": N * 49 / (kms[3] * 1e-3) / 1e9, "axpy": N * 48 / (kms[4] * 1e-3) / 1e9,
+                                    "scale_add": N * 24 / (kms[5] * 1e-3) / 1e9}}
 
     ms_step = ms_mixed / args.steps
     value = ms_step / world  # replicas: whole-job ms per solve
@@ -477,6 +556,8 @@ def main():
     torch.cuda.empty_cache()
     if args.flip_steps > 0:
         out["flip"] = flip_leg(args, dev, ctx, dist, rank, world)
+    if args.diff_dirs >= 0 and rank == 0:
+        out["diff"] = diff_leg(args, ctx)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:

@@ -143,8 +143,9 @@ int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b);
 /* Per-kernel device time of the solver's kernels on the uploaded system (each
  * kernel launched `reps` times, CUDA events on the context stream), in ms per
  * launch: [0] pivot sweep, [1] forward sweep, [2] backward sweep, [3] SpMV,
- * [4] axpy pair, [5] scale-and-add.  For profiling; leaves the solution
- * untouched. */
+ * [4] axpy pair, [5] scale-and-add.  With SC_PREC_MIXED (after a solve) [1]-[5]
+ * are the FP32 kernels the inner solve iterates with.  For profiling; leaves
+ * the solution untouched. */
 int sc_pcg_time_kernels(sc_pcg* pcg, int reps, double* ms_out);
 
 /* Allocation-free ModifiedIncompleteCholesky3D::precond(Adiag, Aneighbour, r,

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include <mutex>
@@ -31,7 +32,7 @@ namespace sc {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kRing = 64;     // boundary ring entries per wavefront CTA
+constexpr int kRing = 32;     // boundary ring entries per wavefront CTA
 constexpr int kStage = 8;     // steps of input staged ahead per compute warp (cp.async ring)
 constexpr int kSpinLimit = 1 << 22;  // bounded waits: ~0.1-1 s, far above any legitimate wait
 
@@ -320,6 +321,12 @@ __device__ __forceinline__ T apply_row_pcg(const Tiled& g, const Cell& c, const 
   return t;
 }
 
+// Each block walks a contiguous range of row blocks (consecutive slots of a
+// tile), so the neighbour rows it reads (x and z neighbours, the upper
+// couplings) were just loaded by the same block; two row blocks per pass.
+// (Measured against two alternatives at 128^3-512^3: per-warp row streaming
+// with register windows, and a multistage cp.async slab pipeline; both were
+// slower.)
 template <class T>
 __global__ void __launch_bounds__(kThreads)
     k_spmv(Tiled g, const T* __restrict__ adiag, const T* __restrict__ al,
@@ -329,24 +336,38 @@ __global__ void __launch_bounds__(kThreads)
   if (use_skip && sc->done != DONE_RUNNING) return;
   double acc = 0.0;
   const int nrb = g.ntiles() * g.nz;
-  // two row blocks per iteration: twice the loads in flight per thread
-  for (int rb0 = blockIdx.x; rb0 < nrb; rb0 += 2 * gridDim.x) {
-    const int rb1 = rb0 + gridDim.x;
+  const int chunk = (nrb + gridDim.x - 1) / gridDim.x;
+  const int rb_end = min(nrb, (int)(blockIdx.x + 1) * chunk);
+  for (int rb0 = blockIdx.x * chunk; rb0 < rb_end; rb0 += 2) {
+    const int rb1 = rb0 + 1;
     Cell c0, c1;
     c0.init(g, rb0, threadIdx.x);
-    c1.init(g, rb1 < nrb ? rb1 : rb0, threadIdx.x);
+    c1.init(g, rb1 < rb_end ? rb1 : rb0, threadIdx.x);
     const T t0 = apply_row_pcg(g, c0, adiag, al, ad, ab, x);
     const T t1 = apply_row_pcg(g, c1, adiag, al, ad, ab, x);
-    const bool a0 = c0.inside && act[c0.e], a1 = rb1 < nrb && c1.inside && act[c1.e];
+    const bool a0 = c0.inside && act[c0.e], a1 = rb1 < rb_end && c1.inside && act[c1.e];
     const T o0 = a0 ? t0 : T(0), o1 = a1 ? t1 : T(0);
     acc += (double)x[c0.e] * (double)o0;
     y[c0.e] = o0;
-    if (rb1 < nrb) {
+    if (rb1 < rb_end) {
       acc += (double)x[c1.e] * (double)o1;
       y[c1.e] = o1;
     }
   }
   reduce_finalize(acc, 0.0, partials, sc, FIN_SPMV);
+}
+
+// b = A x with the reference's activity tests (x may be non-zero on inactive
+// cells): applyCompressedMatrix for the apply entry point.
+__global__ void __launch_bounds__(kThreads)
+    k_apply_checked(Tiled g, const double* __restrict__ adiag, const double* __restrict__ al,
+                    const double* __restrict__ ad, const double* __restrict__ ab,
+                    const uint8_t* __restrict__ act, const double* __restrict__ x, double* __restrict__ b) {
+  SC_ROWBLOCK_LOOP(g) {
+    Cell c;
+    c.init(g, rb, threadIdx.x);
+    b[c.e] = (c.inside && act[c.e]) ? apply_row(g, c, adiag, al, ad, ab, act, x) : 0.0;
+  }
 }
 
 // Entries that couple to an inactive cell, and whole inactive rows, are never
@@ -853,6 +874,8 @@ __device__ void wave_load_y(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int
   if (ly < NS && lane == 0) wave_abort(a, sh, NS);
 }
 
+// One CTA per SM: the sweep is issue-bound, and capping registers for two
+// CTAs per SM measured slower at 128^3, 256^3 and 512^3.
 template <class T, int TY, bool FWD, class Op>
 __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, const Op op) {
   // warps 0..TY-1: tile rows (compute only, no fences: a fence would wait for
@@ -1392,13 +1415,18 @@ int PcgSolver::ensure_pivots() {
 }
 
 template <class T>
+void PcgSolver::launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip) {
+  k_spmv<T><<<nblocks_, kThreads, 0, st>>>(g_, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az, partials_, sc_,
+                                            use_skip);
+}
+
+template <class T>
 void PcgSolver::launch_iteration(SysArrays<T>& A) {
   cudaStream_t st = ctx_->stream;
   const bool f32 = sizeof(T) == 4;
   WaveArgs wf = wave_args(f32, 1, FIN_NONE);
   WaveArgs wb = wave_args(f32, 1, FIN_BWD);
-  k_spmv<T><<<nblocks_, kThreads, 0, st>>>(g_, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az,
-                                            partials_, sc_, 1);
+  launch_spmv<T>(A, st, 1);
   k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.s, A.Az, A.p, A.r, partials_, sc_);
   const int wg = sizeof(T) == 4 ? wave_grid32_ : wave_grid64_;
   FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
@@ -1628,8 +1656,8 @@ int PcgSolver::apply_only(const double* x, double* b) {
   cudaStream_t s = ctx_->stream;
   const int grid = grid_for(g_.total, ctx_->sm_count);
   k_to_tiled<double, double><<<grid, kThreads, 0, s>>>(g_, x, d64_.s, nullptr);
-  k_spmv<double><<<nblocks_, kThreads, 0, s>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab, active_,
-                                               d64_.s, d64_.Az, partials_, sc_, 0);
+  k_apply_checked<<<grid, kThreads, 0, s>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab, active_, d64_.s,
+                                            d64_.Az);
   k_from_tiled<double, double><<<grid, kThreads, 0, s>>>(g_, d64_.Az, b);
   if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("apply");
   return check_dev_error("apply");
@@ -1700,6 +1728,37 @@ int PcgSolver::time_kernels(int reps, double* ms) {
                                                sc_);
   cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
   k_copy<double><<<grid, kThreads, 0, s>>>(g_.total, d64_.r, d64_.s, sc_);
+  // The mixed solver iterates in FP32: time its FP32 kernels (the pivot sweep
+  // is FP64 in both).
+  const bool f32 = opt_.precision == PREC_MIXED && have_f32_;
+  if (f32) {
+    k_init<float><<<nblocks_, kThreads, 0, s>>>(g_, rhs_, 1.0, active_, d32_.r, d32_.p, partials_, sc_);
+    cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
+    k_copy<float><<<grid, kThreads, 0, s>>>(g_.total, d32_.r, d32_.s, sc_);
+  }
+  auto kernel = [&](auto& A, int which) {
+    using T = std::remove_reference_t<decltype(*A.r)>;
+    const bool is32 = sizeof(T) == 4;
+    const int wg = is32 ? wave_grid32_ : wave_grid64_;
+    switch (which) {
+      case 1:
+        launch_wave<T, true>(wave_args(is32, 0, FIN_NONE), FwdOp<T>{{A.r, A.cL, A.cD, A.cB, A.E}, A.q}, s, wg);
+        break;
+      case 2:
+        launch_wave<T, false>(wave_args(is32, 0, FIN_NONE), BwdOp<T>{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z},
+                              s, wg);
+        break;
+      case 3:
+        launch_spmv<T>(A, s, 0);
+        break;
+      case 4:
+        k_axpy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, active_, A.s, A.Az, A.p, A.r, partials_, sc_);
+        break;
+      case 5:
+        k_sa<T><<<nblocks_, kThreads, 0, s>>>(g_.total, active_, A.z, A.s, partials_, sc_);
+        break;
+    }
+  };
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
@@ -1720,27 +1779,11 @@ int PcgSolver::time_kernels(int reps, double* ms) {
                                                     d64_.uU, d64_.uF);
           break;
         }
-        case 1: {
-          FwdOp<double> fo{{d64_.r, d64_.cL, d64_.cD, d64_.cB, d64_.E}, d64_.q};
-          launch_wave<double, true>(wave_args(false, 0, FIN_NONE), fo, s, wave_grid64_);
-          break;
-        }
-        case 2: {
-          BwdOp<double> bo{{d64_.q, d64_.E, d64_.uR, d64_.uU, d64_.uF, d64_.r}, d64_.z};
-          launch_wave<double, false>(wave_args(false, 0, FIN_NONE), bo, s, wave_grid64_);
-          break;
-        }
-        case 3:
-          k_spmv<double><<<nblocks_, kThreads, 0, s>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab,
-                                                       active_, d64_.s, d64_.Az, partials_, sc_, 0);
-          break;
-        case 4:
-          k_axpy<double><<<nblocks_, kThreads, 0, s>>>(g_.total, active_, d64_.s, d64_.Az, d64_.p,
-                                                       d64_.r, partials_, sc_);
-          break;
-        case 5:
-          k_sa<double><<<nblocks_, kThreads, 0, s>>>(g_.total, active_, d64_.z, d64_.s, partials_,
-                                                     sc_);
+        default:
+          if (f32)
+            kernel(d32_, which);
+          else
+            kernel(d64_, which);
           break;
       }
     }

@@ -149,6 +149,8 @@ class PcgSolver {
   int true_residual(PcgStats* st);
   template <class T>
   void launch_iteration(SysArrays<T>& A);
+  template <class T>
+  void launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip);
   int check_dev_error(const char* where);
 
   Context* ctx_;

@@ -488,34 +488,41 @@ def main():
     clocks = clk.summary()
 
     # per-kernel device times on the resident FP64 system -> roofline of the sweeps
-    kt = (ctypes.c_double * 6)()
+    kt = (ctypes.c_double * 8)()
     _capi.check("sc_pcg_time_kernels", L.sc_pcg_time_kernels(solvers["fp64"].handle, 20, kt), ctx.handle)
     kms = list(kt)
-    kt32 = (ctypes.c_double * 6)()
+    kt32 = (ctypes.c_double * 8)()
     _capi.check("sc_pcg_time_kernels", L.sc_pcg_time_kernels(solvers["mixed"].handle, 20, kt32), ctx.handle)
     kms32 = list(kt32)
     pk, pk_src = peaks()
-    # the headline (mixed) solve spends most of its time in the FP32 backward
-    # sweep: q, E, 3 couplings, r read, z written (4 bytes each), active flag
-    bytes_bwd32 = N * (7 * 4 + 1)
+    # The headline (mixed) solve iterates Eisenstat's form in FP32; its top
+    # kernel is the fused forward sweep: v, t, Pinv, Dt, cL, cD, cB, E read and
+    # w written, 4 bytes each.  Its backward sweep reads v, E, uR, uU, uF and
+    # writes t.
+    bytes_fwde32 = N * 9 * 4
+    bytes_bwde32 = N * 6 * 4
     bytes_bwd = N * (7 * 8 + 1)
     bytes_fwd = N * (6 * 8 + 1)
-    achieved = bytes_bwd32 / (kms32[2] * 1e-3) / 1e9
-    traffic = read_traffic("traffic_bytes_per_launch_bwd_fp32") if n == N_GRID else None
-    roofline = {"bound": "hbm", "kernel": "MIC(0) backward sweep, FP32 (k_wave BwdOp<float>), "
+    achieved = bytes_fwde32 / (kms32[7] * 1e-3) / 1e9
+    traffic = read_traffic("traffic_bytes_per_launch_fwd_eisenstat_fp32") if n == N_GRID else None
+    roofline = {"bound": "hbm", "kernel": "fused Eisenstat forward sweep, FP32 (k_wave FwdEisenstatOp<float>), "
                                           "the top kernel of the mixed solve",
                 "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src + " (burst copy)",
-                "traffic": traffic, "algorithmic_bytes_per_launch": bytes_bwd32,
-                "ms_per_launch": kms32[2],
+                "traffic": traffic, "algorithmic_bytes_per_launch": bytes_fwde32,
+                "ms_per_launch": kms32[7],
+                "eisenstat_backward_sweep_fp32": {"ms": kms32[6], "achieved_gbs": bytes_bwde32 / (kms32[6] * 1e-3) / 1e9},
                 "fp64_backward_sweep": {"achieved_gbs": bytes_bwd / (kms[2] * 1e-3) / 1e9,
                                         "traffic": read_traffic("traffic_bytes_per_launch_bwd_fp64")
                                         if n == N_GRID else None},
                 "kernel_ms": {"pivot": kms[0], "forward_sweep": kms[1], "backward_sweep": kms[2],
                               "spmv": kms[3], "axpy": kms[4], "scale_add": kms[5]},
                 "forward_sweep_gbs": bytes_fwd / (kms[1] * 1e-3) / 1e9,
-                "kernel_ms_fp32_inner": {"forward_sweep": kms32[1], "backward_sweep": kms32[2], "spmv": kms32[3],
-                                         "axpy": kms32[4], "scale_add": kms32[5]},
+                "kernel_ms_fp32_inner": {"eisenstat_backward_sweep": kms32[6], "eisenstat_forward_sweep": kms32[7],
+                                         "axpy": kms32[4], "scale_add": kms32[5],
+                                         "init_forward_sweep": kms32[1]},
+                "kernel_ms_fp32_standard_step": {"forward_sweep": kms32[1], "backward_sweep": kms32[2],
+                                                 "spmv": kms32[3]},
                 "kernel_gbs_fp64": {"spmv": N * 49 / (kms[3] * 1e-3) / 1e9, "axpy": N * 48 / (kms[4] * 1e-3) / 1e9,
                                     "scale_add": N * 24 / (kms[5] * 1e-3) / 1e9}}
 

@@ -84,11 +84,27 @@ typedef struct {
   int precision;       /* SC_PREC_* */
   double mic_tau;      /* ModifiedIncompleteCholesky3D tuning, 0.97 (project-solver.h:83) */
   double mic_sigma;    /* ModifiedIncompleteCholesky3D safety, 0.25 (project-solver.h:84) */
-  double inner_rtol;   /* mixed: residual reduction asked of each FP32 inner solve */
-  int max_outer;       /* mixed: maximum defect-correction passes */
+  double inner_rtol;   /* mixed, SC_INNER_PCG: residual reduction asked of each FP32 inner solve */
+  int max_outer;       /* mixed: maximum defect corrections (FP64 residual replacements) */
   int check_symmetry;  /* verify A_Right(p) == A_Left(p+x) etc. on upload */
   int true_residual;   /* recompute ||b - A p|| in FP64 after the solve */
+  int inner_method;    /* mixed: SC_INNER_* iteration of the FP32 inner solve */
+  double reliable_delta; /* mixed, SC_INNER_EISENSTAT: reduction of the FP32 recursive
+                            residual between FP64 residual replacements, 0.1 */
 } sc_pcg_options;
+
+/* Iterations of the mixed solve's FP32 inner MIC(0)-PCG.  SC_INNER_PCG is the
+ * reference's iteration (SpMV, axpy, forward and backward sweep, scale-add).
+ * It restarts after each FP64 defect correction, asking each FP32 solve for a
+ * residual reduction of inner_rtol.  SC_INNER_EISENSTAT (the default) runs CG
+ * on the split system L^-1 A L^-T with Eisenstat's trick (one backward and one
+ * forward sweep apply the operator, so the iteration has no SpMV) and never
+ * restarts: whenever its recursive residual has dropped by reliable_delta, the
+ * FP32 correction is added to the FP64 solution, the residual is recomputed in
+ * FP64 and replaces the FP32 one, and the search direction is kept.  Values of
+ * reliable_delta much below 0.01 let the FP32 recursion drift too far between
+ * replacements.  Both stop on the FP64 residual's test (criterion, tol). */
+enum { SC_INNER_PCG = 0, SC_INNER_EISENSTAT = 1 };
 
 typedef struct {
   int iterations;        /* FP64: the reference's `iter` counter; mixed: inner iterations */
@@ -142,10 +158,11 @@ int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b);
 
 /* Per-kernel device time of the solver's kernels on the uploaded system (each
  * kernel launched `reps` times, CUDA events on the context stream), in ms per
- * launch: [0] pivot sweep, [1] forward sweep, [2] backward sweep, [3] SpMV,
- * [4] axpy pair, [5] scale-and-add.  With SC_PREC_MIXED (after a solve) [1]-[5]
- * are the FP32 kernels the inner solve iterates with.  For profiling; leaves
- * the solution untouched. */
+ * launch, into ms_out[8]: [0] pivot sweep, [1] forward sweep, [2] backward
+ * sweep, [3] SpMV, [4] axpy pair, [5] scale-and-add, [6] backward sweep without
+ * the dot product and [7] fused forward sweep of the Eisenstat inner iteration.
+ * With SC_PREC_MIXED (after a solve) [1]-[7] are FP32 kernels; otherwise [6]
+ * and [7] are 0.  For profiling; leaves the solution untouched. */
 int sc_pcg_time_kernels(sc_pcg* pcg, int reps, double* ms_out);
 
 /* Allocation-free ModifiedIncompleteCholesky3D::precond(Adiag, Aneighbour, r,

@@ -15,7 +15,8 @@ P = ctypes.POINTER
 class sc_pcg_options(ctypes.Structure):
     _fields_ = [("tol", c_double), ("max_iter", c_int), ("criterion", c_int), ("precision", c_int),
                 ("mic_tau", c_double), ("mic_sigma", c_double), ("inner_rtol", c_double),
-                ("max_outer", c_int), ("check_symmetry", c_int), ("true_residual", c_int)]
+                ("max_outer", c_int), ("check_symmetry", c_int), ("true_residual", c_int),
+                ("inner_method", c_int), ("reliable_delta", c_double)]
 
 
 class sc_pcg_stats(ctypes.Structure):
@@ -56,6 +57,7 @@ class sc_diff_config(ctypes.Structure):
 SC_OK = 0
 SC_CRIT_ABS_LINF, SC_CRIT_REL_L2 = 0, 1
 SC_PREC_FP64, SC_PREC_MIXED = 0, 1
+SC_INNER_PCG, SC_INNER_EISENSTAT = 0, 1
 SC_REAL_F64, SC_REAL_F32 = 0, 1
 SC_DONE_CONVERGED, SC_DONE_MAXITER, SC_DONE_BREAKDOWN = 1, 2, 3
 SC_ADVECT_PIC, SC_ADVECT_FLIP = 0, 1

@@ -62,6 +62,8 @@ sc::PcgOptions to_internal(const sc_pcg_options* o) {
   p.max_outer = o->max_outer;
   p.check_symmetry = o->check_symmetry;
   p.true_residual = o->true_residual;
+  p.inner_method = o->inner_method;
+  p.reliable_delta = o->reliable_delta;
   return p;
 }
 
@@ -82,7 +84,8 @@ void to_public(const sc::PcgStats& s, sc_pcg_stats* o) {
 int validate_options(const sc_pcg_options* o) {
   if (!o) return SC_OK;
   if (!(o->tol >= 0.0) || o->max_iter < 1 || o->criterion < 0 || o->criterion > 1 ||
-      o->precision < 0 || o->precision > 1 || !(o->inner_rtol > 0.0) || o->max_outer < 1)
+      o->precision < 0 || o->precision > 1 || !(o->inner_rtol > 0.0) || o->max_outer < 1 ||
+      o->inner_method < 0 || o->inner_method > 1 || !(o->reliable_delta > 0.0 && o->reliable_delta < 1.0))
     return SC_ERR_INVALID;
   return SC_OK;
 }
@@ -171,6 +174,8 @@ void sc_pcg_default_options(sc_pcg_options* o) {
   o->max_outer = d.max_outer;
   o->check_symmetry = d.check_symmetry;
   o->true_residual = d.true_residual;
+  o->inner_method = d.inner_method;
+  o->reliable_delta = d.reliable_delta;
 }
 
 int sc_pcg_create(sc_context* ctx, int nx, int ny, int nz, const sc_pcg_options* opt,

@@ -33,10 +33,27 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kRing = 32;     // boundary ring entries per wavefront CTA
-constexpr int kStage = 8;     // steps of input staged ahead per compute warp (cp.async ring)
+#ifndef SC_WAVE_STAGE_MAX
+#define SC_WAVE_STAGE_MAX 8
+#endif
+// Bytes per cp.async chunk of the staged sweep input (4, 8 or 16); 8 measured
+// best for both precisions at 128^3 and 512^3 (16 costs FP64 sweeps ~4%).
+#ifndef SC_WAVE_CHUNK64
+#define SC_WAVE_CHUNK64 8
+#endif
+#ifndef SC_WAVE_CHUNK32
+#define SC_WAVE_CHUNK32 8
+#endif
+// Ring slots of staged sweep input (steps in flight per compute warp): as many
+// as fit in ~180 KB of shared memory, at most SC_WAVE_STAGE_MAX.
+template <class T, int NV>
+constexpr int wave_stages() {
+  constexpr int fit = (int)(180 * 1024 / ((size_t)Tiled::TY * NV * 32 * sizeof(T)));
+  return fit < SC_WAVE_STAGE_MAX ? fit : SC_WAVE_STAGE_MAX;
+}
 constexpr int kSpinLimit = 1 << 22;  // bounded waits: ~0.1-1 s, far above any legitimate wait
 
-enum { FIN_NONE = 0, FIN_INIT, FIN_SPMV, FIN_AXPY, FIN_BWD, FIN_SA, FIN_NORMS };
+enum { FIN_NONE = 0, FIN_INIT, FIN_SPMV, FIN_AXPY, FIN_BWD, FIN_SA, FIN_NORMS, FIN_EINIT, FIN_EAXPY, FIN_EREPLACE };
 
 __device__ void finalize(int kind, PcgScalars* sc, double sum, double mx) {
   switch (kind) {
@@ -106,6 +123,46 @@ __device__ void finalize(int kind, PcgScalars* sc, double sum, double mx) {
     case FIN_NORMS: {
       sc->rn2 = sum;
       sc->rinf = mx;
+      break;
+    }
+    // Eisenstat iteration (FP32 inner solve): the residual of the split system is
+    // rh = L^-1 r, rho = rh.rh = r.M^-1 r plays sigma's part and the stopping
+    // measure is ||rh|| / ||rh_0||.
+    case FIN_EINIT: {  // rho_0 = rh_0.rh_0
+      sc->sigma = sum;
+      sc->bnorm = sqrt(sum);
+      sc->first = 0;
+      if (!isfinite(sum)) {
+        sc->err |= DEV_ERR_NONFINITE;
+        sc->done = DONE_BREAKDOWN;
+      } else if (sum == 0.0 && sc->done == DONE_RUNNING) {
+        sc->done = DONE_CONVERGED;
+        sc->iter = 0;
+      }
+      break;
+    }
+    case FIN_EREPLACE: {  // rh replaced by L^-1 of the FP64 residual: rho = rh.rh
+      sc->sigma = sum;
+      sc->res = sc->bnorm > 0.0 ? sqrt(sum) / sc->bnorm : 0.0;
+      if (!isfinite(sum)) {
+        sc->err |= DEV_ERR_NONFINITE;
+        sc->done = DONE_BREAKDOWN;
+      }
+      break;
+    }
+    case FIN_EAXPY: {  // rho_new; convergence; beta = rho_new / rho
+      sc->rn2 = sum;
+      sc->rinf = mx;
+      const double res = sc->bnorm > 0.0 ? sqrt(sum) / sc->bnorm : 0.0;
+      sc->res = res;
+      if (!isfinite(res)) {
+        sc->err |= DEV_ERR_NONFINITE;
+        sc->done = DONE_BREAKDOWN;
+      } else if (res < sc->tol) {
+        sc->done = DONE_CONVERGED;
+      }
+      sc->beta = sum / sc->sigma;
+      sc->sigma = sum;
       break;
     }
     default:
@@ -237,7 +294,8 @@ template <class T>
 __global__ void __launch_bounds__(kThreads) k_init(Tiled g, const double* __restrict__ src,
                                                    double scale, const uint8_t* __restrict__ act,
                                                    T* __restrict__ r, T* __restrict__ p,
-                                                   double* partials, PcgScalars* sc) {
+                                                   double* partials, PcgScalars* sc,
+                                                   int fin = FIN_INIT) {
   double s2 = 0.0, mx = 0.0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.total; e += stride) {
@@ -248,7 +306,7 @@ __global__ void __launch_bounds__(kThreads) k_init(Tiled g, const double* __rest
     s2 += dv * dv;
     mx = fmax(mx, fabs(dv));
   }
-  reduce_finalize(s2, mx, partials, sc, FIN_INIT);
+  reduce_finalize(s2, mx, partials, sc, fin);
 }
 
 template <class T>
@@ -404,7 +462,7 @@ template <class T>
 __global__ void __launch_bounds__(kThreads)
     k_axpy(int64_t n, const uint8_t* __restrict__, const T* __restrict__ s,
            const T* __restrict__ Az, T* __restrict__ p, T* __restrict__ r, double* partials,
-           PcgScalars* sc) {
+           PcgScalars* sc, int fin = FIN_AXPY) {
   if (sc->done != DONE_RUNNING) return;
   const T alpha = (T)sc->alpha;
   double s2 = 0.0, mx = 0.0;
@@ -432,7 +490,7 @@ __global__ void __launch_bounds__(kThreads)
       mx = fmax(mx, fabs(dv));
     }
   }
-  reduce_finalize(s2, mx, partials, sc, FIN_AXPY);
+  reduce_finalize(s2, mx, partials, sc, fin);
 }
 
 // scaleAndAdd(s, z, beta): s = z + beta s (util.cc:404-410); z and s are zero
@@ -479,6 +537,20 @@ __global__ void __launch_bounds__(kThreads)
     uR[c.e] = a;
     uU[c.e] = b;
     uF[c.e] = d;
+  }
+}
+
+// Diagonals of the Eisenstat operator (FwdEisenstatOp), from the FP64 pivots:
+// Pinv = 1/E and Dt = 2/E^2 - Adiag where E != 0, else 0.
+__global__ void __launch_bounds__(kThreads)
+    k_eisenstat_diag(int64_t n, const double* __restrict__ E, const double* __restrict__ adiag,
+                     float* __restrict__ pinv, float* __restrict__ dt) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+    const double v = E[e];
+    const double pi = v != 0.0 ? 1.0 / v : 0.0;
+    pinv[e] = (float)pi;
+    dt[e] = v != 0.0 ? (float)(2.0 * pi * pi - adiag[e]) : 0.0f;
   }
 }
 
@@ -540,33 +612,67 @@ __global__ void __launch_bounds__(kThreads)
 // Cell operations of the three sweeps.  Each reads NV arrays at its own cell
 // (staged into shared memory by cp.async) plus the three already-computed
 // neighbour values xn, yn, zn.
-template <class T>
-struct FwdOp {  // L q = r (project-solver.cc:276-288), c* = A_* E(neighbour)
+// compute() returns the value the recurrence passes on to the neighbours and
+// stores the op's outputs at element e itself.
+template <class T, bool SELFDOT = false>
+struct FwdOp {  // L q = r (project-solver.cc:276-288), c* = A_* E(neighbour); SELFDOT: acc q.q
   static constexpr int NV = 5;
   const T* src[NV];  // r, cL, cD, cB, E
   T* out;            // q
-  __device__ __forceinline__ T compute(const T* v, T xn, T yn, T zn, int64_t, double&) const {
+  __device__ __forceinline__ T compute(const T* v, T xn, T yn, T zn, int64_t e, double& acc) const {
     T t = v[0];
     t -= v[1] * xn;
     t -= v[2] * yn;
     t -= v[3] * zn;
-    return t * v[4];
+    const T q = t * v[4];
+    out[e] = q;
+    if (SELFDOT) acc += (double)q * (double)q;
+    return q;
   }
 };
 
-template <class T>
-struct BwdOp {  // L^T z = q (project-solver.cc:293-305), u* = A_*(p+dir) E(p); sigma = z.r
-  static constexpr int NV = 6;
-  const T* src[NV];  // q, E, uR, uU, uF, r
+template <class T, bool DOT = true>
+struct BwdOp {  // L^T z = q (project-solver.cc:293-305), u* = A_*(p+dir) E(p); DOT: sigma = z.r
+  static constexpr int NV = DOT ? 6 : 5;
+  const T* src[NV];  // q, E, uR, uU, uF (, r)
   T* out;            // z
-  __device__ __forceinline__ T compute(const T* v, T xn, T yn, T zn, int64_t, double& acc) const {
+  __device__ __forceinline__ T compute(const T* v, T xn, T yn, T zn, int64_t e, double& acc) const {
     T t = v[0];
     t -= v[2] * xn;
     t -= v[3] * yn;
     t -= v[4] * zn;
     T z = t * v[1];
-    acc += (double)z * (double)v[5];
+    out[e] = z;
+    if constexpr (DOT) acc += (double)z * (double)v[5];
     return z;
+  }
+};
+
+// Eisenstat's form of the preconditioned operator (S. C. Eisenstat, "Efficient
+// implementation of a class of preconditioned conjugate gradient methods",
+// SIAM J. Sci. Stat. Comput. 2 (1981) 1-4).  With the MIC(0) factor
+// L = (P^-2 + F) P (P = diag(E), F the strictly lower part of A) and
+// A = K + K^T - Dt, K = P^-2 + F, Dt = 2 P^-2 - diag(A), the split operator is
+//   L^-1 A L^-T v = P^-1 t + L^-1 (P^-1 v - Dt t),   t = L^-T v,
+// so one backward sweep (t) and this forward sweep apply it: no SpMV.  The
+// recurrence carries q = L^-1 (P^-1 v - Dt t); the output is w = P^-1 t + q
+// and acc gathers v.w.  Pinv = 1/E and Dt are 0 on cells where E = 0.
+template <class T>
+struct FwdEisenstatOp {
+  static constexpr int NV = 8;
+  const T* src[NV];  // v, t, Pinv, Dt, cL, cD, cB, E
+  T* out;            // w
+  __device__ __forceinline__ T compute(const T* v, T xn, T yn, T zn, int64_t e, double& acc) const {
+    T u = v[2] * v[0];
+    u -= v[3] * v[1];
+    u -= v[4] * xn;
+    u -= v[5] * yn;
+    u -= v[6] * zn;
+    const T q = u * v[7];
+    const T w = v[2] * v[1] + q;
+    out[e] = w;
+    acc += (double)v[0] * (double)w;
+    return q;
   }
 };
 
@@ -601,6 +707,7 @@ struct PivotOp {
       if (ee < sigma * adiag) ee = adiag;
       E = 1.0 / sqrt(ee);
     }
+    out[e] = E;
     cL[e] = al * EL;
     cD[e] = ad * ED;
     cB[e] = ab * EB;
@@ -718,13 +825,15 @@ __device__ __forceinline__ void mb_reset(T* p) {
   mb_store_bits(p, Sentinel<T>::bits);
 }
 
-__device__ __forceinline__ void cp_async_elem(double* dst, const double* src) {
+// B-byte copy global -> shared (B = 4, 8 or 16; both addresses B-byte aligned);
+// 16-byte copies bypass L1.
+template <int B, class T>
+__device__ __forceinline__ void cp_async_bytes(T* dst, const T* src) {
   unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_elem(float* dst, const float* src) {
-  unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+  if constexpr (B == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(B) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -959,22 +1068,45 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
           if (--sl < 0) sl = g.nz - 1;
         }
       };
-      // Each lane stages its own element of the NV input rows kStage steps ahead
-      // with cp.async (not waited on by the per-step barrier).
-      T* my_stage = stage + (size_t)ty * Op::NV * 32 + lane;
+      // The warp stages the NV input rows of step s + kStage - 1 into ring slot
+      // (s - 1) mod kStage at the start of step s, as kChunk-byte cp.async chunks
+      // spread over the lanes (CPL per lane, pointers fixed per tile).  The slot
+      // was last read in step s - 1, before that step's barrier; each lane waits
+      // for its own chunks of step s + 1 before the barrier of step s, and the
+      // barrier makes every lane's chunks visible to the warp.
+      constexpr int kStage = wave_stages<T, Op::NV>();
+      constexpr int kChunk = sizeof(T) == 8 ? SC_WAVE_CHUNK64 : SC_WAVE_CHUNK32;  // bytes
+      constexpr int EPC = kChunk / (int)sizeof(T);           // elements per chunk
+      constexpr int CPR = 32 / EPC;                          // chunks per row
+      constexpr int CPL = (Op::NV * CPR + 31) / 32;          // chunks per lane
       constexpr size_t kStageStride = (size_t)TY * Op::NV * 32;  // elements per ring slot
-      auto issue = [&](int sl, int ridx) {
-        const int64_t eg = rowbase + (int64_t)sl * rstride;
+      const T* my_stage = stage + (size_t)ty * Op::NV * 32 + lane;
+      const T* cg[CPL];
+      int coff[CPL];
 #pragma unroll
-        for (int k = 0; k < Op::NV; k++)
-          cp_async_elem(my_stage + ridx * kStageStride + k * 32, op.src[k] + eg);
+      for (int i = 0; i < CPL; i++) {
+        const int j = lane + 32 * i;
+        const int k = j / CPR, c = j - k * CPR;
+        const T* src = op.src[0];
+#pragma unroll
+        for (int kk = 1; kk < Op::NV; kk++)
+          if (k == kk) src = op.src[kk];
+        cg[i] = j < Op::NV * CPR ? src + base + (int64_t)ty * 32 + c * EPC : nullptr;
+        coff[i] = (ty * Op::NV + k) * 32 + c * EPC;
+      }
+      auto issue = [&](int sl, int ridx) {
+        const int64_t so = (int64_t)sl * rstride;
+#pragma unroll
+        for (int i = 0; i < CPL; i++)
+          if (Op::NV * CPR % 32 == 0 || cg[i]) cp_async_bytes<kChunk>(stage + ridx * kStageStride + coff[i], cg[i] + so);
       };
 #pragma unroll
-      for (int r = 0; r < kStage; r++) {
+      for (int r = 0; r < kStage - 1; r++) {
         if (r < NS) issue(pslot, r);
         cp_async_commit();
         advance(pslot);
       }
+      cp_async_wait<kStage - 2>();
       T prev = T(0);
       named_bar_sync(1, NBAR);
       for (int s0 = 0; s0 < NS; s0 += kStage) {
@@ -982,13 +1114,12 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
         for (int u = 0; u < kStage; u++) {
           const int s = s0 + u;
           if (s < NS) {
-            cp_async_wait<kStage - 1>();
+            if (s + kStage - 1 < NS) issue(pslot, (u + kStage - 1) % kStage);
+            cp_async_commit();
+            advance(pslot);
             T v[Op::NV];
 #pragma unroll
             for (int k = 0; k < Op::NV; k++) v[k] = my_stage[u * kStageStride + k * 32];
-            if (s + kStage < NS) issue(pslot, u);
-            cp_async_commit();
-            advance(pslot);
             const int z = FWD ? (s - ty - lane) : (g.nz - 1 - (s - (TY - 1 - ty) - (31 - lane)));
             const bool valid = (z >= 0) && (z < g.nz);
             const T shv = FWD ? __shfl_up_sync(kFull, prev, 1) : __shfl_down_sync(kFull, prev, 1);
@@ -1004,13 +1135,13 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
             if (valid) {
               const int64_t e = rowbase + (int64_t)cslot * rstride;
               val = op.compute(v, xn, yn, prev, e, acc);
-              op.out[e] = val;
               if (xsrc && outx) mb_store(outx + (int64_t)(s - 31) * TY + ty, val);
               if (ysrc && outy) mb_store(outy + (int64_t)(s - (TY - 1)) * 32 + lane, val);
             }
             sh.xch[s & 1][ty][lane] = val;
             prev = val;
             advance(cslot);
+            cp_async_wait<kStage - 2>();
             named_bar_sync(1, NBAR);
           }
         }
@@ -1056,7 +1187,7 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
 
 template <class T, bool FWD, class Op>
 constexpr size_t wave_dyn_smem() {
-  return sizeof(T) * (size_t)kStage * Tiled::TY * Op::NV * 32;
+  return sizeof(T) * (size_t)wave_stages<T, Op::NV>() * Tiled::TY * Op::NV * 32;
 }
 template <class T, bool FWD, class Op>
 void wave_set_attr() {
@@ -1099,12 +1230,12 @@ inline int grid_for(int64_t n, int sm) {
 // PcgSolver (host)
 
 template <>
-cudaGraphExec_t& PcgSolver::graph_for<double>() {
+cudaGraphExec_t& PcgSolver::graph_for<double>(bool) {
   return graph64_;
 }
 template <>
-cudaGraphExec_t& PcgSolver::graph_for<float>() {
-  return graph32_;
+cudaGraphExec_t& PcgSolver::graph_for<float>(bool eis) {
+  return eis ? graph32e_ : graph32_;
 }
 
 void PcgSolver::reset_mailboxes(bool f32) {
@@ -1150,14 +1281,18 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
   wave_set_attr<double, false, BwdOp<double>>();
   wave_set_attr<float, true, FwdOp<float>>();
   wave_set_attr<float, false, BwdOp<float>>();
+  wave_set_attr<float, true, FwdOp<float, true>>();
+  wave_set_attr<float, false, BwdOp<float, false>>();
+  wave_set_attr<float, true, FwdEisenstatOp<float>>();
   nblocks_ = ctx->sm_count * 8;
   const int ntiles = g_.ntiles();
   wave_grid_ = std::min(ntiles, ctx->sm_count);
   {
     const int occ64 = std::min(wave_occupancy<double, true, FwdOp<double>>(),
                                wave_occupancy<double, false, BwdOp<double>>());
-    const int occ32 = std::min(wave_occupancy<float, true, FwdOp<float>>(),
-                               wave_occupancy<float, false, BwdOp<float>>());
+    const int occ32 = std::min({wave_occupancy<float, true, FwdOp<float>>(),
+                                wave_occupancy<float, false, BwdOp<float>>(),
+                                wave_occupancy<float, true, FwdEisenstatOp<float>>()});
     wave_grid64_ = std::min(ntiles, ctx->sm_count * occ64);
     wave_grid32_ = std::min(ntiles, ctx->sm_count * occ32);
   }
@@ -1231,6 +1366,7 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
 PcgSolver::~PcgSolver() {
   if (graph64_) cudaGraphExecDestroy(graph64_);
   if (graph32_) cudaGraphExecDestroy(graph32_);
+  if (graph32e_) cudaGraphExecDestroy(graph32e_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (evt0_) cudaEventDestroy(evt0_);
@@ -1373,9 +1509,10 @@ int PcgSolver::ensure_pivots() {
   if (opt_.precision == PREC_MIXED) {
     if (!have_f32_) {
       const size_t n32 = sizeof(float) * (size_t)g_.total;
-      float** arr32[] = {&d32_.adiag, &d32_.al, &d32_.ad, &d32_.ab, &d32_.E, &d32_.cL,
-                         &d32_.cD,    &d32_.cB, &d32_.uR, &d32_.uU, &d32_.uF, &d32_.r,
-                         &d32_.p,     &d32_.z,  &d32_.s,  &d32_.q,  &d32_.Az};
+      float** arr32[] = {&d32_.adiag, &d32_.al, &d32_.ad, &d32_.ab, &d32_.E,    &d32_.cL,
+                         &d32_.cD,    &d32_.cB, &d32_.uR, &d32_.uU, &d32_.uF,   &d32_.r,
+                         &d32_.p,     &d32_.z,  &d32_.s,  &d32_.q,  &d32_.Az,   &d32_.Pinv,
+                         &d32_.Dt};
       for (float** a : arr32) {
         void* p = nullptr;
         if (cudaMalloc(&p, n32) != cudaSuccess) return ctx_->set_error(-3, "FP32 allocation failed");
@@ -1406,7 +1543,8 @@ int PcgSolver::ensure_pivots() {
                     d32_.cD,    d32_.cB, d32_.uR, d32_.uU, d32_.uF};
     for (int i = 0; i < 11; i++)
       k_convert<double, float><<<grid, kThreads, 0, st>>>(g_.total, s64[i], d32[i]);
-    launches_ += 11;
+    k_eisenstat_diag<<<grid, kThreads, 0, st>>>(g_.total, d64_.E, d64_.adiag, d32_.Pinv, d32_.Dt);
+    launches_ += 12;
   }
   int e = check_dev_error("pivots");
   if (e) return e;
@@ -1421,14 +1559,29 @@ void PcgSolver::launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip) {
 }
 
 template <class T>
-void PcgSolver::launch_iteration(SysArrays<T>& A) {
+void PcgSolver::launch_iteration(SysArrays<T>& A, bool eis) {
   cudaStream_t st = ctx_->stream;
   const bool f32 = sizeof(T) == 4;
+  const int wg = sizeof(T) == 4 ? wave_grid32_ : wave_grid64_;
+  if constexpr (sizeof(T) == 4) {
+    if (eis) {
+      // CG on L^-1 A L^-T: s = ph (search direction), z = t = L^-T ph,
+      // Az = w = L^-1 A L^-T ph, q = rh (split residual), p = x.
+      BwdOp<T, false> bo{{A.s, A.E, A.uR, A.uU, A.uF}, A.z};
+      launch_wave<T, false>(wave_args(true, 1, FIN_NONE), bo, st, wg);
+      FwdEisenstatOp<T> fo{{A.s, A.z, A.Pinv, A.Dt, A.cL, A.cD, A.cB, A.E}, A.Az};
+      launch_wave<T, true>(wave_args(true, 1, FIN_SPMV), fo, st, wg);  // alpha = rho / ph.w
+      // x += alpha t ; rh -= alpha w ; beta = rho_new / rho
+      k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.Az, A.p, A.q, partials_, sc_,
+                                               FIN_EAXPY);
+      k_sa<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.q, A.s, partials_, sc_);
+      return;
+    }
+  }
   WaveArgs wf = wave_args(f32, 1, FIN_NONE);
   WaveArgs wb = wave_args(f32, 1, FIN_BWD);
   launch_spmv<T>(A, st, 1);
   k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.s, A.Az, A.p, A.r, partials_, sc_);
-  const int wg = sizeof(T) == 4 ? wave_grid32_ : wave_grid64_;
   FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
   launch_wave<T, true>(wf, fo, st, wg);
   BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
@@ -1436,9 +1589,33 @@ void PcgSolver::launch_iteration(SysArrays<T>& A) {
   k_sa<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.s, partials_, sc_);
 }
 
+// A CUDA graph of `chunk` iterations, captured on first use.  The legacy
+// default stream cannot be captured: the graph stays null then and callers
+// launch the same kernels directly.
+template <class T>
+int PcgSolver::ensure_graph(SysArrays<T>& A, bool eis) {
+  cudaGraphExec_t& gx = graph_for<T>(eis);
+  if (gx) return 0;
+  cudaStream_t s = ctx_->stream;
+  cudaGraph_t graph = nullptr;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  for (int i = 0; i < opt_.chunk; i++) launch_iteration<T>(A, eis);
+  if (cudaStreamEndCapture(s, &graph) != cudaSuccess || !graph) return check_dev_error("end capture");
+  if (cudaGraphInstantiate(&gx, graph, 0) != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    gx = nullptr;
+    return check_dev_error("instantiate");
+  }
+  cudaGraphDestroy(graph);
+  return 0;
+}
+
 template <class T>
 int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter, bool scale_rhs,
-                       PcgStats* st) {
+                       PcgStats* st, bool eis) {
   cudaStream_t s = ctx_->stream;
   // scalars
   PcgScalars init{};
@@ -1452,38 +1629,31 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
   const double* src = scale_rhs ? d64_.r : rhs_;
   const double scale = scale_rhs ? 1.0 / inner_scale_ : 1.0;
   k_init<T><<<nblocks_, kThreads, 0, s>>>(g_, src, scale, active_, A.r, A.p, partials_, sc_);
-  // z = M^-1 r ; s = z ; sigma = z.r
   const bool f32 = sizeof(T) == 4;
-  WaveArgs wf = wave_args(f32, 1, FIN_NONE);
-  WaveArgs wb = wave_args(f32, 1, FIN_BWD);
   const int wg = sizeof(T) == 4 ? wave_grid32_ : wave_grid64_;
-  FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
-  launch_wave<T, true>(wf, fo, s, wg);
-  BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
-  launch_wave<T, false>(wb, bo, s, wg);
-  k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.z, A.s, sc_);
-  launches_ += 4;
+  eis = eis && f32;
+  if (eis) {
+    // rh = L^-1 r ; s = rh ; rho = rh.rh
+    if constexpr (sizeof(T) == 4) {
+      FwdOp<T, true> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
+      launch_wave<T, true>(wave_args(true, 1, FIN_EINIT), fo, s, wg);
+    }
+    k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.q, A.s, sc_);
+  } else {
+    // z = M^-1 r ; s = z ; sigma = z.r
+    FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
+    launch_wave<T, true>(wave_args(f32, 1, FIN_NONE), fo, s, wg);
+    BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
+    launch_wave<T, false>(wave_args(f32, 1, FIN_BWD), bo, s, wg);
+    k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.z, A.s, sc_);
+  }
+  launches_ += eis ? 3 : 4;
   int e = check_dev_error("pcg init");
   if (e) return e;
-  // graph of `chunk` iterations
-  cudaGraphExec_t& gx = graph_for<T>();
-  if (!gx) {
-    // The legacy default stream cannot be captured: launch the chunk's kernels
-    // directly then (same kernels, same order).
-    cudaGraph_t graph = nullptr;
-    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      for (int i = 0; i < opt_.chunk; i++) launch_iteration<T>(A);
-      if (cudaStreamEndCapture(s, &graph) != cudaSuccess || !graph) return check_dev_error("end capture");
-      if (cudaGraphInstantiate(&gx, graph, 0) != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        gx = nullptr;
-        return check_dev_error("instantiate");
-      }
-      cudaGraphDestroy(graph);
-    } else {
-      cudaGetLastError();
-    }
-  }
+  e = ensure_graph<T>(A, eis);
+  if (e) return e;
+  cudaGraphExec_t gx = graph_for<T>(eis);
+  const int per_iter = eis ? 4 : 5;
   // launch chunks, two in flight, until the device reports done
   const int max_chunks = max_iter / std::max(1, opt_.chunk) + 3;
   cudaEvent_t evs[2] = {ev0_, ev1_};
@@ -1492,8 +1662,8 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
     if (gx)
       cudaGraphLaunch(gx, s);
     else
-      for (int i = 0; i < opt_.chunk; i++) launch_iteration<T>(A);
-    launches_ += 5 * (uint64_t)opt_.chunk;
+      for (int i = 0; i < opt_.chunk; i++) launch_iteration<T>(A, eis);
+    launches_ += per_iter * (uint64_t)opt_.chunk;
     cudaMemcpyAsync(&sc_host_[c & 1], sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(evs[c & 1], s);
   };
@@ -1524,9 +1694,134 @@ int PcgSolver::solve_fp64(PcgStats* st) {
   return run_pcg<double>(d64_, opt_.tol, opt_.criterion, opt_.max_iter, false, st);
 }
 
+// Mixed precision with reliable updates: FP32 CG on the split system
+// L^-1 A L^-T (Eisenstat's iteration) that never restarts, with the FP64
+// solution and residual carried beside it.  After each graph chunk the host
+// reads the recursive split residual ||rh|| / ||rh_0||; once it has dropped by
+// reliable_delta since the last update (or predicts convergence), the FP32
+// correction d is folded into the FP64 state, x += scale d, r -= scale A d,
+// and the split residual is replaced by L^-1 r / scale, keeping the search
+// direction (residual replacement in the manner of H. A. van der Vorst and
+// Q. Ye, "Residual replacement strategies for Krylov subspace iterative methods
+// for the convergence of true residuals", SIAM J. Sci. Comput. 22 (2000)).
+// The solve stops when the FP64 residual meets the stopping test.  Replacing
+// the residual breaks the identity rh.s = rh.rh that CG's step length relies
+// on, so an update that did not lower the FP64 residual, or a recursion whose
+// residual grew a hundredfold, restarts the search direction (s = rh).
+int PcgSolver::solve_mixed_reliable(PcgStats* st) {
+  int e = ensure_pivots();
+  if (e) return e;
+  cudaStream_t s = ctx_->stream;
+  const int grid = grid_for(g_.total, ctx_->sm_count);
+  SysArrays<float>& A = d32_;
+  const int wg = wave_grid32_;
+  // x = 0 ; r = b (FP64)
+  k_fill<double><<<grid, kThreads, 0, s>>>(g_.total, xacc_, 0.0);
+  PcgScalars init{};
+  init.tol = 0.0;  // the FP32 recursion never stops itself
+  init.max_iter = opt_.max_iter;
+  init.criterion = CRIT_REL_L2;
+  init.done = DONE_RUNNING;
+  cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
+  k_init<double><<<nblocks_, kThreads, 0, s>>>(g_, rhs_, 1.0, active_, d64_.r, d64_.p, partials_, sc_,
+                                               FIN_NORMS);
+  launches_ += 2;
+  cudaMemcpyAsync(sc_host_, sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("mixed init");
+  const bool abs_crit = opt_.criterion == CRIT_ABS_LINF;
+  const double bnorm = sqrt(sc_host_->rn2);
+  double meas = abs_crit ? sc_host_->rinf : (bnorm > 0 ? 1.0 : 0.0);
+  int updates = 0, status = DONE_RUNNING, iters = 0;
+  unsigned flags = 0;
+  if (meas < opt_.tol) status = DONE_CONVERGED;
+  const double scale = bnorm;
+  if (status == DONE_RUNNING) {
+    // d = 0 ; r32 = r / scale ; rh = L^-1 r32 ; s = rh ; rho = rh.rh
+    k_init<float><<<nblocks_, kThreads, 0, s>>>(g_, d64_.r, 1.0 / scale, active_, A.r, A.p, partials_, sc_);
+    FwdOp<float, true> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
+    launch_wave<float, true>(wave_args(true, 1, FIN_EINIT), fo, s, wg);
+    k_copy<float><<<nblocks_, kThreads, 0, s>>>(g_.total, A.q, A.s, sc_);
+    launches_ += 3;
+    e = ensure_graph<float>(A, true);
+    if (e) return e;
+  }
+  cudaGraphExec_t gx = graph_for<float>(true);
+  cudaEvent_t evs[2] = {ev0_, ev1_};
+  auto launch_chunk = [&](int slot) {
+    if (gx)
+      cudaGraphLaunch(gx, s);
+    else
+      for (int i = 0; i < opt_.chunk; i++) launch_iteration<float>(A, true);
+    launches_ += 4 * (uint64_t)opt_.chunk;
+    cudaMemcpyAsync(&sc_host_[slot], sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(evs[slot], s);
+  };
+  double res_u = 1.0, meas_u = meas;  // split and stopping residuals at the last update
+  const int max_chunks = opt_.max_iter / std::max(1, opt_.chunk) + 3;
+  int launched = 0, seen = 0;
+  while (status == DONE_RUNNING) {
+    // keep two chunks in flight; look at the older one
+    while (launched - seen < 2 && launched < max_chunks) launch_chunk(launched++ & 1);
+    if (seen == launched) {
+      status = DONE_MAXITER;
+      break;
+    }
+    if (cudaEventSynchronize(evs[seen & 1]) != cudaSuccess) return check_dev_error("mixed chunk");
+    const PcgScalars h = sc_host_[seen & 1];
+    seen++;
+    const bool dev_stop = h.done != DONE_RUNNING || launched >= max_chunks;
+    const double predicted = meas_u * h.res / res_u;
+    const bool grew = !(h.res <= 100.0 * res_u);
+    if (!(dev_stop || grew || h.res < opt_.reliable_delta * res_u || predicted < 0.5 * opt_.tol)) continue;
+    // residual replacement after the chunks in flight
+    if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("mixed chunk");
+    seen = launched;
+    k_mixed_update<<<nblocks_, kThreads, 0, s>>>(g_, d64_.adiag, d64_.al, d64_.ad, d64_.ab, active_, A.p,
+                                                 scale, xacc_, d64_.r, partials_, sc_);
+    k_init<float><<<nblocks_, kThreads, 0, s>>>(g_, d64_.r, 1.0 / scale, active_, A.r, A.p, partials_, sc_,
+                                                FIN_NONE);
+    FwdOp<float, true> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
+    launch_wave<float, true>(wave_args(true, 0, FIN_EREPLACE), fo, s, wg);
+    launches_ += 3;
+    cudaMemcpyAsync(&sc_host_[0], sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("mixed update");
+    const PcgScalars u = sc_host_[0];
+    updates++;
+    iters = u.iter;
+    flags |= u.err;
+    const double rel = bnorm > 0 ? sqrt(u.rn2) / bnorm : 0.0;
+    meas = abs_crit ? u.rinf : rel;
+    if (!std::isfinite(rel)) return ctx_->set_error(-8, "mixed solve: non-finite residual");
+    if (u.err & DEV_ERR_TIMEOUT) return ctx_->set_error(-6, "wavefront wait timed out");
+    if (meas < opt_.tol) {
+      status = DONE_CONVERGED;
+    } else if (u.done == DONE_BREAKDOWN) {
+      status = DONE_BREAKDOWN;
+    } else if (u.done == DONE_MAXITER || launched >= max_chunks || updates >= opt_.max_outer) {
+      status = DONE_MAXITER;
+    } else if (grew || !(meas < meas_u)) {
+      k_copy<float><<<nblocks_, kThreads, 0, s>>>(g_.total, A.q, A.s, sc_);
+      launches_ += 1;
+    }
+    res_u = u.res;
+    meas_u = meas;
+  }
+  if (st) {
+    st->iterations += iters;
+    st->outer = updates;
+    st->residual = meas;
+    st->status = status;
+    st->device_flags |= flags;
+  }
+  cudaMemcpyAsync(d64_.p, xacc_, sizeof(double) * (size_t)g_.total, cudaMemcpyDeviceToDevice, s);
+  return check_dev_error("mixed");
+}
+
 int PcgSolver::solve_mixed(PcgStats* st) {
+  if (opt_.inner_method == INNER_EISENSTAT) return solve_mixed_reliable(st);
   // Defect correction: FP64 residual and solution, FP32 inner MIC-PCG whose
-  // pivots were computed in FP64.  Stops on ||b - A x||_2 / ||b||_2 < tol.
+  // pivots were computed in FP64, restarted after each correction.  Stops on
+  // the FP64 residual's stopping test.
   int e = ensure_pivots();
   if (e) return e;
   cudaStream_t s = ctx_->stream;
@@ -1554,7 +1849,8 @@ int PcgSolver::solve_mixed(PcgStats* st) {
     // the inner solve only needs to reach what is still missing (with margin)
     double want = abs_crit ? opt_.inner_rtol : std::max(opt_.inner_rtol, 0.25 * opt_.tol / rel);
     PcgStats inner{};
-    e = run_pcg<float>(d32_, std::min(want, 0.5), CRIT_REL_L2, opt_.max_iter, true, &inner);
+    e = run_pcg<float>(d32_, std::min(want, 0.5), CRIT_REL_L2, opt_.max_iter, true, &inner,
+                       opt_.inner_method == INNER_EISENSTAT);
     if (e) return e;
     if (st) {
       st->iterations += inner.iterations;
@@ -1757,6 +2053,16 @@ int PcgSolver::time_kernels(int reps, double* ms) {
       case 5:
         k_sa<T><<<nblocks_, kThreads, 0, s>>>(g_.total, active_, A.z, A.s, partials_, sc_);
         break;
+      case 6:
+        if constexpr (sizeof(T) == 4)
+          launch_wave<T, false>(wave_args(true, 0, FIN_NONE), BwdOp<T, false>{{A.s, A.E, A.uR, A.uU, A.uF}, A.z},
+                                s, wg);
+        break;
+      case 7:
+        if constexpr (sizeof(T) == 4)
+          launch_wave<T, true>(wave_args(true, 0, FIN_NONE),
+                               FwdEisenstatOp<T>{{A.s, A.z, A.Pinv, A.Dt, A.cL, A.cD, A.cB, A.E}, A.Az}, s, wg);
+        break;
     }
   };
   cudaEvent_t a, b;
@@ -1793,9 +2099,9 @@ int PcgSolver::time_kernels(int reps, double* ms) {
     cudaEventElapsedTime(&t, a, b);
     return (double)t / reps;
   };
-  for (int k = 0; k < 6; k++) {
+  for (int k = 0; k < 8; k++) {
     cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
-    ms[k] = timed(k);
+    ms[k] = (k < 6 || f32) ? timed(k) : 0.0;
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);

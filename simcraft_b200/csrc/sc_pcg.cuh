@@ -30,6 +30,7 @@ struct Context {
 
 enum { CRIT_ABS_LINF = 0, CRIT_REL_L2 = 1 };
 enum { PREC_FP64 = 0, PREC_MIXED = 1 };
+enum { INNER_PCG = 0, INNER_EISENSTAT = 1 };
 enum { DONE_RUNNING = 0, DONE_CONVERGED = 1, DONE_MAXITER = 2, DONE_BREAKDOWN = 3 };
 
 struct PcgOptions {
@@ -39,10 +40,12 @@ struct PcgOptions {
   int precision = PREC_FP64;
   double tau = 0.97, sigma = 0.25;  // project-solver.h:83-84
   double inner_rtol = 1e-4;  // mixed: relative reduction asked of each FP32 inner solve
-  int max_outer = 20;        // mixed: defect-correction passes
+  int max_outer = 50;        // mixed: defect corrections (FP64 residual replacements)
   int chunk = 8;             // PCG iterations per CUDA-graph launch
   int check_symmetry = 0;    // verify Right/Up/Front == shifted Left/Down/Back
   int true_residual = 1;     // recompute ||b - A p|| in FP64 at the end
+  int inner_method = INNER_EISENSTAT;  // mixed: iteration of the FP32 inner solve
+  double reliable_delta = 0.1;  // mixed, Eisenstat: split-residual reduction between FP64 replacements
 };
 
 struct PcgStats {
@@ -100,6 +103,7 @@ struct SysArrays {  // one precision's copy of everything the PCG touches (tiled
   T *E = nullptr, *cL = nullptr, *cD = nullptr, *cB = nullptr, *uR = nullptr, *uU = nullptr,
     *uF = nullptr;
   T *r = nullptr, *p = nullptr, *z = nullptr, *s = nullptr, *q = nullptr, *Az = nullptr;
+  T *Pinv = nullptr, *Dt = nullptr;  // Eisenstat diagonals (FP32 copy only)
 };
 
 class PcgSolver {
@@ -141,14 +145,18 @@ class PcgSolver {
 
  private:
   int ensure_pivots();
+  // eis: Eisenstat iteration (FP32 inner solve of the mixed path only)
   template <class T>
   int run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter, bool scale_rhs,
-              PcgStats* st);
+              PcgStats* st, bool eis = false);
   int solve_fp64(PcgStats* st);
   int solve_mixed(PcgStats* st);
+  int solve_mixed_reliable(PcgStats* st);
+  template <class T>
+  int ensure_graph(SysArrays<T>& A, bool eis);
   int true_residual(PcgStats* st);
   template <class T>
-  void launch_iteration(SysArrays<T>& A);
+  void launch_iteration(SysArrays<T>& A, bool eis);
   template <class T>
   void launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip);
   int check_dev_error(const char* where);
@@ -186,9 +194,9 @@ class PcgSolver {
   PcgScalars last_{};
   uint64_t launches_ = 0;  // kernels launched so far (graph nodes counted)
   // graphs: one chunk of iterations per precision
-  cudaGraphExec_t graph64_ = nullptr, graph32_ = nullptr;
+  cudaGraphExec_t graph64_ = nullptr, graph32_ = nullptr, graph32e_ = nullptr;
   template <class T>
-  cudaGraphExec_t& graph_for();
+  cudaGraphExec_t& graph_for(bool eis);
 };
 
 // Allocation-free ModifiedIncompleteCholesky3D::precond on device arrays in the

@@ -22,6 +22,7 @@ from ._capi import check, lib, ptr_array
 LEFT, RIGHT, UP, DOWN, FRONT, BACK = range(6)
 CRIT_ABS_LINF, CRIT_REL_L2 = _capi.SC_CRIT_ABS_LINF, _capi.SC_CRIT_REL_L2
 PREC_FP64, PREC_MIXED = _capi.SC_PREC_FP64, _capi.SC_PREC_MIXED
+INNER_PCG, INNER_EISENSTAT = _capi.SC_INNER_PCG, _capi.SC_INNER_EISENSTAT
 
 _contexts = {}
 

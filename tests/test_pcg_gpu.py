@@ -67,3 +67,41 @@ def test_pcg_mixed_reaches_1e10(oracle, torch_mod):
     assert st["true_rel_l2"] < 1e-10, st
     a = S["active"].astype(bool)
     assert rel_l2(pg, p_ref, a) < 1e-8
+
+
+@pytest.mark.parametrize("dims", [(32, 32, 32), (40, 20, 13), (33, 17, 40)])
+@pytest.mark.parametrize("crit,tol", [(1, 1e-10), (0, 1e-6)])
+def test_pcg_mixed_inner_methods(oracle, torch_mod, dims, crit, tol):
+    """Both FP32 inner iterations of the mixed solve (the reference's PCG step and
+    Eisenstat's split form, which applies L^-1 A L^-T with two sweeps and no
+    SpMV) meet the FP64 stopping test and agree with the oracle's solution."""
+    from simcraft_b200.solver import CgSolver3D, INNER_EISENSTAT, INNER_PCG, PREC_MIXED
+    S = poisson_system(oracle, 0, dims=dims, seed=6)
+    p_ref, _, _ = oracle.pcg_solve(S["adiag"], S["an"], S["rhs"], S["active"], tol=1e-13, max_iter=2000,
+                                   criterion=1)
+    a = S["active"].astype(bool)
+    iters = {}
+    for meth in (INNER_PCG, INNER_EISENSTAT):
+        s = CgSolver3D(*dims, tol=tol, max_iter=2000, criterion=crit, precision=PREC_MIXED, inner_method=meth)
+        pg = np.zeros(dims)
+        res = s.solve(S["adiag"], S["an"], S["rhs"], S["active"], pg)
+        st = s.last_stats
+        assert st["status"] == 1 and res < tol, st
+        if crit == 1:
+            assert st["true_rel_l2"] < tol, st
+            assert rel_l2(pg, p_ref, a) < 1e-8
+        else:
+            assert st["true_linf"] < tol, st
+        iters[meth] = st["iterations"]
+    assert iters[INNER_EISENSTAT] <= 1.3 * iters[INNER_PCG] + 5, iters
+
+
+def test_pcg_mixed_eisenstat_zero_rhs(oracle, torch_mod):
+    from simcraft_b200.solver import CgSolver3D, CRIT_REL_L2, PREC_MIXED
+    n = 24
+    S = poisson_system(oracle, n, seed=2)
+    s = CgSolver3D(n, n, n, tol=1e-8, max_iter=100, criterion=CRIT_REL_L2, precision=PREC_MIXED)
+    pg = np.full((n, n, n), 7.0)
+    s.solve(S["adiag"], S["an"], np.zeros((n, n, n)), S["active"], pg)
+    assert s.last_stats["status"] == 1 and s.last_stats["iterations"] == 0
+    assert not pg[S["active"].astype(bool)].any()

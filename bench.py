@@ -496,11 +496,11 @@ def main():
     kms32 = list(kt32)
     pk, pk_src = peaks()
     # The headline (mixed) solve iterates Eisenstat's form in FP32; its top
-    # kernel is the fused forward sweep: v, t, Pinv, Dt, cL, cD, cB, E read and
-    # w written, 4 bytes each.  Its backward sweep reads v, E, uR, uU, uF and
-    # writes t.
+    # kernel is the fused forward sweep: s, t, Pinv, Dt, cL, cD, cB, E read and
+    # w written, 4 bytes each.  Its backward sweep reads rh, s, E, uR, uU, uF and
+    # writes s and t.
     bytes_fwde32 = N * 9 * 4
-    bytes_bwde32 = N * 6 * 4
+    bytes_bwde32 = N * 8 * 4
     bytes_bwd = N * (7 * 8 + 1)
     bytes_fwd = N * (6 * 8 + 1)
     achieved = bytes_fwde32 / (kms32[7] * 1e-3) / 1e9
@@ -519,8 +519,7 @@ def main():
                               "spmv": kms[3], "axpy": kms[4], "scale_add": kms[5]},
                 "forward_sweep_gbs": bytes_fwd / (kms[1] * 1e-3) / 1e9,
                 "kernel_ms_fp32_inner": {"eisenstat_backward_sweep": kms32[6], "eisenstat_forward_sweep": kms32[7],
-                                         "axpy": kms32[4], "scale_add": kms32[5],
-                                         "init_forward_sweep": kms32[1]},
+                                         "axpy": kms32[4], "init_forward_sweep": kms32[1]},
                 "kernel_ms_fp32_standard_step": {"forward_sweep": kms32[1], "backward_sweep": kms32[2],
                                                  "spmv": kms32[3]},
                 "kernel_gbs_fp64": {"spmv": N * 49 / (kms[3] * 1e-3) / 1e9, "axpy": N * 48 / (kms[4] * 1e-3) / 1e9,

@@ -159,9 +159,10 @@ int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b);
 /* Per-kernel device time of the solver's kernels on the uploaded system (each
  * kernel launched `reps` times, CUDA events on the context stream), in ms per
  * launch, into ms_out[8]: [0] pivot sweep, [1] forward sweep, [2] backward
- * sweep, [3] SpMV, [4] axpy pair, [5] scale-and-add, [6] backward sweep without
- * the dot product and [7] fused forward sweep of the Eisenstat inner iteration.
- * With SC_PREC_MIXED (after a solve) [1]-[7] are FP32 kernels; otherwise [6]
+ * sweep, [3] SpMV, [4] axpy pair, [5] scale-and-add, and the two sweeps of the
+ * Eisenstat inner iteration: [6] backward sweep with the search-direction
+ * update, [7] fused forward sweep.  With SC_PREC_MIXED (after a solve) [1]-[7]
+ * are FP32 kernels and the mixed iteration is [6] + [7] + [4]; otherwise [6]
  * and [7] are 0.  For profiling; leaves the solution untouched. */
 int sc_pcg_time_kernels(sc_pcg* pcg, int reps, double* ms_out);
 

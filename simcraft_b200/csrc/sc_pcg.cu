@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include <mutex>
@@ -128,8 +129,9 @@ __device__ void finalize(int kind, PcgScalars* sc, double sum, double mx) {
     // Eisenstat iteration (FP32 inner solve): the residual of the split system is
     // rh = L^-1 r, rho = rh.rh = r.M^-1 r plays sigma's part and the stopping
     // measure is ||rh|| / ||rh_0||.
-    case FIN_EINIT: {  // rho_0 = rh_0.rh_0
+    case FIN_EINIT: {  // rho_0 = rh_0.rh_0 ; the first search direction is rh_0 (beta = 0)
       sc->sigma = sum;
+      sc->beta = 0.0;
       sc->bnorm = sqrt(sum);
       sc->first = 0;
       if (!isfinite(sum)) {
@@ -631,10 +633,10 @@ struct FwdOp {  // L q = r (project-solver.cc:276-288), c* = A_* E(neighbour); S
   }
 };
 
-template <class T, bool DOT = true>
-struct BwdOp {  // L^T z = q (project-solver.cc:293-305), u* = A_*(p+dir) E(p); DOT: sigma = z.r
-  static constexpr int NV = DOT ? 6 : 5;
-  const T* src[NV];  // q, E, uR, uU, uF (, r)
+template <class T>
+struct BwdOp {  // L^T z = q (project-solver.cc:293-305), u* = A_*(p+dir) E(p); sigma = z.r
+  static constexpr int NV = 6;
+  const T* src[NV];  // q, E, uR, uU, uF, r
   T* out;            // z
   __device__ __forceinline__ T compute(const T* v, T xn, T yn, T zn, int64_t e, double& acc) const {
     T t = v[0];
@@ -643,10 +645,40 @@ struct BwdOp {  // L^T z = q (project-solver.cc:293-305), u* = A_*(p+dir) E(p); 
     t -= v[4] * zn;
     T z = t * v[1];
     out[e] = z;
-    if constexpr (DOT) acc += (double)z * (double)v[5];
+    acc += (double)z * (double)v[5];
     return z;
   }
 };
+
+// Eisenstat backward sweep with the search-direction update folded in:
+//   s = rh + beta s  (scaleAndAdd of the CG step), then t = L^-T s.
+// beta comes from the device scalars, read once per CTA (prepare).
+template <class T>
+struct BwdEisenstatOp {
+  static constexpr int NV = 6;
+  const T* src[NV];  // rh, s (previous), E, uR, uU, uF
+  T* out;            // t
+  T* s_out;          // s (in place of src[1]: each element is read before it is written)
+  T beta;
+  __device__ __forceinline__ void prepare(const PcgScalars* sc) { beta = (T)sc->beta; }
+  __device__ __forceinline__ T compute(const T* v, T xn, T yn, T zn, int64_t e, double&) const {
+    const T sv = v[0] + beta * v[1];
+    s_out[e] = sv;
+    T u = sv;
+    u -= v[3] * xn;
+    u -= v[4] * yn;
+    u -= v[5] * zn;
+    const T t = u * v[2];
+    out[e] = t;
+    return t;
+  }
+};
+
+// Ops without per-launch scalars.
+template <class Op, class = void>
+struct HasPrepare : std::false_type {};
+template <class Op>
+struct HasPrepare<Op, std::void_t<decltype(std::declval<Op&>().prepare(nullptr))>> : std::true_type {};
 
 // Eisenstat's form of the preconditioned operator (S. C. Eisenstat, "Efficient
 // implementation of a class of preconditioned conjugate gradient methods",
@@ -986,7 +1018,7 @@ __device__ void wave_load_y(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int
 // One CTA per SM: the sweep is issue-bound, and capping registers for two
 // CTAs per SM measured slower at 128^3, 256^3 and 512^3.
 template <class T, int TY, bool FWD, class Op>
-__global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, const Op op) {
+__global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, const Op op_arg) {
   // warps 0..TY-1: tile rows (compute only, no fences: a fence would wait for
   // the prefetch loads in flight); warp TY: control (flags, ring waits);
   // warps TY+1, TY+2: x and y mailbox loaders.
@@ -996,6 +1028,8 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
   T* stage = reinterpret_cast<T*>(wave_dyn);  // [kStage][TY][NV][32]
   if (a.use_skip && a.sc->done != DONE_RUNNING) return;
   if (a.sc->err & DEV_ERR_TIMEOUT) return;  // an earlier sweep gave up: do not wait again
+  Op op = op_arg;
+  if constexpr (HasPrepare<Op>::value) op.prepare(a.sc);
   const Tiled& g = a.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntiles = g.ntiles();
@@ -1282,7 +1316,7 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
   wave_set_attr<float, true, FwdOp<float>>();
   wave_set_attr<float, false, BwdOp<float>>();
   wave_set_attr<float, true, FwdOp<float, true>>();
-  wave_set_attr<float, false, BwdOp<float, false>>();
+  wave_set_attr<float, false, BwdEisenstatOp<float>>();
   wave_set_attr<float, true, FwdEisenstatOp<float>>();
   nblocks_ = ctx->sm_count * 8;
   const int ntiles = g_.ntiles();
@@ -1292,7 +1326,8 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
                                wave_occupancy<double, false, BwdOp<double>>());
     const int occ32 = std::min({wave_occupancy<float, true, FwdOp<float>>(),
                                 wave_occupancy<float, false, BwdOp<float>>(),
-                                wave_occupancy<float, true, FwdEisenstatOp<float>>()});
+                                wave_occupancy<float, true, FwdEisenstatOp<float>>(),
+                                wave_occupancy<float, false, BwdEisenstatOp<float>>()});
     wave_grid64_ = std::min(ntiles, ctx->sm_count * occ64);
     wave_grid32_ = std::min(ntiles, ctx->sm_count * occ32);
   }
@@ -1565,16 +1600,16 @@ void PcgSolver::launch_iteration(SysArrays<T>& A, bool eis) {
   const int wg = sizeof(T) == 4 ? wave_grid32_ : wave_grid64_;
   if constexpr (sizeof(T) == 4) {
     if (eis) {
-      // CG on L^-1 A L^-T: s = ph (search direction), z = t = L^-T ph,
-      // Az = w = L^-1 A L^-T ph, q = rh (split residual), p = x.
-      BwdOp<T, false> bo{{A.s, A.E, A.uR, A.uU, A.uF}, A.z};
-      launch_wave<T, false>(wave_args(true, 1, FIN_NONE), bo, st, wg);
+      // CG on L^-1 A L^-T: s = search direction, z = t = L^-T s,
+      // Az = w = L^-1 A L^-T s, q = rh (split residual), p = d (FP32 correction).
+      // s = rh + beta s ; t = L^-T s ; iteration count and bound
+      BwdEisenstatOp<T> bo{{A.q, A.s, A.E, A.uR, A.uU, A.uF}, A.z, A.s, T(0)};
+      launch_wave<T, false>(wave_args(true, 1, FIN_SA), bo, st, wg);
       FwdEisenstatOp<T> fo{{A.s, A.z, A.Pinv, A.Dt, A.cL, A.cD, A.cB, A.E}, A.Az};
-      launch_wave<T, true>(wave_args(true, 1, FIN_SPMV), fo, st, wg);  // alpha = rho / ph.w
+      launch_wave<T, true>(wave_args(true, 1, FIN_SPMV), fo, st, wg);  // alpha = rho / s.w
       // x += alpha t ; rh -= alpha w ; beta = rho_new / rho
       k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.Az, A.p, A.q, partials_, sc_,
                                                FIN_EAXPY);
-      k_sa<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.q, A.s, partials_, sc_);
       return;
     }
   }
@@ -1653,7 +1688,7 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
   e = ensure_graph<T>(A, eis);
   if (e) return e;
   cudaGraphExec_t gx = graph_for<T>(eis);
-  const int per_iter = eis ? 4 : 5;
+  const int per_iter = eis ? 3 : 5;
   // launch chunks, two in flight, until the device reports done
   const int max_chunks = max_iter / std::max(1, opt_.chunk) + 3;
   cudaEvent_t evs[2] = {ev0_, ev1_};
@@ -1752,7 +1787,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
       cudaGraphLaunch(gx, s);
     else
       for (int i = 0; i < opt_.chunk; i++) launch_iteration<float>(A, true);
-    launches_ += 4 * (uint64_t)opt_.chunk;
+    launches_ += 3 * (uint64_t)opt_.chunk;
     cudaMemcpyAsync(&sc_host_[slot], sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(evs[slot], s);
   };
@@ -1801,6 +1836,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
       status = DONE_MAXITER;
     } else if (grew || !(meas < meas_u)) {
       k_copy<float><<<nblocks_, kThreads, 0, s>>>(g_.total, A.q, A.s, sc_);
+      cudaMemsetAsync(&sc_->beta, 0, sizeof(double), s);
       launches_ += 1;
     }
     res_u = u.res;
@@ -2055,8 +2091,8 @@ int PcgSolver::time_kernels(int reps, double* ms) {
         break;
       case 6:
         if constexpr (sizeof(T) == 4)
-          launch_wave<T, false>(wave_args(true, 0, FIN_NONE), BwdOp<T, false>{{A.s, A.E, A.uR, A.uU, A.uF}, A.z},
-                                s, wg);
+          launch_wave<T, false>(wave_args(true, 0, FIN_NONE),
+                                BwdEisenstatOp<T>{{A.q, A.s, A.E, A.uR, A.uU, A.uF}, A.z, A.s, T(0)}, s, wg);
         break;
       case 7:
         if constexpr (sizeof(T) == 4)

@@ -44,15 +44,16 @@ FLIP_N = 256
 FRAME_DT = 1.0 / 120.0
 DIFF_N = 64
 DIFF_STEPS = 20
+LARGE_N = 512
 
 
-def build_scene(n):
+def build_scene(n, device=None):
     """Sphere-pool fluid: 24 seeded spheres at 50% fill (seed 2); the 512^3
-    large-solve scene uses 60% fill (seed 9)."""
+    large-solve scene uses 60% fill (seed 9).  `device` evaluates the SDF there."""
     from simcraft_b200 import scenes
 
     fill, seed = (0.6, 9) if n >= 512 else (0.5, 2)
-    sdf, info = scenes.sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=fill, seed=seed)
+    sdf, info = scenes.sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=fill, seed=seed, device=device)
     return np.ascontiguousarray(sdf), info
 
 
@@ -176,6 +177,95 @@ def reference_arm(args, rank):
     }), flush=True)
 
 
+def build_system_device(n, sdf, dev, ctx):
+    """The standalone pressure system of an n^3 scene on the GPU
+    (FvmSolver3D::buildSystem with zero velocity and the empty collider) and its
+    seeded right-hand side: (Adiag, Aneighbour[6], active, active on the host,
+    rhs on the host, rhs info)."""
+    import torch
+
+    from simcraft_b200 import _capi, scenes
+
+    L = _capi.lib()
+    h = 1.0 / n
+    dt = DT_OVER_H * h
+    f64 = dict(dtype=torch.float64, device=dev)
+    sdf_d = torch.from_numpy(sdf).to(dev)
+    u = torch.zeros((n + 1, n, n), **f64)
+    v = torch.zeros((n, n + 1, n), **f64)
+    w = torch.zeros((n, n, n + 1), **f64)
+    adiag = torch.zeros((n, n, n), **f64)
+    an = [torch.zeros((n, n, n), **f64) for _ in range(6)]
+    rhs_b = torch.zeros((n, n, n), **f64)
+    active = torch.zeros((n, n, n), dtype=torch.uint8, device=dev)
+    uw, vw, ww = torch.zeros_like(u), torch.zeros_like(v), torch.zeros_like(w)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    ctx.set_stream(ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    rc = L.sc_fvm_build_system_device(ctx.handle, n, n, n, h, dt, _capi.SC_REAL_F64, ptr(u), ptr(v), ptr(w),
+                                      ptr(sdf_d), None, ptr(adiag), _capi.ptr_array([ptr(a) for a in an]),
+                                      ptr(rhs_b), ptr(active), ptr(uw), ptr(vw), ptr(ww))
+    _capi.check("sc_fvm_build_system_device", rc, ctx.handle)
+    ctx.use_own_stream()
+    torch.cuda.synchronize()
+    del u, v, w, uw, vw, ww, rhs_b, sdf_d
+    act_h = active.cpu().numpy()
+    rhs_h, rinfo = scenes.poisson_rhs(act_h, sdf, seed=3)
+    return adiag, an, active, act_h, np.ascontiguousarray(rhs_h), rinfo
+
+
+def large_solve_leg(args, dev, ctx, replicas):
+    """FP64 against mixed on the 512^3 sphere pool (60% fill, seed 9), both to
+    1e-8 relative residual, device-resident inputs; `--large-steps` timed solves
+    after `--large-warmup` untimed ones, CUDA events on the solver stream."""
+    import torch
+
+    from simcraft_b200 import _capi
+    from simcraft_b200.solver import CgSolver3D, CRIT_REL_L2, PREC_FP64, PREC_MIXED
+
+    L = _capi.lib()
+    n = LARGE_N
+    sdf, info = build_scene(n, device=dev)
+    adiag, an, active, act_h, rhs_h, _ = build_system_device(n, sdf, dev, ctx)
+    del sdf
+    rhs_d = torch.from_numpy(rhs_h).to(dev)
+    pg = torch.zeros((n, n, n), dtype=torch.float64, device=dev)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    an_dev = _capi.ptr_array([ptr(a) for a in an])
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = {"workload": f"standalone pressure solve {n}^3, sphere pool fill {info['fill']:.3f}, "
+                       f"dt/h {DT_OVER_H:.4f}, to {TOL:g} rel. residual",
+           "active_cells": int(act_h.sum()), "warmup": args.large_warmup, "steps": args.large_steps}
+    for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        s = CgSolver3D(n, n, n, context=ctx, tol=TOL, max_iter=5000, criterion=CRIT_REL_L2, precision=prec)
+
+        def solve():
+            st = _capi.sc_pcg_stats()
+            rc = L.sc_pcg_solve_device(s.handle, ptr(adiag), an_dev, ptr(rhs_d), ptr(active), ptr(pg),
+                                       ctypes.byref(st))
+            _capi.check("sc_pcg_solve_device", rc, ctx.handle)
+            return st
+
+        for _ in range(args.large_warmup):
+            solve()
+        torch.cuda.synchronize()
+        replicas.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.large_steps):
+            st = solve()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = replicas.max(e0.elapsed_time(e1)) / max(1, args.large_steps)
+        out[name] = {"ms_per_solve": ms, "iterations": st.iterations, "outer": st.outer,
+                     "true_rel_l2": st.true_rel_l2, "kernel_launches": st.kernel_launches}
+        del s
+        torch.cuda.empty_cache()
+    out["fp64_over_mixed"] = out["fp64"]["ms_per_solve"] / out["mixed"]["ms_per_solve"]
+    del adiag, an, active, rhs_d, pg
+    torch.cuda.empty_cache()
+    return out
+
+
 def flip_leg(args, dev, ctx, dist, rank, world):
     """FLIP substeps/s on the 256^3 FP32 dam break (device-resident particles)."""
     import torch
@@ -217,11 +307,9 @@ def flip_leg(args, dev, ctx, dist, rank, world):
         launches += st["kernel_launches"]
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    from simcraft_b200.replicas import Replicas
+
+    ms = Replicas(rank, world, dist, dev).max(e0.elapsed_time(e1))
     K = args.flip_steps
     out = {"workload": f"FLIP dam break {n}^3, block x<0.5 y<0.5, 8 particles/cell, FP32 particles and grids, "
                        f"CFL factor 1, FLIP 0.95, mixed MIC(0)-PCG to {TOL:g}",
@@ -236,13 +324,14 @@ def flip_leg(args, dev, ctx, dist, rank, world):
     return out
 
 
-def diff_leg(args, ctx):
+def diff_leg(args, ctx, replicas):
     """Differentiable step on the 64^3 control problem: FP32 forward + adjoint
     times (CUDA events around each call on the solver's stream), and the FP64
     adjoint against central differences (eps 1e-3) along seeded directions."""
     import torch
 
     from simcraft_b200.diff import DiffFlip, control_scene, faces_from_cells
+    from simcraft_b200.replicas import fd_check
 
     n, steps = DIFF_N, DIFF_STEPS
     pos, param, target, h = control_scene(n)
@@ -274,19 +363,21 @@ def diff_leg(args, ctx):
     s64 = sims["f64"]
     s64.forward(U, tape="record")
     g64 = s64.backward()
-    rng = np.random.default_rng(8)
-    errs = []
-    for _ in range(args.diff_dirs):
-        d = faces_from_cells(torch.from_numpy(rng.standard_normal(param.shape)).cuda())
-        eps = 1e-3
-        fp = s64.forward([u + eps * x for u, x in zip(U, d)], tape="replay")
-        fm = s64.forward([u - eps * x for u, x in zip(U, d)], tape="replay")
-        fd = (fp - fm) / (2 * eps)
-        ad = sum(float((g * x).sum()) for g, x in zip(g64, d))
-        errs.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+    eps = 1e-3
+
+    def loss_at(d, sign):
+        D = faces_from_cells(torch.from_numpy(d).cuda())
+        return s64.forward([u + sign * eps * x for u, x in zip(U, D)], tape="replay")
+
+    def grad_dot(d):
+        D = faces_from_cells(torch.from_numpy(d).cuda())
+        return sum(float((g * x).sum()) for g, x in zip(g64, D))
+
+    # the directions are split round-robin over the replicas and gathered
+    errs = fd_check(loss_at, grad_dot, param.shape, args.diff_dirs, 8, eps, replicas)
     num = sum(float(((a - b) ** 2).sum()) for a, b in zip(g64, g32))
     den = sum(float((a ** 2).sum()) for a in g64)
-    out.update({"fd_directions": args.diff_dirs, "fd_eps": 1e-3,
+    out.update({"fd_directions": args.diff_dirs, "fd_eps": eps, "fd_ranks": replicas.world,
                 "fd_max_rel_err": max(errs) if errs else None,
                 "fd_median_rel_err": float(np.median(errs)) if errs else None,
                 "f32_vs_f64_grad_rel_l2": (num / den) ** 0.5})
@@ -352,6 +443,9 @@ def main():
     ap.add_argument("--skip-solve", action="store_true",
                     help="run only the FLIP leg (profiling runs; prints the FLIP object)")
     ap.add_argument("--solve-n", type=int, default=N_GRID, help="standalone solve grid size")
+    ap.add_argument("--large-steps", type=int, default=1,
+                    help="timed solves of the 512^3 FP64-vs-mixed leg (0 skips the leg)")
+    ap.add_argument("--large-warmup", type=int, default=2, help="untimed solves of the 512^3 leg")
     ap.add_argument("--diff-dirs", type=int, default=16,
                     help="finite-difference directions of the differentiable leg (-1 skips the leg)")
     args = ap.parse_args()
@@ -380,11 +474,13 @@ def main():
         return
 
     from simcraft_b200 import _capi, scenes
+    from simcraft_b200.replicas import Replicas
     from simcraft_b200.solver import CgSolver3D, Context, CRIT_REL_L2, PREC_FP64, PREC_MIXED
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     ctx = Context(local)
+    replicas = Replicas(rank, world, dist, dev)
     n = args.solve_n
     if args.skip_solve:
         fl = flip_leg(args, dev, ctx, dist, rank, world)
@@ -399,31 +495,11 @@ def main():
     dt = DT_OVER_H * h
     N = n * n * n
     sdf, info = build_scene(n)
-
-    # ---- build the system on the GPU (FvmSolver3D::buildSystem, zero velocity) ----
-    f64 = dict(dtype=torch.float64, device=dev)
-    sdf_d = torch.from_numpy(sdf).to(dev)
-    u = torch.zeros((n + 1, n, n), **f64)
-    v = torch.zeros((n, n + 1, n), **f64)
-    w = torch.zeros((n, n, n + 1), **f64)
-    adiag = torch.zeros((n, n, n), **f64)
-    an = [torch.zeros((n, n, n), **f64) for _ in range(6)]
-    rhs_b = torch.zeros((n, n, n), **f64)
-    active = torch.zeros((n, n, n), dtype=torch.uint8, device=dev)
-    uw, vw, ww = torch.zeros_like(u), torch.zeros_like(v), torch.zeros_like(w)
-    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
-    ctx.set_stream(ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
-    rc = L.sc_fvm_build_system_device(ctx.handle, n, n, n, h, dt, _capi.SC_REAL_F64, ptr(u), ptr(v), ptr(w),
-                                      ptr(sdf_d), None, ptr(adiag), _capi.ptr_array([ptr(a) for a in an]),
-                                      ptr(rhs_b), ptr(active), ptr(uw), ptr(vw), ptr(ww))
-    _capi.check("sc_fvm_build_system_device", rc, ctx.handle)
-    ctx.use_own_stream()
-    torch.cuda.synchronize()
-    act_h = active.cpu().numpy()
-    rhs_h, rinfo = scenes.poisson_rhs(act_h, sdf, seed=3)
-    rhs_h = np.ascontiguousarray(rhs_h)
+    adiag, an, active, act_h, rhs_h, rinfo = build_system_device(n, sdf, dev, ctx)
     rhs_d = torch.from_numpy(rhs_h).to(dev)
     n_active = int(act_h.sum())
+    f64 = dict(dtype=torch.float64, device=dev)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
 
     # pinned host copies for the end-to-end arm (what a host caller passes)
     pin = lambda t: t.cpu().pin_memory()
@@ -474,12 +550,7 @@ def main():
             last = fn(s)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms, last
+        return replicas.max(e0.elapsed_time(e1)), last
 
     with Clocks(local) as clk:
         ms_mixed, st_mixed = timed(solve_device, solvers["mixed"])
@@ -532,7 +603,7 @@ def main():
     out = {
         "metric": METRIC, "value": value, "unit": "ms/solve", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64 (FP32 inner PCG, FP64 defect correction)",
+        "vs_baseline": None, "dtype": "f32+f64 (FP32 Eisenstat-form MIC(0) CG, FP64 residual replacement)",
         "data": "synthetic (seeded sphere pool, no dataset)",
         "config": {"workload": f"standalone pressure solve {n}^3, mixed MIC(0)-PCG to {TOL:g} rel. residual",
                    "grid": [n, n, n], "fill": info["fill"], "active_cells": n_active,
@@ -542,7 +613,7 @@ def main():
         "fp64": {"ms_per_solve": ms_fp64 / args.steps, "iterations": st_fp64.iterations,
                  "true_rel_l2": st_fp64.true_rel_l2},
         "mixed": {"ms_per_solve": ms_step, "inner_iterations": st_mixed.iterations,
-                  "outer_passes": st_mixed.outer, "true_rel_l2": st_mixed.true_rel_l2},
+                  "fp64_replacements": st_mixed.outer, "true_rel_l2": st_mixed.true_rel_l2},
         "mixed_speedup_vs_fp64": (ms_fp64 / ms_mixed),
         "e2e": {"value": e2e_ms / args.steps / world, "unit": "ms/solve", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
@@ -567,10 +638,12 @@ def main():
                                                            np.linalg.norm(pg_cpu[a]))}
     del solvers
     torch.cuda.empty_cache()
+    if args.large_steps > 0:
+        out["solve_512"] = large_solve_leg(args, dev, ctx, replicas)
     if args.flip_steps > 0:
         out["flip"] = flip_leg(args, dev, ctx, dist, rank, world)
-    if args.diff_dirs >= 0 and rank == 0:
-        out["diff"] = diff_leg(args, ctx)
+    if args.diff_dirs >= 0:
+        out["diff"] = diff_leg(args, ctx, replicas)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if dist:

@@ -36,9 +36,13 @@ def _spheres(seed, count, rmin, rmax):
     return centres, radii
 
 
-def sphere_union_sdf(n, centres, radii, chunk=32):
+def sphere_union_sdf(n, centres, radii, chunk=32, device=None):
     """Signed distance to a union of spheres at the cell centres of an n^3 grid
-    (min over spheres of |x - c| - r), float64, shape (n, n, n)."""
+    (min over spheres of |x - c| - r), float64, shape (n, n, n).  With a torch
+    `device` the same double-precision expression is evaluated there, for large
+    grids (values agree with the numpy path to within an ulp of the square root)."""
+    if device is not None:
+        return _sphere_union_sdf_torch(n, centres, radii, chunk, device)
     h = 1.0 / n
     x = (np.arange(n) + 0.5) * h
     out = np.empty((n, n, n))
@@ -52,7 +56,24 @@ def sphere_union_sdf(n, centres, radii, chunk=32):
     return out
 
 
-def sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=0.5, seed=2, probe=64):
+def _sphere_union_sdf_torch(n, centres, radii, chunk, device):
+    import torch
+
+    h = 1.0 / n
+    x = (torch.arange(n, dtype=torch.float64, device=device) + 0.5) * h
+    out = np.empty((n, n, n))
+    for i0 in range(0, n, chunk):
+        xs = x[i0:i0 + chunk]
+        best = torch.full((len(xs), n, n), float("inf"), dtype=torch.float64, device=device)
+        for c, r in zip(centres, radii):
+            d2 = ((xs - float(c[0])) ** 2)[:, None, None] + ((x - float(c[1])) ** 2)[None, :, None] + \
+                ((x - float(c[2])) ** 2)[None, None, :]
+            torch.minimum(best, torch.sqrt(d2) - float(r), out=best)
+        out[i0:i0 + chunk] = best.cpu().numpy()
+    return out
+
+
+def sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=0.5, seed=2, probe=64, device=None):
     """Fluid mask of `count` seeded spheres (centres U[0,1)^3, radii U[rmin,rmax]).
 
     24 spheres of those radii cover only ~25% of the box, so all radii are
@@ -69,7 +90,7 @@ def sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=0.5, seed=2, probe=64):
         else:
             hi = mid
     scale = 0.5 * (lo + hi)
-    sdf = sphere_union_sdf(n, centres, radii * scale)
+    sdf = sphere_union_sdf(n, centres, radii * scale, device=device)
     return sdf, dict(scale=scale, fill=float((sdf <= 0.0).mean()), centres=centres, radii=radii * scale)
 
 

@@ -254,6 +254,32 @@ int sc_flip_advect_device(sc_context* ctx, int64_t n, double* pos, double* vel, 
 int sc_reconstruct_device(sc_context* ctx, int64_t n, const double* pos, int nx, int ny, int nz,
                           double h, double radius, double* sdf, uint8_t* valid);
 
+/* manifold2SDF(exact_band, closest, intersection_cnt, mesh, sdf)
+ * (FluidSim/src/cpu/util.cc:203-310): signed distance from a closed triangle
+ * mesh at the cell centres ((x + 0.5) h + origin[0], ...) of an nx x ny x nz
+ * grid, reference layout.  Exact point-triangle distances within exact_band
+ * cells of each triangle's box, then two rounds of eight fast-sweeping passes
+ * that propagate the closest triangle, then the sign from the parity of the +z
+ * ray crossings below each cell (negative inside).  vertices: nvertices x 3
+ * doubles; triangles: ntriangles x 3 vertex indices.  closest (may be NULL)
+ * receives the triangle each distance came from (-1 for none).  origin is a
+ * host array of 3 doubles (NULL: 0).  flags = SC_MESH_REFERENCE_DISTANCE
+ * reproduces the reference bit for bit, including its distancePointTriangle
+ * (util.cc:87-125), which measures |ap + v ab|, |ap + w ac| and
+ * |ap + v ab + w ac| where the offsets to the closest point on edge AB, edge AC
+ * and the face are ap - v ab, ap - w ac and ap - v ab - w ac, so those
+ * distances come out too large (the sign is unaffected);
+ * SC_MESH_EXACT_DISTANCE uses the true point-triangle distances.  A triangle
+ * index outside [0, nvertices) returns SC_ERR_INVALID.  _device: device
+ * arrays, on the context stream; _host: host arrays (copied in and out). */
+enum { SC_MESH_REFERENCE_DISTANCE = 0, SC_MESH_EXACT_DISTANCE = 1 };
+int sc_mesh_to_sdf_device(sc_context* ctx, int nx, int ny, int nz, double h, const double* origin,
+                          const double* vertices, int64_t nvertices, const int32_t* triangles,
+                          int64_t ntriangles, int exact_band, int flags, double* sdf, int32_t* closest);
+int sc_mesh_to_sdf_host(sc_context* ctx, int nx, int ny, int nz, double h, const double* origin,
+                        const double* vertices, int64_t nvertices, const int32_t* triangles,
+                        int64_t ntriangles, int exact_band, int flags, double* sdf, int32_t* closest);
+
 /* ---------------------------------------------------------------------------
  * Whole simulator: fluid::cpu::FluidSimulator
  * (FluidSim/include/FluidSim/cpu/fluid-simulator.h:25-200,
@@ -303,6 +329,13 @@ int sc_fluid_set_particles(sc_fluid* sim, int64_t n, const double* pos, const do
 /* setCollider (fluid-simulator.h:62-72) given the collider SDF on the cell
  * centres (what manifold2SDF produces); NULL removes it. */
 int sc_fluid_set_collider(sc_fluid* sim, const double* sdf, int device_pointers);
+/* setCollider(const Mesh&) itself (fluid-simulator.h:62-71): the collider SDF
+ * built from a closed triangle mesh with manifold2SDF(3, ...) on the
+ * simulator's grid (origin 0), as sc_mesh_to_sdf_* computes it with `flags`
+ * (SC_MESH_REFERENCE_DISTANCE for the reference's collider). */
+int sc_fluid_set_collider_mesh(sc_fluid* sim, const double* vertices, int64_t nvertices,
+                               const int32_t* triangles, int64_t ntriangles, int flags,
+                               int device_pointers);
 /* CFL() (fluid-simulator.cc:184-203). */
 int sc_fluid_cfl(sc_fluid* sim, double* dt);
 /* substep(dt) (fluid-simulator.cc:140-182). */

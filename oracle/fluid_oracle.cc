@@ -264,6 +264,117 @@ void handle_collision(const double* collider, int nx, int ny, int nz, double h, 
 
 enum { Left = 0, Right = 1, Up = 2, Down = 3, Front = 4, Back = 5 };
 
+// ---------------------------------------------------------------------------
+// Mesh -> signed distance grid: manifold2SDF (FluidSim/src/cpu/util.cc:203-310)
+// and its helpers, in the reference's operation order.  Grid cell (x, y, z)
+// sits at ((x + 0.5) h + ox, ...) (CellCentredGrid::indexToCoord,
+// Spatify/include/Spatify/grids.h:303-308).
+
+// distancePointTriangle (util.cc:87-125): closest point by Voronoi regions.
+// The reference measures |ap + v ab| on edge AB, |ap + w ac| on edge AC and
+// |ap + v ab + w ac| inside the face, where the offset to the closest point is
+// ap - v ab (etc.), so it overstates those distances; `exact` selects the
+// offsets with the minus signs (vertices and edge BC agree in both).
+double dist_point_tri(V3 p, V3 a, V3 b, V3 c, bool exact) {
+  const V3 ab = b - a, ac = c - a, ap = p - a;
+  const double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+  if (d1 <= 0 && d2 <= 0) return std::sqrt(dot3(ap, ap));
+  const V3 bp = p - b;
+  const double d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+  if (d3 >= 0 && d4 <= d3) return std::sqrt(dot3(bp, bp));
+  const double vc = d1 * d4 - d3 * d2;
+  if (vc <= 0 && d1 >= 0 && d3 <= 0) {
+    const double v = d1 / (d1 - d3);
+    const V3 q = exact ? ap - v * ab : ap + v * ab;
+    return std::sqrt(dot3(q, q));
+  }
+  const V3 cp = p - c;
+  const double d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+  if (d6 >= 0 && d5 <= d6) return std::sqrt(dot3(cp, cp));
+  const double vb = d5 * d2 - d1 * d6;
+  if (vb <= 0 && d2 >= 0 && d6 <= 0) {
+    const double w = d2 / (d2 - d6);
+    const V3 q = exact ? ap - w * ac : ap + w * ac;
+    return std::sqrt(dot3(q, q));
+  }
+  const double va = d3 * d6 - d5 * d4;
+  if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+    const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    const V3 q = bp + w * (cp - bp);
+    return std::sqrt(dot3(q, q));
+  }
+  const double denom = 1.0 / (va + vb + vc);
+  const double v = vb * denom, w = vc * denom;
+  const V3 q = exact ? (ap - v * ab) - w * ac : (ap + v * ab) + w * ac;
+  return std::sqrt(dot3(q, q));
+}
+
+// cross / insideTraingle2D (util.cc:127-142): all three edge tests agree.
+inline double cross2(double ax, double ay, double bx, double by) { return ax * by - bx * ay; }
+bool inside_tri_2d(double px, double py, V3 a, V3 b, V3 c) {
+  const int cnt = (cross2(px - a.x, py - a.y, b.x - a.x, b.y - a.y) >= 0.0) +
+                  (cross2(px - b.x, py - b.y, c.x - b.x, c.y - b.y) >= 0.0) +
+                  (cross2(px - c.x, py - c.y, a.x - c.x, a.y - c.y) >= 0.0);
+  return cnt == 3 || cnt == 0;
+}
+
+// solveEquations / calcBiocentricCoord (util.cc:144-157).
+void bary_2d(double px, double py, V3 a, V3 b, V3 c, double* u, double* v, double* w) {
+  const double a1 = a.x - c.x, b1 = b.x - c.x, c1 = px - c.x;
+  const double a2 = a.y - c.y, b2 = b.y - c.y, c2 = py - c.y;
+  const double det = a1 * b2 - a2 * b1;
+  *u = (c1 * b2 - c2 * b1) / det;
+  *v = (a1 * c2 - a2 * c1) / det;
+  *w = 1.0 - (*u) - (*v);
+}
+
+struct MeshGrid {
+  int nx, ny, nz;
+  double h, ox, oy, oz;
+  const double* vert;
+  const int* tri;
+  bool exact;
+  V3 vtx(int t, int k) const { return ld3(vert, tri[3 * t + k]); }
+  V3 coord(int x, int y, int z) const {
+    return {(x + 0.5) * h + ox, (y + 0.5) * h + oy, (z + 0.5) * h + oz};
+  }
+  int64_t at(int x, int y, int z) const { return ((int64_t)x * ny + y) * nz + z; }
+};
+
+// checkNeighbour (util.cc:159-180).  The reference writes abs(); on doubles
+// that is fabs.
+void check_neighbour(const MeshGrid& M, double* sdf, int* closest, int dx, int dy, int dz, int x,
+                     int y, int z) {
+  if (x + dx < 0 || x + dx >= M.nx || y + dy < 0 || y + dy >= M.ny || z + dz < 0 || z + dz >= M.nz)
+    return;
+  const int t = closest[M.at(x + dx, y + dy, z + dz)];
+  if (t == -1) return;
+  const int64_t e = M.at(x, y, z);
+  const double d1 = dist_point_tri(M.coord(x, y, z), M.vtx(t, 0), M.vtx(t, 1), M.vtx(t, 2), M.exact);
+  if (std::fabs(d1) < std::fabs(sdf[e])) {
+    sdf[e] = d1;
+    closest[e] = t;
+  }
+}
+
+// sweep (util.cc:182-201): one Gauss-Seidel pass in the direction (-dx, -dy, -dz).
+void mesh_sweep(const MeshGrid& M, double* sdf, int* closest, int dx, int dy, int dz) {
+  const int xs = dx < 0 ? 0 : M.nx - 1, xe = dx < 0 ? M.nx : -1;
+  const int ys = dy < 0 ? 0 : M.ny - 1, ye = dy < 0 ? M.ny : -1;
+  const int zs = dz < 0 ? 0 : M.nz - 1, ze = dz < 0 ? M.nz : -1;
+  for (int x = xs; x != xe; x -= dx)
+    for (int y = ys; y != ye; y -= dy)
+      for (int z = zs; z != ze; z -= dz) {
+        check_neighbour(M, sdf, closest, 0, dy, dz, x, y, z);
+        check_neighbour(M, sdf, closest, dx, 0, dz, x, y, z);
+        check_neighbour(M, sdf, closest, dx, dy, 0, x, y, z);
+        check_neighbour(M, sdf, closest, 0, 0, dz, x, y, z);
+        check_neighbour(M, sdf, closest, 0, dy, 0, x, y, z);
+        check_neighbour(M, sdf, closest, dx, 0, 0, x, y, z);
+        check_neighbour(M, sdf, closest, dx, dy, dz, x, y, z);
+      }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1267,6 +1378,83 @@ void ora_sim_get_system(const ora_sim* s, double* adiag, double* const* an, doub
   if (rhs) std::memcpy(rhs, s->rhs.data(), sizeof(double) * N);
   if (active) std::memcpy(active, s->active.data(), N);
 }
+// manifold2SDF (FluidSim/src/cpu/util.cc:203-310): exact distances in a band of
+// `exact_band` cells around each triangle's box, crossing counts of the +z rays
+// through the cell centres, two rounds of eight fast sweeps propagating the
+// closest triangle, then the sign from the parity of the crossings below.
+// exact_distance = 0 keeps the reference's point-triangle arithmetic.
+void ora_manifold_to_sdf(int nx, int ny, int nz, double h, double ox, double oy, double oz,
+                         const double* vert, const int* tri, int64_t ntri, int exact_band,
+                         int exact_distance, double* sdf, int* closest, int* icnt) {
+  MeshGrid M{nx, ny, nz, h, ox, oy, oz, vert, tri, exact_distance != 0};
+  const int64_t N = (int64_t)nx * ny * nz;
+  for (int64_t e = 0; e < N; e++) {
+    closest[e] = -1;
+    icnt[e] = 0;
+    sdf[e] = 1e9;
+  }
+  for (int64_t i = 0; i < ntri; i++) {
+    const V3 a = M.vtx((int)i, 0), b = M.vtx((int)i, 1), c = M.vtx((int)i, 2);
+    const double mnx = std::min(std::min(a.x - ox, b.x - ox), c.x - ox);
+    const double mxx = std::max(std::max(a.x - ox, b.x - ox), c.x - ox);
+    const double mny = std::min(std::min(a.y - oy, b.y - oy), c.y - oy);
+    const double mxy = std::max(std::max(a.y - oy, b.y - oy), c.y - oy);
+    const double mnz = std::min(std::min(a.z - oz, b.z - oz), c.z - oz);
+    const double mxz = std::max(std::max(a.z - oz, b.z - oz), c.z - oz);
+    int lx = clampi((int)std::floor(mnx / h - 0.5) - exact_band, 0, nx - 1);
+    int hx = clampi((int)std::ceil(mxx / h - 0.5) + exact_band, 0, nx - 1);
+    int ly = clampi((int)std::floor(mny / h - 0.5) - exact_band, 0, ny - 1);
+    int hy = clampi((int)std::ceil(mxy / h - 0.5) + exact_band, 0, ny - 1);
+    const int lz = clampi((int)std::floor(mnz / h - 0.5) - exact_band, 0, nz - 1);
+    const int hz = clampi((int)std::ceil(mxz / h - 0.5) + exact_band, 0, nz - 1);
+    for (int x = lx; x <= hx; x++)
+      for (int y = ly; y <= hy; y++)
+        for (int z = lz; z <= hz; z++) {
+          const double d = dist_point_tri(M.coord(x, y, z), a, b, c, M.exact);
+          const int64_t e = M.at(x, y, z);
+          if (d < sdf[e]) {
+            sdf[e] = d;
+            closest[e] = (int)i;
+          }
+        }
+    lx = clampi((int)std::floor(mnx / h - 0.5), 0, nx - 1);
+    hx = clampi((int)std::ceil(mxx / h - 0.5), 0, nx - 1);
+    ly = clampi((int)std::floor(mny / h - 0.5), 0, ny - 1);
+    hy = clampi((int)std::ceil(mxy / h - 0.5), 0, ny - 1);
+    for (int j = lx; j <= hx; j++)
+      for (int k = ly; k <= hy; k++) {
+        const V3 o = M.coord(j, k, -1);
+        if (!inside_tri_2d(o.x, o.y, a, b, c)) continue;
+        double u, v, w;
+        bary_2d(o.x, o.y, a, b, c, &u, &v, &w);
+        const double iz = a.z * u + b.z * v + c.z * w;
+        const int l = (int)std::ceil((iz - oz) / h - 0.5);
+        if (l < 0)
+          icnt[M.at(j, k, 0)]++;
+        else if (l < nz)
+          icnt[M.at(j, k, l)]++;
+      }
+  }
+  for (int round = 0; round < 2; round++) {
+    mesh_sweep(M, sdf, closest, 1, 1, 1);
+    mesh_sweep(M, sdf, closest, 1, 1, -1);
+    mesh_sweep(M, sdf, closest, 1, -1, 1);
+    mesh_sweep(M, sdf, closest, 1, -1, -1);
+    mesh_sweep(M, sdf, closest, -1, 1, 1);
+    mesh_sweep(M, sdf, closest, -1, 1, -1);
+    mesh_sweep(M, sdf, closest, -1, -1, 1);
+    mesh_sweep(M, sdf, closest, -1, -1, -1);
+  }
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++) {
+      int tot = 0;
+      for (int k = 0; k < nz; k++) {
+        tot += icnt[M.at(i, j, k)];
+        if (tot & 1) sdf[M.at(i, j, k)] = -sdf[M.at(i, j, k)];
+      }
+    }
+}
+
 int ora_sim_last_iters(const ora_sim* s) { return s->last_iters; }
 double ora_sim_last_residual(const ora_sim* s) { return s->last_residual; }
 

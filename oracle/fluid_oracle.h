@@ -126,6 +126,14 @@ void ora_sim_get_fluid_sdf(const ora_sim* s, double* sdf);
 void ora_sim_get_system(const ora_sim* s, double* adiag, double* const* an, double* rhs,
                         uint8_t* active);
 int ora_sim_last_iters(const ora_sim* s);
+/* manifold2SDF (util.cc:203-310): triangle mesh (vert n x 3, tri ntri x 3, int)
+ * -> signed distance at the cell centres of an nx x ny x nz grid of spacing h
+ * and origin (ox, oy, oz); closest triangle per cell and crossing counts too.
+ * exact_distance = 0: the reference's point-triangle arithmetic (which
+ * overstates edge-AB, edge-AC and face distances); 1: true distances. */
+void ora_manifold_to_sdf(int nx, int ny, int nz, double h, double ox, double oy, double oz,
+                         const double* vert, const int* tri, int64_t ntri, int exact_band,
+                         int exact_distance, double* sdf, int* closest, int* icnt);
 double ora_sim_last_residual(const ora_sim* s);
 
 #ifdef __cplusplus

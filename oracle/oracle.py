@@ -56,6 +56,9 @@ def lib():
             "ora_set_parity_mode": (None, [_int]),
             "ora_get_threads": (_int, []),
             "ora_cubic_weight": (_dbl, [_dbl, _dbl, _dbl, _dbl]),
+            "ora_manifold_to_sdf": (None, [_int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dp,
+                                           ctypes.POINTER(ctypes.c_int), _i64, _int, _int, _dp,
+                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
             "ora_p2g": (None, [_i64, _dp, _dp, _int, _int, _int, _dbl] + [_dp] * 6 + [_u8p] * 3 + [_dp] * 3),
             "ora_sample_velocity": (None, [_i64, _dp, _int, _int, _int, _dbl, _dp, _dp, _dp, _dp]),
             "ora_g2p": (None, [_i64, _dp, _dp, _int, _int, _int, _dbl] + [_dp] * 6 + [_dbl]),
@@ -223,6 +226,20 @@ def mic_precond(adiag, an, r, active, tau=0.97, sigma=0.25, return_scratch=False
     lib().ora_mic_precond(*adiag.shape, _p(adiag), _ptr_array(an), _p(r), _p(active), _p(z), tau, sigma,
                           _p(E), _p(q))
     return (z, E, q) if return_scratch else z
+
+
+def manifold_to_sdf(vertices, triangles, dims, h, origin=(0.0, 0.0, 0.0), exact_band=3, exact_distance=False):
+    """manifold2SDF (util.cc:203-310) on the CPU: (sdf, closest triangle, crossing counts).
+    exact_distance=False keeps the reference's point-triangle arithmetic."""
+    v = np.ascontiguousarray(vertices, np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(triangles, np.int32).reshape(-1, 3)
+    sdf = np.zeros(dims)
+    closest = np.zeros(dims, np.int32)
+    icnt = np.zeros(dims, np.int32)
+    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    lib().ora_manifold_to_sdf(*dims, float(h), *map(float, origin), _p(v), ip(t), len(t), int(exact_band),
+                              int(bool(exact_distance)), _p(sdf), ip(closest), ip(icnt))
+    return sdf, closest, icnt
 
 
 def dot(a, b, active):

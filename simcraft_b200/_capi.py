@@ -62,6 +62,7 @@ SC_REAL_F64, SC_REAL_F32 = 0, 1
 SC_DONE_CONVERGED, SC_DONE_MAXITER, SC_DONE_BREAKDOWN = 1, 2, 3
 SC_ADVECT_PIC, SC_ADVECT_FLIP = 0, 1
 SC_TAPE_NONE, SC_TAPE_RECORD, SC_TAPE_REPLAY = 0, 1, 2
+SC_MESH_REFERENCE_DISTANCE, SC_MESH_EXACT_DISTANCE = 0, 1
 
 _dpp = P(c_void_p)  # array of pointers
 
@@ -111,6 +112,11 @@ SIGNATURES = {
     "sc_fluid_destroy": (None, [c_void_p]),
     "sc_fluid_set_particles": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_int]),
     "sc_fluid_set_collider": (c_int, [c_void_p, c_void_p, c_int]),
+    "sc_fluid_set_collider_mesh": (c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_int, c_int]),
+    "sc_mesh_to_sdf_device": (c_int, [c_void_p, c_int, c_int, c_int, c_double, c_void_p, c_void_p, c_int64,
+                                      c_void_p, c_int64, c_int, c_int, c_void_p, c_void_p]),
+    "sc_mesh_to_sdf_host": (c_int, [c_void_p, c_int, c_int, c_int, c_double, c_void_p, c_void_p, c_int64,
+                                    c_void_p, c_int64, c_int, c_int, c_void_p, c_void_p]),
     "sc_fluid_cfl": (c_int, [c_void_p, P(c_double)]),
     "sc_fluid_substep": (c_int, [c_void_p, c_double, P(sc_fluid_stats)]),
     "sc_fluid_step": (c_int, [c_void_p, c_double, P(sc_fluid_stats)]),

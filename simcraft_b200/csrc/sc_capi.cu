@@ -1,5 +1,7 @@
 // sc_capi.cu -- extern "C" boundary.  No C++ exception or CUDA type crosses it.
+#include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cstring>
 #include <new>
 #include <string>
@@ -8,6 +10,7 @@
 #include "sc_diff.cuh"
 #include "sc_flip.cuh"
 #include "sc_fvm.cuh"
+#include "sc_mesh.cuh"
 #include "sc_pcg.cuh"
 
 // A context is freed when its user handle and every handle created from it
@@ -466,6 +469,70 @@ int sc_reconstruct_device(sc_context* ctx, int64_t n, const double* pos, int nx,
 }
 
 // ---------------------------------------------------------------------------------
+// Mesh -> SDF.
+
+static int mesh_sdf(sc_context* ctx, int nx, int ny, int nz, double h, const double* origin,
+                    const double* vertices, int64_t nvertices, const int32_t* triangles,
+                    int64_t ntriangles, int exact_band, int flags, double* sdf, int32_t* closest,
+                    bool device) {
+  if (!ctx || !grid_ok(nx, ny, nz, h) || nvertices < 0 || ntriangles < 0 || ntriangles > INT_MAX ||
+      (ntriangles > 0 && (!vertices || !triangles)) || exact_band < 0 || !sdf ||
+      (flags != SC_MESH_REFERENCE_DISTANCE && flags != SC_MESH_EXACT_DISTANCE))
+    return SC_ERR_INVALID;
+  cudaSetDevice(ctx->c.device);
+  cudaStream_t st = ctx->c.stream;
+  const int64_t N = (int64_t)nx * ny * nz;
+  sc::MeshSdfArgs a{nx, ny, nz, h, origin ? origin[0] : 0.0, origin ? origin[1] : 0.0,
+                    origin ? origin[2] : 0.0, vertices, nvertices, triangles, ntriangles, exact_band,
+                    flags == SC_MESH_EXACT_DISTANCE};
+  double* d_sdf = sdf;
+  int32_t* d_cl = closest;
+  void *dv = nullptr, *dt = nullptr;
+  if (!device) {
+    if (cudaMallocAsync(&d_sdf, sizeof(double) * (size_t)N, st) != cudaSuccess ||
+        (closest && cudaMallocAsync((void**)&d_cl, sizeof(int32_t) * (size_t)N, st) != cudaSuccess) ||
+        cudaMallocAsync(&dv, sizeof(double) * 3 * (size_t)std::max<int64_t>(nvertices, 1), st) != cudaSuccess ||
+        cudaMallocAsync(&dt, sizeof(int32_t) * 3 * (size_t)std::max<int64_t>(ntriangles, 1), st) != cudaSuccess)
+      return ctx->c.set_error(SC_ERR_NOMEM, "mesh_to_sdf: staging allocation failed");
+    if (nvertices > 0)
+      cudaMemcpyAsync(dv, vertices, sizeof(double) * 3 * (size_t)nvertices, cudaMemcpyHostToDevice, st);
+    if (ntriangles > 0)
+      cudaMemcpyAsync(dt, triangles, sizeof(int32_t) * 3 * (size_t)ntriangles, cudaMemcpyHostToDevice, st);
+    a.vertices = (const double*)dv;
+    a.triangles = (const int32_t*)dt;
+  }
+  std::string msg;
+  int rc = sc::mesh_to_sdf(st, a, d_sdf, d_cl, &msg);
+  if (!device) {
+    if (rc == 0) {
+      cudaMemcpyAsync(sdf, d_sdf, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost, st);
+      if (closest) cudaMemcpyAsync(closest, d_cl, sizeof(int32_t) * (size_t)N, cudaMemcpyDeviceToHost, st);
+    }
+    cudaFreeAsync(d_sdf, st);
+    if (closest) cudaFreeAsync(d_cl, st);
+    cudaFreeAsync(dv, st);
+    cudaFreeAsync(dt, st);
+    cudaStreamSynchronize(st);
+  }
+  if (rc) return ctx->c.set_error(map_status(rc), msg);
+  return finish(ctx, 0, "mesh_to_sdf");
+}
+
+int sc_mesh_to_sdf_device(sc_context* ctx, int nx, int ny, int nz, double h, const double* origin,
+                          const double* vertices, int64_t nvertices, const int32_t* triangles,
+                          int64_t ntriangles, int exact_band, int flags, double* sdf, int32_t* closest) {
+  return mesh_sdf(ctx, nx, ny, nz, h, origin, vertices, nvertices, triangles, ntriangles, exact_band,
+                  flags, sdf, closest, true);
+}
+
+int sc_mesh_to_sdf_host(sc_context* ctx, int nx, int ny, int nz, double h, const double* origin,
+                        const double* vertices, int64_t nvertices, const int32_t* triangles,
+                        int64_t ntriangles, int exact_band, int flags, double* sdf, int32_t* closest) {
+  return mesh_sdf(ctx, nx, ny, nz, h, origin, vertices, nvertices, triangles, ntriangles, exact_band,
+                  flags, sdf, closest, false);
+}
+
+// ---------------------------------------------------------------------------------
 // Simulator.
 
 void sc_fluid_default_config(int nx, int ny, int nz, double h, sc_fluid_config* c) {
@@ -556,6 +623,46 @@ int sc_fluid_set_collider(sc_fluid* sim, const double* sdf, int device_pointers)
   if (!sim) return SC_ERR_INVALID;
   cudaSetDevice(sim->ctx->c.device);
   return fl_rc(sim, sim->sim->set_collider(sdf, device_pointers != 0));
+}
+
+int sc_fluid_set_collider_mesh(sc_fluid* sim, const double* vertices, int64_t nvertices,
+                               const int32_t* triangles, int64_t ntriangles, int flags,
+                               int device_pointers) {
+  if (!sim) return SC_ERR_INVALID;
+  sc_context* ctx = sim->ctx;
+  cudaSetDevice(ctx->c.device);
+  const sc::FluidConfig& c = sim->sim->config();
+  double* d_sdf = nullptr;
+  if (cudaMallocAsync(&d_sdf, sizeof(double) * (size_t)c.nx * c.ny * c.nz, ctx->c.stream) != cudaSuccess)
+    return ctx->c.set_error(SC_ERR_NOMEM, "set_collider_mesh: allocation failed");
+  // setCollider uses an exact band of 3 cells (fluid-simulator.h:69)
+  int rc = device_pointers
+               ? sc_mesh_to_sdf_device(ctx, c.nx, c.ny, c.nz, c.h, nullptr, vertices, nvertices, triangles,
+                                       ntriangles, 3, flags, d_sdf, nullptr)
+               : -1;
+  if (!device_pointers) {
+    // host mesh: stage it, then build on the device
+    void *dv = nullptr, *dt = nullptr;
+    cudaStream_t st = ctx->c.stream;
+    if (cudaMallocAsync(&dv, sizeof(double) * 3 * (size_t)std::max<int64_t>(nvertices, 1), st) != cudaSuccess ||
+        cudaMallocAsync(&dt, sizeof(int32_t) * 3 * (size_t)std::max<int64_t>(ntriangles, 1), st) != cudaSuccess) {
+      cudaFreeAsync(d_sdf, st);
+      return ctx->c.set_error(SC_ERR_NOMEM, "set_collider_mesh: allocation failed");
+    }
+    if (nvertices > 0 && vertices)
+      cudaMemcpyAsync(dv, vertices, sizeof(double) * 3 * (size_t)nvertices, cudaMemcpyHostToDevice, st);
+    if (ntriangles > 0 && triangles)
+      cudaMemcpyAsync(dt, triangles, sizeof(int32_t) * 3 * (size_t)ntriangles, cudaMemcpyHostToDevice, st);
+    rc = sc_mesh_to_sdf_device(ctx, c.nx, c.ny, c.nz, c.h, nullptr, vertices ? (const double*)dv : nullptr,
+                               nvertices, triangles ? (const int32_t*)dt : nullptr, ntriangles, 3, flags,
+                               d_sdf, nullptr);
+    cudaFreeAsync(dv, st);
+    cudaFreeAsync(dt, st);
+  }
+  if (rc == SC_OK) rc = fl_rc(sim, sim->sim->set_collider(d_sdf, true));
+  cudaFreeAsync(d_sdf, ctx->c.stream);
+  cudaStreamSynchronize(ctx->c.stream);
+  return rc;
 }
 
 int sc_fluid_cfl(sc_fluid* sim, double* dt) {

@@ -51,6 +51,7 @@ class FluidSim {
   int get_faces(double* u, double* v, double* w, bool device);
   int get_fluid_sdf(double* s, bool device);
   int64_t num_particles() const { return n_; }
+  const FluidConfig& config() const { return c_; }
 
  private:
   template <class T>

@@ -110,6 +110,25 @@ class FluidSimulator:
             rc = lib().sc_fluid_set_collider(self.handle, _ptr(sdf), 0)
         check("sc_fluid_set_collider", rc, self.ctx.handle)
 
+    def set_collider_mesh(self, vertices, triangles, exact_distance=False):
+        """setCollider(const Mesh&) (fluid-simulator.h:62-71): the collider SDF
+        built on the GPU from a closed triangle mesh (vertices [V,3], triangles
+        [T,3] vertex indices), numpy or CUDA tensors, with manifold2SDF's exact
+        band of 3 cells; exact_distance as in simcraft_b200.mesh.manifold_to_sdf."""
+        flags = int(bool(exact_distance))
+        if _is_torch(vertices):
+            import torch
+
+            v = vertices.to(torch.float64).contiguous()
+            t = triangles.to(torch.int32).contiguous()
+            with _on_torch_stream(self.ctx, v):
+                rc = lib().sc_fluid_set_collider_mesh(self.handle, _ptr(v), v.shape[0], _ptr(t), t.shape[0], flags, 1)
+        else:
+            v = np.ascontiguousarray(vertices, np.float64).reshape(-1, 3)
+            t = np.ascontiguousarray(triangles, np.int32).reshape(-1, 3)
+            rc = lib().sc_fluid_set_collider_mesh(self.handle, _ptr(v), len(v), _ptr(t), len(t), flags, 0)
+        check("sc_fluid_set_collider_mesh", rc, self.ctx.handle)
+
     # -- time stepping ----------------------------------------------------------
     def cfl(self):
         dt = ctypes.c_double()

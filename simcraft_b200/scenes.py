@@ -94,6 +94,63 @@ def sphere_pool(n, count=24, rmin=0.05, rmax=0.2, fill=0.5, seed=2, probe=64, de
     return sdf, dict(scale=scale, fill=float((sdf <= 0.0).mean()), centres=centres, radii=radii * scale)
 
 
+def icosphere(subdiv=2, radius=0.3, centre=(0.5, 0.5, 0.5)):
+    """Closed triangle mesh of a sphere: an icosahedron with each face split in
+    four `subdiv` times, vertices pushed to the sphere.  Returns (vertices
+    [V,3] float64, triangles [T,3] int32); T = 20 * 4^subdiv."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(v, float) / np.linalg.norm(v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdiv):
+        cache, nf = {}, []
+
+        def mid(i, j):
+            key = (min(i, j), max(i, j))
+            if key not in cache:
+                m = verts[i] + verts[j]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    v = np.array(verts) * radius + np.asarray(centre, float)
+    return np.ascontiguousarray(v), np.ascontiguousarray(np.array(faces, np.int32))
+
+
+def torus(n_major=24, n_minor=12, r_major=0.3, r_minor=0.1, centre=(0.5, 0.5, 0.5)):
+    """Closed triangle mesh of a torus around the z axis through `centre`."""
+    u = 2 * np.pi * np.arange(n_major) / n_major
+    w = 2 * np.pi * np.arange(n_minor) / n_minor
+    U, W = np.meshgrid(u, w, indexing="ij")
+    rad = r_major + r_minor * np.cos(W)
+    v = np.stack([rad * np.cos(U), rad * np.sin(U), r_minor * np.sin(W)], -1).reshape(-1, 3)
+    v = v + np.asarray(centre, float)
+    tris = []
+    for i in range(n_major):
+        for j in range(n_minor):
+            a, b = i * n_minor + j, ((i + 1) % n_major) * n_minor + j
+            c, d = ((i + 1) % n_major) * n_minor + (j + 1) % n_minor, i * n_minor + (j + 1) % n_minor
+            tris += [(a, b, c), (a, c, d)]
+    return np.ascontiguousarray(v), np.ascontiguousarray(np.array(tris, np.int32))
+
+
+def box_mesh(lo=(0.3, 0.3, 0.3), hi=(0.7, 0.7, 0.7)):
+    """Closed 12-triangle mesh of an axis-aligned box."""
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    v = np.array([[hi[0] if i & 1 else lo[0], hi[1] if i & 2 else lo[1], hi[2] if i & 4 else lo[2]]
+                  for i in range(8)])
+    tris = [(0, 2, 1), (1, 2, 3), (4, 5, 6), (5, 7, 6), (0, 1, 4), (1, 5, 4), (2, 6, 3), (3, 6, 7),
+            (0, 4, 2), (2, 4, 6), (1, 3, 5), (3, 7, 5)]
+    return np.ascontiguousarray(v), np.ascontiguousarray(np.array(tris, np.int32))
+
+
 def poisson_rhs(active, fluid_sdf, seed=3):
     """Right-hand side U[-1,1] on active cells, mean-subtracted on every
     6-connected active component that has no air (fluid_sdf > 0) face

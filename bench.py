@@ -45,6 +45,7 @@ FRAME_DT = 1.0 / 120.0
 DIFF_N = 64
 DIFF_STEPS = 20
 LARGE_N = 512
+COLLIDER_N = 256
 
 
 def build_scene(n, device=None):
@@ -266,6 +267,48 @@ def large_solve_leg(args, dev, ctx, replicas):
     return out
 
 
+def collider_leg(args, dev, ctx):
+    """setCollider(mesh): manifold2SDF of a closed 20,480-triangle sphere (icosphere
+    subdivided 5 times, radius 0.3) on the GPU at 128^3 and 256^3 (device-resident
+    mesh, CUDA events on torch's stream around the call), and the CPU oracle
+    (sequential, as the reference) on the 128^3 grid."""
+    import torch
+
+    from simcraft_b200 import scenes
+    from simcraft_b200.mesh import manifold_to_sdf
+
+    v, t = scenes.icosphere(5, 0.3)
+    vd, td = torch.from_numpy(v).to(dev), torch.from_numpy(t).to(dev)
+    out = {"workload": f"closed sphere mesh, {len(t)} triangles, exact band 3, reference distance arithmetic",
+           "triangles": len(t)}
+    stream = torch.cuda.current_stream(dev)
+    for n in (128, COLLIDER_N):
+        for _ in range(2):
+            manifold_to_sdf(vd, td, (n, n, n), 1.0 / n, context=ctx)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 3
+        e0.record(stream)
+        for _ in range(reps):
+            sdf = manifold_to_sdf(vd, td, (n, n, n), 1.0 / n, context=ctx)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[f"gpu_ms_{n}"] = e0.elapsed_time(e1) / reps
+        if n == 128:
+            sdf128 = sdf.cpu().numpy()
+        del sdf
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        O.build()
+        t0 = time.perf_counter()
+        ref, _, _ = O.manifold_to_sdf(v, t, (128, 128, 128), 1.0 / 128)
+        out["cpu_baseline"] = {"value": 1e3 * (time.perf_counter() - t0), "unit": "ms", "cores": 1, "kind": "port",
+                               "sample": "the same mesh on the 128^3 grid (the reference's sequential algorithm)",
+                               "bit_exact_vs_gpu": bool(np.array_equal(ref, sdf128))}
+    return out
+
+
 def flip_leg(args, dev, ctx, dist, rank, world):
     """FLIP substeps/s on the 256^3 FP32 dam break (device-resident particles)."""
     import torch
@@ -446,6 +489,7 @@ def main():
     ap.add_argument("--large-steps", type=int, default=1,
                     help="timed solves of the 512^3 FP64-vs-mixed leg (0 skips the leg)")
     ap.add_argument("--large-warmup", type=int, default=2, help="untimed solves of the 512^3 leg")
+    ap.add_argument("--collider", type=int, default=1, help="mesh-to-SDF collider leg (0 skips)")
     ap.add_argument("--diff-dirs", type=int, default=16,
                     help="finite-difference directions of the differentiable leg (-1 skips the leg)")
     args = ap.parse_args()
@@ -642,6 +686,8 @@ def main():
         out["solve_512"] = large_solve_leg(args, dev, ctx, replicas)
     if args.flip_steps > 0:
         out["flip"] = flip_leg(args, dev, ctx, dist, rank, world)
+    if args.collider:
+        out["collider"] = collider_leg(args, dev, ctx)
     if args.diff_dirs >= 0:
         out["diff"] = diff_leg(args, ctx, replicas)
     if rank == 0:

@@ -112,6 +112,16 @@ __device__ __forceinline__ Box tri_box(const MeshGeo& g, D3 a, D3 b, D3 c, int b
   return r;
 }
 
+// Vertex coordinates of every triangle, 9 doubles each (one dependent load per
+// neighbour in the sweeps instead of two).
+__global__ void k_mesh_pack(const double* V, const int32_t* T, int64_t ntri, double* P) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 9 * ntri; i += stride) {
+    const int64_t t = i / 9, r = i - 9 * t;
+    P[i] = V[3 * (int64_t)T[3 * t + r / 3] + r % 3];
+  }
+}
+
 __global__ void k_mesh_check(const int32_t* T, int64_t ntri, int64_t nvert, int* flag) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 3 * ntri; i += stride)
@@ -197,40 +207,137 @@ __global__ void k_mesh_closest(int64_t n, int* closest) {
     if (closest[e] == INT_MAX) closest[e] = -1;
 }
 
-// One hyperplane of sweep(dx, dy, dz) (util.cc:182-201): the pass visits x from
-// the far end when dx > 0 (x = nx-1 first) and from 0 when dx < 0, likewise y
-// and z; oriented coordinates x' = dx < 0 ? x : nx-1-x, etc.
-__global__ void __launch_bounds__(kMeshThreads)
-    k_mesh_sweep(MeshGeo g, const double* V, const int32_t* T, double* sdf, int* closest, int p,
-                 int dx, int dy, int dz) {
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (int64_t)g.nx * g.ny) return;
+// One cell of sweep(dx, dy, dz) (util.cc:182-201) on hyperplane p: the pass
+// visits x from the far end when dx > 0 (x = nx-1 first) and from 0 when
+// dx < 0, likewise y and z; oriented coordinates x' = dx < 0 ? x : nx-1-x, etc.
+// q enumerates (x', y'); z' = p - x' - y'.  Neighbour values written by other
+// blocks in earlier planes are read past L1 (__ldcg).
+__device__ __forceinline__ void sweep_cell(const MeshGeo& g, const double* P, double* sdf, int* closest,
+                                           int64_t q, int p, int dx, int dy, int dz) {
   const int xp = (int)(q / g.ny), yp = (int)(q % g.ny), zp = p - xp - yp;
   if (zp < 0 || zp >= g.nz) return;
   const int x = dx < 0 ? xp : g.nx - 1 - xp;
   const int y = dy < 0 ? yp : g.ny - 1 - yp;
   const int z = dz < 0 ? zp : g.nz - 1 - zp;
   const int64_t e = g.at(x, y, z);
-  double d = sdf[e];
-  int cl = closest[e];
   const D3 pc = g.coord(x, y, z);
-  // checkNeighbour (util.cc:159-180) in the reference's order
+  // checkNeighbour (util.cc:159-180).  The loads of the seven neighbours'
+  // triangles and then of their packed vertices are issued together (two round
+  // trips instead of 21 dependent ones); a triangle already
+  // measured for this cell reuses its distance (same inputs, same result); the
+  // comparisons then run in the reference's order.
   const int off[7][3] = {{0, dy, dz}, {dx, 0, dz}, {dx, dy, 0}, {0, 0, dz},
                          {0, dy, 0},  {dx, 0, 0},  {dx, dy, dz}};
+  int tn[7];
 #pragma unroll
   for (int k = 0; k < 7; k++) {
     const int nx_ = x + off[k][0], ny_ = y + off[k][1], nz_ = z + off[k][2];
-    if (nx_ < 0 || nx_ >= g.nx || ny_ < 0 || ny_ >= g.ny || nz_ < 0 || nz_ >= g.nz) continue;
-    const int t = closest[g.at(nx_, ny_, nz_)];
-    if (t == -1) continue;
-    const double d1 = dist_point_tri(pc, vtx(V, T, t, 0), vtx(V, T, t, 1), vtx(V, T, t, 2), g.exact);
-    if (fabs(d1) < fabs(d)) {
-      d = d1;
-      cl = t;
-    }
+    const bool in = nx_ >= 0 && nx_ < g.nx && ny_ >= 0 && ny_ < g.ny && nz_ >= 0 && nz_ < g.nz;
+    tn[k] = in ? __ldcg(&closest[g.at(nx_, ny_, nz_)]) : -1;
   }
+  double d = __ldcg(&sdf[e]);
+  int cl = __ldcg(&closest[e]);
+  double dk[7];
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    dk[k] = 0.0;
+    if (tn[k] < 0) continue;
+    int same = -1;
+#pragma unroll
+    for (int j = 0; j < k; j++)
+      if (same < 0 && tn[j] == tn[k]) same = j;
+    if (same >= 0) {
+#pragma unroll
+      for (int j = 0; j < k; j++)
+        if (j == same) dk[k] = dk[j];
+      continue;
+    }
+    const double* tp = P + 9 * (int64_t)tn[k];
+    const D3 ta{__ldg(tp), __ldg(tp + 1), __ldg(tp + 2)};
+    const D3 tb{__ldg(tp + 3), __ldg(tp + 4), __ldg(tp + 5)};
+    const D3 tc{__ldg(tp + 6), __ldg(tp + 7), __ldg(tp + 8)};
+    dk[k] = dist_point_tri(pc, ta, tb, tc, g.exact);
+  }
+#pragma unroll
+  for (int k = 0; k < 7; k++)
+    if (tn[k] != -1 && fabs(dk[k]) < fabs(d)) {
+      d = dk[k];
+      cl = tn[k];
+    }
   sdf[e] = d;
   closest[e] = cl;
+}
+
+// The reference's pass order: (1,1,1), (1,1,-1), (1,-1,1), ..., (-1,-1,-1), twice.
+__device__ __host__ __forceinline__ void pass_dir(int d, int& dx, int& dy, int& dz) {
+  dx = (d & 4) ? -1 : 1;
+  dy = (d & 2) ? -1 : 1;
+  dz = (d & 1) ? -1 : 1;
+}
+
+// One plane per launch (fallback when cooperative launches are unavailable).
+__global__ void __launch_bounds__(kMeshThreads)
+    k_mesh_sweep(MeshGeo g, const double* P, double* sdf, int* closest, int p, int dx, int dy, int dz) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < (int64_t)g.nx * g.ny) sweep_cell(g, P, sdf, closest, q, p, dx, dy, dz);
+}
+
+// Grid-wide barrier of a cooperative launch (all blocks co-resident): arrival
+// by a release add, the last arriver publishes the next generation with a
+// release add, the others poll it with acquire loads.  The wait is bounded:
+// after kSweepSpin polls the block raises *err and stops waiting, and every
+// later barrier returns at once.
+constexpr int kSweepSpin = 1 << 24;
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned add_acq_rel(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0 && !*(volatile int*)err) {
+    const unsigned g0 = ld_acquire(gen);
+    if (add_acq_rel(count, 1u) == gridDim.x - 1) {
+      *(volatile unsigned*)count = 0;
+      add_acq_rel(gen, 1u);
+    } else {
+      int spins = 0;
+      while (ld_acquire(gen) == g0) {
+        if (++spins > kSweepSpin || *(volatile int*)err) {
+          atomicOr(err, 1);
+          break;
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// All 16 passes in one cooperative launch, a grid barrier after every plane.
+__global__ void __launch_bounds__(kMeshThreads)
+    k_mesh_sweep_all(MeshGeo g, const double* P, double* sdf, int* closest, unsigned* count, unsigned* gen,
+                     int* err) {
+  const int planes = g.nx + g.ny + g.nz - 2;
+  const int64_t cols = (int64_t)g.nx * g.ny;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int pass = 0; pass < 16; pass++) {
+    int dx, dy, dz;
+    pass_dir(pass & 7, dx, dy, dz);
+    for (int p = 0; p < planes; p++) {
+      // (x', y') pairs whose z' = p - x' - y' lies in [0, nz)
+      const int xlo = max(0, p - (g.ny - 1) - (g.nz - 1)), xhi = min(g.nx - 1, p);
+      for (int64_t q = (int64_t)xlo * g.ny + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+           q < (int64_t)(xhi + 1) * g.ny && q < cols; q += stride)
+        sweep_cell(g, P, sdf, closest, q, p, dx, dy, dz);
+      grid_barrier(count, gen, err);
+      if (*(volatile int*)err) return;
+    }
+  }
 }
 
 // Sign from the parity of the crossings counted at or below each cell (util.cc:301-309).
@@ -252,15 +359,18 @@ int mesh_to_sdf(cudaStream_t st, const MeshSdfArgs& a, double* sdf, int32_t* clo
   const int64_t cols = (int64_t)a.nx * a.ny;
   int* cl = closest;
   int *cnt = nullptr, *flag = nullptr;
+  double* packed = nullptr;
   auto fail = [&](int rc, const char* what) {
     if (msg) *msg = what;
+    if (packed) cudaFreeAsync(packed, st);
     if (cnt) cudaFreeAsync(cnt, st);
     if (flag) cudaFreeAsync(flag, st);
     if (cl && cl != closest) cudaFreeAsync(cl, st);
     return rc;
   };
   if (cudaMallocAsync(&cnt, sizeof(int) * (size_t)N, st) != cudaSuccess ||
-      cudaMallocAsync(&flag, sizeof(int), st) != cudaSuccess ||
+      cudaMallocAsync(&flag, 4 * sizeof(int), st) != cudaSuccess ||
+      cudaMallocAsync(&packed, sizeof(double) * 9 * (size_t)std::max<int64_t>(a.ntriangles, 1), st) != cudaSuccess ||
       (!cl && cudaMallocAsync(&cl, sizeof(int) * (size_t)N, st) != cudaSuccess))
     return fail(-3, "mesh_to_sdf: scratch allocation failed");
   // triangle indices must name vertices
@@ -285,22 +395,54 @@ int mesh_to_sdf(cudaStream_t st, const MeshSdfArgs& a, double* sdf, int32_t* clo
     k_mesh_cross<<<tg, kMeshThreads, 0, st>>>(g, a.vertices, a.triangles, a.ntriangles, cnt);
   }
   k_mesh_closest<<<eblocks, kMeshThreads, 0, st>>>(N, cl);
-  // sweep(1,1,1), (1,1,-1), (1,-1,1), (1,-1,-1), (-1,1,1), ..., twice (util.cc:291-300)
+  if (a.ntriangles > 0)
+    k_mesh_pack<<<(int)std::min<int64_t>((9 * a.ntriangles + kMeshThreads - 1) / kMeshThreads, 4096), kMeshThreads,
+                  0, st>>>(a.vertices, a.triangles, a.ntriangles, packed);
+  // sweep(1,1,1), (1,1,-1), (1,-1,1), (1,-1,-1), (-1,1,1), ..., twice (util.cc:291-300):
+  // one cooperative launch with a grid barrier per plane (co-resident grid),
+  // else one launch per plane
   const int planes = a.nx + a.ny + a.nz - 2;
   const int sblocks = (int)((cols + kMeshThreads - 1) / kMeshThreads);
-  for (int round = 0; round < 2; round++)
-    for (int d = 0; d < 8; d++) {
-      const int dx = (d & 4) ? -1 : 1, dy = (d & 2) ? -1 : 1, dz = (d & 1) ? -1 : 1;
+  bool coop = false;
+  {
+    int dev = 0, sms = 0, can = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&can, cudaDevAttrCooperativeLaunch, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (can && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mesh_sweep_all, kMeshThreads, 0) ==
+                   cudaSuccess && occ > 0) {
+      // one block per SM: a plane holds at most ~(3/4) nx ny cells, and fewer
+      // arrivals make the per-plane barrier cheaper
+      const int grid = (int)std::min<int64_t>((int64_t)sms, (int64_t)sblocks);
+      unsigned* bar = reinterpret_cast<unsigned*>(flag + 1);
+      cudaMemsetAsync(flag, 0, 4 * sizeof(int), st);
+      const double* P = packed;
+      unsigned* gen = bar + 1;
+      void* args[] = {(void*)&g, (void*)&P, (void*)&sdf, (void*)&cl, (void*)&bar, (void*)&gen, (void*)&flag};
+      coop = cudaLaunchCooperativeKernel((const void*)k_mesh_sweep_all, grid, kMeshThreads, args, 0, st) ==
+             cudaSuccess;
+      if (!coop) cudaGetLastError();
+    }
+  }
+  if (!coop)
+    for (int pass = 0; pass < 16; pass++) {
+      int dx, dy, dz;
+      pass_dir(pass & 7, dx, dy, dz);
       for (int p = 0; p < planes; p++)
-        k_mesh_sweep<<<sblocks, kMeshThreads, 0, st>>>(g, a.vertices, a.triangles, sdf, cl, p, dx, dy, dz);
+        k_mesh_sweep<<<sblocks, kMeshThreads, 0, st>>>(g, packed, sdf, cl, p, dx, dy, dz);
     }
   k_mesh_sign<<<sblocks, kMeshThreads, 0, st>>>(g, sdf, cnt);
+  // the sweep's wait status
+  cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(cnt, st);
   cudaFreeAsync(flag, st);
+  cudaFreeAsync(packed, st);
   if (cl != closest) cudaFreeAsync(cl, st);
   cnt = flag = nullptr;
+  packed = nullptr;
   cl = closest;
   if (cudaStreamSynchronize(st) != cudaSuccess) return fail(-2, "mesh_to_sdf");
+  if (coop && hflag) return fail(-6, "mesh_to_sdf: a sweep barrier wait timed out");
   return 0;
 }
 

@@ -1102,11 +1102,13 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
           if (--sl < 0) sl = g.nz - 1;
         }
       };
-      // The warp stages the NV input rows of step s + kStage - 1 into ring slot
-      // (s - 1) mod kStage at the start of step s, as kChunk-byte cp.async chunks
-      // spread over the lanes (CPL per lane, pointers fixed per tile).  The slot
-      // was last read in step s - 1, before that step's barrier; each lane waits
-      // for its own chunks of step s + 1 before the barrier of step s, and the
+      // The warp stages the NV input rows of step s + kStage into ring slot
+      // s mod kStage at the end of step s, as kChunk-byte cp.async chunks spread
+      // over the lanes (CPL per lane, pointers fixed per tile): after the step's
+      // dependent chain, so the copies are issued while the other warps are
+      // still on theirs.  The warp's lanes read that slot at the start of step s
+      // (a __syncwarp orders the reads before the refill); each lane waits for
+      // its own chunks of step s + 1 before the barrier of step s, and the
       // barrier makes every lane's chunks visible to the warp.
       constexpr int kStage = wave_stages<T, Op::NV>();
       constexpr int kChunk = sizeof(T) == 8 ? SC_WAVE_CHUNK64 : SC_WAVE_CHUNK32;  // bytes
@@ -1135,12 +1137,12 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
           if (Op::NV * CPR % 32 == 0 || cg[i]) cp_async_bytes<kChunk>(stage + ridx * kStageStride + coff[i], cg[i] + so);
       };
 #pragma unroll
-      for (int r = 0; r < kStage - 1; r++) {
+      for (int r = 0; r < kStage; r++) {
         if (r < NS) issue(pslot, r);
         cp_async_commit();
         advance(pslot);
       }
-      cp_async_wait<kStage - 2>();
+      cp_async_wait<kStage - 1>();
       T prev = T(0);
       named_bar_sync(1, NBAR);
       for (int s0 = 0; s0 < NS; s0 += kStage) {
@@ -1148,9 +1150,6 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
         for (int u = 0; u < kStage; u++) {
           const int s = s0 + u;
           if (s < NS) {
-            if (s + kStage - 1 < NS) issue(pslot, (u + kStage - 1) % kStage);
-            cp_async_commit();
-            advance(pslot);
             T v[Op::NV];
 #pragma unroll
             for (int k = 0; k < Op::NV; k++) v[k] = my_stage[u * kStageStride + k * 32];
@@ -1175,7 +1174,11 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
             sh.xch[s & 1][ty][lane] = val;
             prev = val;
             advance(cslot);
-            cp_async_wait<kStage - 2>();
+            __syncwarp();
+            if (s + kStage < NS) issue(pslot, u);
+            cp_async_commit();
+            advance(pslot);
+            cp_async_wait<kStage - 1>();
             named_bar_sync(1, NBAR);
           }
         }

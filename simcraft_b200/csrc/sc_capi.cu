@@ -321,9 +321,6 @@ int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b) {
   return map_status(pcg->solver->apply_only(x, b));
 }
 
-int sc_debug_pcg_dump(sc_pcg* pcg, int which, double* out) {
-  return pcg->solver->debug_dump(which, out);
-}
 int sc_pcg_time_kernels(sc_pcg* pcg, int reps, double* ms_out) {
   if (!pcg || reps < 1 || !ms_out) return SC_ERR_INVALID;
   cudaSetDevice(pcg->ctx->c.device);

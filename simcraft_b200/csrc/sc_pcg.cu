@@ -1999,52 +1999,6 @@ int PcgSolver::apply_only(const double* x, double* b) {
 }
 
 
-namespace {
-template <class T>
-__global__ void k_mb_count(int64_t n, const T* mb, unsigned long long* cnt) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  unsigned long long c = 0;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
-    typename Sentinel<T>::Bits b;
-    memcpy(&b, mb + e, sizeof(T));
-    if (b != Sentinel<T>::bits) c++;
-  }
-  if (c) atomicAdd(cnt, c);
-}
-}  // namespace
-
-// Debug: copy an internal tiled FP64 array to a device buffer in reference layout
-// (0 E, 1 cL, 2 cD, 3 cB, 4 uR, 5 uU, 6 uF, 7 q, 8 z); which = 100/101 counts
-// non-sentinel x/y mailbox words into out[0].
-int PcgSolver::debug_dump(int which, double* out) {
-  cudaStream_t s = ctx_->stream;
-  const int grid = grid_for(g_.total, ctx_->sm_count);
-  if (which >= 100) {
-    unsigned long long* cnt = nullptr;
-    cudaMallocAsync(&cnt, 8, s);
-    cudaMemsetAsync(cnt, 0, 8, s);
-    const int ntiles = g_.ntiles();
-    if (which == 100) k_mb_count<double><<<grid, kThreads, 0, s>>>(mb_stride_x_ * ntiles, mbx64_, cnt);
-    else k_mb_count<double><<<grid, kThreads, 0, s>>>(mb_stride_y_ * ntiles, mby64_, cnt);
-    unsigned long long h = 0;
-    cudaMemcpyAsync(&h, cnt, 8, cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
-    cudaFreeAsync(cnt, s);
-    out[0] = (double)h;
-    return check_dev_error("debug");
-  }
-  const double* src[] = {d64_.E, d64_.cL, d64_.cD, d64_.cB, d64_.uR, d64_.uU, d64_.uF, d64_.q, d64_.z};
-  if (which < 0 || which > 8) return -1;
-  double* tmp = nullptr;
-  const int64_t N = (int64_t)g_.nx * g_.ny * g_.nz;
-  cudaMallocAsync(&tmp, sizeof(double) * N, s);
-  k_from_tiled<double, double><<<grid, kThreads, 0, s>>>(g_, src[which], tmp);
-  cudaMemcpyAsync(out, tmp, sizeof(double) * N, cudaMemcpyDeviceToHost, s);
-  cudaFreeAsync(tmp, s);
-  cudaStreamSynchronize(s);
-  return check_dev_error("debug");
-}
-
 int PcgSolver::time_kernels(int reps, double* ms) {
   cudaStream_t s = ctx_->stream;
   int e = ensure_pivots();

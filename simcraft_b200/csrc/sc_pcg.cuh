@@ -124,7 +124,6 @@ class PcgSolver {
   int precond_only(const double* r, double* z);
   // applyCompressedMatrix on the uploaded system (device pointers, reference layout).
   int apply_only(const double* x, double* b);
-  int debug_dump(int which, double* out);
   // Device time per launch of each kernel class (see sc_pcg_time_kernels).
   int time_kernels(int reps, double* ms);
 

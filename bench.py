@@ -214,6 +214,48 @@ def build_system_device(n, sdf, dev, ctx):
     return adiag, an, active, act_h, np.ascontiguousarray(rhs_h), rinfo
 
 
+def tolerance_sweep(n, ctx, adiag, an, rhs_d, active, act_h):
+    """The standalone system at the tolerances 1e-6, 1e-8 and 1e-10 (relative
+    L2), FP64 against mixed: ms per solve (best of 2 after a warm-up, solver
+    events), iterations, and each solution's relative L2 error over the active
+    cells against an FP64 MIC(0)-PCG solve to 1e-12."""
+    import torch
+
+    from simcraft_b200 import _capi
+    from simcraft_b200.solver import CgSolver3D, CRIT_REL_L2, PREC_FP64, PREC_MIXED
+
+    L = _capi.lib()
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    an_dev = _capi.ptr_array([ptr(a) for a in an])
+    mask = torch.from_numpy(act_h.astype(bool)).to(rhs_d.device)
+
+    def solve(s, out):
+        st = _capi.sc_pcg_stats()
+        rc = L.sc_pcg_solve_device(s.handle, ptr(adiag), an_dev, ptr(rhs_d), ptr(active), ptr(out),
+                                   ctypes.byref(st))
+        _capi.check("sc_pcg_solve_device", rc, ctx.handle)
+        return st
+
+    ref = torch.zeros((n, n, n), dtype=torch.float64, device=rhs_d.device)
+    solve(CgSolver3D(n, n, n, context=ctx, tol=1e-12, max_iter=10000, criterion=CRIT_REL_L2, precision=PREC_FP64),
+          ref)
+    ref_norm = float(ref[mask].norm())
+    pg = torch.zeros_like(ref)
+    rows = []
+    for tol in (1e-6, 1e-8, 1e-10):
+        row = {"tolerance": tol}
+        for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+            s = CgSolver3D(n, n, n, context=ctx, tol=tol, max_iter=10000, criterion=CRIT_REL_L2, precision=prec)
+            sts = [solve(s, pg) for _ in range(3)]
+            st = sts[-1]
+            row[name] = {"ms_per_solve": min(x.ms for x in sts[1:]), "iterations": st.iterations,
+                         "true_rel_l2": st.true_rel_l2,
+                         "error_vs_fp64_1e-12": float((pg - ref)[mask].norm()) / ref_norm}
+            del s
+        rows.append(row)
+    return {"reference": "FP64 MIC(0)-PCG to 1e-12 relative residual on the GPU", "rows": rows}
+
+
 def large_solve_leg(args, dev, ctx, replicas):
     """FP64 against mixed on the 512^3 sphere pool (60% fill, seed 9), both to
     1e-8 relative residual, device-resident inputs; `--large-steps` timed solves
@@ -259,11 +301,74 @@ def large_solve_leg(args, dev, ctx, replicas):
         ms = replicas.max(e0.elapsed_time(e1)) / max(1, args.large_steps)
         out[name] = {"ms_per_solve": ms, "iterations": st.iterations, "outer": st.outer,
                      "true_rel_l2": st.true_rel_l2, "kernel_launches": st.kernel_launches}
+        if name == "fp64":
+            pg64 = pg.clone()
+        else:
+            m = torch.from_numpy(act_h.astype(bool)).to(dev)
+            out[name]["rel_l2_vs_fp64_solution"] = float((pg - pg64)[m].norm() / pg64[m].norm())
+            del m, pg64
         del s
         torch.cuda.empty_cache()
     out["fp64_over_mixed"] = out["fp64"]["ms_per_solve"] / out["mixed"]["ms_per_solve"]
     del adiag, an, active, rhs_d, pg
     torch.cuda.empty_cache()
+    return out
+
+
+def flip32_leg(args, ctx):
+    """The 32^3 FP64 dam break of the parity runs (block x<0.5, y<0.5, 8 particles
+    per cell, FLIP 0.95, MIC(0)-PCG to 1e-6 relative, at most 200 iterations):
+    frames/s on the GPU, wall clock around 10 frames of dt = 1/120 from the
+    initial state (host round trips included; a separate simulator warms up
+    first), and the CPU oracle (all host threads) on the same 10 frames, with
+    pressure and positions compared after the last one."""
+    import torch
+
+    from simcraft_b200 import scenes
+    from simcraft_b200.fluid import FluidSimulator
+    from simcraft_b200.solver import CRIT_REL_L2
+
+    n, frames = 32, 10
+    pos, vel, h = scenes.dam_break(n, seed=1)
+    kw = dict(context=ctx, flip_alpha=0.95, pcg_tol=1e-6, pcg_max_iter=200, pcg_criterion=CRIT_REL_L2)
+    warm = FluidSimulator(len(pos), (1.0, 1.0, 1.0), (n, n, n), **kw)
+    warm.set_initial_fluid(pos, vel)
+    for _ in range(3):
+        warm.step(FRAME_DT)
+    del warm
+    sim = FluidSimulator(len(pos), (1.0, 1.0, 1.0), (n, n, n), **kw)
+    sim.set_initial_fluid(pos, vel)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        st = sim.step(FRAME_DT)
+    torch.cuda.synchronize()
+    gpu_ms = (time.perf_counter() - t0) * 1e3 / frames
+    out = {"workload": "FLIP dam break 32^3 FP64, 65,536 particles, FLIP 0.95, PCG to 1e-6 relative (max 200)",
+           "frames": frames, "ms_per_frame": gpu_ms, "frames_per_s": 1e3 / gpu_ms,
+           "device_ms_last_frame": st["ms_total"], "pcg_iterations_last_frame": st["pcg_iterations"]}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        O.build()
+        threads = os.cpu_count() or 1
+        O.set_threads(threads)
+        O.set_parity_mode(False)
+        ref = O.Sim(**O.default_config(n, n, n, h, flip_alpha=0.95, pcg_tol=1e-6, pcg_max_iter=200,
+                                       pcg_criterion=CRIT_REL_L2))
+        ref.set_particles(pos, vel)
+        t0 = time.perf_counter()
+        for _ in range(frames):
+            ref.step(FRAME_DT)
+        cpu_ms = (time.perf_counter() - t0) * 1e3 / frames
+        p_ref, p = ref.pressure(), sim.pressure()
+        x_ref, _ = ref.particles()
+        x, _ = sim.particles()
+        out["cpu_baseline"] = {"value": cpu_ms, "unit": "ms/frame", "cores": threads, "kind": "port",
+                               "sample": f"the same {frames} frames (CPU oracle, OpenMP transfers)",
+                               "pressure_rel_l2_vs_gpu": float(np.linalg.norm(p - p_ref) / np.linalg.norm(p_ref)),
+                               "positions_max_err_over_h": float(np.abs(x - x_ref).max() / h)}
     return out
 
 
@@ -490,6 +595,7 @@ def main():
                     help="timed solves of the 512^3 FP64-vs-mixed leg (0 skips the leg)")
     ap.add_argument("--large-warmup", type=int, default=2, help="untimed solves of the 512^3 leg")
     ap.add_argument("--collider", type=int, default=1, help="mesh-to-SDF collider leg (0 skips)")
+    ap.add_argument("--flip32", type=int, default=1, help="32^3 FP64 dam-break leg (0 skips)")
     ap.add_argument("--diff-dirs", type=int, default=16,
                     help="finite-difference directions of the differentiable leg (-1 skips the leg)")
     args = ap.parse_args()
@@ -682,12 +788,16 @@ def main():
                                                            np.linalg.norm(pg_cpu[a]))}
     del solvers
     torch.cuda.empty_cache()
+    if rank == 0:
+        out["tolerance_sweep"] = tolerance_sweep(n, ctx, adiag, an, rhs_d, active, act_h)
     if args.large_steps > 0:
         out["solve_512"] = large_solve_leg(args, dev, ctx, replicas)
     if args.flip_steps > 0:
         out["flip"] = flip_leg(args, dev, ctx, dist, rank, world)
     if args.collider:
         out["collider"] = collider_leg(args, dev, ctx)
+    if args.flip32:
+        out["flip_32"] = flip32_leg(args, ctx)
     if args.diff_dirs >= 0:
         out["diff"] = diff_leg(args, ctx, replicas)
     if rank == 0:

@@ -315,7 +315,7 @@ def large_solve_leg(args, dev, ctx, replicas):
     return out
 
 
-def flip32_leg(args, ctx):
+def flip32_leg(args, ctx, cpu):
     """The 32^3 FP64 dam break of the parity runs (block x<0.5, y<0.5, 8 particles
     per cell, FLIP 0.95, MIC(0)-PCG to 1e-6 relative, at most 200 iterations):
     frames/s on the GPU, wall clock around 10 frames of dt = 1/120 from the
@@ -347,7 +347,7 @@ def flip32_leg(args, ctx):
     out = {"workload": "FLIP dam break 32^3 FP64, 65,536 particles, FLIP 0.95, PCG to 1e-6 relative (max 200)",
            "frames": frames, "ms_per_frame": gpu_ms, "frames_per_s": 1e3 / gpu_ms,
            "device_ms_last_frame": st["ms_total"], "pcg_iterations_last_frame": st["pcg_iterations"]}
-    if not args.no_cpu:
+    if cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
 
@@ -372,7 +372,7 @@ def flip32_leg(args, ctx):
     return out
 
 
-def collider_leg(args, dev, ctx):
+def collider_leg(args, dev, ctx, cpu):
     """setCollider(mesh): manifold2SDF of a closed 20,480-triangle sphere (icosphere
     subdivided 5 times, radius 0.3) on the GPU at 128^3 and 256^3 (device-resident
     mesh, CUDA events on torch's stream around the call), and the CPU oracle
@@ -401,7 +401,7 @@ def collider_leg(args, dev, ctx):
         if n == 128:
             sdf128 = sdf.cpu().numpy()
         del sdf
-    if not args.no_cpu:
+    if cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
 
@@ -794,10 +794,12 @@ def main():
         out["solve_512"] = large_solve_leg(args, dev, ctx, replicas)
     if args.flip_steps > 0:
         out["flip"] = flip_leg(args, dev, ctx, dist, rank, world)
+    # CPU oracles on the host cores: one process only (as for the solve leg)
+    cpu = rank == 0 and world == 1 and not args.no_cpu
     if args.collider:
-        out["collider"] = collider_leg(args, dev, ctx)
+        out["collider"] = collider_leg(args, dev, ctx, cpu)
     if args.flip32:
-        out["flip_32"] = flip32_leg(args, ctx)
+        out["flip_32"] = flip32_leg(args, ctx, cpu)
     if args.diff_dirs >= 0:
         out["diff"] = diff_leg(args, ctx, replicas)
     if rank == 0:

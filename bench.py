@@ -141,6 +141,15 @@ def cpu_solve_ms(sysm, rhs, threads):
     return (time.perf_counter() - t) * 1e3, it, pg
 
 
+def solve_config(n, info, n_active, world):
+    """The `config` of the headline workload, the same in both arms."""
+    return {"workload": f"standalone pressure solve {n}^3 to {TOL:g} relative residual (sphere pool)",
+            "grid": [n, n, n], "fill": info["fill"], "active_cells": n_active, "dt_over_h": DT_OVER_H,
+            "tolerance": TOL, "criterion": "relative L2",
+            "cache": "inputs larger than L2 (solver working set ~300 MB at 128^3)",
+            "parallelism": f"replicas x{world}"}
+
+
 def reference_arm(args, rank):
     if rank != 0:
         return
@@ -153,7 +162,7 @@ def reference_arm(args, rank):
     O.set_threads(threads)
     O.set_parity_mode(False)
     n = args.solve_n
-    sdf, _ = build_scene(n)
+    sdf, info = build_scene(n)
     h = 1.0 / n
     z = np.zeros
     S = O.build_system((n, n, n), h, DT_OVER_H * h, z((n + 1, n, n)), z((n, n + 1, n)), z((n, n, n + 1)), sdf)
@@ -168,9 +177,9 @@ def reference_arm(args, rank):
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "ms/solve", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded spheres)",
-        "config": {"workload": f"standalone pressure solve {n}^3, FP64 MIC(0)-PCG to {TOL:g} rel. residual",
-                   "grid": [n, n, n], "iterations": it},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sphere pool, no dataset)",
+        "config": solve_config(n, info, int(S["active"].sum()), args.gpus),
+        "solver": f"FP64 MIC(0)-PCG, CPU oracle of the reference path, {it} iterations",
         "cpu_baseline": {"value": v, "unit": "ms/solve", "cores": threads, "kind": "port",
                          "sample": f"one full FP64 solve of the {n}^3 system per step (CPU oracle, "
                                    f"OpenMP where the reference uses TBB, serial MIC(0) as the reference)"},
@@ -755,11 +764,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64 (FP32 Eisenstat-form MIC(0) CG, FP64 residual replacement)",
         "data": "synthetic (seeded sphere pool, no dataset)",
-        "config": {"workload": f"standalone pressure solve {n}^3, mixed MIC(0)-PCG to {TOL:g} rel. residual",
-                   "grid": [n, n, n], "fill": info["fill"], "active_cells": n_active,
-                   "dt_over_h": DT_OVER_H, "tolerance": TOL, "criterion": "relative L2",
-                   "cache": "inputs larger than L2 (solver working set ~300 MB at 128^3)",
-                   "parallelism": f"replicas x{world}"},
+        "config": solve_config(n, info, n_active, world),
+        "solver": "mixed MIC(0)-PCG: FP32 CG on the split system (Eisenstat) with FP64 residual replacement",
         "fp64": {"ms_per_solve": ms_fp64 / args.steps, "iterations": st_fp64.iterations,
                  "true_rel_l2": st_fp64.true_rel_l2},
         "mixed": {"ms_per_solve": ms_step, "inner_iterations": st_mixed.iterations,

@@ -1423,6 +1423,25 @@ int PcgSolver::check_dev_error(const char* where) {
   return 0;
 }
 
+// Staging buffers of the host-array entry points, allocated on first use and
+// kept: a per-call stream-ordered allocation can hand its pages back at the
+// solve's synchronisations and pay for mapping them again on the next call.
+int PcgSolver::ensure_host_stage() {
+  if (hstage_) return 0;
+  const size_t N = (size_t)g_.nx * g_.ny * g_.nz;
+  void *a = nullptr, *b = nullptr;
+  if (cudaMalloc(&a, sizeof(double) * N) != cudaSuccess) return ctx_->set_error(-3, "staging allocation failed");
+  if (cudaMalloc(&b, N) != cudaSuccess) {
+    cudaFree(a);
+    return ctx_->set_error(-3, "staging allocation failed");
+  }
+  allocs_.push_back(a);
+  allocs_.push_back(b);
+  hstage_ = (double*)a;
+  hstage_act_ = (uint8_t*)b;
+  return 0;
+}
+
 int PcgSolver::upload(const double* adiag, const double* const an[6], const double* rhs,
                       const uint8_t* active, bool device) {
   cudaStream_t st = ctx_->stream;
@@ -1434,9 +1453,9 @@ int PcgSolver::upload(const double* adiag, const double* const an[6], const doub
   double* stage = nullptr;
   uint8_t* stage_act = nullptr;
   if (!device) {
-    if (cudaMallocAsync(&stage, sizeof(double) * (size_t)N, st) != cudaSuccess ||
-        cudaMallocAsync(&stage_act, (size_t)N, st) != cudaSuccess)
-      return ctx_->set_error(-3, "upload: staging allocation failed");
+    if (int e = ensure_host_stage()) return e;
+    stage = hstage_;
+    stage_act = hstage_act_;
     cudaMemcpyAsync(stage_act, active, (size_t)N, cudaMemcpyHostToDevice, st);
   }
   const uint8_t* act_ref = device ? active : stage_act;
@@ -1479,8 +1498,6 @@ int PcgSolver::upload(const double* adiag, const double* const an[6], const doub
     if (all) cudaFreeAsync(all, st);
     if (sym_err_ > 1e-4) rc = -7;
   }
-  if (stage) cudaFreeAsync(stage, st);
-  if (stage_act) cudaFreeAsync(stage_act, st);
   pivots_valid_ = false;
   int e = check_dev_error("upload");
   if (e) return e;
@@ -1497,13 +1514,12 @@ int PcgSolver::upload_rhs(const double* rhs, bool device) {
   const double* s = rhs;
   double* stage = nullptr;
   if (!device) {
-    if (cudaMallocAsync(&stage, sizeof(double) * (size_t)N, st) != cudaSuccess)
-      return ctx_->set_error(-3, "upload_rhs: staging allocation failed");
+    if (int e = ensure_host_stage()) return e;
+    stage = hstage_;
     cudaMemcpyAsync(stage, rhs, sizeof(double) * (size_t)N, cudaMemcpyHostToDevice, st);
     s = stage;
   }
   k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g_, s, rhs_, nullptr);
-  if (stage) cudaFreeAsync(stage, st);
   return check_dev_error("upload_rhs");
 }
 
@@ -1517,13 +1533,11 @@ int PcgSolver::download_pressure(double* pg, bool device) {
     launches_ += 1;
     return check_dev_error("download_pressure");
   }
-  double* stage = nullptr;
-  if (cudaMallocAsync(&stage, sizeof(double) * (size_t)N, st) != cudaSuccess)
-    return ctx_->set_error(-3, "download: staging allocation failed");
+  if (int e = ensure_host_stage()) return e;
+  double* stage = hstage_;
   k_from_tiled<double, double><<<grid, kThreads, 0, st>>>(g_, src, stage);
   launches_ += 1;
   cudaMemcpyAsync(pg, stage, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost, st);
-  cudaFreeAsync(stage, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return check_dev_error("download_pressure");
   return check_dev_error("download_pressure");
 }

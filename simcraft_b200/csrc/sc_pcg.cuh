@@ -159,6 +159,9 @@ class PcgSolver {
   template <class T>
   void launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip);
   int check_dev_error(const char* where);
+  int ensure_host_stage();
+  double* hstage_ = nullptr;     // staging of the host-array entry points (N doubles)
+  uint8_t* hstage_act_ = nullptr;  // and of the active flags (N bytes)
 
   Context* ctx_;
   PcgOptions opt_;

@@ -308,8 +308,8 @@ def large_solve_leg(args, dev, ctx, replicas):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = replicas.max(e0.elapsed_time(e1)) / max(1, args.large_steps)
-        out[name] = {"ms_per_solve": ms, "iterations": st.iterations, "outer": st.outer,
-                     "true_rel_l2": st.true_rel_l2, "kernel_launches": st.kernel_launches}
+        out[name] = {"ms_per_solve": ms, "iterations": st.iterations, "iterations_per_s": st.iterations / (ms * 1e-3),
+                     "outer": st.outer, "true_rel_l2": st.true_rel_l2, "kernel_launches": st.kernel_launches}
         if name == "fp64":
             pg64 = pg.clone()
         else:
@@ -767,8 +767,10 @@ def main():
         "config": solve_config(n, info, n_active, world),
         "solver": "mixed MIC(0)-PCG: FP32 CG on the split system (Eisenstat) with FP64 residual replacement",
         "fp64": {"ms_per_solve": ms_fp64 / args.steps, "iterations": st_fp64.iterations,
+                 "iterations_per_s": st_fp64.iterations / (ms_fp64 / args.steps * 1e-3),
                  "true_rel_l2": st_fp64.true_rel_l2},
         "mixed": {"ms_per_solve": ms_step, "inner_iterations": st_mixed.iterations,
+                  "iterations_per_s": st_mixed.iterations / (ms_step * 1e-3),
                   "fp64_replacements": st_mixed.outer, "true_rel_l2": st_mixed.true_rel_l2},
         "mixed_speedup_vs_fp64": (ms_fp64 / ms_mixed),
         "e2e": {"value": e2e_ms / args.steps / world, "unit": "ms/solve", "h2d_bytes_per_step": h2d,

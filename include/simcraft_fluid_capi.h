@@ -271,7 +271,9 @@ int sc_reconstruct_device(sc_context* ctx, int64_t n, const double* pos, int nx,
  * distances come out too large (the sign is unaffected);
  * SC_MESH_EXACT_DISTANCE uses the true point-triangle distances.  A triangle
  * index outside [0, nvertices) returns SC_ERR_INVALID.  _device: device
- * arrays, on the context stream; _host: host arrays (copied in and out). */
+ * arrays, on the context stream; _host: host arrays (copied in and out).  The
+ * context keeps the scratch it needs (about 8 bytes per cell) until it is
+ * destroyed; calls on one context use it one at a time, like its stream. */
 enum { SC_MESH_REFERENCE_DISTANCE = 0, SC_MESH_EXACT_DISTANCE = 1 };
 int sc_mesh_to_sdf_device(sc_context* ctx, int nx, int ny, int nz, double h, const double* origin,
                           const double* vertices, int64_t nvertices, const int32_t* triangles,

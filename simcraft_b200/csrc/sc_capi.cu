@@ -19,6 +19,8 @@ struct sc_context {
   sc::Context c;
   cudaStream_t own = nullptr;
   std::atomic<int> refs{1};
+  void* mesh_scratch = nullptr;  // mesh-to-SDF scratch, grown on demand, kept until destroy
+  size_t mesh_scratch_bytes = 0;
 };
 
 static sc_context* ctx_retain(sc_context* c) {
@@ -27,10 +29,12 @@ static sc_context* ctx_retain(sc_context* c) {
 }
 static void ctx_release(sc_context* c) {
   if (c->refs.fetch_sub(1) == 1) {
-    if (c->own) {
-      cudaSetDevice(c->c.device);
-      cudaStreamDestroy(c->own);
+    cudaSetDevice(c->c.device);
+    if (c->mesh_scratch) {
+      cudaStreamSynchronize(c->c.stream);
+      cudaFree(c->mesh_scratch);
     }
+    if (c->own) cudaStreamDestroy(c->own);
     delete c;
   }
 }
@@ -498,8 +502,23 @@ static int mesh_sdf(sc_context* ctx, int nx, int ny, int nz, double h, const dou
     a.vertices = (const double*)dv;
     a.triangles = (const int32_t*)dt;
   }
+  // scratch kept by the context: a per-call stream-ordered allocation can hand
+  // its pages back at the synchronisations and map them again on the next call
+  const size_t need = sc::mesh_to_sdf_scratch_bytes(a, d_cl == nullptr);
+  if (ctx->mesh_scratch_bytes < need) {
+    cudaStreamSynchronize(st);
+    if (ctx->mesh_scratch) cudaFree(ctx->mesh_scratch);
+    ctx->mesh_scratch = nullptr;
+    ctx->mesh_scratch_bytes = 0;
+    if (cudaMalloc(&ctx->mesh_scratch, need) != cudaSuccess) {
+      ctx->mesh_scratch = nullptr;
+      cudaGetLastError();
+      return ctx->c.set_error(SC_ERR_NOMEM, "mesh_to_sdf: scratch allocation failed");
+    }
+    ctx->mesh_scratch_bytes = need;
+  }
   std::string msg;
-  int rc = sc::mesh_to_sdf(st, a, d_sdf, d_cl, &msg);
+  int rc = sc::mesh_to_sdf(st, a, d_sdf, d_cl, ctx->mesh_scratch, ctx->mesh_scratch_bytes, &msg);
   if (!device) {
     if (rc == 0) {
       cudaMemcpyAsync(sdf, d_sdf, sizeof(double) * (size_t)N, cudaMemcpyDeviceToHost, st);

@@ -354,25 +354,54 @@ __global__ void k_mesh_sign(MeshGeo g, double* sdf, const int* cnt) {
 
 }  // namespace
 
-int mesh_to_sdf(cudaStream_t st, const MeshSdfArgs& a, double* sdf, int32_t* closest, std::string* msg) {
+namespace {
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+}  // namespace
+
+size_t mesh_to_sdf_scratch_bytes(const MeshSdfArgs& a, bool need_closest) {
+  const size_t N = (size_t)a.nx * a.ny * a.nz;
+  return align256(sizeof(int) * N) + align256(4 * sizeof(int)) +
+         align256(sizeof(double) * 9 * (size_t)std::max<int64_t>(a.ntriangles, 1)) +
+         (need_closest ? align256(sizeof(int) * N) : 0);
+}
+
+int mesh_to_sdf(cudaStream_t st, const MeshSdfArgs& a, double* sdf, int32_t* closest, void* scratch,
+                size_t scratch_bytes, std::string* msg) {
   const int64_t N = (int64_t)a.nx * a.ny * a.nz;
   const int64_t cols = (int64_t)a.nx * a.ny;
   int* cl = closest;
   int *cnt = nullptr, *flag = nullptr;
   double* packed = nullptr;
+  const bool own = scratch == nullptr;  // allocate per call
   auto fail = [&](int rc, const char* what) {
     if (msg) *msg = what;
-    if (packed) cudaFreeAsync(packed, st);
-    if (cnt) cudaFreeAsync(cnt, st);
-    if (flag) cudaFreeAsync(flag, st);
-    if (cl && cl != closest) cudaFreeAsync(cl, st);
+    if (own) {
+      if (packed) cudaFreeAsync(packed, st);
+      if (cnt) cudaFreeAsync(cnt, st);
+      if (flag) cudaFreeAsync(flag, st);
+      if (cl && cl != closest) cudaFreeAsync(cl, st);
+    }
     return rc;
   };
-  if (cudaMallocAsync(&cnt, sizeof(int) * (size_t)N, st) != cudaSuccess ||
-      cudaMallocAsync(&flag, 4 * sizeof(int), st) != cudaSuccess ||
-      cudaMallocAsync(&packed, sizeof(double) * 9 * (size_t)std::max<int64_t>(a.ntriangles, 1), st) != cudaSuccess ||
-      (!cl && cudaMallocAsync(&cl, sizeof(int) * (size_t)N, st) != cudaSuccess))
-    return fail(-3, "mesh_to_sdf: scratch allocation failed");
+  if (own) {
+    if (cudaMallocAsync(&cnt, sizeof(int) * (size_t)N, st) != cudaSuccess ||
+        cudaMallocAsync(&flag, 4 * sizeof(int), st) != cudaSuccess ||
+        cudaMallocAsync(&packed, sizeof(double) * 9 * (size_t)std::max<int64_t>(a.ntriangles, 1), st) !=
+            cudaSuccess ||
+        (!cl && cudaMallocAsync(&cl, sizeof(int) * (size_t)N, st) != cudaSuccess))
+      return fail(-3, "mesh_to_sdf: scratch allocation failed");
+  } else {
+    if (scratch_bytes < mesh_to_sdf_scratch_bytes(a, closest == nullptr))
+      return fail(-1, "mesh_to_sdf: scratch too small");
+    char* p = static_cast<char*>(scratch);
+    cnt = reinterpret_cast<int*>(p);
+    p += align256(sizeof(int) * (size_t)N);
+    flag = reinterpret_cast<int*>(p);
+    p += align256(4 * sizeof(int));
+    packed = reinterpret_cast<double*>(p);
+    p += align256(sizeof(double) * 9 * (size_t)std::max<int64_t>(a.ntriangles, 1));
+    if (!cl) cl = reinterpret_cast<int*>(p);
+  }
   // triangle indices must name vertices
   int hflag = 0;
   cudaMemsetAsync(flag, 0, sizeof(int), st);
@@ -434,10 +463,12 @@ int mesh_to_sdf(cudaStream_t st, const MeshSdfArgs& a, double* sdf, int32_t* clo
   k_mesh_sign<<<sblocks, kMeshThreads, 0, st>>>(g, sdf, cnt);
   // the sweep's wait status
   cudaMemcpyAsync(&hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaFreeAsync(cnt, st);
-  cudaFreeAsync(flag, st);
-  cudaFreeAsync(packed, st);
-  if (cl != closest) cudaFreeAsync(cl, st);
+  if (own) {
+    cudaFreeAsync(cnt, st);
+    cudaFreeAsync(flag, st);
+    cudaFreeAsync(packed, st);
+    if (cl != closest) cudaFreeAsync(cl, st);
+  }
   cnt = flag = nullptr;
   packed = nullptr;
   cl = closest;

@@ -21,11 +21,18 @@ struct MeshSdfArgs {
   int exact_distance;       // 0: the reference's point-triangle arithmetic; 1: true distances
 };
 
+// Device scratch mesh_to_sdf needs (crossing counts, closest triangles when the
+// caller passes none, status words, packed triangle vertices).
+size_t mesh_to_sdf_scratch_bytes(const MeshSdfArgs& a, bool need_closest);
+
 // Writes the signed distance (reference layout, z fastest) to `sdf` and, when
 // `closest` is not null, the triangle each cell's distance was taken from (-1:
-// none).  Allocates its scratch on the stream (stream-ordered) and returns 0,
-// -1 with `msg` set for a triangle index outside [0, nvertices), or -3 when an
-// allocation fails.  Synchronises the stream.
-int mesh_to_sdf(cudaStream_t st, const MeshSdfArgs& a, double* sdf, int32_t* closest, std::string* msg);
+// none).  Uses `scratch` (at least mesh_to_sdf_scratch_bytes bytes, 256-byte
+// aligned) when given, else allocates its scratch on the stream.  Returns 0,
+// -1 with `msg` set for a triangle index outside [0, nvertices), -3 when an
+// allocation fails, -6 when a sweep barrier wait timed out.  Synchronises the
+// stream.
+int mesh_to_sdf(cudaStream_t st, const MeshSdfArgs& a, double* sdf, int32_t* closest, void* scratch,
+                size_t scratch_bytes, std::string* msg);
 
 }  // namespace sc

@@ -38,3 +38,38 @@ def test_status_strings_without_gpu():
     assert L.sc_status_string(0) == b"ok"
     assert L.sc_status_string(-6) == b"device wait timed out"
     assert L.sc_version() >= 10000
+
+
+def test_python_structs_match_header_layout(tmp_path):
+    """Every struct of the C ABI has the size and field offsets its ctypes mirror
+    assumes (a probe compiled with the system C compiler against the header)."""
+    import shutil
+    import subprocess
+
+    from simcraft_b200 import _capi
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        import pytest
+
+        pytest.skip("no C compiler")
+    structs = [getattr(_capi, n) for n in ("sc_pcg_options", "sc_pcg_stats", "sc_fluid_config", "sc_fluid_stats",
+                                            "sc_diff_config")]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "simcraft_fluid_capi.h"', "int main(void) {"]
+    for st in structs:
+        lines.append(f'  printf("{st.__name__} size %zu\\n", sizeof({st.__name__}));')
+        for f, _ in st._fields_:
+            lines.append(f'  printf("{st.__name__} {f} %zu\\n", offsetof({st.__name__}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "probe"
+    subprocess.check_call([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = {}
+    for line in subprocess.check_output([str(exe)], text=True).splitlines():
+        name, field, val = line.split()
+        got[(name, field)] = int(val)
+    for st in structs:
+        assert got[(st.__name__, "size")] == ctypes.sizeof(st), st.__name__
+        for f, _ in st._fields_:
+            assert got[(st.__name__, f)] == getattr(st, f).offset, (st.__name__, f)

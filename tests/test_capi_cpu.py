@@ -73,3 +73,31 @@ def test_python_structs_match_header_layout(tmp_path):
         assert got[(st.__name__, "size")] == ctypes.sizeof(st), st.__name__
         for f, _ in st._fields_:
             assert got[(st.__name__, f)] == getattr(st, f).offset, (st.__name__, f)
+
+
+def test_header_compiles_as_cxx_and_links(tmp_path):
+    """A C++ caller includes the header (warnings as errors) and links the
+    library; nothing is called, so no GPU is needed."""
+    import shutil
+    import subprocess
+
+    from simcraft_b200 import build
+
+    cxx = shutil.which("g++")
+    if cxx is None:
+        import pytest
+
+        pytest.skip("no C++ compiler")
+    build.build()
+    src = tmp_path / "caller.cc"
+    src.write_text('#include "simcraft_fluid_capi.h"\n'
+                   "int main(int argc, char**) {\n"
+                   "  sc_pcg_options o;\n"
+                   "  if (argc > 5) sc_pcg_default_options(&o);\n"
+                   "  return argc > 5 ? sc_version() : 0;\n"
+                   "}\n")
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(build.LIB)
+    subprocess.check_call([cxx, "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                           str(src), "-o", str(exe), "-L", libdir, "-lsimcraft_fluid", "-Wl,-rpath," + libdir])
+    assert exe.exists()

@@ -423,6 +423,57 @@ def collider_leg(args, dev, ctx, cpu):
     return out
 
 
+def surface_leg(dev, ctx, sim, h, cpu):
+    """rebuildSurface(mesh, exportFluidSurface()) of the FLIP dam break after its
+    timed substeps, as the reference's app exports the fluid: the device call a
+    user makes (count + fill, CUDA events on torch's stream), the same from host
+    arrays (end to end), and one pass of the CPU oracle (sequential with a hash
+    map, as the reference) on the same SDF, checked bit for bit."""
+    import torch
+
+    from simcraft_b200.surface import rebuild_surface
+
+    sdf_h = sim.export_fluid_surface()
+    n = sdf_h.shape[0]
+    sdf_d = torch.from_numpy(sdf_h).to(dev)
+    for _ in range(3):
+        V, N, I = rebuild_surface(sdf_d, h, context=ctx)
+    stream = torch.cuda.current_stream(dev)
+    reps = 5
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        V, N, I = rebuild_surface(sdf_d, h, context=ctx)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    gpu_ms = e0.elapsed_time(e1) / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        Vh, Nh, Ih = rebuild_surface(sdf_h, h, context=ctx)
+    e2e_ms = 1e3 * (time.perf_counter() - t0) / reps
+    nv, ni = V.shape[0], I.shape[0]
+    alg = 8 * sdf_h.size + 48 * nv + 4 * ni
+    out = {"workload": f"marching cubes of the {n}^3 dam-break fluid SDF after the timed substeps "
+                       f"(FP64 mesh, reference vertex order)",
+           "vertices": int(nv), "triangles": int(ni // 3), "gpu_ms": gpu_ms, "e2e_ms": e2e_ms,
+           "algorithmic_bytes": int(alg), "algorithmic_gb_s": alg / (gpu_ms * 1e-3) / 1e9,
+           "kernel_launches_per_call": 6,
+           "host_equals_device": bool(np.array_equal(Vh, V.cpu().numpy()) and np.array_equal(Ih, I.cpu().numpy()))}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        O.build()
+        t0 = time.perf_counter()
+        Vr, Nr, Ir = O.rebuild_surface(sdf_h, h, counts=(nv, ni))
+        out["cpu_baseline"] = {"value": 1e3 * (time.perf_counter() - t0), "unit": "ms", "cores": 1, "kind": "port",
+                               "sample": f"one pass over the same {n}^3 SDF (the reference's sequential algorithm)",
+                               "bit_exact_vs_gpu": bool(np.array_equal(Vr, Vh) and np.array_equal(Ir, Ih) and
+                                                        np.array_equal(Nr, Nh, equal_nan=True))}
+    return out
+
+
 def flip_leg(args, dev, ctx, dist, rank, world):
     """FLIP substeps/s on the 256^3 FP32 dam break (device-resident particles)."""
     import torch
@@ -476,6 +527,8 @@ def flip_leg(args, dev, ctx, dist, rank, world):
            "pcg_inner_iterations_mean": float(np.mean(iters)), "gpu_launches": int(launches)}
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = flip_cpu_sample(sim, n, h)
+    if args.surface:
+        out["surface"] = surface_leg(dev, ctx, sim, h, rank == 0 and world == 1 and not args.no_cpu)
     del sim
     torch.cuda.empty_cache()
     return out
@@ -605,6 +658,8 @@ def main():
     ap.add_argument("--large-warmup", type=int, default=2, help="untimed solves of the 512^3 leg")
     ap.add_argument("--collider", type=int, default=1, help="mesh-to-SDF collider leg (0 skips)")
     ap.add_argument("--flip32", type=int, default=1, help="32^3 FP64 dam-break leg (0 skips)")
+    ap.add_argument("--surface", type=int, default=1,
+                    help="marching-cubes export of the FLIP leg's fluid (0 skips)")
     ap.add_argument("--diff-dirs", type=int, default=16,
                     help="finite-difference directions of the differentiable leg (-1 skips the leg)")
     args = ap.parse_args()
@@ -802,6 +857,8 @@ def main():
         out["solve_512"] = large_solve_leg(args, dev, ctx, replicas)
     if args.flip_steps > 0:
         out["flip"] = flip_leg(args, dev, ctx, dist, rank, world)
+        if "surface" in out["flip"]:
+            out["surface"] = out["flip"].pop("surface")
     # CPU oracles on the host cores: one process only (as for the solve leg)
     cpu = rank == 0 and world == 1 and not args.no_cpu
     if args.collider:

@@ -1459,3 +1459,106 @@ int ora_sim_last_iters(const ora_sim* s) { return s->last_iters; }
 double ora_sim_last_residual(const ora_sim* s) { return s->last_residual; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// rebuildSurface (FluidSim/src/cpu/rebuild-surface.cc:686-741): marching cubes
+// over the cubes whose lowest corner runs from -1 to n-1 on each axis, samples
+// outside the grid reading 1000 (evalSdf, :655-664).  Vertices are numbered in
+// the order they are first met -- cubes in x, y, z order, a cube's case entries
+// in table order -- and shared through a hash map keyed by the doubled
+// coordinates of the edge midpoint (globalVertexIdx, :643-653).  Serial, as the
+// reference.  The cases come from the library's packed table (the same cases as
+// the reference's triangleConnectionTable3D, pinned by a digest test).
+#include <unordered_map>
+
+#include "../simcraft_b200/csrc/sc_mc_table.h"
+
+namespace {
+
+const uint64_t kMcCases[256] = {SC_MC_CASES_INIT};
+
+struct McOracle {
+  int nx, ny, nz;
+  double hx, hy, hz, ox, oy, oz;
+  const double* sdf;
+  double eval(int x, int y, int z) const {  // evalSdf (:655-660)
+    if (x < 0 || x >= nx || y < 0 || y >= ny || z < 0 || z >= nz) return 1000;
+    return sdf[((int64_t)x * ny + y) * nz + z];
+  }
+  // grad (:666-686): central differences, one-sided where the neighbour index
+  // would leave [-1, n]; the spacing doubles only strictly inside [0, n-1).
+  void grad(int x, int y, int z, double g[3]) const {
+    const int xn = x < nx ? x + 1 : x, xp = x > -1 ? x - 1 : x;
+    const int yn = y < ny ? y + 1 : y, yp = y > -1 ? y - 1 : y;
+    const int zn = z < nz ? z + 1 : z, zp = z > -1 ? z - 1 : z;
+    const double dx = x > -1 && x < nx - 1 ? 2 * hx : hx;
+    const double dy = y > -1 && y < ny - 1 ? 2 * hy : hy;
+    const double dz = z > -1 && z < nz - 1 ? 2 * hz : hz;
+    const double gx = eval(xn, y, z) - eval(xp, y, z);
+    const double gy = eval(x, yn, z) - eval(x, yp, z);
+    const double gz = eval(x, y, zn) - eval(x, y, zp);
+    g[0] = gx / dx;
+    g[1] = gy / dy;
+    g[2] = gz / dz;
+  }
+};
+
+}  // namespace
+
+int64_t ora_rebuild_surface(int nx, int ny, int nz, const double* spacing, const double* origin,
+                            const double* sdf, double* vertices, double* normals, uint32_t* indices,
+                            int64_t vertex_capacity, int64_t index_capacity, int64_t* nindices) {
+  McOracle M{nx, ny, nz, spacing[0], spacing[1], spacing[2], origin[0], origin[1], origin[2], sdf};
+  std::vector<double> V, Nrm;
+  std::vector<uint32_t> I;
+  std::unordered_map<int64_t, int64_t> vmap;
+  const int64_t ky = 2 * (int64_t)ny + 3, kz = 2 * (int64_t)nz + 3;
+  for (int x = -1; x < nx; x++)
+    for (int y = -1; y < ny; y++)
+      for (int z = -1; z < nz; z++) {
+        int mask = 0;
+        for (int c = 0; c < 8; c++)
+          if (M.eval(x + SC_MC_CORNER_X(c), y + SC_MC_CORNER_Y(c), z + SC_MC_CORNER_Z(c)) < 0.0)
+            mask |= 1 << c;
+        const uint64_t w = kMcCases[mask];
+        for (int q = 0; q < SC_MC_COUNT(w); q++) {
+          const int e = SC_MC_ENTRY(w, q), ca = SC_MC_EDGE_A(e), cb = SC_MC_EDGE_B(e);
+          const int ax = x + SC_MC_CORNER_X(ca), ay = y + SC_MC_CORNER_Y(ca), az = z + SC_MC_CORNER_Z(ca);
+          const int bx = x + SC_MC_CORNER_X(cb), by = y + SC_MC_CORNER_Y(cb), bz = z + SC_MC_CORNER_Z(cb);
+          // doubled midpoint, shifted by 2 so that it starts at 0 (globalVertexIdx)
+          const int64_t key = ((int64_t)(ax + bx + 2) * ky + (ay + by + 2)) * kz + (az + bz + 2);
+          auto it = vmap.find(key);
+          int64_t vid;
+          if (it == vmap.end()) {
+            vid = (int64_t)(V.size() / 3);
+            const double pa[3] = {(ax + 0.5) * M.hx + M.ox, (ay + 0.5) * M.hy + M.oy, (az + 0.5) * M.hz + M.oz};
+            const double pb[3] = {(bx + 0.5) * M.hx + M.ox, (by + 0.5) * M.hy + M.oy, (bz + 0.5) * M.hz + M.oz};
+            double na[3], nb[3];
+            M.grad(ax, ay, az, na);
+            M.grad(bx, by, bz, nb);
+            const double va = M.eval(ax, ay, az), vb = M.eval(bx, by, bz);
+            const double t = va / (va - vb);
+            double n[3];
+            for (int d = 0; d < 3; d++) {  // lerp (util.h:26-29): x (1 - t) + y t
+              V.push_back(pa[d] * (1 - t) + pb[d] * t);
+              n[d] = na[d] * (1 - t) + nb[d] * t;
+            }
+            // normalize: v * (1 / sqrt(dot(v, v))), the dot summed x + y, then + z
+            const double inv = 1.0 / std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            for (int d = 0; d < 3; d++) Nrm.push_back(n[d] * inv);
+            vmap.emplace(key, vid);
+          } else {
+            vid = it->second;
+          }
+          I.push_back((uint32_t)vid);
+        }
+      }
+  const int64_t nv = (int64_t)(V.size() / 3), ni = (int64_t)I.size();
+  if (nindices) *nindices = ni;
+  if (vertices && normals && indices && vertex_capacity >= nv && index_capacity >= ni) {
+    std::memcpy(vertices, V.data(), sizeof(double) * V.size());
+    std::memcpy(normals, Nrm.data(), sizeof(double) * Nrm.size());
+    std::memcpy(indices, I.data(), sizeof(uint32_t) * I.size());
+  }
+  return nv;
+}

@@ -135,6 +135,15 @@ void ora_manifold_to_sdf(int nx, int ny, int nz, double h, double ox, double oy,
                          const double* vert, const int* tri, int64_t ntri, int exact_band,
                          int exact_distance, double* sdf, int* closest, int* icnt);
 double ora_sim_last_residual(const ora_sim* s);
+/* rebuildSurface (FluidSim/src/cpu/rebuild-surface.cc:686-741): marching
+ * cubes over the cell-centred SDF (reference layout; sample (x, y, z) at
+ * ((x + 0.5) spacing[0] + origin[0], ...)).  Returns the vertex count and
+ * writes the index count to *nindices; vertices and normals (count x 3) and
+ * indices (3 per triangle) are written only when all three are given and the
+ * capacities hold them. */
+int64_t ora_rebuild_surface(int nx, int ny, int nz, const double* spacing, const double* origin,
+                            const double* sdf, double* vertices, double* normals, uint32_t* indices,
+                            int64_t vertex_capacity, int64_t index_capacity, int64_t* nindices);
 
 #ifdef __cplusplus
 }

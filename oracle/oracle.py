@@ -28,7 +28,8 @@ CRIT_REL_L2 = 1
 def build(force=False):
     """Compile the oracle with its Makefile (g++ -fopenmp)."""
     if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < max(
-        os.path.getmtime(os.path.join(_HERE, f)) for f in ("fluid_oracle.cc", "fluid_oracle.h")
+        os.path.getmtime(os.path.join(_HERE, f))
+        for f in ("fluid_oracle.cc", "fluid_oracle.h", "../simcraft_b200/csrc/sc_mc_table.h")
     ):
         subprocess.check_call(["make", "-s", "-C", _HERE])
     return _LIB
@@ -56,6 +57,9 @@ def lib():
             "ora_set_parity_mode": (None, [_int]),
             "ora_get_threads": (_int, []),
             "ora_cubic_weight": (_dbl, [_dbl, _dbl, _dbl, _dbl]),
+            "ora_rebuild_surface": (_i64, [_int, _int, _int, _dp, _dp, _dp, _dp, _dp,
+                                           ctypes.POINTER(ctypes.c_uint32), _i64, _i64,
+                                           ctypes.POINTER(ctypes.c_int64)]),
             "ora_manifold_to_sdf": (None, [_int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dp,
                                            ctypes.POINTER(ctypes.c_int), _i64, _int, _int, _dp,
                                            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
@@ -240,6 +244,31 @@ def manifold_to_sdf(vertices, triangles, dims, h, origin=(0.0, 0.0, 0.0), exact_
     lib().ora_manifold_to_sdf(*dims, float(h), *map(float, origin), _p(v), ip(t), len(t), int(exact_band),
                               int(bool(exact_distance)), _p(sdf), ip(closest), ip(icnt))
     return sdf, closest, icnt
+
+
+def rebuild_surface(sdf, spacing, origin=(0.0, 0.0, 0.0), counts=None):
+    """rebuildSurface (rebuild-surface.cc:686-741) on the CPU: (vertices [V,3],
+    normals [V,3], indices [I] uint32) of the marching-cubes mesh of a
+    cell-centred SDF.  spacing: a number or three.  counts=(vertices, index
+    entries) when known makes it one pass (else a counting pass comes first)."""
+    sdf = np.ascontiguousarray(sdf, np.float64)
+    nx, ny, nz = sdf.shape
+    sp = np.array([spacing] * 3 if np.isscalar(spacing) else spacing, np.float64)
+    org = np.array(origin, np.float64)
+    ni = ctypes.c_int64(0)
+    if counts is None:
+        nv = lib().ora_rebuild_surface(nx, ny, nz, _p(sp), _p(org), _p(sdf), None, None, None, 0, 0,
+                                       ctypes.byref(ni))
+    else:
+        nv, ni.value = int(counts[0]), int(counts[1])
+    V = np.zeros((nv, 3))
+    N = np.zeros((nv, 3))
+    I = np.zeros(ni.value, np.uint32)
+    lib().ora_rebuild_surface(nx, ny, nz, _p(sp), _p(org), _p(sdf), _p(V), _p(N),
+                              I.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), nv, ni.value,
+                              ctypes.byref(ni))
+    assert ni.value == len(I), "counts do not match the mesh"
+    return V, N, I
 
 
 def dot(a, b, active):

@@ -117,6 +117,10 @@ SIGNATURES = {
                                       c_void_p, c_int64, c_int, c_int, c_void_p, c_void_p]),
     "sc_mesh_to_sdf_host": (c_int, [c_void_p, c_int, c_int, c_int, c_double, c_void_p, c_void_p, c_int64,
                                     c_void_p, c_int64, c_int, c_int, c_void_p, c_void_p]),
+    "sc_rebuild_surface_device": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                          c_void_p, c_void_p, c_int64, c_int64, P(c_int64), P(c_int64)]),
+    "sc_rebuild_surface_host": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_int64, c_int64, P(c_int64), P(c_int64)]),
     "sc_fluid_cfl": (c_int, [c_void_p, P(c_double)]),
     "sc_fluid_substep": (c_int, [c_void_p, c_double, P(sc_fluid_stats)]),
     "sc_fluid_step": (c_int, [c_void_p, c_double, P(sc_fluid_stats)]),

@@ -11,10 +11,10 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsimcraft_fluid.so")
 OBJDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# The particle/grid transfers, the finite-volume build and the mesh SDF restate
+# The particle/grid transfers, the finite-volume build, the mesh SDF and the surface export restate
 # the CPU arithmetic operation by operation: no fused multiply-add contraction there.
 EXTRA = {"sc_flip.cu": ["--fmad=false"], "sc_fvm.cu": ["--fmad=false"], "sc_diff.cu": ["--fmad=false"],
-         "sc_mesh.cu": ["--fmad=false"]}
+         "sc_mesh.cu": ["--fmad=false"], "sc_surface.cu": ["--fmad=false"]}
 
 
 def sources():

@@ -12,6 +12,7 @@
 #include "sc_fvm.cuh"
 #include "sc_mesh.cuh"
 #include "sc_pcg.cuh"
+#include "sc_surface.cuh"
 
 // A context is freed when its user handle and every handle created from it
 // have been destroyed, whatever the order of the destroy calls.
@@ -21,6 +22,10 @@ struct sc_context {
   std::atomic<int> refs{1};
   void* mesh_scratch = nullptr;  // mesh-to-SDF scratch, grown on demand, kept until destroy
   size_t mesh_scratch_bytes = 0;
+  void* surf_scratch = nullptr;  // surface export: SDF staging + counting scratch, likewise
+  size_t surf_scratch_bytes = 0;
+  void* surf_stage = nullptr;    // surface export: mesh staging of the host entry point
+  size_t surf_stage_bytes = 0;
 };
 
 static sc_context* ctx_retain(sc_context* c) {
@@ -30,10 +35,10 @@ static sc_context* ctx_retain(sc_context* c) {
 static void ctx_release(sc_context* c) {
   if (c->refs.fetch_sub(1) == 1) {
     cudaSetDevice(c->c.device);
-    if (c->mesh_scratch) {
-      cudaStreamSynchronize(c->c.stream);
-      cudaFree(c->mesh_scratch);
-    }
+    if (c->mesh_scratch || c->surf_scratch || c->surf_stage) cudaStreamSynchronize(c->c.stream);
+    if (c->mesh_scratch) cudaFree(c->mesh_scratch);
+    if (c->surf_scratch) cudaFree(c->surf_scratch);
+    if (c->surf_stage) cudaFree(c->surf_stage);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
   }
@@ -546,6 +551,101 @@ int sc_mesh_to_sdf_host(sc_context* ctx, int nx, int ny, int nz, double h, const
                         int64_t ntriangles, int exact_band, int flags, double* sdf, int32_t* closest) {
   return mesh_sdf(ctx, nx, ny, nz, h, origin, vertices, nvertices, triangles, ntriangles, exact_band,
                   flags, sdf, closest, false);
+}
+
+// ---------------------------------------------------------------------------------
+// Surface export (marching cubes).
+
+// Grows a device buffer the context keeps to at least `need` bytes (its
+// contents are dropped).
+static bool ctx_grow(sc_context* ctx, void** buf, size_t* have, size_t need) {
+  if (*have >= need) return true;
+  cudaStreamSynchronize(ctx->c.stream);
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *have = 0;
+  if (cudaMalloc(buf, need) != cudaSuccess) {
+    *buf = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  *have = need;
+  return true;
+}
+
+static size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+static int rebuild_surface(sc_context* ctx, int nx, int ny, int nz, const double* spacing,
+                           const double* origin, const double* sdf, double* vertices, double* normals,
+                           uint32_t* indices, int64_t vertex_capacity, int64_t index_capacity,
+                           int64_t* nvertices, int64_t* nindices, bool device) {
+  if (!ctx) return SC_ERR_INVALID;
+  const bool any = vertices || normals || indices, all = vertices && normals && indices;
+  bool ok = nx >= 1 && ny >= 1 && nz >= 1 && (int64_t)(nx + 1) * (ny + 1) * (nz + 1) < ((int64_t)1 << 31) &&
+            spacing && sdf && nvertices && nindices && any == all && vertex_capacity >= 0 && index_capacity >= 0;
+  for (int d = 0; ok && d < 3; d++) ok = spacing[d] > 0.0 && spacing[d] < 1e300;
+  if (!ok) return ctx->c.set_error(SC_ERR_INVALID, "rebuild_surface: invalid argument");
+  cudaSetDevice(ctx->c.device);
+  cudaStream_t st = ctx->c.stream;
+  const size_t N = (size_t)nx * ny * nz;
+  sc::SurfaceArgs a{nx, ny, nz, spacing[0], spacing[1], spacing[2], origin ? origin[0] : 0.0,
+                    origin ? origin[1] : 0.0, origin ? origin[2] : 0.0, sdf};
+  const size_t sdf_bytes = device ? 0 : round256(sizeof(double) * N);
+  if (!ctx_grow(ctx, &ctx->surf_scratch, &ctx->surf_scratch_bytes, sdf_bytes + sc::surface_scratch_bytes(a)))
+    return ctx->c.set_error(SC_ERR_NOMEM, "rebuild_surface: scratch allocation failed");
+  char* scratch = (char*)ctx->surf_scratch;
+  if (!device) {
+    cudaMemcpyAsync(scratch, sdf, sizeof(double) * N, cudaMemcpyHostToDevice, st);
+    a.sdf = (const double*)scratch;
+    scratch += sdf_bytes;
+  }
+  int64_t nv = 0, ni = 0;
+  if (sc::surface_count(st, a, scratch, &nv, &ni))
+    return ctx->c.set_error(SC_ERR_CUDA, std::string("rebuild_surface: ") + cudaGetErrorString(cudaGetLastError()));
+  *nvertices = nv;
+  *nindices = ni;
+  if (!any) return SC_OK;
+  if (vertex_capacity < nv || index_capacity < ni)
+    return ctx->c.set_error(SC_ERR_INVALID, "rebuild_surface: capacity below the mesh size");
+  if (nv > (int64_t)UINT32_MAX - 1)
+    return ctx->c.set_error(SC_ERR_UNSUPPORTED, "rebuild_surface: more vertices than uint32 indices address");
+  if (ni == 0) return SC_OK;
+  double *dv = vertices, *dn = normals;
+  uint32_t* di = indices;
+  const size_t vb = round256(sizeof(double) * 3 * (size_t)nv), ib = round256(sizeof(uint32_t) * (size_t)ni);
+  if (!device) {
+    if (!ctx_grow(ctx, &ctx->surf_stage, &ctx->surf_stage_bytes, 2 * vb + ib))
+      return ctx->c.set_error(SC_ERR_NOMEM, "rebuild_surface: staging allocation failed");
+    dv = (double*)ctx->surf_stage;
+    dn = (double*)((char*)ctx->surf_stage + vb);
+    di = (uint32_t*)((char*)ctx->surf_stage + 2 * vb);
+  }
+  std::string msg;
+  int rc = sc::surface_fill(st, a, scratch, dv, dn, di, &msg);
+  if (rc == 0 && !device) {
+    cudaMemcpyAsync(vertices, dv, sizeof(double) * 3 * (size_t)nv, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(normals, dn, sizeof(double) * 3 * (size_t)nv, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(indices, di, sizeof(uint32_t) * (size_t)ni, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+  }
+  if (rc) return ctx->c.set_error(map_status(rc), msg.empty() ? "rebuild_surface failed" : msg);
+  return finish(ctx, 0, "rebuild_surface");
+}
+
+int sc_rebuild_surface_device(sc_context* ctx, int nx, int ny, int nz, const double* spacing,
+                              const double* origin, const double* sdf, double* vertices, double* normals,
+                              uint32_t* indices, int64_t vertex_capacity, int64_t index_capacity,
+                              int64_t* nvertices, int64_t* nindices) {
+  return rebuild_surface(ctx, nx, ny, nz, spacing, origin, sdf, vertices, normals, indices, vertex_capacity,
+                         index_capacity, nvertices, nindices, true);
+}
+
+int sc_rebuild_surface_host(sc_context* ctx, int nx, int ny, int nz, const double* spacing,
+                            const double* origin, const double* sdf, double* vertices, double* normals,
+                            uint32_t* indices, int64_t vertex_capacity, int64_t index_capacity,
+                            int64_t* nvertices, int64_t* nindices) {
+  return rebuild_surface(ctx, nx, ny, nz, spacing, origin, sdf, vertices, normals, indices, vertex_capacity,
+                         index_capacity, nvertices, nindices, false);
 }
 
 // ---------------------------------------------------------------------------------

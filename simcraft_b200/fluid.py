@@ -178,6 +178,14 @@ class FluidSimulator:
         check("sc_fluid_get_fluid_sdf", lib().sc_fluid_get_fluid_sdf(self.handle, _ptr(s), 0), self.ctx.handle)
         return s
 
+    def rebuild_surface(self):
+        """rebuildSurface(mesh, exportFluidSurface()) (rebuild-surface.cc:732-741,
+        as FluidSim/disabled/fluid-sim.cc:230-238 exports the fluid): the
+        marching-cubes mesh of the fluid SDF, (vertices, normals, indices)."""
+        from .surface import rebuild_surface
+
+        return rebuild_surface(self.export_fluid_surface(), self.h, context=self.ctx)
+
 
 # ---------------------------------------------------------------------------
 # Stage functions on torch CUDA float64 tensors.

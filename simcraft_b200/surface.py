@@ -27,45 +27,78 @@ def _three(x, name):
     return (ctypes.c_double * 3)(*t)
 
 
+# Mesh size of the last export per (context, grid): a repeated export (one per
+# frame) first tries a single call with that size plus headroom.
+_last_counts = {}
+
+
+def _headroom(nv, ni):
+    return nv + nv // 4 + 64, ni + ni // 4 + 192
+
+
 def rebuild_surface(sdf, spacing, origin=(0.0, 0.0, 0.0), context=None):
-    """The marching-cubes mesh of `sdf` (see the module docstring)."""
+    """The marching-cubes mesh of `sdf` (see the module docstring).
+
+    One C-ABI call when the mesh fits the size remembered from the previous
+    export of the same grid on this context (plus a quarter); otherwise a
+    counting call, or the failed call's counts, then one filling call."""
     ctx = context or default_context()
     sp, org = _three(spacing, "spacing"), _three(origin, "origin")
     nv, ni = ctypes.c_int64(0), ctypes.c_int64(0)
-    if _is_torch(sdf):
+    device = _is_torch(sdf)
+    if device:
         import torch
 
         s = sdf.to(torch.float64).contiguous()
-        if s.dim() != 3:
-            raise ValueError("sdf must be 3-D")
-        nx, ny, nz = s.shape
-        with _on_torch_stream(ctx, s):
-            rc = lib().sc_rebuild_surface_device(ctx.handle, nx, ny, nz, sp, org, _ptr(s), None, None, None, 0, 0,
-                                                 ctypes.byref(nv), ctypes.byref(ni))
-            check("sc_rebuild_surface_device", rc, ctx.handle)
-            V = torch.empty((nv.value, 3), dtype=torch.float64, device=s.device)
-            N = torch.empty((nv.value, 3), dtype=torch.float64, device=s.device)
-            I = torch.empty((ni.value,), dtype=torch.int32, device=s.device)
-            if ni.value:
-                rc = lib().sc_rebuild_surface_device(ctx.handle, nx, ny, nz, sp, org, _ptr(s), _ptr(V), _ptr(N),
-                                                     _ptr(I), nv.value, ni.value, ctypes.byref(nv), ctypes.byref(ni))
-                check("sc_rebuild_surface_device", rc, ctx.handle)
-        return V, N, I
-    s = np.ascontiguousarray(sdf, np.float64)
-    if s.ndim != 3:
+        shape = tuple(s.shape)
+        fn_name = "sc_rebuild_surface_device"
+
+        def alloc(cv, ci):
+            return (torch.empty((cv, 3), dtype=torch.float64, device=s.device),
+                    torch.empty((cv, 3), dtype=torch.float64, device=s.device),
+                    torch.empty((ci,), dtype=torch.int32, device=s.device))
+    else:
+        s = np.ascontiguousarray(sdf, np.float64)
+        shape = s.shape
+        fn_name = "sc_rebuild_surface_host"
+
+        def alloc(cv, ci):
+            return np.empty((cv, 3)), np.empty((cv, 3)), np.empty(ci, np.uint32)
+    if len(shape) != 3:
         raise ValueError("sdf must be 3-D")
-    nx, ny, nz = s.shape
-    rc = lib().sc_rebuild_surface_host(ctx.handle, nx, ny, nz, sp, org, _ptr(s), None, None, None, 0, 0,
-                                       ctypes.byref(nv), ctypes.byref(ni))
-    check("sc_rebuild_surface_host", rc, ctx.handle)
-    V = np.empty((nv.value, 3))
-    N = np.empty((nv.value, 3))
-    I = np.empty(ni.value, np.uint32)
-    if ni.value:
-        rc = lib().sc_rebuild_surface_host(ctx.handle, nx, ny, nz, sp, org, _ptr(s), _ptr(V), _ptr(N), _ptr(I),
-                                           nv.value, ni.value, ctypes.byref(nv), ctypes.byref(ni))
-        check("sc_rebuild_surface_host", rc, ctx.handle)
-    return V, N, I
+    nx, ny, nz = shape
+    fn = getattr(lib(), fn_name)
+    key = (ctx.handle.value if hasattr(ctx.handle, "value") else ctx.handle, device, shape)
+
+    def call(out, cv, ci):
+        ptrs = [_ptr(a) for a in out] if out is not None else [None, None, None]
+        return fn(ctx.handle, nx, ny, nz, sp, org, _ptr(s), *ptrs, cv, ci, ctypes.byref(nv), ctypes.byref(ni))
+
+    def run():
+        out = None
+        if key in _last_counts:
+            cv, ci = _headroom(*_last_counts[key])
+            out = alloc(cv, ci)
+            rc = call(out, cv, ci)
+            if rc == 0:
+                return out, nv.value, ni.value
+            if nv.value <= cv and ni.value <= ci:  # not a capacity failure
+                check(fn_name, rc, ctx.handle)
+        else:
+            check(fn_name, call(None, 0, 0), ctx.handle)  # count only
+        cv, ci = nv.value, ni.value
+        out = alloc(cv, ci)
+        if ci:
+            check(fn_name, call(out, cv, ci), ctx.handle)
+        return out, cv, ci
+
+    if device:
+        with _on_torch_stream(ctx, s):
+            (V, N, I), cv, ci = run()
+    else:
+        (V, N, I), cv, ci = run()
+    _last_counts[key] = (cv, ci)
+    return V[:cv], N[:cv], I[:ci]
 
 
 def export_obj(path, vertices, normals, indices):

@@ -315,3 +315,65 @@ def test_kernel_numbering_replayed_on_cpu_equals_oracle(oracle, replay, name):
     v, n, i = replay(sdf, sp, org)
     assert np.array_equal(V, v) and np.array_equal(I, i)
     assert np.array_equal(N, n, equal_nan=True)
+
+
+def test_wrapper_call_protocol_against_a_fake_library(oracle, monkeypatch):
+    """simcraft_b200.surface.rebuild_surface drives the C-ABI contract: a
+    counting call then a filling call the first time; one call when the mesh
+    fits the remembered size; on a capacity failure the counts that call
+    returned, then one filling call.  The fake library implements the contract
+    with the oracle (no GPU)."""
+    import ctypes
+
+    import simcraft_b200.surface as S
+
+    calls = []
+
+    def as_array(p, ctype, shape):
+        addr = p.value if isinstance(p, ctypes.c_void_p) else p
+        return np.ctypeslib.as_array(ctypes.cast(addr, ctypes.POINTER(ctype)), shape)
+
+    class FakeLib:
+        def sc_rebuild_surface_host(self, h, nx, ny, nz, sp, org, sdf_p, vp, np_, ip, cv, ci, pnv, pni):
+            sdf = as_array(sdf_p, ctypes.c_double, (nx, ny, nz)).copy()
+            V, N, I = oracle.rebuild_surface(sdf, list(sp), list(org))
+            pnv._obj.value, pni._obj.value = len(V), len(I)
+            if vp is None:
+                calls.append("count")
+                return 0
+            if cv < len(V) or ci < len(I):
+                calls.append("short")
+                return -1
+            calls.append("fill")
+            if len(V):
+                as_array(vp, ctypes.c_double, (cv, 3))[:len(V)] = V
+                as_array(np_, ctypes.c_double, (cv, 3))[:len(V)] = N
+            if len(I):
+                as_array(ip, ctypes.c_uint32, (ci,))[:len(I)] = I
+            return 0
+
+    class FakeCtx:
+        handle = ctypes.c_void_p(0x5C)
+
+    monkeypatch.setattr(S, "lib", lambda: FakeLib())
+    monkeypatch.setattr(S, "_last_counts", {})
+    ctx = FakeCtx()
+    h = 1.0 / 14
+    small = sphere_sdf((14, 14, 14), (h, h, h), (0, 0, 0), (0.5, 0.5, 0.5), 0.2)
+    big = sphere_sdf((14, 14, 14), (h, h, h), (0, 0, 0), (0.5, 0.5, 0.5), 0.38)
+    other = sphere_sdf((10, 12, 9), (h, h, h), (0, 0, 0), (0.3, 0.4, 0.3), 0.2)
+
+    def run(sdf, expect):
+        calls.clear()
+        got = S.rebuild_surface(sdf, h, context=ctx)
+        assert calls == expect
+        ref = oracle.rebuild_surface(sdf, h)
+        for a, b in zip(got, ref):
+            assert a.shape == b.shape and np.array_equal(a, b, equal_nan=True)
+
+    run(small, ["count", "fill"])
+    run(small, ["fill"])
+    run(big, ["short", "fill"])
+    run(small, ["fill"])  # the remembered size is now the bigger mesh
+    run(other, ["count", "fill"])
+    run(np.ones((14, 14, 14)), ["fill"])  # an empty mesh fits any size

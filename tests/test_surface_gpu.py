@@ -144,3 +144,18 @@ def test_capacity_below_mesh_is_an_error(torch_mod):
                                          Nn.ctypes.data, I.ctypes.data, nv.value, ni.value, ctypes.byref(nv),
                                          ctypes.byref(ni)) == 0
     assert I.max() == nv.value - 1
+
+
+@pytest.mark.parametrize("path", ["host", "device"])
+def test_repeated_exports_single_call_path(oracle, torch_mod, path):
+    """Exports of one grid in a row (the wrapper's one-call path, then a mesh
+    larger than the remembered size, then smaller again) stay bit-exact."""
+    from simcraft_b200.solver import Context
+    from simcraft_b200.surface import rebuild_surface
+
+    ctx = Context(0)
+    h = 1.0 / 40
+    for r in (0.2, 0.2, 0.41, 0.15, 0.3):
+        sdf = sphere_sdf((40, 40, 40), (h, h, h), (0, 0, 0), (0.5, 0.52, 0.48), r)
+        arg = torch_mod.from_numpy(sdf).cuda() if path == "device" else sdf
+        _same(rebuild_surface(arg, h, context=ctx), oracle.rebuild_surface(sdf, h))

@@ -377,3 +377,28 @@ def test_wrapper_call_protocol_against_a_fake_library(oracle, monkeypatch):
     run(small, ["fill"])  # the remembered size is now the bigger mesh
     run(other, ["count", "fill"])
     run(np.ones((14, 14, 14)), ["fill"])  # an empty mesh fits any size
+
+
+def test_export_obj_layout_and_round_trip(oracle, tmp_path):
+    """export_obj writes exportObj's layout (Core/src/obj-io.cc:66-91) and the
+    numbers read back to the same doubles; an unopenable path returns False."""
+    from simcraft_b200.surface import export_obj
+
+    h = 1.0 / 11
+    V, N, I = oracle.rebuild_surface(sphere_sdf((11, 11, 11), (h, h, h), (0, 0, 0), (0.5, 0.5, 0.5), 0.3), h)
+    path = tmp_path / "fluid.obj"
+    assert export_obj(str(path), V, N, I)
+    lines = path.read_text().split("\n")
+    assert lines[-1] == ""
+    lines = lines[:-1]
+    nv, nt = len(V), len(I) // 3
+    assert len(lines) == 2 * nv + nt
+    v = np.array([[float(x) for x in ln.split()[1:]] for ln in lines[:nv] if ln.startswith("v ")])
+    n = np.array([[float(x) for x in ln.split()[1:]] for ln in lines[nv:2 * nv] if ln.startswith("vn ")])
+    assert np.array_equal(v, V) and np.array_equal(n, N)
+    faces = lines[2 * nv:]
+    assert all(ln.startswith("f ") and ln.endswith(" ") for ln in faces)
+    f = np.array([[int(tok.split("//")[0]) for tok in ln.split()[1:]] for ln in faces])
+    g = np.array([[int(tok.split("//")[1]) for tok in ln.split()[1:]] for ln in faces])
+    assert np.array_equal(f, g) and np.array_equal(f - 1, I.reshape(-1, 3).astype(np.int64))
+    assert export_obj(str(tmp_path), V, N, I) is False  # a directory cannot be opened for writing

@@ -282,24 +282,25 @@ int sc_mesh_to_sdf_host(sc_context* ctx, int nx, int ny, int nz, double h, const
                         const double* vertices, int64_t nvertices, const int32_t* triangles,
                         int64_t ntriangles, int exact_band, int flags, double* sdf, int32_t* closest);
 
-/* rebuildSurface(mesh, sdf) (FluidSim/src/cpu/rebuild-surface.cc:686-741):
- * the marching-cubes mesh of a cell-centred SDF of nx x ny x nz samples
- * (reference layout; sample (x, y, z) at ((x + 0.5) spacing[0] + origin[0],
- * ...); spacing and origin are host arrays of 3 doubles, origin NULL: 0).  The
- * cubes run from -1 to n-1 on each axis, samples outside the grid reading
- * 1000, so a region touching the border is closed there.  The mesh equals the
- * reference's bit for bit: vertices and normals (nvertices x 3 doubles each;
- * normal = normalised interpolated central-difference gradient, not finite
- * where that gradient vanishes) in the order the reference creates them, and index entries
- * (3 per triangle, vertex numbers from 0) in its order.  Both counts are
- * always written.  With vertices, normals and indices all NULL the call only
- * counts; with all three given it fills them, returning SC_ERR_INVALID
- * (nothing written) if a capacity (vertices, index entries) is below the
- * count.  The reference appends to the mesh it is given: a caller doing that
- * adds its earlier vertex count to the indices.  _device: device arrays, on the
- * context stream; _host: host arrays (copied in and out).  The context keeps
- * its scratch (about 5 bytes per cell; _host adds the SDF and the mesh) until
- * it is destroyed; calls on one context use it one at a time. */
+/* rebuildSurface(mesh, sdf) (FluidSim/src/cpu/rebuild-surface.cc:686-741): the
+ * marching-cubes mesh of a cell-centred SDF of nx x ny x nz samples (reference
+ * layout; sample (x, y, z) at ((x + 0.5) spacing[0] + origin[0], ...); spacing
+ * and origin are host arrays of 3 doubles, origin NULL: 0).  The cubes run
+ * from -1 to n-1 on each axis, samples outside the grid reading 1000, so a
+ * region touching the border is closed there.  The mesh equals the reference's
+ * bit for bit: vertices and normals (nvertices x 3 doubles each; normal =
+ * normalised interpolated central-difference gradient, not finite where that
+ * gradient vanishes) in the order the reference creates them, and index
+ * entries (3 per triangle, vertex numbers from 0) in its order.  Both counts
+ * are written whenever the arguments are valid.  With vertices, normals and
+ * indices all NULL the call only counts; with all three given it fills them,
+ * returning SC_ERR_INVALID (nothing written) if a capacity (vertices, index
+ * entries) is below the count.  The reference appends to the mesh it is given:
+ * a caller doing that adds its earlier vertex count to the indices.  _device:
+ * device arrays, on the context stream; _host: host arrays (copied in and
+ * out).  The context keeps its scratch (about 5 bytes per cell; _host adds the
+ * SDF and the mesh) until it is destroyed; calls on one context use it one at
+ * a time. */
 int sc_rebuild_surface_device(sc_context* ctx, int nx, int ny, int nz, const double* spacing,
                               const double* origin, const double* sdf, double* vertices, double* normals,
                               uint32_t* indices, int64_t vertex_capacity, int64_t index_capacity,

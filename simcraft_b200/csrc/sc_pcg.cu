@@ -65,7 +65,7 @@ __device__ void finalize(int kind, PcgScalars* sc, double sum, double mx) {
       double res = sc->criterion == CRIT_REL_L2 ? (sc->bnorm > 0.0 ? 1.0 : 0.0) : mx;
       sc->res = res;
       sc->first = 1;
-      if (!(res == res)) {
+      if (!isfinite(sum) || !(res == res)) {  // NaN/Inf in the right-hand side
         sc->err |= DEV_ERR_NONFINITE;
         sc->done = DONE_BREAKDOWN;
         sc->iter = 0;
@@ -1743,7 +1743,10 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
 int PcgSolver::solve_fp64(PcgStats* st) {
   int e = ensure_pivots();
   if (e) return e;
-  return run_pcg<double>(d64_, opt_.tol, opt_.criterion, opt_.max_iter, false, st);
+  e = run_pcg<double>(d64_, opt_.tol, opt_.criterion, opt_.max_iter, false, st);
+  if (e == 0 && (last_.err & DEV_ERR_NONFINITE))
+    return ctx_->set_error(-8, "pcg: NaN or Inf in the system or the right-hand side");
+  return e;
 }
 
 // Mixed precision with reliable updates: FP32 CG on the split system
@@ -1780,6 +1783,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
   launches_ += 2;
   cudaMemcpyAsync(sc_host_, sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("mixed init");
+  if (!std::isfinite(sc_host_->rn2)) return ctx_->set_error(-8, "mixed solve: NaN or Inf in the right-hand side");
   const bool abs_crit = opt_.criterion == CRIT_ABS_LINF;
   const double bnorm = sqrt(sc_host_->rn2);
   double meas = abs_crit ? sc_host_->rinf : (bnorm > 0 ? 1.0 : 0.0);
@@ -1891,6 +1895,7 @@ int PcgSolver::solve_mixed(PcgStats* st) {
                                                sc_);
   cudaMemcpyAsync(sc_host_, sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("mixed init");
+  if (!std::isfinite(sc_host_->rn2)) return ctx_->set_error(-8, "mixed solve: NaN or Inf in the right-hand side");
   const double bnorm = sqrt(sc_host_->rn2);
   double rnorm = bnorm;
   double rel = bnorm > 0 ? 1.0 : 0.0;

@@ -132,7 +132,8 @@ def literal_rebuild_surface(sdf, spacing, origin):
                         p = tuple(pa[k] * (1 - frac) + pb[k] * frac for k in range(3))
                         n = tuple(na[k] * (1 - frac) + nb[k] * frac for k in range(3))
                         dot = n[0] * n[0] + n[1] * n[1] + n[2] * n[2]
-                        inv = 1.0 / math.sqrt(dot) if dot > 0.0 else math.inf  # IEEE 1/0
+                        # 1 / sqrt(dot) with IEEE semantics: 1/0 = inf, NaN stays NaN
+                        inv = math.nan if dot != dot else (math.inf if dot == 0.0 else 1.0 / math.sqrt(dot))
                         vmap[g] = len(verts)
                         verts.append(p)
                         norms.append(tuple(c * inv for c in n))
@@ -156,6 +157,9 @@ def scenes():
     yield "all_inside", -np.ones((3, 3, 3)), (0.5, 0.5, 0.5), (0.0, 0.0, 0.0)
     yield "empty", np.ones((4, 3, 5)), (0.5, 0.5, 0.5), (0.0, 0.0, 0.0)
     yield "single_cell", -np.ones((1, 1, 1)), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0)
+    holes = sphere_sdf((8, 9, 7), (0.125, 0.125, 0.125), (0, 0, 0), (0.5, 0.55, 0.45), 0.3)
+    holes[rng.random(holes.shape) < 0.15] = np.inf  # +inf samples: positive, non-finite gradients
+    yield "inf_holes", holes, (0.125, 0.125, 0.125), (0.0, 0.0, 0.0)
 
 
 @pytest.mark.parametrize("name", [s[0] for s in scenes()])
@@ -164,7 +168,7 @@ def test_oracle_equals_literal_restatement(oracle, name):
     V, N, I = oracle.rebuild_surface(sdf, sp, org)
     v, n, i = literal_rebuild_surface(sdf, sp, org)
     assert V.shape == v.shape and I.shape == i.shape
-    assert np.array_equal(V, v) and np.array_equal(I, i)
+    assert np.array_equal(V, v, equal_nan=True) and np.array_equal(I, i)
     assert np.array_equal(N, n, equal_nan=True)
     if name == "empty":
         assert len(V) == 0 and len(I) == 0
@@ -298,14 +302,24 @@ def replay(tmp_path_factory):
     return run
 
 
-@pytest.mark.parametrize("name", [s[0] for s in scenes()] + ["sphere_32", "noise_20"])
+def _nan_inf_field():
+    f = sphere_sdf((12, 11, 13), (0.09,) * 3, (0, 0, 0), (0.5, 0.5, 0.55), 0.33)
+    u = np.random.default_rng(8).random(f.shape)
+    f[u < 0.06] = np.nan
+    f[(u >= 0.06) & (u < 0.12)] = np.inf
+    f[(u >= 0.12) & (u < 0.15)] = -np.inf
+    return f
+
+
+@pytest.mark.parametrize("name", [s[0] for s in scenes()] + ["sphere_32", "noise_20", "nan_inf"])
 def test_kernel_numbering_replayed_on_cpu_equals_oracle(oracle, replay, name):
     """Owner cubes, ranks and the scan order give the reference's vertex
-    numbering: the replay equals the oracle bit for bit."""
+    numbering: the replay equals the oracle bit for bit (NaN where it has NaN)."""
     extra = {
         "sphere_32": (sphere_sdf((32, 30, 28), (1 / 32,) * 3, (0, 0, 0), (0.5, 0.45, 0.4), 0.31), (1 / 32,) * 3,
                       (0.0, 0.0, 0.0)),
         "noise_20": (np.random.default_rng(4).standard_normal((20, 21, 19)), (0.05, 0.06, 0.07), (0.3, 0.2, 0.1)),
+        "nan_inf": (_nan_inf_field(), (0.09,) * 3, (0.0, 0.0, 0.0)),
     }
     if name in extra:
         sdf, sp, org = extra[name]
@@ -313,7 +327,7 @@ def test_kernel_numbering_replayed_on_cpu_equals_oracle(oracle, replay, name):
         sdf, sp, org = next((s[1], s[2], s[3]) for s in scenes() if s[0] == name)
     V, N, I = oracle.rebuild_surface(sdf, sp, org)
     v, n, i = replay(sdf, sp, org)
-    assert np.array_equal(V, v) and np.array_equal(I, i)
+    assert np.array_equal(V, v, equal_nan=True) and np.array_equal(I, i)
     assert np.array_equal(N, n, equal_nan=True)
 
 

@@ -101,3 +101,49 @@ def test_header_compiles_as_cxx_and_links(tmp_path):
     subprocess.check_call([cxx, "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
                            str(src), "-o", str(exe), "-L", libdir, "-lsimcraft_fluid", "-Wl,-rpath," + libdir])
     assert exe.exists()
+
+
+def test_null_handles_are_rejected():
+    """Host-side fault injection at the boundary: every exported function that
+    takes a handle, given NULL for it (and ones, zeros or NULLs for the rest),
+    returns SC_ERR_INVALID (a status), 0 (a count) or nothing, and touches
+    neither the handle nor the device."""
+    import ctypes
+
+    from simcraft_b200 import _capi
+
+    L = _capi.lib()
+    probed = 0
+    for name, (rt, at) in sorted(_capi.SIGNATURES.items()):
+        if not at or at[0] is not ctypes.c_void_p:
+            continue
+        args = [1 if t in (ctypes.c_int, ctypes.c_int64, ctypes.c_uint32) else 1.0 if t is ctypes.c_double else None
+                for t in at]
+        r = getattr(L, name)(*args)
+        if rt is None or rt is ctypes.c_void_p:  # nothing, or a NULL pointer
+            assert r is None, name
+        elif rt is ctypes.c_char_p:
+            assert r == b"no context", name
+        elif name in ("sc_fluid_num_particles", "sc_diff_last_pcg_iterations"):
+            assert r == 0, name
+        else:
+            assert r == -1, (name, r)  # SC_ERR_INVALID
+        probed += 1
+    assert probed >= 50
+
+
+def test_context_creation_fails_cleanly_without_a_device():
+    import ctypes
+
+    import torch
+
+    from simcraft_b200 import _capi
+
+    if torch.cuda.is_available():
+        import pytest
+
+        pytest.skip("a device is present")
+    h = ctypes.c_void_p(1234)
+    assert _capi.lib().sc_context_create(0, ctypes.byref(h)) == -2  # SC_ERR_CUDA
+    assert h.value is None
+    assert _capi.lib().sc_context_create(0, None) == -1

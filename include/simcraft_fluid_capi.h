@@ -131,8 +131,10 @@ int sc_pcg_set_options(sc_pcg* pcg, const sc_pcg_options* opt);
 
 /* CgSolver3D::solve(Adiag, Aneighbour, rhs, active, pg) -> residual
  * (project-solver.h:107-111, project-solver.cc:308-346), host arrays.
- * an: 6 arrays in Directions order; only Left/Down/Back are read unless
- * check_symmetry is set (the matrix must be symmetric, project-solver.cc:41-57). */
+ * an: 6 arrays in Directions order; only Left/Down/Back are read (the others
+ * may be NULL) unless check_symmetry is set, which reads all six and returns
+ * SC_ERR_INVALID if one is missing (the matrix must be symmetric,
+ * project-solver.cc:41-57). */
 int sc_pcg_solve_host(sc_pcg* pcg, const double* adiag, const double* const* an,
                       const double* rhs, const uint8_t* active, double* pg,
                       sc_pcg_stats* stats);

@@ -258,6 +258,9 @@ int sc_pcg_upload(sc_pcg* pcg, const double* adiag, const double* const* an, con
                   const uint8_t* active, int device_pointers) {
   if (!pcg || !adiag || !an || !rhs || !active || !an[0] || !an[3] || !an[5])
     return SC_ERR_INVALID;
+  // the symmetry check reads the upper couplings too
+  if (pcg->solver->options().check_symmetry && (!an[1] || !an[2] || !an[4]))
+    return pcg->ctx->c.set_error(SC_ERR_INVALID, "check_symmetry needs all six neighbour arrays");
   cudaSetDevice(pcg->ctx->c.device);
   return map_status(pcg->solver->upload(adiag, an, rhs, active, device_pointers != 0));
 }

@@ -125,13 +125,14 @@ struct Tiled {
 // One element of a tiled array seen from a thread of a TY*32-thread block that
 // owns the row block (tile, slot): thread (ty, tx) = (threadIdx.x / 32, % 32).
 // Gives the coordinates and the element offsets of the six face neighbours
-// without any division per element.
+// without any division per element.  Host and device, so that the index
+// arithmetic can be checked on the CPU.
 struct Cell {
   int x, y, z;
   int tx, ty, slot, X, Y;
   int64_t tbase, e;
   bool inside;
-  __device__ __forceinline__ void init(const Tiled& g, int rb, int tid) {
+  __host__ __device__ __forceinline__ void init(const Tiled& g, int rb, int tid) {
     const int tile = rb / g.nz;
     slot = rb - tile * g.nz;
     Y = tile / g.ntx;
@@ -147,34 +148,34 @@ struct Cell {
     e = (int64_t)rb * (Tiled::TY * 32) + tid;
     inside = x < g.nx && y < g.ny;
   }
-  __device__ __forceinline__ int64_t at(int64_t base, int s, int ty_, int tx_) const {
+  __host__ __device__ __forceinline__ int64_t at(int64_t base, int s, int ty_, int tx_) const {
     return base + ((int64_t)s * Tiled::TY + ty_) * 32 + tx_;
   }
   // neighbour offsets; callers check the domain bounds first
-  __device__ __forceinline__ int64_t xm(const Tiled& g) const {
+  __host__ __device__ __forceinline__ int64_t xm(const Tiled& g) const {
     if (tx > 0) return at(tbase, slot == 0 ? g.nz - 1 : slot - 1, ty, tx - 1);
     int s = slot + 31;
     while (s >= g.nz) s -= g.nz;
     return at(tbase - g.tile_elems, s, ty, 31);
   }
-  __device__ __forceinline__ int64_t xp(const Tiled& g) const {
+  __host__ __device__ __forceinline__ int64_t xp(const Tiled& g) const {
     if (tx < 31) return at(tbase, slot == g.nz - 1 ? 0 : slot + 1, ty, tx + 1);
     int s = slot - 31;
     while (s < 0) s += g.nz;
     return at(tbase + g.tile_elems, s, ty, 0);
   }
-  __device__ __forceinline__ int64_t ym(const Tiled& g) const {
+  __host__ __device__ __forceinline__ int64_t ym(const Tiled& g) const {
     if (ty > 0) return e - 32;
     return at(tbase - (int64_t)g.ntx * g.tile_elems, slot, Tiled::TY - 1, tx);
   }
-  __device__ __forceinline__ int64_t yp(const Tiled& g) const {
+  __host__ __device__ __forceinline__ int64_t yp(const Tiled& g) const {
     if (ty < Tiled::TY - 1) return e + 32;
     return at(tbase + (int64_t)g.ntx * g.tile_elems, slot, 0, tx);
   }
-  __device__ __forceinline__ int64_t zm(const Tiled& g) const {
+  __host__ __device__ __forceinline__ int64_t zm(const Tiled& g) const {
     return at(tbase, slot == 0 ? g.nz - 1 : slot - 1, ty, tx);
   }
-  __device__ __forceinline__ int64_t zp(const Tiled& g) const {
+  __host__ __device__ __forceinline__ int64_t zp(const Tiled& g) const {
     return at(tbase, slot == g.nz - 1 ? 0 : slot + 1, ty, tx);
   }
 };

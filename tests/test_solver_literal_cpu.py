@@ -8,7 +8,11 @@ loop orders and the same operation order (IEEE doubles):
   fallback, then the forward and the reversed backward sweep;
 * CgSolver3D::solve (project-solver.cc:308-346) with dotProduct, saxpy,
   scaleAndAdd and LinfNorm (util.cc:380-410, util.h:56-63): zero start,
-  absolute L-inf stop, `iter` from 1, the first preconditioner applied to rhs.
+  absolute L-inf stop, `iter` from 1, the first preconditioner applied to rhs;
+* FvmSolver3D::buildSystem (project-solver.cc:59-228) with fractionInside
+  (util.cc:319-378) and SDF<3>::eval (sdf.h:35-60, whose node weights are the
+  mirror of trilinear): face weights, theta clamps, ghost-fluid diagonals,
+  the right-hand side, and the `j < width - 1` bound of the up face.
 
 The reference ships no test or fixture for these functions and cannot be built
 here, so this second, independent restatement is what catches a transcription
@@ -215,3 +219,203 @@ def test_pcg_equals_literal(oracle, name):
     act = S["active"] > 0
     assert it == lit and res == lres and it > 1
     assert np.array_equal(pg[act], lpg[act])
+
+
+# --- buildSystem (project-solver.cc:59-228), SDF::eval (sdf.h:35-60),
+# --- fractionInside (util.cc:319-378)
+
+def literal_eval(grid, h, p):
+    """SDF<3>::eval on a cell-centred grid with origin 0: node (x, y, z) takes
+    the weight tx ty tz (the mirror of trilinear), as the reference."""
+    W, H, D = grid.shape
+    ix, iy, iz = (int(c / h - 0.5) for c in p)  # Vec3i(...) truncates toward zero
+
+    def clamp(a, lo, hi):
+        return lo if a < lo else (hi if a > hi else a)
+
+    x, y, z = clamp(ix, 0, W - 1), clamp(iy, 0, H - 1), clamp(iz, 0, D - 1)
+    xn, yn, zn = clamp(ix + 1, 0, W - 1), clamp(iy + 1, 0, H - 1), clamp(iz + 1, 0, D - 1)
+    pos = ((x + 0.5) * h, (y + 0.5) * h, (z + 0.5) * h)
+    tx = clamp((p[0] - pos[0]) / h, 0.0, 1.0)
+    ty = clamp((p[1] - pos[1]) / h, 0.0, 1.0)
+    tz = clamp((p[2] - pos[2]) / h, 0.0, 1.0)
+    g = grid
+    return (tx * ty * tz * g[x, y, z] + tx * ty * (1 - tz) * g[x, y, zn] + tx * (1 - ty) * tz * g[x, yn, z] +
+            tx * (1 - ty) * (1 - tz) * g[x, yn, zn] + (1 - tx) * ty * tz * g[xn, y, z] +
+            (1 - tx) * ty * (1 - tz) * g[xn, y, zn] + (1 - tx) * (1 - ty) * tz * g[xn, yn, z] +
+            (1 - tx) * (1 - ty) * (1 - tz) * g[xn, yn, zn])
+
+
+def literal_fraction_inside(lu, ru, rd, ld):
+    n = int(lu <= 0.0) + int(ru <= 0.0) + int(rd <= 0.0) + int(ld <= 0.0)  # numpy bools would OR
+    if n == 0:
+        return 0.0
+    if n == 4:
+        return 1.0
+    while lu > 0.0:
+        lu, ru, rd, ld = ld, lu, ru, rd  # cycle
+    if n == 1:
+        fracu = ru / (ru - lu)
+        fracl = ld / (ld - lu)
+        return fracu * fracl * 0.5
+    if n == 2:
+        if ru <= 0.0:
+            return 0.5 * (ld / (ld - lu) + rd / (rd - ru))
+        if ld <= 0.0:
+            return 0.5 * (ru / (ru - lu) + rd / (rd - ld))
+        if rd <= 0.0:
+            fracu = ru / (ru - lu)
+            fracd = ld / (ld - rd)
+            fracl = ld / (ld - lu)
+            fracr = ru / (ru - rd)
+            if lu + ru + rd + ld <= 0.0:
+                return 1.0 - 0.5 * ((1.0 - fracu) * (1.0 - fracl) + (1.0 - fracd) * (1.0 - fracr))
+            return 0.5 * (fracu * fracl + fracd * fracr)
+    while lu <= 0.0:
+        lu, ru, rd, ld = ld, lu, ru, rd
+    fracu = ru / (ru - lu)
+    fracl = ld / (ld - lu)
+    return 1.0 - 0.5 * fracu * fracl
+
+
+def literal_build_system(dims, h, dt, u, v, w, F, C):
+    nx, ny, nz = dims
+    uw, vw, ww = np.zeros((nx + 1, ny, nz)), np.zeros((nx, ny + 1, nz)), np.zeros((nx, ny, nz + 1))
+    hh = 0.5 * h
+    for i in range(nx + 1):
+        for j in range(ny):
+            for k in range(nz):
+                if i == 0 or i == nx or (F[i - 1, j, k] > 0.0 and F[i, j, k] > 0.0):
+                    continue
+                p = (i * h, (j + 0.5) * h, (k + 0.5) * h)
+                bu = literal_eval(C, h, (p[0] + 0.0, p[1] + hh, p[2] - hh))
+                bd = literal_eval(C, h, (p[0] + 0.0, p[1] - hh, p[2] - hh))
+                fd = literal_eval(C, h, (p[0] + 0.0, p[1] - hh, p[2] + hh))
+                fu = literal_eval(C, h, (p[0] + 0.0, p[1] + hh, p[2] + hh))
+                uw[i, j, k] = 1.0 - literal_fraction_inside(bu, bd, fd, fu)
+    for i in range(nx):
+        for j in range(ny + 1):
+            for k in range(nz):
+                if j == 0 or j == ny or (F[i, j - 1, k] > 0.0 and F[i, j, k] > 0.0):
+                    continue
+                p = ((i + 0.5) * h, j * h, (k + 0.5) * h)
+                lb = literal_eval(C, h, (p[0] - hh, p[1] + 0.0, p[2] - hh))
+                rb = literal_eval(C, h, (p[0] + hh, p[1] + 0.0, p[2] - hh))
+                rf = literal_eval(C, h, (p[0] + hh, p[1] + 0.0, p[2] + hh))
+                lf = literal_eval(C, h, (p[0] - hh, p[1] + 0.0, p[2] + hh))
+                vw[i, j, k] = 1.0 - literal_fraction_inside(lb, rb, rf, lf)
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz + 1):
+                if k == 0 or k == nz or (F[i, j, k - 1] > 0.0 and F[i, j, k] > 0.0):
+                    continue
+                p = ((i + 0.5) * h, (j + 0.5) * h, k * h)
+                ld = literal_eval(C, h, (p[0] - hh, p[1] - hh, p[2] + 0.0))
+                lu = literal_eval(C, h, (p[0] - hh, p[1] + hh, p[2] + 0.0))
+                ru = literal_eval(C, h, (p[0] + hh, p[1] + hh, p[2] + 0.0))
+                rd = literal_eval(C, h, (p[0] + hh, p[1] - hh, p[2] + 0.0))
+                ww[i, j, k] = 1.0 - literal_fraction_inside(ld, lu, ru, rd)
+    adiag = np.zeros(dims)
+    an = [np.zeros(dims) for _ in range(6)]
+    rhs = np.zeros(dims)
+    active = np.zeros(dims, np.uint8)
+    factor = dt / h
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                if (uw[i, j, k] == 0.0 and uw[i + 1, j, k] == 0.0 and vw[i, j, k] == 0.0 and vw[i, j + 1, k] == 0.0
+                        and ww[i, j, k] == 0.0 and ww[i, j, k + 1] == 0.0):
+                    continue
+                if F[i, j, k] > 0.0:
+                    continue
+                active[i, j, k] = 1
+                sd = F[i, j, k]
+                a = 0.0
+                if i > 0:
+                    if F[i - 1, j, k] > 0.0:
+                        th = min(F[i - 1, j, k] / (F[i - 1, j, k] - sd), 0.99)
+                        a += uw[i, j, k] * factor / (1.0 - th)
+                    else:
+                        a += uw[i, j, k] * factor
+                        an[LEFT][i, j, k] -= uw[i, j, k] * factor
+                    rhs[i, j, k] += uw[i, j, k] * u[i, j, k]
+                if i < nx - 1:
+                    if F[i + 1, j, k] > 0.0:
+                        th = max(sd / (sd - F[i + 1, j, k]), 0.01)
+                        a += uw[i + 1, j, k] * factor / th
+                    else:
+                        a += uw[i + 1, j, k] * factor
+                        an[RIGHT][i, j, k] -= uw[i + 1, j, k] * factor
+                    rhs[i, j, k] -= uw[i + 1, j, k] * u[i + 1, j, k]
+                if j > 0:
+                    if F[i, j - 1, k] > 0.0:
+                        th = min(F[i, j - 1, k] / (F[i, j - 1, k] - sd), 0.99)
+                        a += vw[i, j, k] * factor / (1.0 - th)
+                    else:
+                        a += vw[i, j, k] * factor
+                        an[DOWN][i, j, k] -= vw[i, j, k] * factor
+                    rhs[i, j, k] += vw[i, j, k] * v[i, j, k]
+                if j < nx - 1:  # the reference bounds `up` by the width (:186)
+                    if F[i, j + 1, k] > 0.0:
+                        th = max(sd / (sd - F[i, j + 1, k]), 0.01)
+                        a += vw[i, j + 1, k] * factor / th
+                    else:
+                        a += vw[i, j + 1, k] * factor
+                        an[UP][i, j, k] -= vw[i, j + 1, k] * factor
+                    rhs[i, j, k] -= vw[i, j + 1, k] * v[i, j + 1, k]
+                if k > 0:
+                    if F[i, j, k - 1] > 0.0:
+                        th = min(F[i, j, k - 1] / (F[i, j, k - 1] - sd), 0.99)
+                        a += ww[i, j, k] * factor / (1.0 - th)
+                    else:
+                        a += ww[i, j, k] * factor
+                        an[BACK][i, j, k] -= ww[i, j, k] * factor
+                    rhs[i, j, k] += ww[i, j, k] * w[i, j, k]
+                if k < nz - 1:
+                    if F[i, j, k + 1] > 0.0:
+                        th = max(sd / (sd - F[i, j, k + 1]), 0.01)
+                        a += ww[i, j, k + 1] * factor / th
+                    else:
+                        a += ww[i, j, k + 1] * factor
+                        an[FRONT][i, j, k] -= ww[i, j, k + 1] * factor
+                    rhs[i, j, k] -= ww[i, j, k + 1] * w[i, j, k + 1]
+                adiag[i, j, k] = a
+    return dict(adiag=adiag, an=an, rhs=rhs, active=active, uwt=uw, vwt=vw, wwt=ww)
+
+
+@pytest.mark.parametrize("case", ["empty_collider", "sphere_collider", "narrow_x"])
+def test_build_system_equals_literal(oracle, case):
+    dims = (6, 9, 7) if case == "narrow_x" else (8, 8, 7)
+    h = 1.0 / 8
+    dt = 0.3 * h
+    rng = np.random.default_rng(17)
+    x = [(np.arange(n) + 0.5) * h for n in dims]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    F = np.minimum(np.sqrt((X - 0.45) ** 2 + (Y - 0.4) ** 2 + (Z - 0.5) ** 2) - 0.33, Y - 0.3)
+    nx, ny, nz = dims
+    u, v, w = rng.uniform(-1, 1, (nx + 1, ny, nz)), rng.uniform(-1, 1, (nx, ny + 1, nz)), rng.uniform(-1, 1, (nx, ny, nz + 1))
+    if case == "sphere_collider":
+        C = np.sqrt((X - 0.6) ** 2 + (Y - 0.35) ** 2 + (Z - 0.45) ** 2) - 0.2
+    else:
+        C = np.full(dims, 1e9)
+    got = oracle.build_system(dims, h, dt, u, v, w, F, C)
+    ref = literal_build_system(dims, h, dt, u, v, w, F, C)
+    for key in ("adiag", "rhs", "active", "uwt", "vwt", "wwt"):
+        assert np.array_equal(got[key], ref[key]), key
+    for d in range(6):
+        assert np.array_equal(got["an"][d], ref["an"][d]), d
+    assert ref["active"].any()
+    if case == "sphere_collider":
+        assert ((ref["uwt"] > 0) & (ref["uwt"] < 1)).any()  # partial faces
+
+
+def test_fraction_inside_and_eval_equal_literal(oracle):
+    rng = np.random.default_rng(23)
+    for c in rng.uniform(-1, 1, (3000, 4)):
+        assert oracle.fraction_inside(*c) == literal_fraction_inside(*c), c
+    for c in rng.integers(-1, 2, (300, 4)).astype(np.float64):  # exact zeros on corners
+        assert oracle.fraction_inside(*c) == literal_fraction_inside(*c), c
+    h = 1.0 / 8
+    g = rng.uniform(-1, 1, (8, 7, 9))
+    for p in rng.uniform(-0.2, 1.2, (500, 3)):  # inside, and clamped outside the grid
+        assert oracle.sdf_eval(g, h, p) == literal_eval(g, h, tuple(p)), p

@@ -12,7 +12,9 @@ loop orders and the same operation order (IEEE doubles):
 * FvmSolver3D::buildSystem (project-solver.cc:59-228) with fractionInside
   (util.cc:319-378) and SDF<3>::eval (sdf.h:35-60, whose node weights are the
   mirror of trilinear): face weights, theta clamps, ghost-fluid diagonals,
-  the right-hand side, and the `j < width - 1` bound of the up face.
+  the right-hand side, and the `j < width - 1` bound of the up face;
+* FvmSolver3D::project (project-solver.cc:348-435): fluid-fluid faces, the
+  ghost-fluid faces on either side, walls.
 
 The reference ships no test or fixture for these functions and cannot be built
 here, so this second, independent restatement is what catches a transcription
@@ -419,3 +421,65 @@ def test_fraction_inside_and_eval_equal_literal(oracle):
     g = rng.uniform(-1, 1, (8, 7, 9))
     for p in rng.uniform(-0.2, 1.2, (500, 3)):  # inside, and clamped outside the grid
         assert oracle.sdf_eval(g, h, p) == literal_eval(g, h, tuple(p)), p
+
+
+# --- FvmSolver3D::project (project-solver.cc:348-435)
+
+def literal_project(dims, h, dt, u, v, w, pg, F, uw, vw, ww):
+    nx, ny, nz = dims
+    u, v, w = u.copy(), v.copy(), w.copy()
+
+    def face(vel, idx, wt, n_along, axis_i, lo_idx, hi_idx):
+        if wt <= 0.0:
+            return
+        if axis_i == 0 or axis_i == n_along:
+            vel[idx] = 0.0
+            return
+        sl, sr = F[lo_idx], F[hi_idx]
+        if sl >= 0.0 and sr >= 0.0:
+            return
+        if sl < 0.0 and sr < 0.0:
+            vel[idx] -= (pg[hi_idx] - pg[lo_idx]) * dt / h
+            return
+        if sl < 0.0:
+            th = max(sl / (sl - sr), 0.01)
+            vel[idx] += pg[lo_idx] * dt / h / th
+        else:
+            th = min(sl / (sl - sr), 0.99)
+            vel[idx] -= pg[hi_idx] * dt / h / (1.0 - th)
+
+    for i in range(nx + 1):
+        for j in range(ny):
+            for k in range(nz):
+                face(u, (i, j, k), uw[i, j, k], nx, i, (i - 1, j, k), (i, j, k))
+    for i in range(nx):
+        for j in range(ny + 1):
+            for k in range(nz):
+                face(v, (i, j, k), vw[i, j, k], ny, j, (i, j - 1, k), (i, j, k))
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz + 1):
+                face(w, (i, j, k), ww[i, j, k], nz, k, (i, j, k - 1), (i, j, k))
+    return u, v, w
+
+
+def test_project_equals_literal(oracle):
+    dims = (8, 9, 7)
+    h = 1.0 / 9
+    dt = 0.4 * h
+    rng = np.random.default_rng(29)
+    x = [(np.arange(n) + 0.5) * h for n in dims]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    F = np.minimum(np.sqrt((X - 0.4) ** 2 + (Y - 0.45) ** 2 + (Z - 0.4) ** 2) - 0.3, Y - 0.35)
+    C = np.sqrt((X - 0.55) ** 2 + (Y - 0.3) ** 2 + (Z - 0.4) ** 2) - 0.17
+    nx, ny, nz = dims
+    u, v, w = rng.uniform(-1, 1, (nx + 1, ny, nz)), rng.uniform(-1, 1, (nx, ny + 1, nz)), rng.uniform(-1, 1, (nx, ny, nz + 1))
+    S = oracle.build_system(dims, h, dt, u, v, w, F, C)
+    pg = rng.uniform(-2, 2, dims)
+    got = oracle.project(dims, h, dt, u, v, w, pg, F, S["uwt"], S["vwt"], S["wwt"])
+    ref = literal_project(dims, h, dt, u, v, w, pg, F, S["uwt"], S["vwt"], S["wwt"])
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
+    # every branch is reached: fluid-fluid, both ghost sides, walls
+    sl, sr = F[:-1], F[1:]
+    assert ((sl < 0) & (sr < 0)).any() and ((sl < 0) & (sr >= 0)).any() and ((sl >= 0) & (sr < 0)).any()

@@ -7,6 +7,8 @@ the same operation order):
   nearest() (Spatify/include/Spatify/grids.h:287-292) truncating toward zero;
 * FlipAdvectionSolver3D::solveG2P (advect-solver.cc:157-169) and the PIC form
   (advect-solver.cc:7-17);
+* solveP2G (advect-solver.cc:188-271) in serial particle order: splat, weight
+  sums, normalisation, validity, u_last;
 * advect (advect-solver.cc:170-187): Ralston RK3 through sampleVelocity, then
   handleCollision (advect-solver.cc:100-137) with SDF<3>::grad
   (FluidSim/include/FluidSim/cpu/sdf.h:62-118: the mirrored trilinear blend of
@@ -181,3 +183,48 @@ def test_advect_and_collision_equal_literal(oracle, scene, collider):
         rp, rv = literal_advect(oracle, p, v, S["h"], S["grids"], C, S["box"], dt, fired)
         assert list(gp[i]) == rp and list(gv[i]) == rv, i
     assert fired["box"] > 0 and (fired["collider"] > 0) == collider, fired
+
+
+def literal_p2g(oracle, pos, vel, dims, h):
+    """FlipAdvectionSolver3D::solveP2G (advect-solver.cc:188-271) with the
+    particles taken in order (the reference's parallel loop races on shared
+    nodes; serial order is the oracle's parity mode)."""
+    nx, ny, nz = dims
+    shapes = ((nx + 1, ny, nz), (nx, ny + 1, nz), (nx, ny, nz + 1))
+    g = [np.zeros(s) for s in shapes]
+    wsum = [np.zeros(s) for s in shapes]
+    for p, v in zip(pos.tolist(), vel.tolist()):
+        idx = [_nearest(p, off, h) for off in OFFSETS]
+        for i in range(-1, 3):
+            for j in range(-1, 3):
+                for k in range(-1, 3):
+                    for a in range(3):
+                        n = (idx[a][0] + i, idx[a][1] + j, idx[a][2] + k)
+                        if not all(0 <= n[b] < shapes[a][b] for b in range(3)):
+                            continue
+                        pn = [(n[b] + OFFSETS[a][b]) * h + 0.0 for b in range(3)]
+                        wt = oracle.cubic_weight(h, [p[b] - pn[b] for b in range(3)])
+                        g[a][n] += v[a] * wt
+                        wsum[a][n] += wt
+    valid = []
+    for a in range(3):
+        pos_w = wsum[a] > 0.0
+        g[a] = np.where(pos_w, g[a] / np.where(pos_w, wsum[a], 1.0), 0.0)
+        valid.append(pos_w.astype(np.uint8))
+    return g, wsum, valid
+
+
+def test_p2g_equals_literal(oracle, scene):
+    S = scene
+    rng = np.random.default_rng(43)
+    ext = np.array(S["dims"]) * S["h"]
+    pos = rng.uniform(0.0, 1.0, (60, 3)) * ext * np.array([0.6, 1.0, 1.0])  # leaves empty faces
+    vel = rng.uniform(-1, 1, (60, 3))
+    got = oracle.p2g(pos, vel, S["dims"], S["h"], flip=True)
+    g, wsum, valid = literal_p2g(oracle, pos, vel, S["dims"], S["h"])
+    for a, c in enumerate("uvw"):
+        assert np.array_equal(got[c], g[a]), c
+        assert np.array_equal(got[c + "w"], wsum[a]), c
+        assert np.array_equal(got[c + "valid"], valid[a]), c
+        assert np.array_equal(got[c + "last"], g[a]), c  # u_last: the normalised grid itself
+        assert valid[a].any() and not valid[a].all()

@@ -29,9 +29,11 @@ inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 inline V3 operator*(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
 inline double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// glm::normalize, which the reference uses (Core/include/Core/utils.h:18):
+// v * inversesqrt(dot(v, v)), inversesqrt(x) = 1 / sqrt(x).
 inline V3 normalize3(V3 a) {
-  double l = std::sqrt(dot3(a, a));
-  return {a.x / l, a.y / l, a.z / l};
+  const double inv = 1.0 / std::sqrt(dot3(a, a));
+  return {a.x * inv, a.y * inv, a.z * inv};
 }
 
 // Dense 3-D view, spatify::LinearHashXYZ order (Spatify/include/Spatify/hash.h:23-26).

@@ -200,10 +200,11 @@ __device__ void handle_collision(const double* col, const Geo& G, double h, T& p
     if (d < 0.0) {
       double n[3];
       sdf_grad(col, G, h, (double)px, (double)py, (double)pz, n);
-      const double l = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-      n[0] /= l;
-      n[1] /= l;
-      n[2] /= l;
+      // glm::normalize: n * (1 / sqrt(dot(n, n)))
+      const double inv = 1.0 / sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      n[0] *= inv;
+      n[1] *= inv;
+      n[2] *= inv;
       px = (T)((double)px - d * n[0]);
       py = (T)((double)py - d * n[1]);
       pz = (T)((double)pz - d * n[2]);
@@ -817,8 +818,9 @@ __global__ void __launch_bounds__(kT) k_collider(Geo G, double h, T* g, const do
     if (sdf_eval(col, G.nx, G.ny, G.nz, h, px, py, pz) < 0.0) {
       double nrm[3];
       sdf_grad(col, G, h, px, py, pz, nrm);
-      const double l = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
-      const double nc = nrm[AX] / l;
+      // glm::normalize: nrm * (1 / sqrt(dot(nrm, nrm)))
+      const double inv = 1.0 / sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+      const double nc = nrm[AX] * inv;
       const double x = (double)g[id];
       g[id] = (T)(x - x * nc);
     }

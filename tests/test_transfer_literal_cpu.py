@@ -103,6 +103,8 @@ def literal_collide(C, h, box, p, v, fired=None):
             nrm = [g[a] * inv for a in range(3)]
             p = [p[a] - d * nrm[a] for a in range(3)]
             m = min(v[0] * nrm[0] + v[1] * nrm[1] + v[2] * nrm[2], 0.0)
+            if fired is not None and m < 0.0:
+                fired["inflow"] += 1
             v = [v[a] - m * nrm[a] for a in range(3)]
     for a in range(3):
         if fired is not None and (p[a] < 0.0 or p[a] > box[a]):
@@ -177,12 +179,18 @@ def test_advect_and_collision_equal_literal(oracle, scene, collider):
     S = scene
     C = S["C"] if collider else None
     dt = 0.05
-    gp, gv = oracle.advect(S["pos"], S["vel"], S["dims"], S["h"], *S["grids"], C, dt)
-    fired = {"collider": 0, "box": 0}
-    for i, (p, v) in enumerate(zip(S["pos"], S["vel"])):
+    rng = np.random.default_rng(47)
+    centre = np.array([0.45, 0.5, 0.35])
+    inside = centre + rng.uniform(-0.1, 0.1, (20, 3))  # in the collider sphere (radius 0.22)
+    pos = np.concatenate([S["pos"], inside])
+    vel = np.concatenate([S["vel"], (centre - inside) * 5.0])  # moving inward
+    gp, gv = oracle.advect(pos, vel, S["dims"], S["h"], *S["grids"], C, dt)
+    fired = {"collider": 0, "box": 0, "inflow": 0}
+    for i, (p, v) in enumerate(zip(pos, vel)):
         rp, rv = literal_advect(oracle, p, v, S["h"], S["grids"], C, S["box"], dt, fired)
         assert list(gp[i]) == rp and list(gv[i]) == rv, i
-    assert fired["box"] > 0 and (fired["collider"] > 0) == collider, fired
+    # the push-out and the removal of the inflowing velocity both ran
+    assert fired["box"] > 0 and (fired["collider"] > 0) == collider and (fired["inflow"] > 0) == collider, fired
 
 
 def literal_p2g(oracle, pos, vel, dims, h):

@@ -162,3 +162,125 @@ def test_torus_with_origin_and_partial_grid(oracle):
 def test_empty_mesh(oracle):
     sdf, cl, icnt = oracle.manifold_to_sdf(np.zeros((0, 3)), np.zeros((0, 3), np.int32), (4, 5, 6), 0.25)
     assert (sdf == 1e9).all() and (cl == -1).all() and not icnt.any()
+
+
+def literal_manifold_to_sdf(v, t, dims, h, origin, exact_band):
+    """manifold2SDF (util.cc:203-310) with checkNeighbour/sweep (:159-201),
+    insideTraingle2D/solveEquations/calcBiocentricCoord (:128-157), statement
+    by statement in plain Python floats, reference point-triangle distance."""
+    W, H, D = dims
+    ox, oy, oz = origin
+    V = [tuple(float(c) for c in p) for p in v]
+    T = [tuple(int(c) for c in tri) for tri in t]
+    sdf = np.full(dims, 1e9)
+    closest = np.full(dims, -1, np.int32)
+    cnt = np.zeros(dims, np.int32)
+
+    def clamp(a, lo, hi):
+        return lo if a < lo else (hi if a > hi else a)
+
+    def centre(x, y, z):
+        return ((x + 0.5) * h + ox, (y + 0.5) * h + oy, (z + 0.5) * h + oz)
+
+    def cross2(a, b):
+        return a[0] * b[1] - b[0] * a[1]
+
+    def inside2(p, a, b, c):
+        ap, ab = (p[0] - a[0], p[1] - a[1]), (b[0] - a[0], b[1] - a[1])
+        bp, bc = (p[0] - b[0], p[1] - b[1]), (c[0] - b[0], c[1] - b[1])
+        cp, ca = (p[0] - c[0], p[1] - c[1]), (a[0] - c[0], a[1] - c[1])
+        n = int(cross2(ap, ab) >= 0.0) + int(cross2(bp, bc) >= 0.0) + int(cross2(cp, ca) >= 0.0)
+        return n == 3 or n == 0
+
+    for i, (ia, ib, ic) in enumerate(T):
+        a, b, c = V[ia], V[ib], V[ic]
+        lo = [clamp(int(math.floor(min(min(a[q] - o, b[q] - o), c[q] - o) / h - 0.5)) - exact_band, 0, n - 1)
+              for q, (o, n) in enumerate(zip(origin, dims))]
+        hi = [clamp(int(math.ceil(max(max(a[q] - o, b[q] - o), c[q] - o) / h - 0.5)) + exact_band, 0, n - 1)
+              for q, (o, n) in enumerate(zip(origin, dims))]
+        for x in range(lo[0], hi[0] + 1):
+            for y in range(lo[1], hi[1] + 1):
+                for z in range(lo[2], hi[2] + 1):
+                    d = ref_dist(centre(x, y, z), a, b, c, False)
+                    if d < sdf[x, y, z]:
+                        sdf[x, y, z] = d
+                        closest[x, y, z] = i
+        lo = [clamp(int(math.floor(min(min(a[q] - o, b[q] - o), c[q] - o) / h - 0.5)), 0, n - 1)
+              for q, (o, n) in enumerate(zip(origin[:2], dims[:2]))]
+        hi = [clamp(int(math.ceil(max(max(a[q] - o, b[q] - o), c[q] - o) / h - 0.5)), 0, n - 1)
+              for q, (o, n) in enumerate(zip(origin[:2], dims[:2]))]
+        for j in range(lo[0], hi[0] + 1):
+            for k in range(lo[1], hi[1] + 1):
+                orig = centre(j, k, -1)
+                pp = (orig[0], orig[1])
+                if not inside2(pp, a, b, c):
+                    continue
+                a1, b1, c1 = a[0] - c[0], b[0] - c[0], pp[0] - c[0]
+                a2, b2, c2 = a[1] - c[1], b[1] - c[1], pp[1] - c[1]
+                det = a1 * b2 - a2 * b1
+                u = (c1 * b2 - c2 * b1) / det
+                vv = (a1 * c2 - a2 * c1) / det
+                w = 1.0 - u - vv
+                inter_z = a[2] * u + b[2] * vv + c[2] * w
+                l = int(math.ceil((inter_z - oz) / h - 0.5))
+                if l < 0:
+                    cnt[j, k, 0] += 1
+                elif l < D:
+                    cnt[j, k, l] += 1
+
+    def check(dx, dy, dz, x, y, z):
+        nx_, ny_, nz_ = x + dx, y + dy, z + dz
+        if nx_ < 0 or nx_ >= W or ny_ < 0 or ny_ >= H or nz_ < 0 or nz_ >= D:
+            return
+        tri = closest[nx_, ny_, nz_]
+        if tri == -1:
+            return
+        ia, ib, ic = T[tri]
+        d1 = ref_dist(centre(x, y, z), V[ia], V[ib], V[ic], False)
+        if abs(d1) < abs(sdf[x, y, z]):
+            sdf[x, y, z] = d1
+            closest[x, y, z] = tri
+
+    def sweep(dx, dy, dz):
+        xs = range(W - 1, -1, -1) if dx > 0 else range(W)
+        ys = range(H - 1, -1, -1) if dy > 0 else range(H)
+        zs = range(D - 1, -1, -1) if dz > 0 else range(D)
+        for x in xs:
+            for y in ys:
+                for z in zs:
+                    check(0, dy, dz, x, y, z)
+                    check(dx, 0, dz, x, y, z)
+                    check(dx, dy, 0, x, y, z)
+                    check(0, 0, dz, x, y, z)
+                    check(0, dy, 0, x, y, z)
+                    check(dx, 0, 0, x, y, z)
+                    check(dx, dy, dz, x, y, z)
+
+    for _ in range(2):
+        for dx, dy, dz in ((1, 1, 1), (1, 1, -1), (1, -1, 1), (1, -1, -1), (-1, 1, 1), (-1, 1, -1), (-1, -1, 1),
+                           (-1, -1, -1)):
+            sweep(dx, dy, dz)
+    for i in range(W):
+        for j in range(H):
+            tot = 0
+            for k in range(D):
+                tot += int(cnt[i, j, k])
+                if tot & 1:
+                    sdf[i, j, k] = -sdf[i, j, k]
+    return sdf, closest, cnt
+
+
+@pytest.mark.parametrize("case", ["icosphere_band1", "torus_origin"])
+def test_manifold_to_sdf_equals_literal(oracle, case):
+    if case == "icosphere_band1":
+        v, t = scenes.icosphere(1, 0.3, (0.48, 0.52, 0.5))
+        dims, h, origin, band = (10, 11, 9), 0.1, (0.0, 0.0, 0.0), 1
+    else:
+        v, t = scenes.torus(10, 6, 0.28, 0.1, (0.5, 0.5, 0.5))
+        dims, h, origin, band = (11, 9, 10), 1.0 / 10, (0.03, 0.06, -0.02), 2
+    sdf, cl, icnt = oracle.manifold_to_sdf(v, t, dims, h, origin=origin, exact_band=band)
+    ls, lc, li = literal_manifold_to_sdf(v, t, dims, h, origin, band)
+    assert np.array_equal(icnt, li)
+    assert np.array_equal(cl, lc)
+    assert np.array_equal(sdf, ls)
+    assert (ls < 0).any() and (lc >= 0).all()

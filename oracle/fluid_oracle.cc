@@ -1049,6 +1049,32 @@ struct ora_sim {
   int64_t fsize[3];
 };
 
+// smoothFluidSurface (fluid-simulator.cc:39-74): min-preserving neighbour
+// average, ping-ponging fluidSurface and fluidSurfaceBuf.
+static void sim_smooth(ora_sim* s, int iters) {
+  const int nx = s->c.nx, ny = s->c.ny, nz = s->c.nz;
+  for (int it = 0; it < iters; it++) {
+    const double* src = s->sdf[s->scur].data();
+    double* dst = s->sdf[1 - s->scur].data();
+    for (int i = 0; i < nx; i++)
+      for (int j = 0; j < ny; j++)
+        for (int k = 0; k < nz; k++) {
+          int64_t id = k + (int64_t)j * nz + (int64_t)i * ny * nz;
+          double sum = 0;
+          int cnt = 0;
+          if (i > 0) { sum += src[id - (int64_t)ny * nz]; cnt++; }
+          if (i < nx - 1) { sum += src[id + (int64_t)ny * nz]; cnt++; }
+          if (j > 0) { sum += src[id - nz]; cnt++; }
+          if (j < ny - 1) { sum += src[id + nz]; cnt++; }
+          if (k > 0) { sum += src[id - 1]; cnt++; }
+          if (k < nz - 1) { sum += src[id + 1]; cnt++; }
+          dst[id] = sum / cnt;
+          if (src[id] < dst[id]) dst[id] = src[id];
+        }
+    s->scur = 1 - s->scur;
+  }
+}
+
 static void sim_alloc(ora_sim* s) {
   int nx = s->c.nx, ny = s->c.ny, nz = s->c.nz;
   int64_t N = (int64_t)nx * ny * nz;
@@ -1166,27 +1192,7 @@ void ora_sim_substep(ora_sim* s, double dt) {  // fluid-simulator.cc:140-182
     s->scur = 1 - s->scur;
     s->svcur = 1 - s->svcur;
   }
-  // smoothFluidSurface (fluid-simulator.cc:39-74): min-preserving neighbour average.
-  for (int it = 0; it < c.smooth_iters; it++) {
-    const double* src = s->sdf[s->scur].data();
-    double* dst = s->sdf[1 - s->scur].data();
-    for (int i = 0; i < nx; i++)
-      for (int j = 0; j < ny; j++)
-        for (int k = 0; k < nz; k++) {
-          int64_t id = k + (int64_t)j * nz + (int64_t)i * ny * nz;
-          double sum = 0;
-          int cnt = 0;
-          if (i > 0) { sum += src[id - (int64_t)ny * nz]; cnt++; }
-          if (i < nx - 1) { sum += src[id + (int64_t)ny * nz]; cnt++; }
-          if (j > 0) { sum += src[id - nz]; cnt++; }
-          if (j < ny - 1) { sum += src[id + nz]; cnt++; }
-          if (k > 0) { sum += src[id - 1]; cnt++; }
-          if (k < nz - 1) { sum += src[id + 1]; cnt++; }
-          dst[id] = sum / cnt;
-          if (src[id] < dst[id]) dst[id] = src[id];
-        }
-    s->scur = 1 - s->scur;
-  }
+  sim_smooth(s, c.smooth_iters);
   const double* fluid = s->sdf[s->scur].data();
   // P2G (:155-156)
   U = s->g[0][s->gcur[0]].data();
@@ -1370,6 +1376,14 @@ void ora_sim_get_faces(const ora_sim* s, double* u, double* v, double* w) {
 void ora_sim_get_fluid_sdf(const ora_sim* s, double* sdf) {
   std::memcpy(sdf, s->sdf[s->scur].data(), sizeof(double) * s->sdf[s->scur].size());
 }
+// FluidSimulator::reconstruct (cpu/fluid-simulator.h:115-119): the particles'
+// surface into the current fluidSurface and sdfValid; the reference passes
+// radius = 1.2 h / sqrt(2).
+void ora_sim_reconstruct(ora_sim* s, double radius) {
+  ora_reconstruct(s->n, s->pos.data(), s->c.nx, s->c.ny, s->c.nz, s->c.h, radius,
+                  s->sdf[s->scur].data(), s->sdfv[s->svcur].data());
+}
+void ora_sim_smooth_fluid_surface(ora_sim* s, int iters) { sim_smooth(s, iters); }
 void ora_sim_get_system(const ora_sim* s, double* adiag, double* const* an, double* rhs,
                         uint8_t* active) {
   size_t N = s->adiag.size();

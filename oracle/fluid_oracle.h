@@ -123,6 +123,12 @@ void ora_sim_get_particles(const ora_sim* s, double* pos, double* vel);
 void ora_sim_get_pressure(const ora_sim* s, double* p);
 void ora_sim_get_faces(const ora_sim* s, double* u, double* v, double* w);
 void ora_sim_get_fluid_sdf(const ora_sim* s, double* sdf);
+/* FluidSimulator::reconstruct() (cpu/fluid-simulator.h:115-119, radius
+ * 1.2 h / sqrt 2 in the reference) and smoothFluidSurface(iters)
+ * (fluid-simulator.cc:39-74) on the simulator's own surface buffers, as the
+ * reference's export path calls them between steps. */
+void ora_sim_reconstruct(ora_sim* s, double radius);
+void ora_sim_smooth_fluid_surface(ora_sim* s, int iters);
 void ora_sim_get_system(const ora_sim* s, double* adiag, double* const* an, double* rhs,
                         uint8_t* active);
 int ora_sim_last_iters(const ora_sim* s);

@@ -60,6 +60,8 @@ def lib():
             "ora_rebuild_surface": (_i64, [_int, _int, _int, _dp, _dp, _dp, _dp, _dp,
                                            ctypes.POINTER(ctypes.c_uint32), _i64, _i64,
                                            ctypes.POINTER(ctypes.c_int64)]),
+            "ora_sim_reconstruct": (None, [ctypes.c_void_p, _dbl]),
+            "ora_sim_smooth_fluid_surface": (None, [ctypes.c_void_p, _int]),
             "ora_manifold_to_sdf": (None, [_int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dp,
                                            ctypes.POINTER(ctypes.c_int), _i64, _int, _int, _dp,
                                            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
@@ -359,6 +361,14 @@ class Sim:
         u, v, w = np.zeros(su), np.zeros(sv), np.zeros(sw)
         lib().ora_sim_get_faces(self._h, _p(u), _p(v), _p(w))
         return u, v, w
+
+    def reconstruct(self, radius=None):
+        """FluidSimulator::reconstruct(): radius 1.2 h / sqrt(2) by default."""
+        h = self.cfg["h"]
+        lib().ora_sim_reconstruct(self._h, 1.2 * h / np.sqrt(2.0) if radius is None else radius)
+
+    def smooth_fluid_surface(self, iters):
+        lib().ora_sim_smooth_fluid_surface(self._h, int(iters))
 
     def fluid_sdf(self):
         s = np.zeros(self.dims)

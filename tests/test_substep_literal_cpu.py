@@ -132,6 +132,32 @@ class LiteralSim:
         self.C = collider
         self.alpha, self.tol, self.max_iter = alpha, tol, max_iter
 
+    def smooth(self, iters):
+        """smoothFluidSurface (fluid-simulator.cc:39-74)."""
+        n = self.n
+        for _ in range(iters):
+            S, B = self.surf, self.surfbuf
+            for i in range(n):
+                for j in range(n):
+                    for k in range(n):
+                        s, c = 0.0, 0
+                        for (a, b, e, ok) in ((i - 1, j, k, i > 0), (i + 1, j, k, i < n - 1), (i, j - 1, k, j > 0),
+                                              (i, j + 1, k, j < n - 1), (i, j, k - 1, k > 0),
+                                              (i, j, k + 1, k < n - 1)):
+                            if ok:
+                                s += S[a, b, e]
+                                c += 1
+                        B[i, j, k] = s / c
+                        if S[i, j, k] < B[i, j, k]:
+                            B[i, j, k] = S[i, j, k]
+            self.surf, self.surfbuf = B, S
+
+    def reconstruct(self):
+        """FluidSimulator::reconstruct (cpu/fluid-simulator.h:115-119)."""
+        sdf, valid = literal_reconstruct(self.pos, self.dims, self.h, 1.2 * self.h / math.sqrt(2.0))
+        self.surf[...] = sdf
+        self.sval[...] = valid
+
     def substep(self, dt):
         O, n, h, dims = self.O, self.n, self.h, self.dims
         for a in range(3):  # clear()
@@ -155,22 +181,7 @@ class LiteralSim:
         self.sval[...] = valid
         self.surf, self.surfbuf, self.sval, self.svalbuf = _extrapolate(self.surf, self.surfbuf, self.sval,
                                                                         self.svalbuf, 10, zero_invalid=False)
-        for _ in range(5):  # smoothFluidSurface
-            S, B = self.surf, self.surfbuf
-            for i in range(n):
-                for j in range(n):
-                    for k in range(n):
-                        s, c = 0.0, 0
-                        for (a, b, e, ok) in ((i - 1, j, k, i > 0), (i + 1, j, k, i < n - 1), (i, j - 1, k, j > 0),
-                                              (i, j + 1, k, j < n - 1), (i, j, k - 1, k > 0),
-                                              (i, j, k + 1, k < n - 1)):
-                            if ok:
-                                s += S[a, b, e]
-                                c += 1
-                        B[i, j, k] = s / c
-                        if S[i, j, k] < B[i, j, k]:
-                            B[i, j, k] = S[i, j, k]
-            self.surf, self.surfbuf = B, S
+        self.smooth(5)
         # P2G into the cleared grids, serial particle order
         wsum = [np.zeros_like(x) for x in self.g]
         for p, v in zip(self.pos, self.vel):
@@ -266,3 +277,32 @@ def test_substep_equals_literal(oracle, collider):
         adiag, an, rhs, act = sim.system()
         assert np.array_equal(adiag, lit.system["adiag"]) and np.array_equal(rhs, lit.system["rhs"])
         assert np.array_equal(act, lit.system["active"]) and lit.iters > 1
+
+
+def test_export_calls_between_substeps_equal_literal(oracle):
+    """The reference's export path (FluidSim/disabled/fluid-sim.cc:231-235)
+    calls reconstruct() and smoothFluidSurface(5) between frames; both act on
+    the simulator's surface buffers, so they change the stale values the next
+    substep's extrapolation reads.  The oracle follows the literal simulator
+    through substep, reconstruct, smooth, substep."""
+    from simcraft_b200 import scenes
+
+    n = 8
+    pos, vel, h = scenes.dam_break(n, ppc=2, seed=7)
+    sim = oracle.Sim(**oracle.default_config(n, n, n, h))
+    sim.set_particles(pos, vel)
+    lit = LiteralSim(oracle, n, h, pos, vel, None)
+    dt = 1.0 / 120
+    sim.substep(dt)
+    lit.substep(dt)
+    sim.reconstruct()
+    lit.reconstruct()
+    assert np.array_equal(sim.fluid_sdf(), lit.surf)
+    sim.smooth_fluid_surface(5)
+    lit.smooth(5)
+    assert np.array_equal(sim.fluid_sdf(), lit.surf)
+    sim.substep(dt)
+    lit.substep(dt)
+    p, v = sim.particles()
+    assert np.array_equal(p, np.array(lit.pos)) and np.array_equal(v, np.array(lit.vel))
+    assert np.array_equal(sim.fluid_sdf(), lit.surf) and np.array_equal(sim.pressure(), lit.pg)

@@ -384,6 +384,17 @@ int sc_fluid_get_pressure(sc_fluid* sim, double* pg, int device_pointers);
 int sc_fluid_get_faces(sc_fluid* sim, double* u, double* v, double* w, int device_pointers);
 /* exportFluidSurface() (fluid-simulator.h:187-189): the smoothed fluid SDF. */
 int sc_fluid_get_fluid_sdf(sc_fluid* sim, double* sdf, int device_pointers);
+/* FluidSimulator::reconstruct() (FluidSim/include/FluidSim/cpu/fluid-simulator.h
+ * :115-119): the surface of the particles as they are now, into the
+ * simulator's fluid SDF (what sc_fluid_get_fluid_sdf returns).  radius <= 0
+ * selects the reference's 1.2 h / sqrt(2).  smoothFluidSurface(iters)
+ * (FluidSim/src/cpu/fluid-simulator.cc:39-74): min-preserving neighbour
+ * averaging of that SDF.  Both act on the simulator's own surface buffers, as
+ * the reference's, so calling them between steps (as its export path does)
+ * changes the stale buffer values the next substep's SDF extrapolation reads,
+ * exactly as in the reference. */
+int sc_fluid_reconstruct(sc_fluid* sim, double radius);
+int sc_fluid_smooth_fluid_surface(sc_fluid* sim, int iters);
 
 /* ---------------------------------------------------------------------------
  * Differentiable FLIP/PIC substeps (no counterpart in the reference).

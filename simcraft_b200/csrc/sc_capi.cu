@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <string>
@@ -849,6 +850,19 @@ int sc_fluid_get_fluid_sdf(sc_fluid* sim, double* sdf, int device_pointers) {
   if (!sim || !sdf) return SC_ERR_INVALID;
   cudaSetDevice(sim->ctx->c.device);
   return fl_rc(sim, sim->sim->get_fluid_sdf(sdf, device_pointers != 0));
+}
+
+int sc_fluid_reconstruct(sc_fluid* sim, double radius) {
+  if (!sim || !(radius < 1e300)) return SC_ERR_INVALID;  // rejects NaN and Inf
+  cudaSetDevice(sim->ctx->c.device);
+  const double h = sim->sim->config().h;
+  return fl_rc(sim, sim->sim->reconstruct(radius > 0.0 ? radius : 1.2 * h / std::sqrt(2.0)));
+}
+
+int sc_fluid_smooth_fluid_surface(sc_fluid* sim, int iters) {
+  if (!sim || iters < 0) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  return fl_rc(sim, sim->sim->smooth_fluid_surface(iters));
 }
 
 // ---------------------------------------------------------------------------------

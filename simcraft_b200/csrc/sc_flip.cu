@@ -329,6 +329,58 @@ int FluidSim::substep(double dt, StepStats* st) {
   return c_.f32 ? substep_t<float>(dt, st) : substep_t<double>(dt, st);
 }
 
+// FluidSimulator::reconstruct (cpu/fluid-simulator.h:115-119): the surface of
+// the particles as they are now into the current fluidSurface and sdfValid,
+// sorted by cell first exactly as the substep sorts them (cell, then index), so
+// later substeps see the same particle order.
+template <class T>
+int FluidSim::reconstruct_t(double radius) {
+  cudaStream_t st = ctx_->stream;
+  const Geo G{c_.nx, c_.ny, c_.nz};
+  const double h = c_.h;
+  const int64_t N = (int64_t)c_.nx * c_.ny * c_.nz;
+  const int64_t n = n_;
+  PartsT<T> P{(T*)px_, (T*)py_, (T*)pz_, (T*)vx_, (T*)vy_, (T*)vz_};
+  PartsT<T> S{(T*)spx_, (T*)spy_, (T*)spz_, (T*)svx_, (T*)svy_, (T*)svz_};
+  if (n > 0) {
+    SortBufs sb{key_, cnt_, start_, cursor_, bsum_};
+    launches_ += sort_particles<T>(st, n, G, h, P, id_, S, sid_, sb);
+    std::swap(px_, spx_);
+    std::swap(py_, spy_);
+    std::swap(pz_, spz_);
+    std::swap(vx_, svx_);
+    std::swap(vy_, svy_);
+    std::swap(vz_, svz_);
+    std::swap(id_, sid_);
+    P = PartsT<T>{(T*)px_, (T*)py_, (T*)pz_, (T*)vx_, (T*)vy_, (T*)vz_};
+  } else {
+    cudaMemsetAsync(cnt_, 0, sizeof(int) * N, st);
+    cudaMemsetAsync(start_, 0, sizeof(int) * N, st);
+  }
+  k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, radius, start_, cnt_, P.px, P.py, P.pz, sdf_[scur_],
+                                           sdfv_[svcur_]);
+  launches_ += 1;
+  return err("reconstruct");
+}
+
+int FluidSim::reconstruct(double radius) {
+  return c_.f32 ? reconstruct_t<float>(radius) : reconstruct_t<double>(radius);
+}
+
+// smoothFluidSurface (fluid-simulator.cc:39-74) on the simulator's surface
+// buffers, flipping them once per pass as the substep does.
+int FluidSim::smooth_fluid_surface(int iters) {
+  cudaStream_t st = ctx_->stream;
+  const Geo G{c_.nx, c_.ny, c_.nz};
+  const int64_t N = (int64_t)c_.nx * c_.ny * c_.nz;
+  for (int it = 0; it < iters; it++) {
+    k_smooth_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_]);
+    scur_ = 1 - scur_;
+  }
+  launches_ += iters;
+  return err("smooth_fluid_surface");
+}
+
 int FluidSim::step(double frame_dt, StepStats* st) {  // fluid-simulator.cc:205-220
   double t = 0;
   while (t < frame_dt) {

@@ -50,12 +50,18 @@ class FluidSim {
   int get_pressure(double* p, bool device);
   int get_faces(double* u, double* v, double* w, bool device);
   int get_fluid_sdf(double* s, bool device);
+  // FluidSimulator::reconstruct() and smoothFluidSurface(iters) on the
+  // simulator's own surface buffers (cpu/fluid-simulator.h:115-121).
+  int reconstruct(double radius);
+  int smooth_fluid_surface(int iters);
   int64_t num_particles() const { return n_; }
   const FluidConfig& config() const { return c_; }
 
  private:
   template <class T>
   int substep_t(double dt, StepStats* st);
+  template <class T>
+  int reconstruct_t(double radius);
   int alloc_particles(int64_t n);
   int err(const char* where);
 

@@ -178,6 +178,18 @@ class FluidSimulator:
         check("sc_fluid_get_fluid_sdf", lib().sc_fluid_get_fluid_sdf(self.handle, _ptr(s), 0), self.ctx.handle)
         return s
 
+    def reconstruct(self, radius=None):
+        """FluidSimulator::reconstruct() (cpu/fluid-simulator.h:115-119): the
+        particles' surface into the fluid SDF, radius 1.2 h / sqrt(2) unless
+        given."""
+        check("sc_fluid_reconstruct", lib().sc_fluid_reconstruct(self.handle, float(radius or 0.0)),
+              self.ctx.handle)
+
+    def smooth_fluid_surface(self, iters):
+        """smoothFluidSurface(iters) (fluid-simulator.cc:39-74) on the fluid SDF."""
+        check("sc_fluid_smooth_fluid_surface", lib().sc_fluid_smooth_fluid_surface(self.handle, int(iters)),
+              self.ctx.handle)
+
     def rebuild_surface(self):
         """rebuildSurface(mesh, exportFluidSurface()) (rebuild-surface.cc:732-741,
         as FluidSim/disabled/fluid-sim.cc:230-238 exports the fluid): the

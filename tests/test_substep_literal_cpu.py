@@ -20,7 +20,9 @@ restatement of FluidSimulator::substep (FluidSim/src/cpu/fluid-simulator.cc:
 The restatement reuses the literal pieces of test_solver_literal_cpu and
 test_transfer_literal_cpu; after each of two substeps of a small dam break
 (with and without a collider) particles, pressure, faces, the fluid SDF and the
-assembled system must equal the oracle's bit for bit."""
+assembled system must equal the oracle's bit for bit.  Also restated: CFL and
+the frame loop (fluid-simulator.cc:184-220), and the export path's
+reconstruct() / smoothFluidSurface() between substeps."""
 import math
 
 import numpy as np
@@ -151,6 +153,28 @@ class LiteralSim:
                         if S[i, j, k] < B[i, j, k]:
                             B[i, j, k] = S[i, j, k]
             self.surf, self.surfbuf = B, S
+
+    def cfl(self, factor):
+        """FluidSimulator::CFL (fluid-simulator.cc:184-203): h / |u| over the
+        non-zero face velocities, floored at 1e-3, times the CFL factor."""
+        h = self.h
+        c = h / 1e-6
+        for G in self.g:
+            for u in G.ravel().tolist():
+                if u != 0.0:
+                    c = min(c, h / abs(u))
+        return factor * max(1e-3, c)
+
+    def step(self, frame_dt, factor):
+        """FluidSimulator::step (fluid-simulator.cc:205-220)."""
+        t = 0.0
+        count = 0
+        while t < frame_dt:
+            dt = min(self.cfl(factor), frame_dt - t)
+            self.substep(dt)
+            t += dt
+            count += 1
+        return count
 
     def reconstruct(self):
         """FluidSimulator::reconstruct (cpu/fluid-simulator.h:115-119)."""
@@ -306,3 +330,27 @@ def test_export_calls_between_substeps_equal_literal(oracle):
     p, v = sim.particles()
     assert np.array_equal(p, np.array(lit.pos)) and np.array_equal(v, np.array(lit.vel))
     assert np.array_equal(sim.fluid_sdf(), lit.surf) and np.array_equal(sim.pressure(), lit.pg)
+
+
+def test_frame_loop_equals_literal(oracle):
+    """step(frame) (fluid-simulator.cc:205-220): substeps of min(CFL, rest of the
+    frame) until the frame is covered; a CFL factor of 0.2 makes the second
+    frame take several substeps."""
+    from simcraft_b200 import scenes
+
+    n = 8
+    pos, vel, h = scenes.dam_break(n, ppc=2, seed=9)
+    vel = np.random.default_rng(10).uniform(-0.5, 0.5, pos.shape)
+    factor = 0.2
+    sim = oracle.Sim(**oracle.default_config(n, n, n, h, cfl_factor=factor))
+    sim.set_particles(pos, vel)
+    lit = LiteralSim(oracle, n, h, pos, vel, None)
+    counts = []
+    for frame in range(2):
+        sim.step(0.05)
+        counts.append(lit.step(0.05, factor))
+        p, v = sim.particles()
+        assert np.array_equal(p, np.array(lit.pos)) and np.array_equal(v, np.array(lit.vel)), frame
+        assert np.array_equal(sim.pressure(), lit.pg), frame
+    assert counts[0] == 1 and counts[1] > 1, counts  # the grids are empty before the first substep
+    assert sim.cfl() == lit.cfl(factor)

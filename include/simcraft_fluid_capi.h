@@ -53,7 +53,8 @@ extern "C" {
 typedef struct sc_context sc_context;
 typedef struct sc_pcg sc_pcg;
 
-/* Library identity. */
+/* Library identity: major * 10000 + minor * 100 (1.1 added the surface export
+ * and the simulator's reconstruct / smoothing calls). */
 int sc_version(void);
 const char* sc_status_string(int status);
 

@@ -107,7 +107,7 @@ int validate_options(const sc_pcg_options* o) {
 
 extern "C" {
 
-int sc_version(void) { return 10000; }
+int sc_version(void) { return 10100; }  // 1.1: surface export, simulator export calls
 
 const char* sc_status_string(int status) {
   switch (status) {

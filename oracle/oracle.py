@@ -125,6 +125,10 @@ def set_threads(n):
     lib().ora_set_threads(int(n))
 
 
+def get_threads():
+    return lib().ora_get_threads()
+
+
 def set_parity_mode(on):
     lib().ora_set_parity_mode(1 if on else 0)
 

@@ -114,3 +114,38 @@ def test_dam_break_step_invariants(oracle):
     assert np.isfinite(p).all() and np.isfinite(v).all()
     assert p.min() >= 0.0 and p.max() <= 1.0
     assert v[:, 1].mean() < 0  # gravity pulls the column down
+
+
+def test_timing_mode_does_the_same_work(oracle):
+    """bench.py times the oracle in its timing mode (parallel P2G with
+    per-thread accumulation, OpenMP where the reference uses TBB).  That mode
+    must compute what the parity mode computes, up to summation order: P2G
+    grids, then a whole simulated frame."""
+    from simcraft_b200 import scenes
+
+    pos, vel, h = scenes.dam_break(16, seed=2)
+    vel = np.random.default_rng(3).uniform(-1, 1, pos.shape)
+    threads = oracle.get_threads()
+    try:
+        oracle.set_threads(max(4, threads))
+        oracle.set_parity_mode(True)
+        a = oracle.p2g(pos, vel, (16, 16, 16), h)
+        cfg = oracle.default_config(16, 16, 16, h, pcg_tol=1e-10, pcg_criterion=1)
+        s1 = oracle.Sim(**cfg)
+        s1.set_particles(pos, vel)
+        s1.step(1.0 / 120)
+        oracle.set_parity_mode(False)
+        b = oracle.p2g(pos, vel, (16, 16, 16), h)
+        s2 = oracle.Sim(**cfg)
+        s2.set_particles(pos, vel)
+        s2.step(1.0 / 120)
+    finally:
+        oracle.set_parity_mode(True)
+        oracle.set_threads(threads)
+    for k in ("u", "v", "w", "uw", "vw", "ww"):
+        np.testing.assert_allclose(b[k], a[k], rtol=1e-12, atol=1e-14)
+    for k in ("uvalid", "vvalid", "wvalid"):
+        assert np.array_equal(a[k], b[k])
+    p1, p2 = s1.pressure(), s2.pressure()
+    assert np.linalg.norm(p2 - p1) / np.linalg.norm(p1) < 1e-8
+    assert np.abs(s2.particles()[0] - s1.particles()[0]).max() < 1e-8 * h

@@ -395,6 +395,10 @@ int sc_fluid_get_fluid_sdf(sc_fluid* sim, double* sdf, int device_pointers);
  * changes the stale buffer values the next substep's SDF extrapolation reads,
  * exactly as in the reference. */
 int sc_fluid_reconstruct(sc_fluid* sim, double radius);
+/* exportColliderSurface() (cpu/fluid-simulator.h:191-193): the collider SDF on
+ * the simulator's grid, reference layout; 1e9 everywhere when no collider is
+ * set (what manifold2SDF leaves for an empty mesh). */
+int sc_fluid_get_collider_sdf(sc_fluid* sim, double* sdf, int device_pointers);
 int sc_fluid_smooth_fluid_surface(sc_fluid* sim, int iters);
 
 /* ---------------------------------------------------------------------------

@@ -122,6 +122,7 @@ SIGNATURES = {
     "sc_rebuild_surface_host": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                         c_void_p, c_void_p, c_int64, c_int64, P(c_int64), P(c_int64)]),
     "sc_fluid_reconstruct": (c_int, [c_void_p, c_double]),
+    "sc_fluid_get_collider_sdf": (c_int, [c_void_p, c_void_p, c_int]),
     "sc_fluid_smooth_fluid_surface": (c_int, [c_void_p, c_int]),
     "sc_fluid_cfl": (c_int, [c_void_p, P(c_double)]),
     "sc_fluid_substep": (c_int, [c_void_p, c_double, P(sc_fluid_stats)]),

@@ -852,6 +852,12 @@ int sc_fluid_get_fluid_sdf(sc_fluid* sim, double* sdf, int device_pointers) {
   return fl_rc(sim, sim->sim->get_fluid_sdf(sdf, device_pointers != 0));
 }
 
+int sc_fluid_get_collider_sdf(sc_fluid* sim, double* sdf, int device_pointers) {
+  if (!sim || !sdf) return SC_ERR_INVALID;
+  cudaSetDevice(sim->ctx->c.device);
+  return fl_rc(sim, sim->sim->get_collider_sdf(sdf, device_pointers != 0));
+}
+
 int sc_fluid_reconstruct(sc_fluid* sim, double radius) {
   if (!sim || !(radius < 1e300)) return SC_ERR_INVALID;  // rejects NaN and Inf
   cudaSetDevice(sim->ctx->c.device);

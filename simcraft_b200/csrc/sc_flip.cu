@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 
+#include <vector>
 #include "sc_flip.cuh"
 #include "sc_fvm.cuh"
 
@@ -426,6 +427,26 @@ int FluidSim::get_fluid_sdf(double* s, bool device) {
                   ctx_->stream);
   if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return err("get_fluid_sdf");
   return err("get_fluid_sdf");
+}
+
+// exportColliderSurface (cpu/fluid-simulator.h:191-193): the collider SDF; an
+// empty collider is 1e9 everywhere, as manifold2SDF leaves it.
+int FluidSim::get_collider_sdf(double* s, bool device) {
+  const int64_t N = (int64_t)c_.nx * c_.ny * c_.nz;
+  if (!collider_ && !device) {
+    std::fill(s, s + N, 1e9);
+    return 0;
+  }
+  std::vector<double> empty;
+  if (collider_) {
+    cudaMemcpyAsync(s, collider_, sizeof(double) * N, device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                    ctx_->stream);
+  } else {
+    empty.assign((size_t)N, 1e9);
+    cudaMemcpyAsync(s, empty.data(), sizeof(double) * N, cudaMemcpyHostToDevice, ctx_->stream);
+  }
+  if (cudaStreamSynchronize(ctx_->stream) != cudaSuccess) return err("get_collider_sdf");
+  return err("get_collider_sdf");
 }
 
 int FluidSim::get_faces(double* u, double* v, double* w, bool device) {

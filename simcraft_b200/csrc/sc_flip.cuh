@@ -50,6 +50,7 @@ class FluidSim {
   int get_pressure(double* p, bool device);
   int get_faces(double* u, double* v, double* w, bool device);
   int get_fluid_sdf(double* s, bool device);
+  int get_collider_sdf(double* s, bool device);  // 1e9 everywhere when there is none
   // FluidSimulator::reconstruct() and smoothFluidSurface(iters) on the
   // simulator's own surface buffers (cpu/fluid-simulator.h:115-121).
   int reconstruct(double radius);

@@ -178,6 +178,13 @@ class FluidSimulator:
         check("sc_fluid_get_fluid_sdf", lib().sc_fluid_get_fluid_sdf(self.handle, _ptr(s), 0), self.ctx.handle)
         return s
 
+    def export_collider_surface(self):
+        """exportColliderSurface() (cpu/fluid-simulator.h:191-193): the collider
+        SDF, 1e9 everywhere when there is none."""
+        s = np.zeros(self.dims)
+        check("sc_fluid_get_collider_sdf", lib().sc_fluid_get_collider_sdf(self.handle, _ptr(s), 0), self.ctx.handle)
+        return s
+
     def reconstruct(self, radius=None):
         """FluidSimulator::reconstruct() (cpu/fluid-simulator.h:115-119): the
         particles' surface into the fluid SDF, radius 1.2 h / sqrt(2) unless

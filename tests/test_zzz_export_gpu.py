@@ -42,3 +42,22 @@ def test_export_calls_between_frames_follow_the_oracle(oracle, gpu):
     assert np.linalg.norm(p_gpu - p_ref) / np.linalg.norm(p_ref) < 1e-5
     assert np.abs(sim.positions() - ref.particles()[0]).max() < 1e-4 * h
     np.testing.assert_allclose(sim.export_fluid_surface(), ref.fluid_sdf(), rtol=0, atol=1e-6 * h)
+
+
+def test_export_collider_surface(gpu):
+    """exportColliderSurface(): 1e9 everywhere without a collider, the given
+    SDF after setCollider(sdf), and empty again after removing it."""
+    from simcraft_b200 import scenes
+    from simcraft_b200.fluid import FluidSimulator
+
+    n = 12
+    pos, vel, h = scenes.dam_break(n, seed=2)
+    sim = FluidSimulator(len(pos), (1.0, 1.0, 1.0), (n, n, n))
+    assert (sim.export_collider_surface() == 1e9).all()
+    x = (np.arange(n) + 0.5) * h
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    C = np.sqrt((X - 0.6) ** 2 + (Y - 0.3) ** 2 + (Z - 0.5) ** 2) - 0.2
+    sim.set_collider(C)
+    assert np.array_equal(sim.export_collider_surface(), C)
+    sim.set_collider(None)
+    assert (sim.export_collider_surface() == 1e9).all()

@@ -21,6 +21,10 @@ namespace {
 
 int g_threads = 1;
 int g_parity = 1;
+// Bucket order of the reconstruction's neighbour search: 0 = (cell, particle
+// id), stable; 1 = the reference's own, std::sort of the particle indices by
+// Morton key (ns-util.h:46-79), which is not stable.
+int g_bucket_order = 0;
 
 struct V3 {
   double x, y, z;
@@ -383,6 +387,7 @@ extern "C" {
 
 void ora_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
 void ora_set_parity_mode(int on) { g_parity = on; }
+void ora_set_bucket_order(int mode) { g_bucket_order = mode; }
 int ora_get_threads(void) { return g_threads; }
 
 double ora_cubic_weight(double h, double dx, double dy, double dz) {
@@ -537,9 +542,32 @@ void ora_reconstruct(int64_t n, const double* pos, int nx, int ny, int nz, doubl
     key[i] = iz + (int64_t)iy * nz + (int64_t)ix * ny * nz;
   }
   std::vector<int64_t> order((size_t)n);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+  if (g_bucket_order == 1) {
+    // ParticleNeighbourSearcher::update (ns-util.h:36-79): int indices sorted by
+    // std::sort on the Morton key of the (clamped) cell.  The permutation inside
+    // a bucket, and so the particle that forNeighbours skips, is the one this
+    // unstable sort leaves; the buckets themselves are the same either way.
+    auto morton10 = [](int x) {
+      x = (x | (x << 16)) & 0x030000FF;
+      x = (x | (x << 8)) & 0x0300F00F;
+      x = (x | (x << 4)) & 0x030C30C3;
+      x = (x | (x << 2)) & 0x09249249;
+      return x;
+    };
+    std::vector<int> mkey((size_t)n), idx((size_t)n);
+    for (int64_t i = 0; i < n; i++) {
+      const int64_t c = key[i];
+      const int iz = (int)(c % nz), iy = (int)((c / nz) % ny), ix = (int)(c / ((int64_t)ny * nz));
+      mkey[i] = morton10(ix) | (morton10(iy) << 1) | (morton10(iz) << 2);
+      idx[i] = (int)i;
+    }
+    std::sort(idx.begin(), idx.end(), [&](int a, int b) { return mkey[a] < mkey[b]; });
+    for (int64_t i = 0; i < n; i++) order[i] = idx[i];
+  } else {
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+  }
   std::vector<int64_t> beg((size_t)ncell, -1), end((size_t)ncell, -1);
   for (int64_t i = 0; i < n; i++) {
     int64_t c = key[order[i]];

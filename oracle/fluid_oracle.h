@@ -5,10 +5,13 @@
  * path in simcraft_b200 and the timed CPU baseline of bench.py; nothing in the
  * product links or calls it.  Every function follows the reference CPU code
  * loop for loop (file:line cited beside each declaration, paths relative to the
- * SimCraft tree).  The reference itself cannot be compiled (glm/TBB missing,
- * Core/transfer-stencil.h absent), so parity of the transfer-kernel shape is
- * "unpinned": the cubic B-spline below is the documented policy for the
- * missing CubicKernel::weight.
+ * SimCraft tree).  It is pinned bit for bit against the reference's own
+ * sources, compiled from the reference tree by `make ref` (ref_capi.cc,
+ * oracle/_ref, tests/test_ref_pin_cpu.py) with stand-ins for the absent
+ * glm/oneTBB/spdlog headers.  Core/transfer-stencil.h is absent from the
+ * reference snapshot, so the transfer kernel's shape is the one unpinned part:
+ * the cubic B-spline below is the documented policy for the missing
+ * CubicKernel::weight, and the reference build uses the same policy.
  *
  * Layout (identical to spatify::LinearHashXYZ, Spatify/include/Spatify/hash.h:25):
  *   idx(i,j,k) = k + j*sz + i*sy*sz      (z fastest)
@@ -28,6 +31,11 @@ extern "C" {
  * parity_mode=1 keeps FLIP P2G serial (the reference's parallel P2G is racy). */
 void ora_set_threads(int n);
 void ora_set_parity_mode(int on);
+/* Bucket order of the reconstruction (ora_reconstruct, the simulator's
+ * substep): 0 (default) = (cell, particle id), the order the GPU path uses;
+ * 1 = the reference's std::sort by Morton key (ns-util.h:46-79), not stable,
+ * so the skipped last particle of a bucket is the one that sort leaves last. */
+void ora_set_bucket_order(int mode);
 int ora_get_threads(void);
 
 /* Cubic B-spline weight policy for the missing Core/transfer-stencil.h. */

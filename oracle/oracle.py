@@ -55,6 +55,7 @@ def lib():
         sig = {
             "ora_set_threads": (None, [_int]),
             "ora_set_parity_mode": (None, [_int]),
+            "ora_set_bucket_order": (None, [_int]),
             "ora_get_threads": (_int, []),
             "ora_cubic_weight": (_dbl, [_dbl, _dbl, _dbl, _dbl]),
             "ora_rebuild_surface": (_i64, [_int, _int, _int, _dp, _dp, _dp, _dp, _dp,
@@ -123,6 +124,12 @@ def _ptr_array(arrs):
 
 def set_threads(n):
     lib().ora_set_threads(int(n))
+
+
+def set_bucket_order(mode):
+    """0: (cell, particle id) bucket order (the GPU path's); 1: the reference's
+    std::sort by Morton key, as ns-util.h:46-79 runs it."""
+    lib().ora_set_bucket_order(int(mode))
 
 
 def get_threads():

@@ -73,6 +73,14 @@ int sc_context_use_own_stream(sc_context* ctx);
 void* sc_context_stream(sc_context* ctx);
 int sc_context_synchronize(sc_context* ctx);
 const char* sc_context_last_error(sc_context* ctx);
+/* Bound of the device-side spin-waits of this context's later calls (the
+ * pressure solver's wavefront mailboxes, the mesh collider's sweep barriers),
+ * in polls; polls <= 0 restores each wait's default (about 0.1-1 s).  A wait
+ * that reaches the bound gives up: the call returns SC_ERR_TIMEOUT and the
+ * handle stays usable (the solver refills its mailboxes and recomputes its
+ * pivots on the next call).  No reference counterpart: the reference waits on
+ * nothing.  Meant for failure-detection tests and watchdog settings. */
+int sc_context_set_wait_limit(sc_context* ctx, int polls);
 
 /* ---------------------------------------------------------------------------
  * Pressure solver: CgSolver3D + ModifiedIncompleteCholesky3D
@@ -169,13 +177,15 @@ int sc_pcg_apply_device(sc_pcg* pcg, const double* x, double* b);
  * and [7] are 0.  For profiling; leaves the solution untouched. */
 int sc_pcg_time_kernels(sc_pcg* pcg, int reps, double* ms_out);
 
-/* Allocation-free ModifiedIncompleteCholesky3D::precond(Adiag, Aneighbour, r,
- * active, z) (project-solver.cc:230-306) on device arrays in the reference
- * layout; an is a host array of 6 device pointers (only Left, Down and Back are
- * read).  No counterpart in the reference: it exists for callers that cannot
- * call cudaMalloc, such as engines whose device memory is owned by their own
- * pool allocator, or hot loops where cudaMalloc's device-wide synchronisation is
- * not acceptable.  It allocates nothing: its scratch is one static device array
+/* Library-only entry point, no counterpart in the reference: the same MIC(0)
+ * preconditioner z = M^-1 r as sc_pcg_precond_device, computed without
+ * allocating, on device arrays in the reference layout; an is a host array of
+ * 6 device pointers (only Left, Down and Back are read).  It exists for callers
+ * that cannot call cudaMalloc, such as engines whose device memory is owned by
+ * their own pool allocator, or hot loops where cudaMalloc's device-wide
+ * synchronisation is not acceptable.  As in sc_pcg_precond_device, entries the
+ * reference never reads (couplings to inactive cells, inactive rows) may hold
+ * any value, NaN included.  It allocates nothing: its scratch is one static device array
  * of about 4.4 MB that every GPU loading the library holds until exit, which
  * limits the grid to 32768 tiled cells (ceil(nx/32)*32 * ceil(ny/8)*8 * nz,
  * e.g. 32^3) in at most 8 column tiles; larger grids return SC_ERR_INVALID with
@@ -453,6 +463,8 @@ int sc_diff_get_density(sc_diff* d, double* rho, int device_pointers);
 int sc_diff_get_particles(sc_diff* d, double* pos, double* vel, int device_pointers);
 /* pressure-solve iterations of the last substep run */
 int sc_diff_last_pcg_iterations(sc_diff* d);
+/* pressure of the last substep run (nx*ny*nz doubles, reference layout) */
+int sc_diff_get_pressure(sc_diff* d, double* p, int device_pointers);
 
 #ifdef __cplusplus
 }

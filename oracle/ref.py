@@ -16,9 +16,11 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "_ref", "libsimcraft_ref.so")
+# the timing build: the same sources with oneTBB's loops on OpenMP threads
+_LIB_PAR = os.path.join(_HERE, "_ref", "libsimcraft_ref_par.so")
 _SRC = ("ref_capi.cc", "refshim/prelude.h", "refshim/glm/glm.hpp", "refshim/tbb/tbb.h",
         "refshim/spdlog/spdlog.h", "refshim/Core/transfer-stencil.h")
-_lib = None
+_libs = {}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _u8p = ctypes.POINTER(ctypes.c_uint8)
@@ -37,8 +39,8 @@ def reference_tree():
 def build(force=False):
     """Build the library when the reference tree is present and the library is
     missing or older than its wrapper sources.  Returns the path or None."""
-    stale = not os.path.exists(_LIB) or os.path.getmtime(_LIB) < max(
-        os.path.getmtime(os.path.join(_HERE, f)) for f in _SRC)
+    newest = max(os.path.getmtime(os.path.join(_HERE, f)) for f in _SRC)
+    stale = any(not os.path.exists(p) or os.path.getmtime(p) < newest for p in (_LIB, _LIB_PAR))
     if (force or stale) and os.path.isdir(os.path.join(reference_tree(), "FluidSim")):
         subprocess.check_call(["make", "-s", "-C", _HERE, "ref", "REF=" + reference_tree()])
     return _LIB if os.path.exists(_LIB) else None
@@ -51,17 +53,20 @@ def available():
         return False
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if build() is None:
-            raise RuntimeError("oracle/_ref/libsimcraft_ref.so is not built and the reference tree is absent")
-        L = ctypes.CDLL(_LIB)
+def lib(parallel=False):
+    """The parity build (serial), or with parallel=True the timing build."""
+    if parallel not in _libs:
+        path = _LIB_PAR if parallel else _LIB
+        if build() is None or not os.path.exists(path):
+            raise RuntimeError(path + " is not built and the reference tree is absent")
+        L = ctypes.CDLL(path)
         sig = {
             "ref_apply_matrix": (None, [_int, _int, _int, _dp, ctypes.POINTER(_dp), _dp, _u8p, _dp]),
             "ref_mic_precond": (None, [_int, _int, _int, _dp, ctypes.POINTER(_dp), _dp, _u8p, _dp, _dbl, _dbl,
                                        _dp, _dp]),
-            "ref_cg_solve": (_dbl, [_int, _int, _int, _dp, ctypes.POINTER(_dp), _dp, _u8p, _dp, _dbl, _int]),
+            "ref_cg_solve": (_dbl, [_int, _int, _int, _dp, ctypes.POINTER(_dp), _dp, _u8p, _dp, _dbl, _int,
+                                    ctypes.POINTER(_int), _dp]),
+            "ref_set_threads": (None, [_int]),
             "ref_dot": (_dbl, [_int, _int, _int, _dp, _dp, _u8p]),
             "ref_saxpy": (None, [_int, _int, _int, _dp, _dp, _dbl, _u8p]),
             "ref_scale_and_add": (None, [_int, _int, _int, _dp, _dp, _dbl, _u8p]),
@@ -100,8 +105,8 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
-        _lib = L
-    return _lib
+        _libs[parallel] = L
+    return _libs[parallel]
 
 
 def _p(a):
@@ -140,12 +145,22 @@ def mic_precond(adiag, an, r, active, tau=0.97, sigma=0.25, return_scratch=False
     return (z, E, q) if return_scratch else z
 
 
-def cg_solve(adiag, an, rhs, active, tol=1e-6, max_iter=300):
+def cg_solve(adiag, an, rhs, active, tol=1e-6, max_iter=300, parallel=False, threads=None, stats=None):
     """CgSolver3D::solve: the reference's stopping test (absolute L-inf < tol,
-    at most max_iter - 1 iterations).  Returns (pressure, residual)."""
+    at most max_iter - 1 iterations).  Returns (pressure, residual); `stats`
+    (a dict) receives the reference's iteration count and the solve's wall ms.
+    parallel=True runs the timing build on `threads` OpenMP threads."""
     pg = np.zeros_like(adiag)
     an = [np.ascontiguousarray(a) for a in an]
-    res = lib().ref_cg_solve(*adiag.shape, _p(adiag), _ptr_array(an), _p(rhs), _p(active), _p(pg), tol, max_iter)
+    L = lib(parallel)
+    if parallel:
+        L.ref_set_threads(int(threads or os.cpu_count() or 1))
+    it, ms = _int(0), _dbl(0.0)
+    res = L.ref_cg_solve(*adiag.shape, _p(adiag), _ptr_array(an), _p(rhs), _p(active), _p(pg), tol, max_iter,
+                         ctypes.byref(it), ctypes.byref(ms))
+    if stats is not None:
+        stats["iterations"] = it.value
+        stats["ms"] = ms.value
     return pg, res
 
 

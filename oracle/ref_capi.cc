@@ -21,6 +21,8 @@
  */
 #include "refshim/prelude.h"
 
+#include <chrono>
+
 #define private public
 #define protected public
 #include <FluidSim/src/cpu/project-solver.cc>
@@ -129,9 +131,13 @@ void ref_mic_precond(int nx, int ny, int nz, const double* adiag, const double* 
 
 /* CgSolver3D::solve (project-solver.cc:308-346) with the MIC(0) preconditioner;
  * tolerance and max_iterations replace the defaults of project-solver.h:129-130.
- * Returns the reference's residual (absolute L-inf). */
+ * Returns the reference's residual (absolute L-inf); *iters (may be NULL)
+ * receives the count the reference prints ("PCG iterations: N", :344), 0 when
+ * it converged before iterating.  ms (may be NULL) receives the wall time of
+ * the solve call alone. */
 double ref_cg_solve(int nx, int ny, int nz, const double* adiag, const double* const* an,
-                    const double* rhs, const uint8_t* active, double* pg, double tol, int max_iter) {
+                    const double* rhs, const uint8_t* active, double* pg, double tol, int max_iter,
+                    int* iters, double* ms) {
   System S(nx, ny, nz, adiag, an, active);
   Array3D<Real> RHS(nx, ny, nz), P(nx, ny, nz);
   put(RHS, rhs);
@@ -140,9 +146,30 @@ double ref_cg_solve(int nx, int ny, int nz, const double* adiag, const double* c
   cg.setPreconditioner(PreconditionerMethod::ModifiedIncompleteCholesky);
   cg.tolerance = tol;
   cg.max_iterations = max_iter;
+  std::ostringstream sink;
+  std::streambuf* o = std::cout.rdbuf(sink.rdbuf());
+  const auto t0 = std::chrono::steady_clock::now();
   const Real res = cg.solve(S.adiag, S.an, RHS, S.active, P);
+  const auto t1 = std::chrono::steady_clock::now();
+  std::cout.rdbuf(o);
+  if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  if (iters) {
+    *iters = 0;
+    const std::string out = sink.str(), key = "PCG iterations: ";
+    const size_t at = out.rfind(key);
+    if (at != std::string::npos) *iters = std::atoi(out.c_str() + at + key.size());
+  }
   get(P, pg);
   return res;
+}
+
+/* Threads of the timing build (SIMCRAFT_REF_PARALLEL); the parity build is serial. */
+void ref_set_threads(int n) {
+#ifdef SIMCRAFT_REF_PARALLEL
+  omp_set_num_threads(n < 1 ? 1 : n);
+#else
+  (void)n;
+#endif
 }
 
 /* Masked BLAS-1 (util.cc:380-410, util.h:56-63) on an nx x ny x nz array. */

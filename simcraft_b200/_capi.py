@@ -77,6 +77,7 @@ SIGNATURES = {
     "sc_context_stream": (c_void_p, [c_void_p]),
     "sc_context_synchronize": (c_int, [c_void_p]),
     "sc_context_last_error": (c_char_p, [c_void_p]),
+    "sc_context_set_wait_limit": (c_int, [c_void_p, c_int]),
     "sc_pcg_default_options": (None, [P(sc_pcg_options)]),
     "sc_pcg_create": (c_int, [c_void_p, c_int, c_int, c_int, P(sc_pcg_options), P(c_void_p)]),
     "sc_pcg_destroy": (None, [c_void_p]),
@@ -142,6 +143,7 @@ SIGNATURES = {
     "sc_diff_get_density": (c_int, [c_void_p, c_void_p, c_int]),
     "sc_diff_get_particles": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "sc_diff_last_pcg_iterations": (c_int, [c_void_p]),
+    "sc_diff_get_pressure": (c_int, [c_void_p, c_void_p, c_int]),
 }
 
 _lib = None

@@ -170,6 +170,12 @@ int sc_context_synchronize(sc_context* ctx) {
   return SC_OK;
 }
 
+int sc_context_set_wait_limit(sc_context* ctx, int polls) {
+  if (!ctx) return SC_ERR_INVALID;
+  ctx->c.wait_limit = polls > 0 ? polls : 0;
+  return SC_OK;
+}
+
 const char* sc_context_last_error(sc_context* ctx) {
   return ctx ? ctx->c.last_error.c_str() : "no context";
 }
@@ -494,7 +500,7 @@ static int mesh_sdf(sc_context* ctx, int nx, int ny, int nz, double h, const dou
   const int64_t N = (int64_t)nx * ny * nz;
   sc::MeshSdfArgs a{nx, ny, nz, h, origin ? origin[0] : 0.0, origin ? origin[1] : 0.0,
                     origin ? origin[2] : 0.0, vertices, nvertices, triangles, ntriangles, exact_band,
-                    flags == SC_MESH_EXACT_DISTANCE};
+                    flags == SC_MESH_EXACT_DISTANCE, ctx->c.wait_limit};
   double* d_sdf = sdf;
   int32_t* d_cl = closest;
   void *dv = nullptr, *dt = nullptr;
@@ -996,6 +1002,12 @@ int sc_diff_get_particles(sc_diff* d, double* pos, double* vel, int device_point
   if (!d) return SC_ERR_INVALID;
   cudaSetDevice(d->ctx->c.device);
   return df_rc(d, d->sim->get_particles(pos, vel, device_pointers != 0));
+}
+
+int sc_diff_get_pressure(sc_diff* d, double* p, int device_pointers) {
+  if (!d || !p) return SC_ERR_INVALID;
+  cudaSetDevice(d->ctx->c.device);
+  return df_rc(d, d->sim->get_pressure(p, device_pointers != 0));
 }
 
 int sc_diff_last_pcg_iterations(sc_diff* d) { return d ? d->sim->last_pcg_iterations() : 0; }

@@ -1050,6 +1050,11 @@ int DiffSim::get_density(double* rho, bool device) {
   return err("get_density");
 }
 
+int DiffSim::get_pressure(double* p, bool device) {
+  if (!have_forward_) return ctx_->set_error(-1, "get_pressure needs a forward first");
+  return pcg_->download_pressure(p, device);
+}
+
 int DiffSim::get_particles(double* pos, double* vel, bool device) {
   cudaStream_t st = ctx_->stream;
   const int64_t n = n_;

@@ -56,6 +56,8 @@ class DiffSim {
   int backward(double* const gU[3]);
   int get_density(double* rho, bool device);
   int get_particles(double* pos, double* vel, bool device);
+  // pressure of the last pressure solve run (reference layout)
+  int get_pressure(double* p, bool device);
   int64_t num_particles() const { return n_; }
   int last_pcg_iterations() const { return last_iters_; }
   int64_t launches() const { return launches_; }

@@ -285,8 +285,8 @@ __global__ void __launch_bounds__(kMeshThreads)
 // Grid-wide barrier of a cooperative launch (all blocks co-resident): arrival
 // by a release add, the last arriver publishes the next generation with a
 // release add, the others poll it with acquire loads.  The wait is bounded:
-// after kSweepSpin polls the block raises *err and stops waiting, and every
-// later barrier returns at once.
+// after `limit` polls (kSweepSpin by default) the block raises *err and stops
+// waiting, and every later barrier returns at once.
 constexpr int kSweepSpin = 1 << 24;
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
@@ -298,7 +298,7 @@ __device__ __forceinline__ unsigned add_acq_rel(unsigned* p, unsigned v) {
   asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
   return old;
 }
-__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, int* err) {
+__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, int* err, int limit) {
   __syncthreads();
   if (threadIdx.x == 0 && !*(volatile int*)err) {
     const unsigned g0 = ld_acquire(gen);
@@ -308,7 +308,7 @@ __device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, int
     } else {
       int spins = 0;
       while (ld_acquire(gen) == g0) {
-        if (++spins > kSweepSpin || *(volatile int*)err) {
+        if (++spins > limit || *(volatile int*)err) {
           atomicOr(err, 1);
           break;
         }
@@ -321,7 +321,7 @@ __device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, int
 // All 16 passes in one cooperative launch, a grid barrier after every plane.
 __global__ void __launch_bounds__(kMeshThreads)
     k_mesh_sweep_all(MeshGeo g, const double* P, double* sdf, int* closest, unsigned* count, unsigned* gen,
-                     int* err) {
+                     int* err, int limit) {
   const int planes = g.nx + g.ny + g.nz - 2;
   const int64_t cols = (int64_t)g.nx * g.ny;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(kMeshThreads)
       for (int64_t q = (int64_t)xlo * g.ny + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
            q < (int64_t)(xhi + 1) * g.ny && q < cols; q += stride)
         sweep_cell(g, P, sdf, closest, q, p, dx, dy, dz);
-      grid_barrier(count, gen, err);
+      grid_barrier(count, gen, err, limit);
       if (*(volatile int*)err) return;
     }
   }
@@ -447,7 +447,9 @@ int mesh_to_sdf(cudaStream_t st, const MeshSdfArgs& a, double* sdf, int32_t* clo
       cudaMemsetAsync(flag, 0, 4 * sizeof(int), st);
       const double* P = packed;
       unsigned* gen = bar + 1;
-      void* args[] = {(void*)&g, (void*)&P, (void*)&sdf, (void*)&cl, (void*)&bar, (void*)&gen, (void*)&flag};
+      int limit = a.wait_limit > 0 ? a.wait_limit : kSweepSpin;
+      void* args[] = {(void*)&g, (void*)&P, (void*)&sdf, (void*)&cl, (void*)&bar, (void*)&gen, (void*)&flag,
+                      (void*)&limit};
       coop = cudaLaunchCooperativeKernel((const void*)k_mesh_sweep_all, grid, kMeshThreads, args, 0, st) ==
              cudaSuccess;
       if (!coop) cudaGetLastError();

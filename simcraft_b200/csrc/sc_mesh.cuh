@@ -19,6 +19,7 @@ struct MeshSdfArgs {
   int64_t ntriangles;
   int exact_band;           // cells around each triangle's box with exact distances (3 in setCollider)
   int exact_distance;       // 0: the reference's point-triangle arithmetic; 1: true distances
+  int wait_limit;           // polls before a sweep barrier wait gives up (0: the default)
 };
 
 // Device scratch mesh_to_sdf needs (crossing counts, closest triangles when the

@@ -52,7 +52,7 @@ constexpr int wave_stages() {
   constexpr int fit = (int)(180 * 1024 / ((size_t)Tiled::TY * NV * 32 * sizeof(T)));
   return fit < SC_WAVE_STAGE_MAX ? fit : SC_WAVE_STAGE_MAX;
 }
-constexpr int kSpinLimit = 1 << 22;  // bounded waits: ~0.1-1 s, far above any legitimate wait
+constexpr int kSpinLimit = 1 << 22;  // default bound of the waits: ~0.1-1 s, far above any legitimate wait
 
 enum { FIN_NONE = 0, FIN_INIT, FIN_SPMV, FIN_AXPY, FIN_BWD, FIN_SA, FIN_NORMS, FIN_EINIT, FIN_EAXPY, FIN_EREPLACE };
 
@@ -902,7 +902,7 @@ __device__ __forceinline__ bool wave_should_stop(const WaveArgs& a, int& spins,
   if (*s_abort) return true;
   ++spins;
   if ((spins & 63) == 0 && ld_relaxed_gpu_u32(&a.sc->err)) return true;
-  return spins > kSpinLimit;
+  return spins > a.spin_limit;
 }
 
 // Mailboxes.  The producer tile writes each boundary value it computes into
@@ -1061,9 +1061,9 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
     if (warp == TY) {
       // control warp: keeps the compute warps one step behind the rings
       auto wait_avail = [&](int s) {
-        int spins = 0;
+        long long spins = 0;
         while (((hasX && sh.availX <= s) || (hasY && sh.availY <= s)) && !sh.abort) {
-          if (++spins > kSpinLimit * 4) {
+          if (++spins > 4ll * a.spin_limit) {
             if (lane == 0) wave_abort(a, sh, NS);
             break;
           }
@@ -1303,7 +1303,20 @@ WaveArgs PcgSolver::wave_args(bool f32, int use_skip, int fin) const {
   w.tile_partials = tile_partials_;
   w.use_skip = use_skip;
   w.fin_kind = fin;
+  w.spin_limit = spin_limit();
   return w;
+}
+
+int PcgSolver::spin_limit() const { return ctx_->wait_limit > 0 ? ctx_->wait_limit : kSpinLimit; }
+
+int PcgSolver::recover_after_timeout() {
+  cudaStream_t st = ctx_->stream;
+  reset_mailboxes(false);
+  if (have_f32_) reset_mailboxes(true);
+  cudaMemsetAsync(sc_, 0, sizeof(PcgScalars), st);
+  pivots_valid_ = false;
+  cudaStreamSynchronize(st);
+  return ctx_->set_error(-6, "wavefront wait timed out");
 }
 
 PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt)
@@ -1547,6 +1560,8 @@ int PcgSolver::ensure_pivots() {
   cudaStream_t st = ctx_->stream;
   const int grid = grid_for(g_.total, ctx_->sm_count);
   WaveArgs wa = wave_args(false, 0, FIN_NONE);
+  // the pivot sweep reports a timeout through the status word: start it clean
+  cudaMemsetAsync(&sc_->err, 0, sizeof(unsigned), st);
   k_mask_system<<<grid, kThreads, 0, st>>>(g_, active_, d64_.adiag, d64_.al, d64_.ad, d64_.ab);
   // uR/uU/uF hold the pivot's diagonal products until k_upper overwrites them
   // q holds Adiag masked by the active flag until the forward sweep overwrites it
@@ -1558,6 +1573,13 @@ int PcgSolver::ensure_pivots() {
   k_upper<double><<<grid, kThreads, 0, st>>>(g_, d64_.cL, d64_.cD, d64_.cB, d64_.uR, d64_.uU,
                                               d64_.uF);
   launches_ += 4;
+  {
+    // the solve's scalars are set over the status word next: read it first
+    unsigned* herr = reinterpret_cast<unsigned*>(sc_host_ + 1);
+    cudaMemcpyAsync(herr, &sc_->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_dev_error("pivots");
+    if (*herr & DEV_ERR_TIMEOUT) return recover_after_timeout();
+  }
   if (opt_.precision == PREC_MIXED) {
     if (!have_f32_) {
       const size_t n32 = sizeof(float) * (size_t)g_.total;
@@ -1646,6 +1668,14 @@ void PcgSolver::launch_iteration(SysArrays<T>& A, bool eis) {
 // launch the same kernels directly.
 template <class T>
 int PcgSolver::ensure_graph(SysArrays<T>& A, bool eis) {
+  if (graph_limit_ != spin_limit()) {  // the wait bound is a kernel argument baked into the graphs
+    for (cudaGraphExec_t* g : {&graph64_, &graph32_, &graph32e_})
+      if (*g) {
+        cudaGraphExecDestroy(*g);
+        *g = nullptr;
+      }
+    graph_limit_ = spin_limit();
+  }
   cudaGraphExec_t& gx = graph_for<T>(eis);
   if (gx) return 0;
   cudaStream_t s = ctx_->stream;
@@ -1736,7 +1766,7 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
     st->residual = last_.res;
     st->device_flags |= last_.err;
   }
-  if (last_.err & DEV_ERR_TIMEOUT) return ctx_->set_error(-6, "wavefront wait timed out");
+  if (last_.err & DEV_ERR_TIMEOUT) return recover_after_timeout();
   return check_dev_error("pcg");
 }
 
@@ -1848,7 +1878,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
     const double rel = bnorm > 0 ? sqrt(u.rn2) / bnorm : 0.0;
     meas = abs_crit ? u.rinf : rel;
     if (!std::isfinite(rel)) return ctx_->set_error(-8, "mixed solve: non-finite residual");
-    if (u.err & DEV_ERR_TIMEOUT) return ctx_->set_error(-6, "wavefront wait timed out");
+    if (u.err & DEV_ERR_TIMEOUT) return recover_after_timeout();
     if (meas < opt_.tol) {
       status = DONE_CONVERGED;
     } else if (u.done == DONE_BREAKDOWN) {
@@ -2002,7 +2032,7 @@ int PcgSolver::precond_only(const double* r, double* z) {
   cudaMemcpyAsync(sc_host_, sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("precond");
   last_ = *sc_host_;
-  if (sc_host_->err & DEV_ERR_TIMEOUT) return ctx_->set_error(-6, "wavefront wait timed out");
+  if (sc_host_->err & DEV_ERR_TIMEOUT) return recover_after_timeout();
   return check_dev_error("precond");
 }
 
@@ -2224,11 +2254,20 @@ int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int n
   const int ntiles = g.ntiles();
   const int NS = g.nz + 31 + Tiled::TY - 1;
   const int64_t sx = (int64_t)NS * Tiled::TY, sy = (int64_t)NS * 32;
-  cudaMemsetAsync(ticket, 0, sizeof(int) * 2, st);
-  cudaMemsetAsync(scal, 0, sizeof(PcgScalars), st);
+  // An error left pending by earlier, unrelated work is not this call's.
+  cudaGetLastError();
+  auto failed = [&](cudaError_t e, const char* step) {
+    if (e == cudaSuccess) return false;
+    *msg = std::string(step) + ": " + cudaGetErrorString(e);
+    return true;
+  };
+  if (failed(cudaMemsetAsync(ticket, 0, sizeof(int) * 2, st), "clearing the tile tickets") ||
+      failed(cudaMemsetAsync(scal, 0, sizeof(PcgScalars), st), "clearing the status word"))
+    return -2;
   const int rgrid = grid_for(sy * ntiles, sm_count);
   k_mb_reset<double><<<rgrid, kThreads, 0, st>>>(sx * ntiles, mbx);
   k_mb_reset<double><<<rgrid, kThreads, 0, st>>>(sy * ntiles, mby);
+  if (failed(cudaGetLastError(), "resetting the mailboxes")) return -2;
   int2 ord[kNoAllocMaxTiles];
   int no = 0;
   for (int d = 0; d <= g.ntx + g.nty - 2; d++)
@@ -2236,8 +2275,11 @@ int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int n
       int Y = d - X;
       if (Y >= 0 && Y < g.nty) ord[no++] = make_int2(X, Y);
     }
-  cudaMemcpyAsync(order, ord, sizeof(int2) * no, cudaMemcpyHostToDevice, st);
-  // system and right-hand side into the tiled layout
+  if (failed(cudaMemcpyAsync(order, ord, sizeof(int2) * no, cudaMemcpyHostToDevice, st), "uploading the tile order"))
+    return -2;
+  // system and right-hand side into the tiled layout, then the entries the
+  // reference never reads (couplings to inactive cells, inactive rows) cleared
+  // of non-finite values, as the allocating entry point does
   const int grid = grid_for(g.total, sm_count);
   k_to_tiled<uint8_t, uint8_t><<<grid, kThreads, 0, st>>>(g, active, act, nullptr);
   k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g, adiag, t_adiag, nullptr);
@@ -2245,6 +2287,8 @@ int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int n
   k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g, an[3], t_ad, nullptr);
   k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g, an[5], t_ab, nullptr);
   k_to_tiled<double, double><<<grid, kThreads, 0, st>>>(g, r, t_r, nullptr);
+  k_mask_system<<<grid, kThreads, 0, st>>>(g, act, t_adiag, t_al, t_ad, t_ab);
+  if (failed(cudaGetLastError(), "converting the system to the tiled layout")) return -2;
   // pivots, couplings, forward and backward sweeps
   WaveArgs wa{};
   wa.g = g;
@@ -2260,6 +2304,7 @@ int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int n
   wa.tile_partials = tile_partials;
   wa.use_skip = 0;
   wa.fin_kind = FIN_NONE;
+  wa.spin_limit = kSpinLimit;
   const int wgrid = std::min(ntiles, sm_count);
   k_pivot_diag<<<grid, kThreads, 0, st>>>(g, t_adiag, t_al, t_ad, t_ab, act, tau, t_q, t_uR, t_uU,
                                           t_uF);
@@ -2271,18 +2316,13 @@ int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int n
   BwdOp<double> bo{{t_q, t_E, t_uR, t_uU, t_uF, t_r}, t_z};
   launch_wave<double, false>(wa, bo, st, wgrid);
   k_from_tiled<double, double><<<grid, kThreads, 0, st>>>(g, t_z, z);
+  if (failed(cudaGetLastError(), "launching the pivot and sweep kernels")) return -2;
   unsigned err = 0;
-  cudaMemcpyAsync(&err, &scal->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) {
-    *msg = cudaGetErrorString(e);
+  if (failed(cudaMemcpyAsync(&err, &scal->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st),
+             "reading the status word") ||
+      failed(cudaStreamSynchronize(st), "running the preconditioner") ||
+      failed(cudaGetLastError(), "running the preconditioner"))
     return -2;
-  }
-  e = cudaGetLastError();
-  if (e != cudaSuccess) {
-    *msg = cudaGetErrorString(e);
-    return -2;
-  }
   if (err & DEV_ERR_TIMEOUT) {
     *msg = "wavefront wait timed out";
     return -6;

@@ -21,6 +21,10 @@ struct Context {
   int sm_count = 148;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // Bound of the device's spin-waits (wavefront mailboxes, grid barriers), in
+  // polls; 0 selects each wait's default.  A wait that reaches it gives up and
+  // the call returns SC_ERR_TIMEOUT.
+  int wait_limit = 0;
   std::string last_error;
   int set_error(int code, const std::string& msg) {
     last_error = msg;
@@ -88,6 +92,7 @@ struct WaveArgs {
   double* tile_partials;  // per tile share of the sweep's dot product
   int use_skip;
   int fin_kind;
+  int spin_limit;  // polls before a mailbox wait gives up (the control warp waits 4x as long)
 };
 
 // Wavefront scheduling state (one per sweep kernel; reset by the kernel's last CTA).
@@ -159,6 +164,12 @@ class PcgSolver {
   template <class T>
   void launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip);
   int check_dev_error(const char* where);
+  // After a wavefront wait gave up: refill the mailboxes with the sentinel
+  // (an aborted consumer leaves entries unconsumed), clear the status word and
+  // drop the pivots, so the next solve starts from a clean state.
+  int recover_after_timeout();
+  int spin_limit() const;
+  int graph_limit_ = 0;  // spin limit baked into the captured graphs
   int ensure_host_stage();
   double* hstage_ = nullptr;     // staging of the host-array entry points (N doubles)
   uint8_t* hstage_act_ = nullptr;  // and of the active flags (N bytes)

@@ -134,6 +134,12 @@ class DiffFlip:
     def last_pcg_iterations(self):
         return lib().sc_diff_last_pcg_iterations(self.handle)
 
+    def pressure(self):
+        """Pressure of the last substep of the last forward (reference layout)."""
+        p = np.zeros(self.dims)
+        check("sc_diff_get_pressure", lib().sc_diff_get_pressure(self.handle, _ptr(p), 0), self.ctx.handle)
+        return p
+
 
 class FlipLoss(torch.autograd.Function):
     """loss = FlipLoss.apply(param, sim): param is a (3, nx, ny, nz) CUDA tensor;

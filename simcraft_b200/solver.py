@@ -50,6 +50,11 @@ class Context:
     def stream(self):
         return lib().sc_context_stream(self.handle)
 
+    def set_wait_limit(self, polls):
+        """Bound the device spin-waits of later calls to `polls` polls (<= 0: the
+        defaults); a wait that reaches it makes the call fail with SC_ERR_TIMEOUT."""
+        check("sc_context_set_wait_limit", lib().sc_context_set_wait_limit(self.handle, int(polls)), self.handle)
+
     def __del__(self):
         if getattr(self, "handle", None) and _capi._lib is not None:
             _capi._lib.sc_context_destroy(self.handle)

@@ -1,6 +1,7 @@
-"""bench.py's reference arm on the CPU (it runs the oracle of the reference path,
-no GPU): one JSON line on stdout with the keys and types the benchmark line
-carries, at a small grid so the test takes seconds."""
+"""bench.py's reference arm on the CPU (it runs the reference's own CPU solver,
+or the oracle restatement where that library is absent; no GPU): one JSON line
+on stdout with the keys and types the benchmark line carries, at a small grid
+so the test takes seconds."""
 import json
 import os
 import subprocess
@@ -28,6 +29,10 @@ def test_reference_arm_prints_one_contract_line():
     assert d["dtype"] == "f64" and "synthetic" in d["data"]
     assert isinstance(d["config"], dict) and "workload" in d["config"] and d["config"]["grid"] == [16, 16, 16]
     cb = d["cpu_baseline"]
-    assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+
+    kind = "reference" if ref.available() else "port"
+    assert cb["value"] == d["value"] and cb["kind"] == kind and cb["cores"] >= 1 and cb["sample"]
     e = d["e2e"]
     assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0

@@ -121,3 +121,61 @@ def test_control_problem_64(torch_mod):
     num = sum(float(((a - b) ** 2).sum()) for a, b in zip(g64, g32))
     den = sum(float((a ** 2).sum()) for a in g64)
     assert (num / den) ** 0.5 < 1e-2
+
+
+def _density_np(pos, dims, h):
+    """rho_c = sum_p N(x_p - x_c) on the cell centres over the stencil
+    nearest + {-1..2}, N the tensor-product cubic B-spline (the loss's density)."""
+    def bs(r):
+        r = np.abs(r)
+        return np.where(r < 1.0, 2.0 / 3.0 - r * r + 0.5 * r ** 3, np.where(r < 2.0, (2.0 - r) ** 3 / 6.0, 0.0))
+    rho = np.zeros(dims)
+    base = np.floor(pos / h).astype(np.int64) - 1
+    for a in range(4):
+        for b in range(4):
+            for c in range(4):
+                idx = base + np.array([a, b, c])
+                w = (bs(pos[:, 0] / h - (idx[:, 0] + 0.5)) * bs(pos[:, 1] / h - (idx[:, 1] + 0.5))
+                     * bs(pos[:, 2] / h - (idx[:, 2] + 0.5)))
+                ok = np.all((idx >= 0) & (idx < np.array(dims)), axis=1)
+                np.add.at(rho, (idx[ok, 0], idx[ok, 1], idx[ok, 2]), w[ok])
+    return rho
+
+
+@pytest.mark.parametrize("n,advection", [(16, "flip"), (20, "pic")])
+def test_forward_matches_oracle_simulator(oracle, torch_mod, n, advection):
+    """The differentiable step's forward (FP64, no tape) is the simulator's
+    substep with a fixed dt: against the oracle's simulator (fluid-simulator.cc:
+    140-182) given the velocities the oracle samples from the same face field U
+    (sampleVelocity, util.cc:40-85), with the same MIC(0) tau = 0 and relative
+    1e-10 pressure solves: pressure within 1e-5 relative L2 and positions within
+    1e-4 h after each of 4 substeps, and the density loss within 1e-10 relative."""
+    torch = torch_mod
+    from simcraft_b200.diff import DiffFlip, control_scene, faces_from_cells
+    pos, param, target, h = control_scene(n)
+    dims, dt = (n, n, n), 1.0 / 120
+    U = faces_from_cells(torch.from_numpy(param).cuda())
+    vel0 = oracle.sample_velocity(pos, dims, h, *[u.cpu().numpy() for u in U])
+    flip = advection == "flip"
+    cfg = oracle.default_config(n, n, n, h, flip=int(flip), flip_alpha=0.95, pcg_tol=1e-10, pcg_max_iter=2000,
+                                pcg_criterion=1, mic_tau=0.0)
+    ref = oracle.Sim(**cfg)
+    ref.set_particles(pos, vel0)
+    loss = None
+    for k in range(1, 5):
+        ref.substep(dt)
+        sim = DiffFlip(dims, h, dt, k, flip_alpha=0.95, advection=advection, checkpoint_every=2)
+        sim.set_particles(pos)
+        sim.set_target(target)
+        loss = sim.forward(U, tape="none")
+        p_ref = ref.pressure()
+        assert np.abs(p_ref).max() > 0
+        perr = np.linalg.norm(sim.pressure() - p_ref) / np.linalg.norm(p_ref)
+        x, v = sim.particles()
+        x_ref, v_ref = ref.particles()
+        xerr = np.abs(x - x_ref).max() / h
+        assert perr <= 1e-5 and xerr <= 1e-4, (k, perr, xerr)
+    rho_ref = _density_np(ref.particles()[0], dims, h)
+    np.testing.assert_allclose(sim.density(), rho_ref, rtol=0, atol=1e-9)
+    loss_ref = float(((rho_ref - target) ** 2).sum())
+    assert abs(loss - loss_ref) <= 1e-10 * loss_ref, (loss, loss_ref)

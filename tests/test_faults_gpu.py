@@ -154,3 +154,78 @@ def test_surface_with_nan_and_inf_samples(oracle, gpu, path):
     np.testing.assert_array_equal(V, ref[0])  # NaN where the oracle has NaN
     np.testing.assert_array_equal(N, ref[1])
     np.testing.assert_array_equal(I.astype(np.int64), ref[2].astype(np.int64))
+
+
+SC_ERR_TIMEOUT = -6
+
+
+def test_wavefront_wait_timeout_is_reported_and_the_solver_recovers(oracle, gpu):
+    """The bounded waits of the wavefront sweeps: with the bound cut to one poll
+    (sc_context_set_wait_limit), a consumer tile gives up on a mailbox its
+    producer has not written yet; the solve returns SC_ERR_TIMEOUT in both
+    precisions and through the preconditioner entry point, nothing faults, and
+    with the default bound back the same handles solve again, bit for bit as a
+    fresh solver does."""
+    import torch
+    from simcraft_b200._capi import CapiError
+    from simcraft_b200.solver import CgSolver3D, Context, CRIT_REL_L2, PREC_FP64, PREC_MIXED
+
+    dims = (64, 32, 48)  # 2 x 4 column tiles: every sweep hands values between tiles
+    S = poisson_system(oracle, 0, dims=dims, seed=6)
+    ctx = Context(0)
+    fresh = {}
+    for prec in (PREC_FP64, PREC_MIXED):
+        f = CgSolver3D(*dims, tol=1e-8, max_iter=500, criterion=CRIT_REL_L2, precision=prec)
+        fresh[prec] = np.zeros(dims)
+        f.solve(S["adiag"], S["an"], S["rhs"], S["active"], fresh[prec])
+    for prec in (PREC_FP64, PREC_MIXED):
+        s = CgSolver3D(*dims, context=ctx, tol=1e-8, max_iter=500, criterion=CRIT_REL_L2, precision=prec)
+        pg = np.zeros(dims)
+        s.solve(S["adiag"], S["an"], S["rhs"], S["active"], pg)  # graphs captured with the default bound
+        for _ in range(2):
+            ctx.set_wait_limit(1)
+            with pytest.raises(CapiError) as ei:
+                s.solve(S["adiag"], S["an"], S["rhs"], S["active"], np.zeros(dims))
+            assert ei.value.status == SC_ERR_TIMEOUT
+            ctx.set_wait_limit(0)
+            pg = np.zeros(dims)
+            s.solve(S["adiag"], S["an"], S["rhs"], S["active"], pg)
+            assert s.last_stats["status"] == SC_DONE_CONVERGED
+            np.testing.assert_array_equal(pg, fresh[prec])
+    # the preconditioner entry point
+    s = CgSolver3D(*dims, context=ctx)
+    s.upload(S["adiag"], S["an"], S["rhs"], S["active"])
+    x = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, dims)).cuda()
+    z0 = torch.zeros(dims, dtype=torch.float64, device="cuda")
+    s.precond(x, z0)
+    ctx.set_wait_limit(1)
+    with pytest.raises(CapiError) as ei:
+        s.precond(x, torch.zeros_like(z0))
+    assert ei.value.status == SC_ERR_TIMEOUT
+    ctx.set_wait_limit(0)
+    z1 = torch.zeros_like(z0)
+    s.precond(x, z1)
+    assert torch.equal(z0, z1)
+
+
+def test_mesh_sweep_barrier_timeout_is_reported_and_recovers(gpu):
+    """The bounded grid barrier of the collider's fast-sweeping launch: with the
+    bound cut to one poll a block gives up waiting for the others; the call
+    returns SC_ERR_TIMEOUT, and with the default bound back the same context
+    builds the SDF bit for bit as before."""
+    from simcraft_b200 import scenes
+    from simcraft_b200._capi import CapiError
+    from simcraft_b200.mesh import manifold_to_sdf
+    from simcraft_b200.solver import Context
+
+    ctx = Context(0)
+    v, t = scenes.icosphere(3, 0.3, (0.5, 0.5, 0.5))
+    n = 64
+    ref = manifold_to_sdf(v, t, (n, n, n), 1.0 / n, context=ctx)
+    ctx.set_wait_limit(1)
+    with pytest.raises(CapiError) as ei:
+        manifold_to_sdf(v, t, (n, n, n), 1.0 / n, context=ctx)
+    assert ei.value.status == SC_ERR_TIMEOUT
+    ctx.set_wait_limit(0)
+    again = manifold_to_sdf(v, t, (n, n, n), 1.0 / n, context=ctx)
+    np.testing.assert_array_equal(again, ref)

@@ -263,3 +263,41 @@ def test_simulator_edge_cases(oracle, torch_mod):
     sim.step(1.0 / 120)
     x1, _ = sim.particles()
     assert np.abs(x1 - pos[perm]).max() < 0.5 * h
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_dam_break_64_ten_frames(oracle, torch_mod, precision):
+    """The largest stand-in for the 256^3 dam break that the CPU oracle runs in
+    seconds: 64^3, block x < 0.5, y < 0.5 (262,144 particles), FLIP 0.95, frames
+    of 1/240 (dt/h = 0.267, the regime where the reference's MIC(0) converges),
+    10 frames.  f64: the FP64 solver, pressure within 1e-5 relative L2 after
+    every frame and positions within 1e-4 h after 10 frames.  f32: FP32
+    particles and grids with the mixed solver (FP32 Eisenstat CG, FP64
+    residual replacement) to 1e-8; single-precision rounding of positions and
+    grids bounds the agreement: pressure within 1e-3 relative L2 after every
+    frame, positions within 1e-2 h after 10 frames."""
+    from simcraft_b200.fluid import FluidSimulator
+    from simcraft_b200.solver import CRIT_REL_L2, PREC_FP64, PREC_MIXED
+    n = 64
+    pos, vel, h = scenes.dam_break(n, seed=1)
+    ocfg = oracle.default_config(n, n, n, h, flip=1, flip_alpha=0.95, pcg_tol=1e-8, pcg_max_iter=800,
+                                 pcg_criterion=CRIT_REL_L2)
+    ref = oracle.Sim(**ocfg)
+    ref.set_particles(pos, vel)
+    f32 = precision == "f32"
+    sim = FluidSimulator(len(pos), (1.0, 1.0, 1.0), (n, n, n), precision=precision, flip_alpha=0.95,
+                         pcg_tol=1e-8, pcg_max_iter=800, pcg_criterion=CRIT_REL_L2,
+                         pcg_precision=PREC_MIXED if f32 else PREC_FP64)
+    sim.set_initial_fluid(pos, vel)
+    errs = []
+    for step in range(10):
+        assert ref.step(1.0 / 240) == 1
+        st = sim.step(1.0 / 240)
+        assert st["substeps"] == 1 and st["pcg_residual"] < 1e-8
+        errs.append(_rel(sim.pressure(), ref.pressure()))
+        assert errs[-1] <= (1e-3 if f32 else 1e-5), (step, errs)
+    x_ref, _ = ref.particles()
+    x, _ = sim.particles()
+    dx = np.abs(x - x_ref).max() / h
+    assert dx <= (1e-2 if f32 else 1e-4), (dx, errs)
+    assert np.abs(x_ref - pos).max() > 0.5 * h  # the block has started to fall

@@ -1075,6 +1075,12 @@ struct ora_sim {
   int last_iters = 0;
   double last_residual = 0.0;
   int64_t fsize[3];
+  // fluid-SDF tape (checker of the differentiable step, not part of the
+  // reference): 1 records the fluid SDF each substep uses, 2 uses the recorded
+  // ones in their order instead of reconstructing
+  int sdf_tape = 0;
+  size_t sdf_tape_pos = 0;
+  std::vector<std::vector<double>> sdf_tape_data;
 };
 
 // smoothFluidSurface (fluid-simulator.cc:39-74): min-preserving neighbour
@@ -1136,6 +1142,21 @@ ora_sim* ora_sim_create(const ora_sim_config* cfg) {
   sim_alloc(s);
   return s;
 }
+void ora_sim_sdf_tape(ora_sim* s, int mode) {
+  s->sdf_tape = mode;
+  s->sdf_tape_pos = 0;
+  if (mode == 1) s->sdf_tape_data.clear();
+}
+int ora_sim_sdf_tape_get(ora_sim* s, int64_t k, double* sdf) {
+  if (k < 0 || k >= (int64_t)s->sdf_tape_data.size()) return -1;
+  std::copy(s->sdf_tape_data[k].begin(), s->sdf_tape_data[k].end(), sdf);
+  return 0;
+}
+int ora_sim_sdf_tape_put(ora_sim* s, const double* sdf) {
+  s->sdf_tape_data.emplace_back(sdf, sdf + (int64_t)s->c.nx * s->c.ny * s->c.nz);
+  return 0;
+}
+
 void ora_sim_destroy(ora_sim* s) { delete s; }
 void ora_sim_set_particles(ora_sim* s, int64_t n, const double* pos, const double* vel) {
   s->n = n;
@@ -1184,6 +1205,12 @@ void ora_sim_substep(ora_sim* s, double dt) {  // fluid-simulator.cc:140-182
   // advect on the just-cleared grids (:143)
   ora_advect(s->n, s->pos.data(), s->vel.data(), nx, ny, nz, h, U, Vv, W, s->collider.data(),
              dt);
+  const bool replay = s->sdf_tape == 2 && s->sdf_tape_pos < s->sdf_tape_data.size();
+  if (replay) {
+    std::copy(s->sdf_tape_data[s->sdf_tape_pos].begin(), s->sdf_tape_data[s->sdf_tape_pos].end(),
+              s->sdf[s->scur].begin());
+    s->sdf_tape_pos++;
+  } else {
   // reconstruct into the current primary SDF (:146-148)
   ora_reconstruct(s->n, s->pos.data(), nx, ny, nz, h, c.recon_factor * h,
                   s->sdf[s->scur].data(), s->sdfv[s->svcur].data());
@@ -1221,6 +1248,8 @@ void ora_sim_substep(ora_sim* s, double dt) {  // fluid-simulator.cc:140-182
     s->svcur = 1 - s->svcur;
   }
   sim_smooth(s, c.smooth_iters);
+  if (s->sdf_tape == 1) s->sdf_tape_data.push_back(s->sdf[s->scur]);
+  }
   const double* fluid = s->sdf[s->scur].data();
   // P2G (:155-156)
   U = s->g[0][s->gcur[0]].data();

@@ -149,6 +149,15 @@ void ora_manifold_to_sdf(int nx, int ny, int nz, double h, double ox, double oy,
                          const double* vert, const int* tri, int64_t ntri, int exact_band,
                          int exact_distance, double* sdf, int* closest, int* icnt);
 double ora_sim_last_residual(const ora_sim* s);
+/* Fluid-SDF tape of the simulator (for checking the differentiable step, which
+ * holds the fluid SDF of its recorded run fixed; the reference has no such
+ * mode): mode 1 clears the tape and records the fluid SDF each later substep
+ * uses; mode 2 makes the later substeps use the taped SDFs in order, skipping
+ * reconstruction, SDF extrapolation and smoothing; 0 turns the tape off.
+ * _get copies taped SDF k out, _put appends one. */
+void ora_sim_sdf_tape(ora_sim* s, int mode);
+int ora_sim_sdf_tape_get(ora_sim* s, int64_t k, double* sdf);
+int ora_sim_sdf_tape_put(ora_sim* s, const double* sdf);
 /* rebuildSurface (FluidSim/src/cpu/rebuild-surface.cc:686-741): marching
  * cubes over the cell-centred SDF (reference layout; sample (x, y, z) at
  * ((x + 0.5) spacing[0] + origin[0], ...)).  Returns the vertex count and

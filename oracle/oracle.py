@@ -100,6 +100,9 @@ def lib():
             "ora_sim_get_system": (None, [ctypes.c_void_p, _dp, ctypes.POINTER(_dp), _dp, _u8p]),
             "ora_sim_last_iters": (_int, [ctypes.c_void_p]),
             "ora_sim_last_residual": (_dbl, [ctypes.c_void_p]),
+            "ora_sim_sdf_tape": (None, [ctypes.c_void_p, _int]),
+            "ora_sim_sdf_tape_get": (_int, [ctypes.c_void_p, _i64, _dp]),
+            "ora_sim_sdf_tape_put": (_int, [ctypes.c_void_p, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -399,3 +402,24 @@ class Sim:
 
     def last_residual(self):
         return lib().ora_sim_last_residual(self._h)
+
+    def sdf_tape(self, mode, sdfs=None):
+        """Fluid-SDF tape: 1 records the SDF each later substep uses, 2 replays
+        the taped ones (or `sdfs`, a list of arrays, when given) instead of
+        reconstructing, 0 turns it off."""
+        lib().ora_sim_sdf_tape(self._h, 1 if sdfs is not None else int(mode))
+        if sdfs is not None:
+            for a in sdfs:
+                lib().ora_sim_sdf_tape_put(self._h, _p(np.ascontiguousarray(a, np.float64)))
+            lib().ora_sim_sdf_tape(self._h, 2)
+            # mode 2 rewinds the tape without clearing it
+
+    def taped_sdfs(self):
+        out = []
+        k = 0
+        while True:
+            a = np.zeros(self.dims)
+            if lib().ora_sim_sdf_tape_get(self._h, k, _p(a)) != 0:
+                return out
+            out.append(a)
+            k += 1

@@ -417,6 +417,100 @@ __global__ void __launch_bounds__(kThreads)
   reduce_finalize(acc, 0.0, partials, sc, FIN_SPMV);
 }
 
+// The PCG's SpMV as a stream over the z-slots of each tile.  In the tiled
+// layout the z-neighbours of a cell are its own lane's entries at the previous
+// and next slot, and its x-neighbours are the previous and next lanes' entries
+// at those slots.  A warp that owns row ty of a tile and walks the slots in
+// order therefore holds every x and z neighbour in a three-slot register window
+// (x neighbours by shuffle); the y neighbours are the adjacent rows of the same
+// slot, read through L1 where the block's other warps have just loaded them.
+// Each array element comes from HBM once, and no cell pays for a division or a
+// tile-edge branch: only the two edge lanes of a row reach into the next tiles.
+// The sum is the same as apply_row_pcg's, term for term.  A work item is the
+// TY row warps of one tile over a run of consecutive slots.
+template <class T>
+__global__ void __launch_bounds__(kThreads, 4)
+    k_spmv_stream(Tiled g, const T* __restrict__ adiag, const T* __restrict__ al, const T* __restrict__ ad,
+                  const T* __restrict__ ab, const uint8_t* __restrict__ act, const T* __restrict__ x,
+                  T* __restrict__ y, double* partials, PcgScalars* sc, int use_skip, int chunks) {
+  if (use_skip && sc->done != DONE_RUNNING) return;
+  constexpr int TY = Tiled::TY, RS = Tiled::TY * 32;  // elements per slot of a tile
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int nz = g.nz;
+  double acc = 0.0;
+  const int items = g.ntiles() * chunks;
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    const int tile = it / chunks, ch = it - tile * chunks;
+    const int s0 = (int)((int64_t)nz * ch / chunks), s1 = (int)((int64_t)nz * (ch + 1) / chunks);
+    const int Y = tile / g.ntx, X = tile - Y * g.ntx;
+    const int xg = X * 32 + tx, yg = Y * TY + ty;
+    const bool inside = xg < g.nx && yg < g.ny;
+    const bool hx = xg > 0, px = xg < g.nx - 1, hy = yg > 0, py = yg < g.ny - 1;
+    const int64_t tb = (int64_t)tile * g.tile_elems;
+    const int64_t row = tb + ty * 32 + tx;
+    // the rows of the same slot at y - 1 and y + 1 (read only when hy / py)
+    const int64_t rym = ty > 0 ? row - 32 : tb - (int64_t)g.ntx * g.tile_elems + (TY - 1) * 32 + tx;
+    const int64_t ryp = ty < TY - 1 ? row + 32 : tb + (int64_t)g.ntx * g.tile_elems + tx;
+    // the lanes across the x edges: lane 0's x - 1 is lane 31 of tile X - 1 at
+    // slot s + 31, lane 31's x + 1 is lane 0 of tile X + 1 at slot s - 31
+    const int64_t rxm = tb - g.tile_elems + ty * 32 + 31, rxp = tb + g.tile_elems + ty * 32;
+    auto wrap = [nz](int v) { return v >= nz ? v - nz : (v < 0 ? v + nz : v); };
+    int sm = wrap(s0 - 1), sp = wrap(s0 + 1), s31 = wrap(wrap(s0 + 31 % nz)), sm31 = wrap(wrap(s0 - 31 % nz));
+    int z = wrap(s0 - tx % nz);
+    T x_m = __ldg(x + row + (int64_t)sm * RS), x_c = __ldg(x + row + (int64_t)s0 * RS),
+      x_p = __ldg(x + row + (int64_t)sp * RS);
+    T al_c = __ldg(al + row + (int64_t)s0 * RS), al_p = __ldg(al + row + (int64_t)sp * RS);
+    T ab_c = __ldg(ab + row + (int64_t)s0 * RS), ab_p = __ldg(ab + row + (int64_t)sp * RS);
+    for (int s = s0; s < s1; s++) {
+      const int64_t e = row + (int64_t)s * RS;
+      const int s2 = wrap(sp + 1);
+      // next window entries first: their latency overlaps this slot's work
+      const T x_n = __ldg(x + row + (int64_t)s2 * RS), al_n = __ldg(al + row + (int64_t)s2 * RS),
+              ab_n = __ldg(ab + row + (int64_t)s2 * RS);
+      const T d = __ldg(adiag + e), adc = __ldg(ad + e);
+      const bool a = inside && __ldg(act + e);
+      const bool hz = z > 0, pz = z < nz - 1;
+      const T ym = hy ? __ldg(x + rym + (int64_t)s * RS) : x_c;
+      const T yp = py ? __ldg(x + ryp + (int64_t)s * RS) : x_c;
+      const T adp = py ? __ldg(ad + ryp + (int64_t)s * RS) : T(0);
+      T xm = __shfl_up_sync(kFull, x_m, 1), xp = __shfl_down_sync(kFull, x_p, 1),
+        alp = __shfl_down_sync(kFull, al_p, 1);
+      if (tx == 0) xm = hx ? __ldg(x + rxm + (int64_t)s31 * RS) : x_c;
+      if (tx == 31) {
+        xp = px ? __ldg(x + rxp + (int64_t)sm31 * RS) : x_c;
+        alp = px ? __ldg(al + rxp + (int64_t)sm31 * RS) : T(0);
+      }
+      if (!hx) xm = x_c;
+      if (!px) xp = x_c;
+      const T cxm = hx ? al_c : T(0), cym = hy ? adc : T(0), czm = hz ? ab_c : T(0);
+      const T cxp = px ? alp : T(0), cyp = py ? adp : T(0), czp = pz ? ab_p : T(0);
+      T t = d * x_c;
+      t += cxm * xm;
+      t += cym * ym;
+      t += czm * (hz ? x_m : x_c);
+      t += cxp * xp;
+      t += cyp * yp;
+      t += czp * (pz ? x_p : x_c);
+      const T o = a ? t : T(0);
+      y[e] = o;
+      acc += (double)x_c * (double)o;
+      x_m = x_c;
+      x_c = x_p;
+      x_p = x_n;
+      al_c = al_p;
+      al_p = al_n;
+      ab_c = ab_p;
+      ab_p = ab_n;
+      sm = s;
+      sp = s2;
+      s31 = wrap(s31 + 1);
+      sm31 = wrap(sm31 + 1);
+      z = wrap(z + 1);
+    }
+  }
+  reduce_finalize(acc, 0.0, partials, sc, FIN_SPMV);
+}
+
 // b = A x with the reference's activity tests (x may be non-zero on inactive
 // cells): applyCompressedMatrix for the apply entry point.
 __global__ void __launch_bounds__(kThreads)
@@ -1059,11 +1153,13 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
     const int cX = FWD ? tid + 1 : tid - 1, cY = FWD ? tid + g.ntx : tid - g.ntx;
     const int64_t base = g.tile_base(X, Y);
     if (warp == TY) {
-      // control warp: keeps the compute warps one step behind the rings
+      // control warp: keeps the compute warps one step behind the rings; it
+      // waits up to four times the loaders' bound
+      const int ctl_limit = a.spin_limit > (1 << 28) ? (1 << 30) : 4 * a.spin_limit;
       auto wait_avail = [&](int s) {
-        long long spins = 0;
+        int spins = 0;
         while (((hasX && sh.availX <= s) || (hasY && sh.availY <= s)) && !sh.abort) {
-          if (++spins > 4ll * a.spin_limit) {
+          if (++spins > ctl_limit) {
             if (lane == 0) wave_abort(a, sh, NS);
             break;
           }
@@ -1209,15 +1305,20 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
       sh.last = (prev == (int)gridDim.x - 1);
     }
     __syncthreads();
-    if (sh.last && threadIdx.x == 0) {
+    if (sh.last && warp == 0) {
+      // the tiles' shares, lane l summing tiles l, l + 32, ... in order, then a
+      // fixed shuffle tree: the same sum whichever CTA gets here
       __threadfence();
       double S = 0.0;
-      for (int b = 0; b < ntiles; b++) S += __ldcg(&a.tile_partials[b]);
-      *a.ticket = 0;
-      *a.exits = 0;
-      if (a.fin_kind != FIN_NONE) finalize(a.fin_kind, a.sc, S, 0.0);
-      if (a.sc->err & DEV_ERR_TIMEOUT) a.sc->done = DONE_BREAKDOWN;
-      __threadfence();
+      for (int b = lane; b < ntiles; b += 32) S += __ldcg(&a.tile_partials[b]);
+      S = warp_sum(S);
+      if (lane == 0) {
+        *a.ticket = 0;
+        *a.exits = 0;
+        if (a.fin_kind != FIN_NONE) finalize(a.fin_kind, a.sc, S, 0.0);
+        if (a.sc->err & DEV_ERR_TIMEOUT) a.sc->done = DONE_BREAKDOWN;
+        __threadfence();
+      }
     }
   }
 }
@@ -1628,8 +1729,12 @@ int PcgSolver::ensure_pivots() {
 
 template <class T>
 void PcgSolver::launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip) {
-  k_spmv<T><<<nblocks_, kThreads, 0, st>>>(g_, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az, partials_, sc_,
-                                            use_skip);
+  // slot runs per tile: about 1024 work items in all, runs of at least 16 slots
+  const int ntiles = g_.ntiles();
+  const int chunks = std::max(1, std::min((1024 + ntiles - 1) / ntiles, g_.nz / 16));
+  const int grid = std::min(nblocks_, ntiles * chunks);
+  k_spmv_stream<T><<<grid, kThreads, 0, st>>>(g_, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az, partials_, sc_,
+                                              use_skip, chunks);
 }
 
 template <class T>

@@ -179,3 +179,59 @@ def test_forward_matches_oracle_simulator(oracle, torch_mod, n, advection):
     np.testing.assert_allclose(sim.density(), rho_ref, rtol=0, atol=1e-9)
     loss_ref = float(((rho_ref - target) ** 2).sum())
     assert abs(loss - loss_ref) <= 1e-10 * loss_ref, (loss, loss_ref)
+
+
+def _oracle_loss(oracle, pos, U, target, dims, h, dt, steps, flip, sdfs=None):
+    """The differentiable step's loss computed by the oracle's FP64 simulator
+    (the reference's substep, fluid-simulator.cc:140-182) with MIC(0) tau = 0 and
+    pressure solves to 1e-14 relative, from velocities sampleVelocity takes
+    from U.  sdfs=None records the fluid SDF of every substep and returns
+    (loss, sdfs); given sdfs, the substeps use them instead of reconstructing
+    (the structure the adjoint holds fixed) and the loss is returned."""
+    vel0 = oracle.sample_velocity(pos, dims, h, *U)
+    cfg = oracle.default_config(*dims, h, flip=int(flip), flip_alpha=0.95, pcg_tol=1e-14, pcg_max_iter=4000,
+                                pcg_criterion=1, mic_tau=0.0)
+    sim = oracle.Sim(**cfg)
+    sim.set_particles(pos, vel0)
+    sim.sdf_tape(1, sdfs)
+    for _ in range(steps):
+        sim.substep(dt)
+    rho = _density_np(sim.particles()[0], dims, h)
+    loss = float(((rho - target) ** 2).sum())
+    return (loss, sim.taped_sdfs()) if sdfs is None else loss
+
+
+@pytest.mark.parametrize("n,steps,advection", [(8, 3, "flip"), (12, 2, "flip"), (10, 2, "pic")])
+def test_adjoint_matches_oracle_central_differences(oracle, torch_mod, n, steps, advection):
+    """An FP64 reference gradient independent of this repository's adjoint:
+    central differences of the oracle's forward with the structure the adjoint
+    holds fixed (the fluid SDF of each substep, taped from the oracle's own base
+    run; at eps = 1e-5 no stencil base or wall clamp changes between the two
+    evaluations) against the GPU adjoint: relative error below 1e-5."""
+    torch = torch_mod
+    from simcraft_b200.diff import DiffFlip, control_scene, faces_from_cells
+    pos, param, target, h = control_scene(n)
+    dims, dt, flip = (n, n, n), 1.0 / 120, advection == "flip"
+    U = faces_from_cells(torch.from_numpy(param).cuda())
+    sim = DiffFlip(dims, h, dt, steps, flip_alpha=0.95, advection=advection, checkpoint_every=1, pcg_tol=1e-13)
+    sim.set_particles(pos)
+    sim.set_target(target)
+    loss = sim.forward(U, tape="none")
+    grads = sim.backward()
+    Uh = [u.cpu().numpy() for u in U]
+    loss_ref, sdfs = _oracle_loss(oracle, pos, Uh, target, dims, h, dt, steps, flip)
+    assert len(sdfs) == steps and abs(loss - loss_ref) <= 1e-10 * loss
+    # replaying its own SDFs leaves the oracle's base loss unchanged
+    assert _oracle_loss(oracle, pos, Uh, target, dims, h, dt, steps, flip, sdfs) == loss_ref
+    rng = np.random.default_rng(8)
+    eps = 1e-5
+    errs = []
+    for _ in range(6):
+        d = faces_from_cells(torch.from_numpy(rng.standard_normal(param.shape)).cuda())
+        dh = [x.cpu().numpy() for x in d]
+        lp = _oracle_loss(oracle, pos, [u + eps * x for u, x in zip(Uh, dh)], target, dims, h, dt, steps, flip, sdfs)
+        lm = _oracle_loss(oracle, pos, [u - eps * x for u, x in zip(Uh, dh)], target, dims, h, dt, steps, flip, sdfs)
+        fd = (lp - lm) / (2 * eps)
+        ad = sum(float((g * x).sum()) for g, x in zip(grads, d))
+        errs.append(abs(fd - ad) / max(abs(fd), abs(ad)))
+    assert max(errs) < 1e-5, errs

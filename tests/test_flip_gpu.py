@@ -300,4 +300,4 @@ def test_dam_break_64_ten_frames(oracle, torch_mod, precision):
     x, _ = sim.particles()
     dx = np.abs(x - x_ref).max() / h
     assert dx <= (1e-2 if f32 else 1e-4), (dx, errs)
-    assert np.abs(x_ref - pos).max() > 0.5 * h  # the block has started to fall
+    assert np.abs(x_ref - pos).max() > 0.2 * h  # the block has started to fall (0.29 h in 10 frames)

@@ -110,16 +110,14 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def read_traffic(key):
-    """Per-launch DRAM traffic of a sweep from the committed ncu summary (128^3)."""
-    path = os.path.join(ROOT, "profiles", "pcg_sweeps_128.md")
+def read_traffic(key, n):
+    """Per-launch DRAM traffic of a sweep at n^3 as measured by ncu
+    (profiles/dram_traffic.json, written from the captures), or None."""
     try:
-        for line in open(path):
-            if line.startswith(key + ":"):
-                return float(line.split(":")[1])
-    except OSError:
-        pass
-    return None
+        d = json.load(open(os.path.join(ROOT, "profiles", "dram_traffic.json")))
+    except (OSError, ValueError):
+        return None
+    return float(d[key]) if d.get("grid") == n and key in d else None
 
 
 def peaks():
@@ -302,7 +300,7 @@ def tolerance_sweep(n, ctx, adiag, an, rhs_d, active, act_h):
     return {"reference": "FP64 MIC(0)-PCG to 1e-12 relative residual on the GPU", "rows": rows}
 
 
-def large_solve_leg(args, dev, ctx, replicas):
+def large_solve_leg(args, dev, ctx, replicas, cpu=False):
     """FP64 against mixed on the 512^3 sphere pool (60% fill, seed 9), both to
     1e-8 relative residual, device-resident inputs; `--large-steps` timed solves
     after `--large-warmup` untimed ones, CUDA events on the solver stream."""
@@ -356,6 +354,30 @@ def large_solve_leg(args, dev, ctx, replicas):
         del s
         torch.cuda.empty_cache()
     out["fp64_over_mixed"] = out["fp64"]["ms_per_solve"] / out["mixed"]["ms_per_solve"]
+    if cpu:
+        # the reference's own CgSolver3D on the host cores: a capped run of a few
+        # iterations, its per-iteration time extrapolated to the FP64 count
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ref as R
+
+        if R.available():
+            threads = os.cpu_count() or 1
+            host = {"adiag": adiag.cpu().numpy(), "an": [a.cpu().numpy() for a in an], "active": act_h}
+            capped = 3
+            st = {}
+            R.cg_solve(host["adiag"], host["an"], rhs_h, host["active"], tol=0.0, max_iter=capped + 1,
+                       parallel=True, threads=threads, stats=st)
+            # one preconditioner application precedes the loop: capped + 1 applications
+            per_iter = st["ms"] / (capped + 1)
+            iters = out["fp64"]["iterations"]
+            out["cpu_baseline"] = {"value": per_iter * iters, "unit": "ms/solve", "cores": threads,
+                                   "kind": "reference", "extrapolated": True,
+                                   "ms_per_iteration": per_iter,
+                                   "sample": f"the reference's CgSolver3D::solve on the same {n}^3 system, "
+                                             f"capped at {capped} iterations ({st['ms']:.0f} ms); the total is "
+                                             f"that per-iteration time x the FP64 solve's {iters} iterations "
+                                             f"(extrapolated)"}
+            del host
     del adiag, an, active, rhs_d, pg
     torch.cuda.empty_cache()
     return out
@@ -433,7 +455,7 @@ def collider_leg(args, dev, ctx, cpu):
     out = {"workload": f"closed sphere mesh, {len(t)} triangles, exact band 3, reference distance arithmetic",
            "triangles": len(t)}
     stream = torch.cuda.current_stream(dev)
-    for n in (128, COLLIDER_N):
+    for n in (128, args.collider_n):
         for _ in range(2):
             manifold_to_sdf(vd, td, (n, n, n), 1.0 / n, context=ctx)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -561,7 +583,11 @@ def flip_leg(args, dev, ctx, dist, rank, world):
            "particles": n_particles, "steps": K, "warmup": args.warmup,
            "steps_per_s": world * K / (ms * 1e-3), "ms_per_step": ms / K,
            "split_ms_per_step": {k: v / K for k, v in split.items()},
-           "pcg_inner_iterations_mean": float(np.mean(iters)), "gpu_launches": int(launches)}
+           "pcg_inner_iterations_mean": float(np.mean(iters)), "gpu_launches": int(launches),
+           "steps_note": (f"{K} of the configuration's 100 substeps are timed (--flip-steps 100 times all of "
+                          f"them): each substep takes about a second, and the default run keeps the timed work "
+                          f"near a minute; the timed substeps follow the warm-up ones from the same initial "
+                          f"block, where the flow and the iteration counts are still developing")}
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = flip_cpu_sample(sim, n, h)
     if args.surface:
@@ -627,7 +653,11 @@ def diff_leg(args, ctx, replicas):
     out.update({"fd_directions": args.diff_dirs, "fd_eps": eps, "fd_ranks": replicas.world,
                 "fd_max_rel_err": max(errs) if errs else None,
                 "fd_median_rel_err": float(np.median(errs)) if errs else None,
-                "f32_vs_f64_grad_rel_l2": (num / den) ** 0.5})
+                "f32_vs_f64_grad_rel_l2": (num / den) ** 0.5,
+                "cpu_baseline": {"value": None, "kind": "none",
+                                 "note": "the reference has no differentiable step: there is no CPU adjoint to "
+                                         "time (the FP64 reference gradient of the tests is central differences "
+                                         "of the oracle's forward, tests/test_diff_gpu.py)"}})
     del sims, s32, s64
     torch.cuda.empty_cache()
     return out
@@ -694,6 +724,7 @@ def main():
                     help="timed solves of the 512^3 FP64-vs-mixed leg (0 skips the leg)")
     ap.add_argument("--large-warmup", type=int, default=2, help="untimed solves of the 512^3 leg")
     ap.add_argument("--collider", type=int, default=1, help="mesh-to-SDF collider leg (0 skips)")
+    ap.add_argument("--collider-n", type=int, default=COLLIDER_N, help="the collider leg's larger grid")
     ap.add_argument("--flip32", type=int, default=1, help="32^3 FP64 dam-break leg (0 skips)")
     ap.add_argument("--surface", type=int, default=1,
                     help="marching-cubes export of the FLIP leg's fluid (0 skips)")
@@ -826,7 +857,7 @@ def main():
     bytes_bwd = N * (7 * 8 + 1)
     bytes_fwd = N * (6 * 8 + 1)
     achieved = bytes_fwde32 / (kms32[7] * 1e-3) / 1e9
-    traffic = read_traffic("traffic_bytes_per_launch_fwd_eisenstat_fp32") if n == N_GRID else None
+    traffic = read_traffic("fwd_eisenstat_fp32", n)
     roofline = {"bound": "hbm", "kernel": "fused Eisenstat forward sweep, FP32 (k_wave FwdEisenstatOp<float>), "
                                           "the top kernel of the mixed solve",
                 "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
@@ -835,8 +866,7 @@ def main():
                 "ms_per_launch": kms32[7],
                 "eisenstat_backward_sweep_fp32": {"ms": kms32[6], "achieved_gbs": bytes_bwde32 / (kms32[6] * 1e-3) / 1e9},
                 "fp64_backward_sweep": {"achieved_gbs": bytes_bwd / (kms[2] * 1e-3) / 1e9,
-                                        "traffic": read_traffic("traffic_bytes_per_launch_bwd_fp64")
-                                        if n == N_GRID else None},
+                                        "traffic": read_traffic("bwd_fp64", n)},
                 "kernel_ms": {"pivot": kms[0], "forward_sweep": kms[1], "backward_sweep": kms[2],
                               "spmv": kms[3], "axpy": kms[4], "scale_add": kms[5]},
                 "forward_sweep_gbs": bytes_fwd / (kms[1] * 1e-3) / 1e9,
@@ -893,7 +923,8 @@ def main():
     if rank == 0:
         out["tolerance_sweep"] = tolerance_sweep(n, ctx, adiag, an, rhs_d, active, act_h)
     if args.large_steps > 0:
-        out["solve_512"] = large_solve_leg(args, dev, ctx, replicas)
+        out["solve_512"] = large_solve_leg(args, dev, ctx, replicas,
+                                           cpu=rank == 0 and world == 1 and not args.no_cpu)
     if args.flip_steps > 0:
         out["flip"] = flip_leg(args, dev, ctx, dist, rank, world)
         if "surface" in out["flip"]:

@@ -1,6 +1,6 @@
 """Builds the sm_100a shared library libsimcraft_fluid.so in-tree with nvcc.
 
-Usage: python -m simcraft_b200.build [--force] [--bounds-check]
+Usage: python -m simcraft_b200.build [--force] [-v]
 """
 import os
 import subprocess
@@ -35,7 +35,7 @@ def nvcc():
     return "nvcc"
 
 
-def build(force=False, bounds_check=False, verbose=False):
+def build(force=False, verbose=False):
     if not force and os.path.exists(LIB):
         lt = os.path.getmtime(LIB)
         if all(os.path.getmtime(f) <= lt for f in _deps()):
@@ -43,8 +43,6 @@ def build(force=False, bounds_check=False, verbose=False):
     os.makedirs(OBJDIR, exist_ok=True)
     flags = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
              "-ccbin", "g++"] + ARCH
-    if bounds_check:
-        flags.append("-DSC_BOUNDS_CHECK=1")
     if verbose:
         flags += ["-Xptxas", "-v"]
     objs = []
@@ -71,6 +69,5 @@ def build(force=False, bounds_check=False, verbose=False):
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, bounds_check="--bounds-check" in sys.argv,
-          verbose="-v" in sys.argv)
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
     print(LIB)

@@ -16,7 +16,6 @@ enum : unsigned {
   DEV_ERR_TIMEOUT = 1u,     // a bounded spin-wait gave up
   DEV_ERR_NONFINITE = 2u,   // NaN/Inf in a reduction
   DEV_ERR_BREAKDOWN = 4u,   // PCG breakdown (s.As == 0)
-  DEV_ERR_BOUNDS = 8u,      // index check failed (bounds-checked build only)
 };
 
 constexpr int kWarp = 32;
@@ -179,6 +178,15 @@ struct Cell {
     return at(tbase, slot == g.nz - 1 ? 0 : slot + 1, ty, tx);
   }
 };
+
+// (x, y, z) of a linear index in an nx x ny x nz grid, z fastest, with
+// 32-bit divisions (every grid here holds fewer than 2^31 cells)
+__host__ __device__ __forceinline__ void decode3(int64_t id, int ny, int nz, int& x, int& y, int& z) {
+  const unsigned u = (unsigned)id, q = u / (unsigned)nz, r = q / (unsigned)ny;
+  z = (int)(u - q * (unsigned)nz);
+  y = (int)(q - r * (unsigned)ny);
+  x = (int)r;
+}
 
 // Reference-layout index helpers.
 __host__ __device__ __forceinline__ int64_t lin(int i, int j, int k, int sy, int sz) {

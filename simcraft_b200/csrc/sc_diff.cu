@@ -348,9 +348,8 @@ __global__ void __launch_bounds__(kT) k_adj_walls(Geo G, T* lg) {
   const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
   const int64_t n = (int64_t)fx * fy * fz;
   GRID_LOOP(id, n) {
-    const int c = (int)(id % fz);
-    const int b = (int)((id / fz) % fy);
-    const int a = (int)(id / ((int64_t)fy * fz));
+    int a, b, c;
+    decode3(id, fy, fz, a, b, c);
     const int q = AX == 0 ? a : (AX == 1 ? b : c), qm = AX == 0 ? fx - 1 : (AX == 1 ? fy - 1 : fz - 1);
     if (q == 0 || q == qm) lg[id] = T(0);
   }
@@ -422,9 +421,8 @@ __global__ void __launch_bounds__(kT)
   const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
   const int64_t n = (int64_t)fx * fy * fz;
   GRID_LOOP(id, n) {
-    const int c = (int)(id % fz);
-    const int b = (int)((id / fz) % fy);
-    const int a = (int)(id / ((int64_t)fy * fz));
+    int a, b, c;
+    decode3(id, fy, fz, a, b, c);
     const int q = AX == 0 ? a : (AX == 1 ? b : c);
     const int qn = AX == 0 ? nx : (AX == 1 ? ny : nz);
     double s = 0.0;
@@ -457,9 +455,8 @@ __global__ void __launch_bounds__(kT)
   };
   GRID_LOOP(id, n) {
     if (!vs[id]) continue;
-    const int c = (int)(id % fz);
-    const int b = (int)((id / fz) % fy);
-    const int a = (int)(id / sx);
+    int a, b, c;
+    decode3(id, fy, fz, a, b, c);
     T s = T(0);
     if (a > 0 && !vs[id - sx]) s += ld[id - sx] / (T)count(id - sx, a - 1, b, c);
     if (a < fx - 1 && !vs[id + sx]) s += ld[id + sx] / (T)count(id + sx, a + 1, b, c);
@@ -482,9 +479,8 @@ __global__ void __launch_bounds__(kT) k_adj_dirichlet(Geo G, T* lg, const T* lul
   const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
   const int64_t n = (int64_t)fx * fy * fz;
   GRID_LOOP(id, n) {
-    const int c = (int)(id % fz);
-    const int b = (int)((id / fz) % fy);
-    const int a = (int)(id / ((int64_t)fy * fz));
+    int a, b, c;
+    decode3(id, fy, fz, a, b, c);
     const int q = AX == 0 ? a : (AX == 1 ? b : c), qm = AX == 0 ? fx - 1 : (AX == 1 ? fy - 1 : fz - 1);
     lg[id] = ((q == 0 || q == qm) ? T(0) : lg[id]) + lul[id];
   }

@@ -459,9 +459,8 @@ __global__ void __launch_bounds__(kT)
   const int64_t N = (int64_t)G.nx * G.ny * G.nz;
   const double r2 = 2 * radius;
   GRID_LOOP(id, N) {
-    const int k = (int)(id % G.nz);
-    const int j = (int)((id / G.nz) % G.ny);
-    const int i = (int)(id / ((int64_t)G.ny * G.nz));
+    int i, j, k;
+    decode3(id, G.ny, G.nz, i, j, k);
     const double cx = radd(rmul(radd((double)i, 0.5), h), 0.0);
     const double cy = radd(rmul(radd((double)j, 0.5), h), 0.0);
     const double cz = radd(rmul(radd((double)k, 0.5), h), 0.0);
@@ -518,9 +517,8 @@ __global__ void __launch_bounds__(kT)
       vd[id] = 1;
       continue;
     }
-    const int k = (int)(id % G.nz);
-    const int j = (int)((id / G.nz) % G.ny);
-    const int i = (int)(id / sx);
+    int i, j, k;
+    decode3(id, G.ny, G.nz, i, j, k);
     double sum = 0.0;
     int cnt = 0;
     if (i > 0 && vs[id - sx]) { sum = radd(sum, src[id - sx]); cnt++; }
@@ -544,9 +542,8 @@ __global__ void __launch_bounds__(kT)
   const int64_t N = (int64_t)G.nx * G.ny * G.nz;
   const int64_t sx = (int64_t)G.ny * G.nz, sy = G.nz;
   GRID_LOOP(id, N) {
-    const int k = (int)(id % G.nz);
-    const int j = (int)((id / G.nz) % G.ny);
-    const int i = (int)(id / sx);
+    int i, j, k;
+    decode3(id, G.ny, G.nz, i, j, k);
     double sum = 0.0;
     int cnt = 0;
     if (i > 0) { sum = radd(sum, src[id - sx]); cnt++; }
@@ -738,9 +735,8 @@ __global__ void __launch_bounds__(kT) k_dirichlet(Geo G, T* g, uint8_t* valid) {
   const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
   const int64_t n = (int64_t)fx * fy * fz;
   GRID_LOOP(id, n) {
-    const int c = (int)(id % fz);
-    const int b = (int)((id / fz) % fy);
-    const int a = (int)(id / ((int64_t)fy * fz));
+    int a, b, c;
+    decode3(id, fy, fz, a, b, c);
     const int q = AX == 0 ? a : (AX == 1 ? b : c), qm = AX == 0 ? fx - 1 : (AX == 1 ? fy - 1 : fz - 1);
     if (q == 0 || q == qm) {
       g[id] = T(0);
@@ -764,9 +760,8 @@ __global__ void __launch_bounds__(kT)
       vd[id] = 1;
       continue;
     }
-    const int c = (int)(id % fz);
-    const int b = (int)((id / fz) % fy);
-    const int a = (int)(id / sx);
+    int a, b, c;
+    decode3(id, fy, fz, a, b, c);
     T sum = T(0);
     int cnt = 0;
     if (a > 0 && vs[id - sx]) { sum = radd(sum, src[id - sx]); cnt++; }
@@ -792,7 +787,8 @@ __global__ void __launch_bounds__(kT) k_force(Geo G, T* v, const uint8_t* valid,
   const int64_t n = (int64_t)G.nx * fy * G.nz;
   const T d = (T)gdt;
   GRID_LOOP(id, n) {
-    const int j = (int)((id / G.nz) % fy);
+    int i, j, k;
+    decode3(id, fy, G.nz, i, j, k);
     if (valid[id] && j > 0 && j < G.ny) v[id] = rsub(v[id], d);
   }
 }
@@ -803,9 +799,8 @@ __global__ void __launch_bounds__(kT) k_collider(Geo G, double h, T* g, const do
   const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
   const int64_t n = (int64_t)fx * fy * fz;
   GRID_LOOP(id, n) {
-    const int c = (int)(id % fz);
-    const int b = (int)((id / fz) % fy);
-    const int a = (int)(id / ((int64_t)fy * fz));
+    int a, b, c;
+    decode3(id, fy, fz, a, b, c);
     const int q = AX == 0 ? a : (AX == 1 ? b : c), qm = AX == 0 ? fx - 1 : (AX == 1 ? fy - 1 : fz - 1);
     if (q == 0 || q == qm) {
       g[id] = T(0);

@@ -27,9 +27,8 @@ __global__ void __launch_bounds__(kT)
   const int64_t n = (int64_t)fx * fy * fz;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n;
        id += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(id % fz);
-    const int j = (int)((id / fz) % fy);
-    const int i = (int)(id / ((int64_t)fy * fz));
+    int i, j, k;
+    decode3(id, fy, fz, i, j, k);
     const int c = AX == 0 ? i : (AX == 1 ? j : k);
     const int cmax = AX == 0 ? nx : (AX == 1 ? ny : nz);
     double out = 0.0;
@@ -199,9 +198,8 @@ __global__ void __launch_bounds__(kT)
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n;
        id += (int64_t)gridDim.x * blockDim.x) {
     if (wt[id] <= 0.0) continue;
-    const int k = (int)(id % fz);
-    const int j = (int)((id / fz) % fy);
-    const int i = (int)(id / ((int64_t)fy * fz));
+    int i, j, k;
+    decode3(id, fy, fz, i, j, k);
     const int c = AX == 0 ? i : (AX == 1 ? j : k);
     const int cmax = AX == 0 ? nx : (AX == 1 ? ny : nz);
     if (c == 0 || c == cmax) {

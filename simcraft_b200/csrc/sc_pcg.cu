@@ -27,6 +27,8 @@
 #include <mutex>
 #include <string>
 
+#include <cooperative_groups.h>
+
 #include "sc_pcg.cuh"
 
 namespace sc {
@@ -982,6 +984,44 @@ struct WaveShared {
   double ssum[TY + 3];
 };
 
+// Hand-off ring between the CTAs of a thread-block cluster (distributed shared
+// memory): the y-boundary row a tile passes to the next tile of the same
+// cluster goes straight into that CTA's ring.  One 64-bit word per lane and
+// entry holds the FP32 value in its low half and a stamp (the cluster tile's
+// ticket << 12 | the entry) in its high half, written with one store, so a
+// consumer that sees the stamp it expects sees the value: no fence and no
+// reset.  Each CTA fills its ring with an impossible stamp at launch.
+constexpr int kClRing = 32;
+constexpr unsigned kClNoStamp = 0xffffffffu;
+__device__ __forceinline__ unsigned cl_stamp(int ticket, int e) { return ((unsigned)ticket << 12) | (unsigned)e; }
+__device__ __forceinline__ void st_relaxed_cluster_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.cluster.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_cluster_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.cluster.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_relaxed_cluster_s32(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.cluster.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+template <class T>
+__device__ __forceinline__ T cl_value(unsigned long long w) {
+  if constexpr (sizeof(T) == 4)
+    return __uint_as_float((unsigned)(w & 0xffffffffull));
+  else
+    return T(0);
+}
+template <class T>
+__device__ __forceinline__ unsigned long long cl_word(int ticket, int e, T v) {
+  if constexpr (sizeof(T) == 4)
+    return ((unsigned long long)cl_stamp(ticket, e) << 32) | (unsigned long long)__float_as_uint(v);
+  else
+    return 0ull;
+}
+
 // Give up: flag the error and release the compute warps.
 template <class T, int TY>
 __device__ __forceinline__ void wave_abort(const WaveArgs& a, WaveShared<T, TY>& sh, int NS) {
@@ -992,11 +1032,11 @@ __device__ __forceinline__ void wave_abort(const WaveArgs& a, WaveShared<T, TY>&
 }
 
 __device__ __forceinline__ bool wave_should_stop(const WaveArgs& a, int& spins,
-                                                 volatile int* s_abort) {
+                                                 volatile int* s_abort, int limit) {
   if (*s_abort) return true;
   ++spins;
   if ((spins & 63) == 0 && ld_relaxed_gpu_u32(&a.sc->err)) return true;
-  return spins > a.spin_limit;
+  return spins > limit;
 }
 
 // Mailboxes.  The producer tile writes each boundary value it computes into
@@ -1008,7 +1048,7 @@ __device__ __forceinline__ bool wave_should_stop(const WaveArgs& a, int& spins,
 // which leaves the mailboxes ready for the next sweep.  No fences are needed:
 // every mailbox word carries exactly one value per sweep.
 template <class T, int TY, bool FWD>
-__device__ void wave_load_x(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int NS) {
+__device__ void wave_load_x(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int NS, int limit) {
   const Tiled& g = a.g;
   const int lane = threadIdx.x & 31;
   constexpr int EPB = 32 / TY;  // entries per 32 lanes
@@ -1016,7 +1056,7 @@ __device__ void wave_load_x(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int
   while (lx < NS) {
     const int want = min(NS, sh.done + kRing);
     if (lx >= want) {
-      if (wave_should_stop(a, spins, &sh.abort)) break;
+      if (wave_should_stop(a, spins, &sh.abort, limit)) break;
       continue;
     }
     // poll up to 8*EPB entries: lane handles (entry lx + k*EPB + lane/TY, ty = lane%TY)
@@ -1056,20 +1096,20 @@ __device__ void wave_load_x(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int
       spins = 0;
       continue;
     }
-    if (wave_should_stop(a, spins, &sh.abort)) break;
+    if (wave_should_stop(a, spins, &sh.abort, limit)) break;
   }
   if (lx < NS && lane == 0) wave_abort(a, sh, NS);
 }
 
 template <class T, int TY, bool FWD>
-__device__ void wave_load_y(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int NS) {
+__device__ void wave_load_y(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int NS, int limit) {
   const Tiled& g = a.g;
   const int lane = threadIdx.x & 31;
   int ly = 0, spins = 0;
   while (ly < NS) {
     const int want = min(NS, sh.done + kRing);
     if (ly >= want) {
-      if (wave_should_stop(a, spins, &sh.abort)) break;
+      if (wave_should_stop(a, spins, &sh.abort, limit)) break;
       continue;
     }
     typename Sentinel<T>::Bits v[8];
@@ -1104,26 +1144,46 @@ __device__ void wave_load_y(const WaveArgs& a, WaveShared<T, TY>& sh, T* mb, int
       spins = 0;
       continue;
     }
-    if (wave_should_stop(a, spins, &sh.abort)) break;
+    if (wave_should_stop(a, spins, &sh.abort, limit)) break;
   }
   if (ly < NS && lane == 0) wave_abort(a, sh, NS);
 }
 
 // One CTA per SM: the sweep is issue-bound, and capping registers for two
 // CTAs per SM measured slower at 128^3, 256^3 and 512^3.
-template <class T, int TY, bool FWD, class Op>
+//
+// CL > 0 (FP32 only): the grid is made of thread-block clusters of CL CTAs.  A
+// ticket then names a cluster tile, CL tiles stacked along y in one column
+// (X, Yc * CL + rank), and a tile hands its y-boundary row to the next tile of
+// its cluster through that CTA's shared memory (kClRing) instead of a global
+// mailbox; only the hand-offs between clusters (along y at the cluster edges,
+// and along x) use the mailboxes.  The CTAs of a cluster take each ticket
+// together and meet at a cluster barrier after each cluster tile.
+template <class T, int TY, bool FWD, class Op, int CL = 0>
 __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, const Op op_arg) {
   // warps 0..TY-1: tile rows (compute only, no fences: a fence would wait for
   // the prefetch loads in flight); warp TY: control (flags, ring waits);
   // warps TY+1, TY+2: x and y mailbox loaders.
+  constexpr bool CLU = CL > 0;
+  static_assert(!CLU || sizeof(T) == 4, "cluster hand-off rings carry FP32 values");
   constexpr int NBAR = (TY + 1) * 32;
   __shared__ WaveShared<T, TY> sh;
+  __shared__ unsigned long long ringY[CLU ? kClRing : 1][32];
   extern __shared__ __align__(16) unsigned char wave_dyn[];
   T* stage = reinterpret_cast<T*>(wave_dyn);  // [kStage][TY][NV][32]
   if (a.use_skip && a.sc->done != DONE_RUNNING) return;
-  if (a.sc->err & DEV_ERR_TIMEOUT) return;  // an earlier sweep gave up: do not wait again
+  // an earlier sweep gave up: do not wait again (a cluster decides together,
+  // below, since CTAs could read the status word at different moments)
+  if (!CLU && (a.sc->err & DEV_ERR_TIMEOUT)) return;
+  int rank = 0;
+  if constexpr (CLU) {
+    rank = (int)cooperative_groups::this_cluster().block_rank();
+    for (int i = threadIdx.x; i < kClRing * 32; i += blockDim.x) ringY[i / 32][i % 32] = (unsigned long long)kClNoStamp << 32;
+    cooperative_groups::this_cluster().sync();  // every CTA of the cluster runs before any remote access
+  }
   Op op = op_arg;
   if constexpr (HasPrepare<Op>::value) op.prepare(a.sc);
+  const int slim = a.sc->spin_limit > 0 ? a.sc->spin_limit : kSpinLimit;  // bound of every wait
   const Tiled& g = a.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntiles = g.ntiles();
@@ -1131,19 +1191,46 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
   T* mbx = reinterpret_cast<T*>(a.mbx);
   T* mby = reinterpret_cast<T*>(a.mby);
   double acc = 0.0;
+  // a cluster launch takes tickets for cluster tiles: ntx columns of ceil(nty/CL)
+  const int nticket = CLU ? g.ntx * ((g.nty + (CLU ? CL : 1) - 1) / (CLU ? CL : 1)) : ntiles;
   for (;;) {
-    if (threadIdx.x == 0) {
-      sh.tile = atomicAdd(a.ticket, 1);
-      sh.done = 0;
-      sh.availX = 0;
-      sh.availY = 0;
-      sh.abort = 0;
+    if constexpr (CLU) {
+      if (threadIdx.x == 0) {
+        sh.done = 0;
+        sh.availX = 0;
+        sh.availY = 0;
+        sh.abort = 0;
+      }
+      if (rank == 0 && threadIdx.x == 0) {
+        const int tk = atomicAdd(a.ticket, 1);
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        for (int r = 0; r < CL; r++) *cl.map_shared_rank(&sh.tile, r) = tk;
+      }
+      cooperative_groups::this_cluster().sync();
+    } else {
+      if (threadIdx.x == 0) {
+        sh.tile = atomicAdd(a.ticket, 1);
+        sh.done = 0;
+        sh.availX = 0;
+        sh.availY = 0;
+        sh.abort = 0;
+      }
+      __syncthreads();
     }
-    __syncthreads();
     const int t = sh.tile;
-    if (t >= ntiles) break;
-    const int2 XY = a.order[FWD ? t : ntiles - 1 - t];
-    const int X = XY.x, Y = XY.y;
+    if (t >= nticket) break;
+    int X, Y;
+    if constexpr (CLU) {
+      const int2 XY = a.order[FWD ? t : nticket - 1 - t];
+      X = XY.x;
+      Y = XY.y * CL + rank;
+    } else {
+      const int2 XY = a.order[FWD ? t : ntiles - 1 - t];
+      X = XY.x;
+      Y = XY.y;
+    }
+    // a cluster tile at the top edge can have CTAs without a tile
+    if (Y < g.nty) {
     const int tid = Y * g.ntx + X;
     const bool hasX = FWD ? (X > 0) : (X < g.ntx - 1);
     const bool hasY = FWD ? (Y > 0) : (Y < g.nty - 1);
@@ -1151,17 +1238,38 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
     const bool outX = FWD ? (X < g.ntx - 1) : (X > 0);
     const bool outY = FWD ? (Y < g.nty - 1) : (Y > 0);
     const int cX = FWD ? tid + 1 : tid - 1, cY = FWD ? tid + g.ntx : tid - g.ntx;
+    // y boundary rows within a cluster travel through the rings
+    const bool ydin = CLU && hasY && (FWD ? rank > 0 : rank < CL - 1);
+    const bool ydout = CLU && outY && (FWD ? rank < CL - 1 : rank > 0);
     const int64_t base = g.tile_base(X, Y);
     if (warp == TY) {
       // control warp: keeps the compute warps one step behind the rings; it
       // waits up to four times the loaders' bound
-      const int ctl_limit = a.spin_limit > (1 << 28) ? (1 << 30) : 4 * a.spin_limit;
+      const int ctl_limit = slim > (1 << 28) ? (1 << 30) : 4 * slim;
       auto wait_avail = [&](int s) {
         int spins = 0;
-        while (((hasX && sh.availX <= s) || (hasY && sh.availY <= s)) && !sh.abort) {
-          if (++spins > ctl_limit) {
-            if (lane == 0) wave_abort(a, sh, NS);
-            break;
+        if (ydin) {
+          // this lane's word of ring entry s, where the consumer row needs it
+          // (the same z test as the mailbox loader's)
+          const int zc = FWD ? s - lane : g.nz - 1 - (s - (31 - lane));
+          const bool need = zc >= 0 && zc < g.nz;
+          const unsigned want = cl_stamp(t, s);
+          const unsigned long long* w = &ringY[s % kClRing][lane];
+          for (;;) {
+            const bool mine = !need || (unsigned)(ld_relaxed_cluster_u64(w) >> 32) == want;
+            const bool ok = mine && !(hasX && sh.availX <= s);
+            if (__all_sync(kFull, ok) || __any_sync(kFull, sh.abort)) break;
+            if (++spins > ctl_limit) {
+              if (lane == 0) wave_abort(a, sh, NS);
+              break;
+            }
+          }
+        } else {
+          while (((hasX && sh.availX <= s) || (hasY && sh.availY <= s)) && !sh.abort) {
+            if (++spins > ctl_limit) {
+              if (lane == 0) wave_abort(a, sh, NS);
+              break;
+            }
           }
         }
         __syncwarp();
@@ -1176,15 +1284,27 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
       }
       if (lane == 0) sh.done = NS;
     } else if (warp == TY + 1) {
-      if (hasX) wave_load_x<T, TY, FWD>(a, sh, mbx + (int64_t)tid * a.mb_stride_x, NS);
+      if (hasX) wave_load_x<T, TY, FWD>(a, sh, mbx + (int64_t)tid * a.mb_stride_x, NS, slim);
     } else if (warp == TY + 2) {
-      if (hasY) wave_load_y<T, TY, FWD>(a, sh, mby + (int64_t)tid * a.mb_stride_y, NS);
+      if (hasY && !ydin) wave_load_y<T, TY, FWD>(a, sh, mby + (int64_t)tid * a.mb_stride_y, NS, slim);
     } else {
       const int ty = warp;
       T* outx = outX ? mbx + (int64_t)cX * a.mb_stride_x : nullptr;
-      T* outy = outY ? mby + (int64_t)cY * a.mb_stride_y : nullptr;
+      T* outy = (outY && !ydout) ? mby + (int64_t)cY * a.mb_stride_y : nullptr;
       const bool xsrc = FWD ? (lane == 31) : (lane == 0);        // lane feeding the x consumer
       const bool ysrc = FWD ? (ty == TY - 1) : (ty == 0);        // warp feeding the y consumer
+      // the ring of the cluster CTA this tile feeds along y, and its progress
+      unsigned long long* rring = nullptr;
+      const int* rdone = nullptr;
+      int cdone = 0;  // the consumer's completed steps, as last read
+      if constexpr (CLU) {
+        if (ydout && ysrc) {
+          cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+          const int cr = FWD ? rank + 1 : rank - 1;
+          rring = cl.map_shared_rank(&ringY[0][0], cr);
+          rdone = const_cast<const int*>(cl.map_shared_rank(const_cast<int*>(&sh.done), cr));
+        }
+      }
       // slot of the row this warp touches at step s: forward (s - ty) mod nz,
       // backward (nz + 29 + TY - s - ty) mod nz; advanced incrementally.
       int cslot = wave_slot<TY, FWD>(g, 0, ty);
@@ -1255,17 +1375,47 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
             const bool xedge = FWD ? (lane == 0) : (lane == 31);
             const T xn = xedge ? (hasX ? sh.bufX[s % kRing][ty] : T(0)) : shv;
             T yn;
+            // the y neighbour across the tile edge: a cluster ring entry or the
+            // mailbox ring the loader filled
+            T yedge = T(0);
+            if (hasY) {
+              if (CLU && ydin)
+                yedge = cl_value<T>(*(volatile unsigned long long*)&ringY[s % kClRing][lane]);
+              else
+                yedge = sh.bufY[s % kRing][lane];
+            }
             if (FWD)
-              yn = ty > 0 ? sh.xch[(s + 1) & 1][ty - 1][lane] : (hasY ? sh.bufY[s % kRing][lane] : T(0));
+              yn = ty > 0 ? sh.xch[(s + 1) & 1][ty - 1][lane] : yedge;
             else
-              yn = ty < TY - 1 ? sh.xch[(s + 1) & 1][ty + 1][lane]
-                               : (hasY ? sh.bufY[s % kRing][lane] : T(0));
+              yn = ty < TY - 1 ? sh.xch[(s + 1) & 1][ty + 1][lane] : yedge;
+            if constexpr (CLU) {
+              // before writing entry s - (TY-1) into the consumer's ring, that
+              // slot's previous entry must have been used (its step completed)
+              if (rring && s >= TY - 1 && s - (TY - 1) - kClRing >= cdone) {
+                int spins = 0;
+                for (;;) {
+                  cdone = ld_relaxed_cluster_s32(rdone);
+                  if (s - (TY - 1) - kClRing < cdone) break;
+                  if (++spins > slim) {
+                    atomicOr(&a.sc->err, DEV_ERR_TIMEOUT);
+                    break;
+                  }
+                }
+              }
+            }
             T val = T(0);
             if (valid) {
               const int64_t e = rowbase + (int64_t)cslot * rstride;
               val = op.compute(v, xn, yn, prev, e, acc);
               if (xsrc && outx) mb_store(outx + (int64_t)(s - 31) * TY + ty, val);
-              if (ysrc && outy) mb_store(outy + (int64_t)(s - (TY - 1)) * 32 + lane, val);
+              if (ysrc) {
+                if (CLU && rring) {
+                  const int en = s - (TY - 1);
+                  st_relaxed_cluster_u64(rring + (en % kClRing) * 32 + lane, cl_word<T>(t, en, val));
+                } else if (outy) {
+                  mb_store(outy + (int64_t)(s - (TY - 1)) * 32 + lane, val);
+                }
+              }
             }
             sh.xch[s & 1][ty][lane] = val;
             prev = val;
@@ -1295,6 +1445,8 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
       }
     }
     __syncthreads();
+    }  // Y < nty
+    if constexpr (CLU) cooperative_groups::this_cluster().sync();  // no ring traffic crosses cluster tiles
   }
   // CTA partial of the accumulated dot product, then exit accounting.  The last
   // CTA to exit finalizes the reduction and resets the ticket counters.
@@ -1348,6 +1500,62 @@ void launch_wave(const WaveArgs& a, const Op& op, cudaStream_t st, int grid) {
   k_wave<T, Tiled::TY, FWD, Op><<<grid, (Tiled::TY + 3) * 32, wave_dyn_smem<T, FWD, Op>(), st>>>(a, op);
 }
 
+// Cluster launches of the FP32 sweeps (CL CTAs per cluster along y).
+template <int CL>
+cudaLaunchAttribute cluster_attr() {
+  cudaLaunchAttribute at{};
+  at.id = cudaLaunchAttributeClusterDimension;
+  at.val.clusterDim.x = CL;
+  at.val.clusterDim.y = 1;
+  at.val.clusterDim.z = 1;
+  return at;
+}
+template <class T, bool FWD, class Op, int CL>
+void wave_set_attr_cl() {
+  cudaFuncSetAttribute(k_wave<T, Tiled::TY, FWD, Op, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)wave_dyn_smem<T, FWD, Op>());
+  if (CL > 8) cudaFuncSetAttribute(k_wave<T, Tiled::TY, FWD, Op, CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+// Clusters of the sweep that fit on the GPU at once (0: cannot launch).
+template <class T, bool FWD, class Op, int CL>
+int wave_max_clusters() {
+  wave_set_attr_cl<T, FWD, Op, CL>();
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(CL * 64);
+  cfg.blockDim = dim3((Tiled::TY + 3) * 32);
+  cfg.dynamicSmemBytes = wave_dyn_smem<T, FWD, Op>();
+  cudaLaunchAttribute at = cluster_attr<CL>();
+  cfg.attrs = &at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_wave<T, Tiled::TY, FWD, Op, CL>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+template <class T, bool FWD, class Op, int CL>
+void launch_wave_cl(const WaveArgs& a, const Op& op, cudaStream_t st, int nclusters) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(nclusters * CL);
+  cfg.blockDim = dim3((Tiled::TY + 3) * 32);
+  cfg.dynamicSmemBytes = wave_dyn_smem<T, FWD, Op>();
+  cfg.stream = st;
+  cudaLaunchAttribute at = cluster_attr<CL>();
+  cfg.attrs = &at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_wave<T, Tiled::TY, FWD, Op, CL>, a, op);
+}
+// The FP32 sweep kinds (all of them take the cluster path together).
+template <int CL>
+int fp32_max_clusters() {
+  return std::min({wave_max_clusters<float, true, FwdOp<float>, CL>(),
+                   wave_max_clusters<float, false, BwdOp<float>, CL>(),
+                   wave_max_clusters<float, true, FwdOp<float, true>, CL>(),
+                   wave_max_clusters<float, false, BwdEisenstatOp<float>, CL>(),
+                   wave_max_clusters<float, true, FwdEisenstatOp<float>, CL>()});
+}
+
 // Fill the mailboxes with the sentinel (at allocation and after an error).
 template <class T>
 __global__ void k_mb_reset(int64_t n, T* mb) {
@@ -1389,6 +1597,24 @@ void PcgSolver::reset_mailboxes(bool f32) {
   }
 }
 
+// FP32 sweeps go through clusters when the solver set them up; everything
+// else (FP64, or no clusters) through the plain persistent grid.
+template <class T, bool FWD, class Op>
+void PcgSolver::launch_sweep(const WaveArgs& a, const Op& op, cudaStream_t st, int grid) {
+  if constexpr (sizeof(T) == 4) {
+    if (cl_size_ > 0) {
+      WaveArgs c = a;
+      c.order = order_cl_;
+      if (cl_size_ == 16)
+        launch_wave_cl<T, FWD, Op, 16>(c, op, st, cl_grid_);
+      else
+        launch_wave_cl<T, FWD, Op, 8>(c, op, st, cl_grid_);
+      return;
+    }
+  }
+  launch_wave<T, FWD>(a, op, st, grid);
+}
+
 WaveArgs PcgSolver::wave_args(bool f32, int use_skip, int fin) const {
   WaveArgs w{};
   w.g = g_;
@@ -1404,7 +1630,6 @@ WaveArgs PcgSolver::wave_args(bool f32, int use_skip, int fin) const {
   w.tile_partials = tile_partials_;
   w.use_skip = use_skip;
   w.fin_kind = fin;
-  w.spin_limit = spin_limit();
   return w;
 }
 
@@ -1504,6 +1729,28 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
     }
   cudaMemcpyAsync(order, ord.data(), sizeof(int2) * ord.size(), cudaMemcpyHostToDevice,
                   ctx->stream);
+  // FP32 sweeps in clusters of 16 (or 8) CTAs along y, when the tile rows fill
+  // such clusters, the GPU can run them, and the ring stamps hold the entries
+  if (NS < 4096) {
+    for (int CL : {16, 8}) {
+      if (g_.nty < CL) continue;
+      const int n = CL == 16 ? fp32_max_clusters<16>() : fp32_max_clusters<8>();
+      if (n < 1) continue;
+      const int nyc = (g_.nty + CL - 1) / CL;
+      std::vector<int2> oc;
+      for (int d = 0; d <= g_.ntx + nyc - 2; d++)
+        for (int X = 0; X < g_.ntx; X++) {
+          const int Yc = d - X;
+          if (Yc >= 0 && Yc < nyc) oc.push_back(make_int2(X, Yc));
+        }
+      order_cl_ = (int2*)alloc(sizeof(int2) * oc.size());
+      if (!order_cl_) break;
+      cudaMemcpyAsync(order_cl_, oc.data(), sizeof(int2) * oc.size(), cudaMemcpyHostToDevice, ctx->stream);
+      cl_size_ = CL;
+      cl_grid_ = std::min(n, (int)oc.size());
+      break;
+    }
+  }
   if (cudaMallocHost(&sc_host_, sizeof(PcgScalars) * 2) != cudaSuccess) {
     init_status_ = -3;
     return;
@@ -1661,8 +1908,11 @@ int PcgSolver::ensure_pivots() {
   cudaStream_t st = ctx_->stream;
   const int grid = grid_for(g_.total, ctx_->sm_count);
   WaveArgs wa = wave_args(false, 0, FIN_NONE);
-  // the pivot sweep reports a timeout through the status word: start it clean
+  // the pivot sweep reports a timeout through the status word: start it clean,
+  // with this context's wait bound
   cudaMemsetAsync(&sc_->err, 0, sizeof(unsigned), st);
+  pivot_limit_ = spin_limit();
+  cudaMemcpyAsync(&sc_->spin_limit, &pivot_limit_, sizeof(int), cudaMemcpyHostToDevice, st);
   k_mask_system<<<grid, kThreads, 0, st>>>(g_, active_, d64_.adiag, d64_.al, d64_.ad, d64_.ab);
   // uR/uU/uF hold the pivot's diagonal products until k_upper overwrites them
   // q holds Adiag masked by the active flag until the forward sweep overwrites it
@@ -1748,9 +1998,9 @@ void PcgSolver::launch_iteration(SysArrays<T>& A, bool eis) {
       // Az = w = L^-1 A L^-T s, q = rh (split residual), p = d (FP32 correction).
       // s = rh + beta s ; t = L^-T s ; iteration count and bound
       BwdEisenstatOp<T> bo{{A.q, A.s, A.E, A.uR, A.uU, A.uF}, A.z, A.s, T(0)};
-      launch_wave<T, false>(wave_args(true, 1, FIN_SA), bo, st, wg);
+      launch_sweep<T, false>(wave_args(true, 1, FIN_SA), bo, st, wg);
       FwdEisenstatOp<T> fo{{A.s, A.z, A.Pinv, A.Dt, A.cL, A.cD, A.cB, A.E}, A.Az};
-      launch_wave<T, true>(wave_args(true, 1, FIN_SPMV), fo, st, wg);  // alpha = rho / s.w
+      launch_sweep<T, true>(wave_args(true, 1, FIN_SPMV), fo, st, wg);  // alpha = rho / s.w
       // x += alpha t ; rh -= alpha w ; beta = rho_new / rho
       k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.Az, A.p, A.q, partials_, sc_,
                                                FIN_EAXPY);
@@ -1762,9 +2012,9 @@ void PcgSolver::launch_iteration(SysArrays<T>& A, bool eis) {
   launch_spmv<T>(A, st, 1);
   k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.s, A.Az, A.p, A.r, partials_, sc_);
   FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
-  launch_wave<T, true>(wf, fo, st, wg);
+  launch_sweep<T, true>(wf, fo, st, wg);
   BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
-  launch_wave<T, false>(wb, bo, st, wg);
+  launch_sweep<T, false>(wb, bo, st, wg);
   k_sa<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.s, partials_, sc_);
 }
 
@@ -1773,14 +2023,6 @@ void PcgSolver::launch_iteration(SysArrays<T>& A, bool eis) {
 // launch the same kernels directly.
 template <class T>
 int PcgSolver::ensure_graph(SysArrays<T>& A, bool eis) {
-  if (graph_limit_ != spin_limit()) {  // the wait bound is a kernel argument baked into the graphs
-    for (cudaGraphExec_t* g : {&graph64_, &graph32_, &graph32e_})
-      if (*g) {
-        cudaGraphExecDestroy(*g);
-        *g = nullptr;
-      }
-    graph_limit_ = spin_limit();
-  }
   cudaGraphExec_t& gx = graph_for<T>(eis);
   if (gx) return 0;
   cudaStream_t s = ctx_->stream;
@@ -1806,6 +2048,7 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
   cudaStream_t s = ctx_->stream;
   // scalars
   PcgScalars init{};
+  init.spin_limit = spin_limit();
   init.tol = tol;
   init.max_iter = max_iter;
   init.criterion = criterion;
@@ -1823,15 +2066,15 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
     // rh = L^-1 r ; s = rh ; rho = rh.rh
     if constexpr (sizeof(T) == 4) {
       FwdOp<T, true> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
-      launch_wave<T, true>(wave_args(true, 1, FIN_EINIT), fo, s, wg);
+      launch_sweep<T, true>(wave_args(true, 1, FIN_EINIT), fo, s, wg);
     }
     k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.q, A.s, sc_);
   } else {
     // z = M^-1 r ; s = z ; sigma = z.r
     FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
-    launch_wave<T, true>(wave_args(f32, 1, FIN_NONE), fo, s, wg);
+    launch_sweep<T, true>(wave_args(f32, 1, FIN_NONE), fo, s, wg);
     BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
-    launch_wave<T, false>(wave_args(f32, 1, FIN_BWD), bo, s, wg);
+    launch_sweep<T, false>(wave_args(f32, 1, FIN_BWD), bo, s, wg);
     k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.z, A.s, sc_);
   }
   launches_ += eis ? 3 : 4;
@@ -1908,6 +2151,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
   // x = 0 ; r = b (FP64)
   k_fill<double><<<grid, kThreads, 0, s>>>(g_.total, xacc_, 0.0);
   PcgScalars init{};
+  init.spin_limit = spin_limit();
   init.tol = 0.0;  // the FP32 recursion never stops itself
   init.max_iter = opt_.max_iter;
   init.criterion = CRIT_REL_L2;
@@ -1930,7 +2174,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
     // d = 0 ; r32 = r / scale ; rh = L^-1 r32 ; s = rh ; rho = rh.rh
     k_init<float><<<nblocks_, kThreads, 0, s>>>(g_, d64_.r, 1.0 / scale, active_, A.r, A.p, partials_, sc_);
     FwdOp<float, true> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
-    launch_wave<float, true>(wave_args(true, 1, FIN_EINIT), fo, s, wg);
+    launch_sweep<float, true>(wave_args(true, 1, FIN_EINIT), fo, s, wg);
     k_copy<float><<<nblocks_, kThreads, 0, s>>>(g_.total, A.q, A.s, sc_);
     launches_ += 3;
     e = ensure_graph<float>(A, true);
@@ -1972,7 +2216,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
     k_init<float><<<nblocks_, kThreads, 0, s>>>(g_, d64_.r, 1.0 / scale, active_, A.r, A.p, partials_, sc_,
                                                 FIN_NONE);
     FwdOp<float, true> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
-    launch_wave<float, true>(wave_args(true, 0, FIN_EREPLACE), fo, s, wg);
+    launch_sweep<float, true>(wave_args(true, 0, FIN_EREPLACE), fo, s, wg);
     launches_ += 3;
     cudaMemcpyAsync(&sc_host_[0], sc_, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("mixed update");
@@ -2022,6 +2266,7 @@ int PcgSolver::solve_mixed(PcgStats* st) {
   k_fill<double><<<grid, kThreads, 0, s>>>(g_.total, xacc_, 0.0);
   launches_ += 2;
   PcgScalars init{};
+  init.spin_limit = spin_limit();
   init.tol = 0.0;
   init.max_iter = 1;
   init.criterion = CRIT_REL_L2;
@@ -2124,6 +2369,7 @@ int PcgSolver::precond_only(const double* r, double* z) {
   if (e) return e;
   k_to_tiled<double, double><<<grid, kThreads, 0, s>>>(g_, r, d64_.r, nullptr);
   PcgScalars init{};
+  init.spin_limit = spin_limit();
   init.done = DONE_RUNNING;
   init.first = 1;
   cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
@@ -2160,6 +2406,7 @@ int PcgSolver::time_kernels(int reps, double* ms) {
   const int grid = grid_for(g_.total, ctx_->sm_count);
   // a benign state: r = rhs, s = r, scalars running with a tiny alpha/beta
   PcgScalars init{};
+  init.spin_limit = spin_limit();
   init.done = DONE_RUNNING;
   init.first = 1;
   init.max_iter = 1 << 30;
@@ -2185,10 +2432,10 @@ int PcgSolver::time_kernels(int reps, double* ms) {
     const int wg = is32 ? wave_grid32_ : wave_grid64_;
     switch (which) {
       case 1:
-        launch_wave<T, true>(wave_args(is32, 0, FIN_NONE), FwdOp<T>{{A.r, A.cL, A.cD, A.cB, A.E}, A.q}, s, wg);
+        this->template launch_sweep<T, true>(wave_args(is32, 0, FIN_NONE), FwdOp<T>{{A.r, A.cL, A.cD, A.cB, A.E}, A.q}, s, wg);
         break;
       case 2:
-        launch_wave<T, false>(wave_args(is32, 0, FIN_NONE), BwdOp<T>{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z},
+        this->template launch_sweep<T, false>(wave_args(is32, 0, FIN_NONE), BwdOp<T>{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z},
                               s, wg);
         break;
       case 3:
@@ -2202,12 +2449,12 @@ int PcgSolver::time_kernels(int reps, double* ms) {
         break;
       case 6:
         if constexpr (sizeof(T) == 4)
-          launch_wave<T, false>(wave_args(true, 0, FIN_NONE),
+          this->template launch_sweep<T, false>(wave_args(true, 0, FIN_NONE),
                                 BwdEisenstatOp<T>{{A.q, A.s, A.E, A.uR, A.uU, A.uF}, A.z, A.s, T(0)}, s, wg);
         break;
       case 7:
         if constexpr (sizeof(T) == 4)
-          launch_wave<T, true>(wave_args(true, 0, FIN_NONE),
+          this->template launch_sweep<T, true>(wave_args(true, 0, FIN_NONE),
                                FwdEisenstatOp<T>{{A.s, A.z, A.Pinv, A.Dt, A.cL, A.cD, A.cB, A.E}, A.Az}, s, wg);
         break;
     }
@@ -2409,7 +2656,6 @@ int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int n
   wa.tile_partials = tile_partials;
   wa.use_skip = 0;
   wa.fin_kind = FIN_NONE;
-  wa.spin_limit = kSpinLimit;
   const int wgrid = std::min(ntiles, sm_count);
   k_pivot_diag<<<grid, kThreads, 0, st>>>(g, t_adiag, t_al, t_ad, t_ab, act, tau, t_q, t_uR, t_uU,
                                           t_uF);

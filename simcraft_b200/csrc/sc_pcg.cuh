@@ -74,7 +74,7 @@ struct PcgScalars {
   unsigned err;
   unsigned count;  // last-block counter
   int first;       // 1 until the first preconditioner application has set sigma
-  int pad;
+  int spin_limit;  // polls before a sweep's wait gives up (0: the default bound)
 };
 
 struct PcgScalars;
@@ -92,7 +92,9 @@ struct WaveArgs {
   double* tile_partials;  // per tile share of the sweep's dot product
   int use_skip;
   int fin_kind;
-  int spin_limit;  // polls before a mailbox wait gives up (the control warp waits 4x as long)
+  // Nothing more: growing this parameter block past its 128 bytes measured the
+  // sweeps ~30% slower.  The wait bound travels in PcgScalars::spin_limit, and a
+  // cluster launch passes its cluster-tile order through `order`.
 };
 
 // Wavefront scheduling state (one per sweep kernel; reset by the kernel's last CTA).
@@ -169,7 +171,13 @@ class PcgSolver {
   // drop the pivots, so the next solve starts from a clean state.
   int recover_after_timeout();
   int spin_limit() const;
-  int graph_limit_ = 0;  // spin limit baked into the captured graphs
+  int pivot_limit_ = 0;  // host copy of the bound uploaded for the pivot sweep
+  // FP32 sweeps in thread-block clusters of cl_size_ CTAs along y (0: none),
+  // cl_grid_ clusters; the cluster tile order (anti-diagonals of (X, Yc))
+  int cl_size_ = 0, cl_grid_ = 0;
+  int2* order_cl_ = nullptr;
+  template <class T, bool FWD, class Op>
+  void launch_sweep(const WaveArgs& a, const Op& op, cudaStream_t st, int grid);
   int ensure_host_stage();
   double* hstage_ = nullptr;     // staging of the host-array entry points (N doubles)
   uint8_t* hstage_act_ = nullptr;  // and of the active flags (N bytes)

@@ -7,7 +7,7 @@ reference source.  The library keeps the same tables in its own packed form
 header and compares its digests with these, so the transcription is pinned to
 the reference without a second copy of the tables in the repository.
 
-Run (needs the reference source tree): python tests/golden/make_mc_table_pin.py [reference_root]
+Run (needs the reference source tree): python tests/golden/make_mc_table_pin.py REFERENCE_ROOT
 """
 import json
 import os
@@ -15,7 +15,6 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 
 
 def _initializer(src, name):
@@ -52,8 +51,8 @@ def digests(cases, corners, edges):
     }
 
 
-def main():
-    path = os.path.join(REF, "FluidSim", "src", "cpu", "rebuild-surface.cc")
+def main(ref_root):
+    path = os.path.join(ref_root, "FluidSim", "src", "cpu", "rebuild-surface.cc")
     src = re.sub(r"//[^\n]*", "", open(path).read())
     vo = _ints(_initializer(src, "vertexOffset ="))
     ec = _ints(_initializer(src, "edgeConnection["))
@@ -71,4 +70,6 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_mc_table_pin.py REFERENCE_ROOT (the SimCraft source tree)")
+    main(sys.argv[1])

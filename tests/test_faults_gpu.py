@@ -166,11 +166,22 @@ def test_wavefront_wait_timeout_is_reported_and_the_solver_recovers(oracle, gpu)
     precisions and through the preconditioner entry point, nothing faults, and
     with the default bound back the same handles solve again, bit for bit as a
     fresh solver does."""
+    _timeout_round_trip(oracle, (64, 32, 48))  # 2 x 4 column tiles: mailbox hand-offs
+
+
+def test_wavefront_wait_timeout_in_cluster_sweeps(oracle, gpu):
+    """The same on a grid whose FP32 sweeps run in thread-block clusters (9 tile
+    rows: a cluster of 8 and a partial one, 40% fluid): a ring wait, a mailbox wait or the
+    backpressure wait gives up, the solve reports SC_ERR_TIMEOUT, and the handle
+    solves again bit for bit."""
+    _timeout_round_trip(oracle, (72, 72, 40), precond=False)
+
+
+def _timeout_round_trip(oracle, dims, precond=True):
     import torch
     from simcraft_b200._capi import CapiError
     from simcraft_b200.solver import CgSolver3D, Context, CRIT_REL_L2, PREC_FP64, PREC_MIXED
 
-    dims = (64, 32, 48)  # 2 x 4 column tiles: every sweep hands values between tiles
     S = poisson_system(oracle, 0, dims=dims, seed=6)
     ctx = Context(0)
     fresh = {}
@@ -192,6 +203,8 @@ def test_wavefront_wait_timeout_is_reported_and_the_solver_recovers(oracle, gpu)
             s.solve(S["adiag"], S["an"], S["rhs"], S["active"], pg)
             assert s.last_stats["status"] == SC_DONE_CONVERGED
             np.testing.assert_array_equal(pg, fresh[prec])
+    if not precond:
+        return
     # the preconditioner entry point
     s = CgSolver3D(*dims, context=ctx)
     s.upload(S["adiag"], S["an"], S["rhs"], S["active"])

@@ -174,3 +174,32 @@ def test_config2_128_sphere_pool(oracle, torch_mod):
         m.solve(S["adiag"], S["an"], rhs, S["active"], pm)
         assert m.last_stats["status"] == 1 and m.last_stats["true_rel_l2"] < tol, m.last_stats
         assert rel_l2(pm, p12, a) < bound, (tol, rel_l2(pm, p12, a))
+
+
+# nx >= ny throughout: the reference's buildSystem bounds its up faces by the
+# width (project-solver.cc:186), which leaves nx < ny systems asymmetric
+@pytest.mark.parametrize("dims", [(64, 64, 40), (72, 72, 40), (128, 128, 24), (136, 136, 20)])
+def test_pcg_mixed_cluster_sweeps(oracle, torch_mod, dims):
+    """Grids whose column tiles fill thread-block clusters along y (tiles of 8
+    rows: ny = 64 fills one cluster of 8, 72 gives a cluster of 8 and a partial
+    one, 128 fills one of 16, 136 leaves CTAs of its second cluster of 16
+    without a tile), so the FP32 sweeps of the mixed solve hand their y
+    boundary rows through distributed shared memory: both inner iterations meet
+    the FP64 stopping test and agree with the oracle's solution."""
+    from simcraft_b200.solver import CgSolver3D, INNER_EISENSTAT, INNER_PCG, PREC_MIXED
+    S = poisson_system(oracle, 0, dims=dims, seed=6)
+    assert S["active"].mean() > 0.1
+    p_ref, _, _ = oracle.pcg_solve(S["adiag"], S["an"], S["rhs"], S["active"], tol=1e-13, max_iter=3000,
+                                   criterion=1)
+    a = S["active"].astype(bool)
+    for meth in (INNER_EISENSTAT, INNER_PCG):
+        s = CgSolver3D(*dims, tol=1e-10, max_iter=3000, criterion=1, precision=PREC_MIXED, inner_method=meth)
+        pg = np.zeros(dims)
+        s.solve(S["adiag"], S["an"], S["rhs"], S["active"], pg)
+        st = s.last_stats
+        assert st["status"] == 1 and st["true_rel_l2"] < 1e-10, (meth, st)
+        assert rel_l2(pg, p_ref, a) < 1e-8
+        # the solve is deterministic: the same handle solves again bit for bit
+        pg2 = np.zeros(dims)
+        s.solve(S["adiag"], S["an"], S["rhs"], S["active"], pg2)
+        np.testing.assert_array_equal(pg, pg2)

@@ -345,6 +345,24 @@ def large_solve_leg(args, dev, ctx, replicas, cpu=False):
         ms = replicas.max(e0.elapsed_time(e1)) / max(1, args.large_steps)
         out[name] = {"ms_per_solve": ms, "iterations": st.iterations, "iterations_per_s": st.iterations / (ms * 1e-3),
                      "outer": st.outer, "true_rel_l2": st.true_rel_l2, "kernel_launches": st.kernel_launches}
+        # per-kernel device times on this system (sc_pcg_time_kernels) and the
+        # algorithmic bandwidth of each: FP64 SpMV N(6s+1), axpy N(6s), scale-add
+        # N(3s), sweeps N(6s+1) / N(7s+1); FP32 Eisenstat sweeps N*8*4 / N*9*4
+        kt = (ctypes.c_double * 8)()
+        _capi.check("sc_pcg_time_kernels", L.sc_pcg_time_kernels(s.handle, 5, kt), ctx.handle)
+        km = list(kt)
+        N = n * n * n
+        gbs = lambda b, t: b / (t * 1e-3) / 1e9 if t > 0 else None
+        if name == "fp64":
+            out[name]["kernel_ms"] = {"forward_sweep": km[1], "backward_sweep": km[2], "spmv": km[3], "axpy": km[4],
+                                      "scale_add": km[5]}
+            out[name]["kernel_gbs"] = {"forward_sweep": gbs(N * 49, km[1]), "backward_sweep": gbs(N * 57, km[2]),
+                                       "spmv": gbs(N * 49, km[3]), "axpy": gbs(N * 48, km[4]),
+                                       "scale_add": gbs(N * 24, km[5])}
+        else:
+            out[name]["kernel_ms"] = {"eisenstat_backward_sweep": km[6], "eisenstat_forward_sweep": km[7], "axpy": km[4]}
+            out[name]["kernel_gbs"] = {"eisenstat_backward_sweep": gbs(N * 32, km[6]),
+                                       "eisenstat_forward_sweep": gbs(N * 36, km[7]), "axpy": gbs(N * 24, km[4])}
         if name == "fp64":
             pg64 = pg.clone()
         else:
@@ -606,7 +624,7 @@ def diff_leg(args, ctx, replicas):
     from simcraft_b200.diff import DiffFlip, control_scene, faces_from_cells
     from simcraft_b200.replicas import fd_check
 
-    n, steps = DIFF_N, DIFF_STEPS
+    n, steps = args.diff_n, DIFF_STEPS
     pos, param, target, h = control_scene(n)
     U = faces_from_cells(torch.from_numpy(param).cuda())
     out = {"workload": f"differentiable FLIP control {n}^3, fluid y<0.25, {len(pos)} particles, "
@@ -728,6 +746,7 @@ def main():
     ap.add_argument("--flip32", type=int, default=1, help="32^3 FP64 dam-break leg (0 skips)")
     ap.add_argument("--surface", type=int, default=1,
                     help="marching-cubes export of the FLIP leg's fluid (0 skips)")
+    ap.add_argument("--diff-n", type=int, default=DIFF_N, help="grid of the differentiable leg (profiling runs)")
     ap.add_argument("--diff-dirs", type=int, default=16,
                     help="finite-difference directions of the differentiable leg (-1 skips the leg)")
     args = ap.parse_args()

@@ -1191,8 +1191,9 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
   T* mbx = reinterpret_cast<T*>(a.mbx);
   T* mby = reinterpret_cast<T*>(a.mby);
   double acc = 0.0;
-  // a cluster launch takes tickets for cluster tiles: ntx columns of ceil(nty/CL)
-  const int nticket = CLU ? g.ntx * ((g.nty + (CLU ? CL : 1) - 1) / (CLU ? CL : 1)) : ntiles;
+  // the tickets: entries of the order list (tiles, or cluster tiles of CL
+  // tiles along y), whose length sits in the header entry before the first
+  const int nticket = a.order[-1].x;
   for (;;) {
     if constexpr (CLU) {
       if (threadIdx.x == 0) {
@@ -1219,28 +1220,29 @@ __global__ void __launch_bounds__((TY + 3) * 32, 1) k_wave(const WaveArgs a, con
     }
     const int t = sh.tile;
     if (t >= nticket) break;
-    int X, Y;
-    if constexpr (CLU) {
-      const int2 XY = a.order[FWD ? t : nticket - 1 - t];
-      X = XY.x;
-      Y = XY.y * CL + rank;
-    } else {
-      const int2 XY = a.order[FWD ? t : ntiles - 1 - t];
-      X = XY.x;
-      Y = XY.y;
-    }
+    // entry: x = X | neighbour bits << 16, y = the tile row (cluster tile row);
+    // bit 0/1: the unit at X - 1 / X + 1 is swept, bit 2/3: the unit below /
+    // above.  A unit that is not swept (no active cell) holds zeros and has
+    // zero couplings to this one, so its boundary values are zeros.
+    const int2 XY = a.order[FWD ? t : nticket - 1 - t];
+    const int X = XY.x & 0xffff, nb = XY.x >> 16;
+    const int Y = CLU ? XY.y * CL + rank : XY.y;
     // a cluster tile at the top edge can have CTAs without a tile
     if (Y < g.nty) {
     const int tid = Y * g.ntx + X;
-    const bool hasX = FWD ? (X > 0) : (X < g.ntx - 1);
-    const bool hasY = FWD ? (Y > 0) : (Y < g.nty - 1);
+    // producers within this cluster tile (along y, through the rings), and
+    // consumers within it
+    const bool inner_in = CLU && (FWD ? rank > 0 : rank < CL - 1);
+    const bool inner_out = CLU && (FWD ? rank < CL - 1 : rank > 0);
+    const bool hasX = FWD ? (nb & 1) : (nb & 2);
+    const bool hasY = (FWD ? Y > 0 : Y < g.nty - 1) && (inner_in || (FWD ? (nb & 4) : (nb & 8)));
     // consumers of this tile's boundary values
-    const bool outX = FWD ? (X < g.ntx - 1) : (X > 0);
-    const bool outY = FWD ? (Y < g.nty - 1) : (Y > 0);
+    const bool outX = FWD ? (nb & 2) : (nb & 1);
+    const bool outY = (FWD ? Y < g.nty - 1 : Y > 0) && (inner_out || (FWD ? (nb & 8) : (nb & 4)));
     const int cX = FWD ? tid + 1 : tid - 1, cY = FWD ? tid + g.ntx : tid - g.ntx;
     // y boundary rows within a cluster travel through the rings
-    const bool ydin = CLU && hasY && (FWD ? rank > 0 : rank < CL - 1);
-    const bool ydout = CLU && outY && (FWD ? rank < CL - 1 : rank > 0);
+    const bool ydin = CLU && hasY && inner_in;
+    const bool ydout = CLU && outY && inner_out;
     const int64_t base = g.tile_base(X, Y);
     if (warp == TY) {
       // control warp: keeps the compute warps one step behind the rings; it
@@ -1564,6 +1566,96 @@ __global__ void k_mb_reset(int64_t n, T* mb) {
     mb_reset(mb + e);
 }
 
+// Per tile: 1 when any of its cells is active (one block per tile).
+__global__ void __launch_bounds__(kThreads) k_tile_activity(Tiled g, const uint8_t* __restrict__ act,
+                                                            uint8_t* __restrict__ tile_act) {
+  // tile_elems = 256 nz bytes, and each tile starts 256-byte aligned
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(act + (int64_t)blockIdx.x * g.tile_elems);
+  const int64_t nw = g.tile_elems / 4;
+  int any = 0;
+  for (int64_t i = threadIdx.x; i < nw; i += blockDim.x) any |= __ldg(w + i) != 0u;
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) tile_act[blockIdx.x] = any ? 1 : 0;
+}
+
+// The sweep order of the iterations: the entries of `all` (n units in
+// dependency order, tiles when CL == 0, else cluster tiles of CL tiles along
+// y) whose unit holds an active tile, in the same order, each with the bits
+// of its swept neighbours (x: X | bits << 16), and their count in the header
+// entry dst[-1].  The dot-product shares of tiles left out are set to zero
+// (nothing writes them while their unit is left out).  One block.
+__global__ void __launch_bounds__(1024) k_compact_order(int ntx, int nty, int CL, const uint8_t* __restrict__ tile_act,
+                                                        const int2* __restrict__ all, int n, int2* __restrict__ dst,
+                                                        double* __restrict__ tile_partials) {
+  __shared__ int wsum[32];
+  __shared__ int carry;
+  const int nyu = CL ? (nty + CL - 1) / CL : nty;
+  auto swept = [&](int X, int Yu) -> bool {
+    if (X < 0 || X >= ntx || Yu < 0 || Yu >= nyu) return false;
+    if (!CL) return tile_act[Yu * ntx + X] != 0;
+    for (int r = 0; r < CL; r++) {
+      const int Y = Yu * CL + r;
+      if (Y < nty && tile_act[Y * ntx + X]) return true;
+    }
+    return false;
+  };
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int b0 = 0; b0 < n; b0 += blockDim.x) {
+    const int i = b0 + threadIdx.x;
+    bool on = false;
+    int2 e = make_int2(0, 0);
+    if (i < n) {
+      const int X = all[i].x & 0xffff, Yu = all[i].y;
+      on = swept(X, Yu);
+      const int bits = (swept(X - 1, Yu) ? 1 : 0) | (swept(X + 1, Yu) ? 2 : 0) | (swept(X, Yu - 1) ? 4 : 0) |
+                       (swept(X, Yu + 1) ? 8 : 0);
+      e = make_int2(X | (bits << 16), Yu);
+      if (!on)
+        for (int r = 0; r < (CL ? CL : 1); r++) {
+          const int Y = CL ? Yu * CL + r : Yu;
+          if (Y < nty) tile_partials[Y * ntx + X] = 0.0;
+        }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, on);
+    if (lane == 0) wsum[warp] = __popc(m);
+    __syncthreads();
+    int before = carry;
+    for (int w = 0; w < warp; w++) before += wsum[w];
+    before += __popc(m & ((1u << lane) - 1u));
+    if (on) dst[before] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += wsum[w];
+      carry += t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) dst[-1] = make_int2(carry, 0);
+}
+
+// Writes a header entry (the count) followed by the units of an ntx x nyu
+// grid in anti-diagonal order, each with the bits of the neighbours that
+// exist, into `o` (ntx nyu + 1 entries).
+void all_units_order(int ntx, int nyu, int2* o) {
+  int n = 0;
+  o[n++] = make_int2(ntx * nyu, 0);
+  for (int d = 0; d <= ntx + nyu - 2; d++)
+    for (int X = 0; X < ntx; X++) {
+      const int Y = d - X;
+      if (Y < 0 || Y >= nyu) continue;
+      const int bits = (X > 0 ? 1 : 0) | (X < ntx - 1 ? 2 : 0) | (Y > 0 ? 4 : 0) | (Y < nyu - 1 ? 8 : 0);
+      o[n++] = make_int2(X | (bits << 16), Y);
+    }
+}
+std::vector<int2> all_units_order(int ntx, int nyu) {
+  std::vector<int2> o((size_t)ntx * nyu + 1);
+  all_units_order(ntx, nyu, o.data());
+  return o;
+}
+
 inline int grid_for(int64_t n, int sm) {
   int64_t b = (n + kThreads - 1) / kThreads;
   int64_t cap = (int64_t)sm * 4;
@@ -1604,7 +1696,7 @@ void PcgSolver::launch_sweep(const WaveArgs& a, const Op& op, cudaStream_t st, i
   if constexpr (sizeof(T) == 4) {
     if (cl_size_ > 0) {
       WaveArgs c = a;
-      c.order = order_cl_;
+      c.order = a.order == ws_.order_all ? order_cl_all_ : order_cl_;
       if (cl_size_ == 16)
         launch_wave_cl<T, FWD, Op, 16>(c, op, st, cl_grid_);
       else
@@ -1615,7 +1707,7 @@ void PcgSolver::launch_sweep(const WaveArgs& a, const Op& op, cudaStream_t st, i
   launch_wave<T, FWD>(a, op, st, grid);
 }
 
-WaveArgs PcgSolver::wave_args(bool f32, int use_skip, int fin) const {
+WaveArgs PcgSolver::wave_args(bool f32, int use_skip, int fin, bool all_tiles) const {
   WaveArgs w{};
   w.g = g_;
   w.mbx = f32 ? (void*)mbx32_ : (void*)mbx64_;
@@ -1624,7 +1716,7 @@ WaveArgs PcgSolver::wave_args(bool f32, int use_skip, int fin) const {
   w.mb_stride_y = mb_stride_y_;
   w.ticket = ws_.ticket;
   w.exits = ws_.exits;
-  w.order = ws_.order_fwd;
+  w.order = all_tiles ? ws_.order_all : ws_.order_fwd;
   w.sc = sc_;
   w.partials = partials_;
   w.tile_partials = tile_partials_;
@@ -1696,20 +1788,24 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
   sc_ = (PcgScalars*)alloc(sizeof(PcgScalars));
   ws_.ticket = (int*)alloc(sizeof(int) * 2);
   tile_partials_ = (double*)alloc(sizeof(double) * (size_t)ntiles);
-  int2* order = (int2*)alloc(sizeof(int2) * (size_t)ntiles);
+  tile_act_ = (uint8_t*)alloc((size_t)ntiles);
+  // order lists: a header entry (the count) and up to ntiles entries
+  int2* order_all = (int2*)alloc(sizeof(int2) * (size_t)(ntiles + 1));
+  int2* order = (int2*)alloc(sizeof(int2) * (size_t)(ntiles + 1));
   // mailboxes (FP64; the FP32 ones are allocated with the FP32 arrays)
   const int NS = nz + 31 + Tiled::TY - 1;
   mb_stride_x_ = (int64_t)NS * Tiled::TY;
   mb_stride_y_ = (int64_t)NS * 32;
   mbx64_ = (double*)alloc(sizeof(double) * (size_t)(mb_stride_x_ * ntiles));
   mby64_ = (double*)alloc(sizeof(double) * (size_t)(mb_stride_y_ * ntiles));
-  if (!active_ || !partials_ || !sc_ || !ws_.ticket || !order || !mbx64_ || !mby64_ ||
-      !tile_partials_) {
+  if (!active_ || !partials_ || !sc_ || !ws_.ticket || !order || !order_all || !mbx64_ || !mby64_ ||
+      !tile_partials_ || !tile_act_) {
     init_status_ = -3;
     return;
   }
   ws_.exits = ws_.ticket + 1;
-  ws_.order_fwd = order;
+  ws_.order_all = order_all + 1;
+  ws_.order_fwd = order + 1;
   cudaMemsetAsync(ws_.ticket, 0, sizeof(int) * 2, ctx->stream);
   for (double** a : arr64) cudaMemsetAsync(*a, 0, n64, ctx->stream);
   cudaMemsetAsync(active_, 0, (size_t)g_.total, ctx->stream);
@@ -1720,34 +1816,33 @@ PcgSolver::PcgSolver(Context* ctx, int nx, int ny, int nz, const PcgOptions& opt
   reset_mailboxes(false);
   // tile order: anti-diagonals of the tile grid, so every tile's forward
   // predecessors (X-1,Y), (X,Y-1) hold smaller tickets; reversed for backward.
-  std::vector<int2> ord;
-  ord.reserve(ntiles);
-  for (int d = 0; d <= g_.ntx + g_.nty - 2; d++)
-    for (int X = 0; X < g_.ntx; X++) {
-      int Y = d - X;
-      if (Y >= 0 && Y < g_.nty) ord.push_back(make_int2(X, Y));
-    }
-  cudaMemcpyAsync(order, ord.data(), sizeof(int2) * ord.size(), cudaMemcpyHostToDevice,
-                  ctx->stream);
+  // Until the first system selects its active tiles, both lists hold all.
+  std::vector<int2> ord = all_units_order(g_.ntx, g_.nty);
+  cudaMemcpyAsync(order_all, ord.data(), sizeof(int2) * ord.size(), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(order, ord.data(), sizeof(int2) * ord.size(), cudaMemcpyHostToDevice, ctx->stream);
   // FP32 sweeps in clusters of 16 (or 8) CTAs along y, when the tile rows fill
-  // such clusters, the GPU can run them, and the ring stamps hold the entries
+  // such clusters, the GPU can run all of them at once, and the ring stamps
+  // hold the entries.  A cluster holds its CTAs until its last tile ends, so
+  // when cluster tiles have to queue for free clusters (256^3 and up) the
+  // plain persistent grid is faster: with clusters of 16 the 512^3 mixed solve
+  // measured 2.93 s against 1.80 s without, each FP32 sweep 2.3 ms.
   if (NS < 4096) {
     for (int CL : {16, 8}) {
       if (g_.nty < CL) continue;
       const int n = CL == 16 ? fp32_max_clusters<16>() : fp32_max_clusters<8>();
       if (n < 1) continue;
       const int nyc = (g_.nty + CL - 1) / CL;
-      std::vector<int2> oc;
-      for (int d = 0; d <= g_.ntx + nyc - 2; d++)
-        for (int X = 0; X < g_.ntx; X++) {
-          const int Yc = d - X;
-          if (Yc >= 0 && Yc < nyc) oc.push_back(make_int2(X, Yc));
-        }
-      order_cl_ = (int2*)alloc(sizeof(int2) * oc.size());
-      if (!order_cl_) break;
-      cudaMemcpyAsync(order_cl_, oc.data(), sizeof(int2) * oc.size(), cudaMemcpyHostToDevice, ctx->stream);
+      if (g_.ntx * nyc > n) continue;
+      std::vector<int2> oc = all_units_order(g_.ntx, nyc);
+      int2* ca = (int2*)alloc(sizeof(int2) * oc.size());
+      int2* cc = (int2*)alloc(sizeof(int2) * oc.size());
+      if (!ca || !cc) break;
+      cudaMemcpyAsync(ca, oc.data(), sizeof(int2) * oc.size(), cudaMemcpyHostToDevice, ctx->stream);
+      cudaMemcpyAsync(cc, oc.data(), sizeof(int2) * oc.size(), cudaMemcpyHostToDevice, ctx->stream);
+      order_cl_all_ = ca + 1;
+      order_cl_ = cc + 1;
       cl_size_ = CL;
-      cl_grid_ = std::min(n, (int)oc.size());
+      cl_grid_ = std::min(n, g_.ntx * nyc);
       break;
     }
   }
@@ -1907,7 +2002,7 @@ int PcgSolver::ensure_pivots() {
   if (pivots_valid_) return 0;
   cudaStream_t st = ctx_->stream;
   const int grid = grid_for(g_.total, ctx_->sm_count);
-  WaveArgs wa = wave_args(false, 0, FIN_NONE);
+  WaveArgs wa = wave_args(false, 0, FIN_NONE, true);
   // the pivot sweep reports a timeout through the status word: start it clean,
   // with this context's wait bound
   cudaMemsetAsync(&sc_->err, 0, sizeof(unsigned), st);
@@ -1971,10 +2066,35 @@ int PcgSolver::ensure_pivots() {
     k_eisenstat_diag<<<grid, kThreads, 0, st>>>(g_.total, d64_.E, d64_.adiag, d32_.Pinv, d32_.Dt);
     launches_ += 12;
   }
+  select_active_tiles();
   int e = check_dev_error("pivots");
   if (e) return e;
   pivots_valid_ = true;
   return 0;
+}
+
+// The tiles the iteration sweeps visit: those with an active cell (with
+// clusters: the cluster tiles holding one).  A tile left out is never written
+// by a sweep, so the vectors the iterations carry start at zero everywhere;
+// on a tile without an active cell they then stay zero, as a sweep over it
+// would leave them (its pivots and couplings are zero).
+void PcgSolver::select_active_tiles() {
+  cudaStream_t st = ctx_->stream;
+  const int ntiles = g_.ntiles();
+  k_tile_activity<<<ntiles, kThreads, 0, st>>>(g_, active_, tile_act_);
+  k_compact_order<<<1, 1024, 0, st>>>(g_.ntx, g_.nty, 0, tile_act_, ws_.order_all, ntiles, ws_.order_fwd,
+                                      tile_partials_);
+  launches_ += 2;
+  if (cl_size_ > 0) {
+    const int nyc = (g_.nty + cl_size_ - 1) / cl_size_;
+    k_compact_order<<<1, 1024, 0, st>>>(g_.ntx, g_.nty, cl_size_, tile_act_, order_cl_all_, g_.ntx * nyc,
+                                        order_cl_, tile_partials_);
+    launches_ += 1;
+  }
+  const size_t n64 = sizeof(double) * (size_t)g_.total, n32 = sizeof(float) * (size_t)g_.total;
+  for (double* v : {d64_.r, d64_.p, d64_.z, d64_.s, d64_.q, d64_.Az}) cudaMemsetAsync(v, 0, n64, st);
+  if (have_f32_)
+    for (float* v : {d32_.r, d32_.p, d32_.z, d32_.s, d32_.q, d32_.Az}) cudaMemsetAsync(v, 0, n32, st);
 }
 
 template <class T>
@@ -2467,7 +2587,7 @@ int PcgSolver::time_kernels(int reps, double* ms) {
     for (int i = 0; i < reps; i++) {
       switch (which) {
         case 0: {
-          WaveArgs wa = wave_args(false, 0, FIN_NONE);
+          WaveArgs wa = wave_args(false, 0, FIN_NONE, true);
           PivotOp op{{d64_.q, d64_.al, d64_.ad, d64_.ab, d64_.uR, d64_.uU, d64_.uF},
                      opt_.sigma, d64_.E, d64_.cL, d64_.cD, d64_.cB};
           // the diag terms live in uR/uU/uF only until k_upper; rebuild them
@@ -2537,7 +2657,7 @@ constexpr size_t kNaActBytes = na_align(kNoAllocMaxTiled);
 constexpr size_t kNaMbxBytes = na_align(sizeof(double) * kNoAllocMaxTiles * kNoAllocMaxNS * Tiled::TY);
 constexpr size_t kNaMbyBytes = na_align(sizeof(double) * kNoAllocMaxTiles * kNoAllocMaxNS * 32);
 constexpr size_t kNaSmallBytes =
-    na_align(sizeof(double) * kNoAllocMaxTiles + sizeof(int) * 2 + sizeof(int2) * kNoAllocMaxTiles) +
+    na_align(sizeof(double) * kNoAllocMaxTiles + sizeof(int) * 2 + sizeof(int2) * (kNoAllocMaxTiles + 1)) +
     na_align(sizeof(PcgScalars));
 constexpr size_t kNoAllocBytes =
     kNaArrBytes * kNoAllocArrays + kNaActBytes + kNaMbxBytes + kNaMbyBytes + kNaSmallBytes;
@@ -2595,9 +2715,9 @@ int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int n
   q += kNaMbyBytes;
   double* tile_partials = (double*)q;
   int* ticket = (int*)(tile_partials + kNoAllocMaxTiles);
-  int2* order = (int2*)(ticket + 2);
+  int2* order = (int2*)(ticket + 2);  // header entry, then the tiles
   PcgScalars* scal = (PcgScalars*)(q + na_align(sizeof(double) * kNoAllocMaxTiles + sizeof(int) * 2 +
-                                                sizeof(int2) * kNoAllocMaxTiles));
+                                                sizeof(int2) * (kNoAllocMaxTiles + 1)));
   double *t_adiag = arr[0], *t_al = arr[1], *t_ad = arr[2], *t_ab = arr[3], *t_E = arr[4],
          *t_cL = arr[5], *t_cD = arr[6], *t_cB = arr[7], *t_uR = arr[8], *t_uU = arr[9],
          *t_uF = arr[10], *t_r = arr[11], *t_q = arr[12], *t_z = arr[13];
@@ -2620,14 +2740,11 @@ int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int n
   k_mb_reset<double><<<rgrid, kThreads, 0, st>>>(sx * ntiles, mbx);
   k_mb_reset<double><<<rgrid, kThreads, 0, st>>>(sy * ntiles, mby);
   if (failed(cudaGetLastError(), "resetting the mailboxes")) return -2;
-  int2 ord[kNoAllocMaxTiles];
-  int no = 0;
-  for (int d = 0; d <= g.ntx + g.nty - 2; d++)
-    for (int X = 0; X < g.ntx; X++) {
-      int Y = d - X;
-      if (Y >= 0 && Y < g.nty) ord[no++] = make_int2(X, Y);
-    }
-  if (failed(cudaMemcpyAsync(order, ord, sizeof(int2) * no, cudaMemcpyHostToDevice, st), "uploading the tile order"))
+  // every tile is swept (the order of all tiles, its count in the header)
+  int2 ord[kNoAllocMaxTiles + 1];
+  all_units_order(g.ntx, g.nty, ord);
+  if (failed(cudaMemcpyAsync(order, ord, sizeof(int2) * (ntiles + 1), cudaMemcpyHostToDevice, st),
+             "uploading the tile order"))
     return -2;
   // system and right-hand side into the tiled layout, then the entries the
   // reference never reads (couplings to inactive cells, inactive rows) cleared
@@ -2650,7 +2767,7 @@ int mic_precond_noalloc(cudaStream_t st, int device, int sm_count, int nx, int n
   wa.mb_stride_y = sy;
   wa.ticket = ticket;
   wa.exits = ticket + 1;
-  wa.order = order;
+  wa.order = order + 1;
   wa.sc = scal;
   wa.partials = tile_partials;
   wa.tile_partials = tile_partials;

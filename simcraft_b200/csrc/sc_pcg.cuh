@@ -93,15 +93,19 @@ struct WaveArgs {
   int use_skip;
   int fin_kind;
   // Nothing more: growing this parameter block past its 128 bytes measured the
-  // sweeps ~30% slower.  The wait bound travels in PcgScalars::spin_limit, and a
-  // cluster launch passes its cluster-tile order through `order`.
+  // sweeps ~30% slower.  The wait bound travels in PcgScalars::spin_limit, a
+  // cluster launch passes its cluster-tile order through `order`, and the
+  // order's length sits in the header entry order[-1].x.
 };
 
 // Wavefront scheduling state (one per sweep kernel; reset by the kernel's last CTA).
 struct WaveSync {
   int* ticket;        // next tile ticket
   int* exits;         // CTAs that found no more tiles
-  int2* order_fwd;    // ticket -> tile (X,Y) for forward sweeps
+  // ticket -> tile for forward sweeps, entries after a header entry holding
+  // their count: every tile (pivot sweep), and the tiles with an active cell
+  int2* order_all;
+  int2* order_fwd;
 };
 
 template <class T>
@@ -175,7 +179,12 @@ class PcgSolver {
   // FP32 sweeps in thread-block clusters of cl_size_ CTAs along y (0: none),
   // cl_grid_ clusters; the cluster tile order (anti-diagonals of (X, Yc))
   int cl_size_ = 0, cl_grid_ = 0;
-  int2* order_cl_ = nullptr;
+  int2* order_cl_all_ = nullptr;  // every cluster tile (header + entries)
+  int2* order_cl_ = nullptr;      // the cluster tiles with an active cell
+  // Per tile: any active cell (set with the pivots); the sweeps of the
+  // iterations visit only those tiles (or cluster tiles holding one).
+  uint8_t* tile_act_ = nullptr;
+  void select_active_tiles();
   template <class T, bool FWD, class Op>
   void launch_sweep(const WaveArgs& a, const Op& op, cudaStream_t st, int grid);
   int ensure_host_stage();
@@ -206,7 +215,8 @@ class PcgSolver {
   float *mbx32_ = nullptr, *mby32_ = nullptr;
   int64_t mb_stride_x_ = 0, mb_stride_y_ = 0;
   void reset_mailboxes(bool f32);
-  WaveArgs wave_args(bool f32, int use_skip, int fin) const;
+  // all_tiles: sweep every tile (the pivot sweep), else the active ones
+  WaveArgs wave_args(bool f32, int use_skip, int fin, bool all_tiles = false) const;
   std::vector<void*> allocs_;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;    // chunk polling
   cudaEvent_t evt0_ = nullptr, evt1_ = nullptr;  // solve timing

@@ -313,12 +313,29 @@ __global__ void __launch_bounds__(kThreads) k_init(Tiled g, const double* __rest
   reduce_finalize(s2, mx, partials, sc, fin);
 }
 
+// The iteration kernels below visit only the tiles of a sweep order list
+// (tiles[-1].x entries; the tiles holding an active cell): the vectors they
+// update are zero on every other tile and stay so.  Work unit: one slot of a
+// tile, its TY x 32 = 256 consecutive elements, one per thread of the block.
+static_assert(Tiled::TY * 32 == kThreads, "a tile slot is one element per thread");
+__device__ __forceinline__ int slot_count(const Tiled& g, const int2* __restrict__ tiles) {
+  return tiles[-1].x * g.nz;
+}
+__device__ __forceinline__ int64_t slot_elem(const Tiled& g, const int2* __restrict__ tiles, int c) {
+  const int t = c / g.nz, sl = c - t * g.nz;
+  const int2 XY = tiles[t];
+  return ((int64_t)(XY.y * g.ntx + (XY.x & 0xffff)) * g.nz + sl) * kThreads + threadIdx.x;
+}
+
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_copy(int64_t n, const T* __restrict__ a,
+__global__ void __launch_bounds__(kThreads) k_copy(Tiled g, const int2* __restrict__ tiles, const T* __restrict__ a,
                                                    T* __restrict__ b, const PcgScalars* sc) {
   if (sc->done != DONE_RUNNING) return;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) b[e] = a[e];
+  const int nch = slot_count(g, tiles);
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int64_t e = slot_elem(g, tiles, c);
+    b[e] = a[e];
+  }
 }
 
 // applyCompressedMatrix (project-solver.cc:16-39) on the tiled layout.  The
@@ -432,17 +449,20 @@ __global__ void __launch_bounds__(kThreads)
 // TY row warps of one tile over a run of consecutive slots.
 template <class T>
 __global__ void __launch_bounds__(kThreads, 4)
-    k_spmv_stream(Tiled g, const T* __restrict__ adiag, const T* __restrict__ al, const T* __restrict__ ad,
-                  const T* __restrict__ ab, const uint8_t* __restrict__ act, const T* __restrict__ x,
-                  T* __restrict__ y, double* partials, PcgScalars* sc, int use_skip, int chunks) {
+    k_spmv_stream(Tiled g, const int2* __restrict__ tiles, const T* __restrict__ adiag, const T* __restrict__ al,
+                  const T* __restrict__ ad, const T* __restrict__ ab, const uint8_t* __restrict__ act,
+                  const T* __restrict__ x, T* __restrict__ y, double* partials, PcgScalars* sc, int use_skip,
+                  int chunks) {
   if (use_skip && sc->done != DONE_RUNNING) return;
   constexpr int TY = Tiled::TY, RS = Tiled::TY * 32;  // elements per slot of a tile
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int nz = g.nz;
   double acc = 0.0;
-  const int items = g.ntiles() * chunks;
+  // the listed tiles (those with an active cell; y stays zero on the others)
+  const int items = tiles[-1].x * chunks;
   for (int it = blockIdx.x; it < items; it += gridDim.x) {
-    const int tile = it / chunks, ch = it - tile * chunks;
+    const int li = it / chunks, ch = it - li * chunks;
+    const int tile = tiles[li].y * g.ntx + (tiles[li].x & 0xffff);
     const int s0 = (int)((int64_t)nz * ch / chunks), s1 = (int)((int64_t)nz * (ch + 1) / chunks);
     const int Y = tile / g.ntx, X = tile - Y * g.ntx;
     const int xg = X * 32 + tx, yg = Y * TY + ty;
@@ -558,19 +578,22 @@ __global__ void __launch_bounds__(kThreads)
 // are the plain updates here; four independent elements per thread per pass.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-    k_axpy(int64_t n, const uint8_t* __restrict__, const T* __restrict__ s,
+    k_axpy(Tiled g, const int2* __restrict__ tiles, const T* __restrict__ s,
            const T* __restrict__ Az, T* __restrict__ p, T* __restrict__ r, double* partials,
            PcgScalars* sc, int fin = FIN_AXPY) {
   if (sc->done != DONE_RUNNING) return;
   const T alpha = (T)sc->alpha;
   double s2 = 0.0, mx = 0.0;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += 4 * stride) {
+  const int nch = slot_count(g, tiles);
+  for (int c0 = blockIdx.x; c0 < nch; c0 += 4 * gridDim.x) {
     T sv[4], av[4], pv[4], rv[4];
+    int64_t ee[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      const int64_t e = e0 + k * stride;
-      const bool in = e < n;
+      const int c = c0 + k * (int)gridDim.x;
+      const bool in = c < nch;
+      const int64_t e = in ? slot_elem(g, tiles, c) : 0;
+      ee[k] = in ? e : -1;
       sv[k] = in ? s[e] : T(0);
       av[k] = in ? Az[e] : T(0);
       pv[k] = in ? p[e] : T(0);
@@ -578,8 +601,8 @@ __global__ void __launch_bounds__(kThreads)
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      const int64_t e = e0 + k * stride;
-      if (e >= n) continue;
+      const int64_t e = ee[k];
+      if (e < 0) continue;
       p[e] = pv[k] + alpha * sv[k];
       const T rn = rv[k] + (-alpha) * av[k];
       r[e] = rn;
@@ -595,24 +618,26 @@ __global__ void __launch_bounds__(kThreads)
 // on inactive cells.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-    k_sa(int64_t n, const uint8_t* __restrict__, const T* __restrict__ z, T* __restrict__ s,
+    k_sa(Tiled g, const int2* __restrict__ tiles, const T* __restrict__ z, T* __restrict__ s,
          double* partials, PcgScalars* sc) {
   if (sc->done != DONE_RUNNING) return;
   const T beta = (T)sc->beta;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += 4 * stride) {
+  const int nch = slot_count(g, tiles);
+  for (int c0 = blockIdx.x; c0 < nch; c0 += 4 * gridDim.x) {
     T zv[4], sv[4];
+    int64_t ee[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      const int64_t e = e0 + k * stride;
-      zv[k] = e < n ? z[e] : T(0);
-      sv[k] = e < n ? s[e] : T(0);
+      const int c = c0 + k * (int)gridDim.x;
+      const bool in = c < nch;
+      const int64_t e = in ? slot_elem(g, tiles, c) : 0;
+      ee[k] = in ? e : -1;
+      zv[k] = in ? z[e] : T(0);
+      sv[k] = in ? s[e] : T(0);
     }
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const int64_t e = e0 + k * stride;
-      if (e < n) s[e] = zv[k] + beta * sv[k];
-    }
+    for (int k = 0; k < 4; k++)
+      if (ee[k] >= 0) s[ee[k]] = zv[k] + beta * sv[k];
   }
   reduce_finalize(0.0, 0.0, partials, sc, FIN_SA);
 }
@@ -2103,7 +2128,7 @@ void PcgSolver::launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip) {
   const int ntiles = g_.ntiles();
   const int chunks = std::max(1, std::min((1024 + ntiles - 1) / ntiles, g_.nz / 16));
   const int grid = std::min(nblocks_, ntiles * chunks);
-  k_spmv_stream<T><<<grid, kThreads, 0, st>>>(g_, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az, partials_, sc_,
+  k_spmv_stream<T><<<grid, kThreads, 0, st>>>(g_, ws_.order_fwd, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az, partials_, sc_,
                                               use_skip, chunks);
 }
 
@@ -2122,7 +2147,7 @@ void PcgSolver::launch_iteration(SysArrays<T>& A, bool eis) {
       FwdEisenstatOp<T> fo{{A.s, A.z, A.Pinv, A.Dt, A.cL, A.cD, A.cB, A.E}, A.Az};
       launch_sweep<T, true>(wave_args(true, 1, FIN_SPMV), fo, st, wg);  // alpha = rho / s.w
       // x += alpha t ; rh -= alpha w ; beta = rho_new / rho
-      k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.Az, A.p, A.q, partials_, sc_,
+      k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_, ws_.order_fwd, A.z, A.Az, A.p, A.q, partials_, sc_,
                                                FIN_EAXPY);
       return;
     }
@@ -2130,12 +2155,12 @@ void PcgSolver::launch_iteration(SysArrays<T>& A, bool eis) {
   WaveArgs wf = wave_args(f32, 1, FIN_NONE);
   WaveArgs wb = wave_args(f32, 1, FIN_BWD);
   launch_spmv<T>(A, st, 1);
-  k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.s, A.Az, A.p, A.r, partials_, sc_);
+  k_axpy<T><<<nblocks_, kThreads, 0, st>>>(g_, ws_.order_fwd, A.s, A.Az, A.p, A.r, partials_, sc_);
   FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
   launch_sweep<T, true>(wf, fo, st, wg);
   BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
   launch_sweep<T, false>(wb, bo, st, wg);
-  k_sa<T><<<nblocks_, kThreads, 0, st>>>(g_.total, active_, A.z, A.s, partials_, sc_);
+  k_sa<T><<<nblocks_, kThreads, 0, st>>>(g_, ws_.order_fwd, A.z, A.s, partials_, sc_);
 }
 
 // A CUDA graph of `chunk` iterations, captured on first use.  The legacy
@@ -2188,14 +2213,14 @@ int PcgSolver::run_pcg(SysArrays<T>& A, double tol, int criterion, int max_iter,
       FwdOp<T, true> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
       launch_sweep<T, true>(wave_args(true, 1, FIN_EINIT), fo, s, wg);
     }
-    k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.q, A.s, sc_);
+    k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_, ws_.order_fwd, A.q, A.s, sc_);
   } else {
     // z = M^-1 r ; s = z ; sigma = z.r
     FwdOp<T> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
     launch_sweep<T, true>(wave_args(f32, 1, FIN_NONE), fo, s, wg);
     BwdOp<T> bo{{A.q, A.E, A.uR, A.uU, A.uF, A.r}, A.z};
     launch_sweep<T, false>(wave_args(f32, 1, FIN_BWD), bo, s, wg);
-    k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, A.z, A.s, sc_);
+    k_copy<T><<<nblocks_, kThreads, 0, s>>>(g_, ws_.order_fwd, A.z, A.s, sc_);
   }
   launches_ += eis ? 3 : 4;
   int e = check_dev_error("pcg init");
@@ -2295,7 +2320,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
     k_init<float><<<nblocks_, kThreads, 0, s>>>(g_, d64_.r, 1.0 / scale, active_, A.r, A.p, partials_, sc_);
     FwdOp<float, true> fo{{A.r, A.cL, A.cD, A.cB, A.E}, A.q};
     launch_sweep<float, true>(wave_args(true, 1, FIN_EINIT), fo, s, wg);
-    k_copy<float><<<nblocks_, kThreads, 0, s>>>(g_.total, A.q, A.s, sc_);
+    k_copy<float><<<nblocks_, kThreads, 0, s>>>(g_, ws_.order_fwd, A.q, A.s, sc_);
     launches_ += 3;
     e = ensure_graph<float>(A, true);
     if (e) return e;
@@ -2355,7 +2380,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
     } else if (u.done == DONE_MAXITER || launched >= max_chunks || updates >= opt_.max_outer) {
       status = DONE_MAXITER;
     } else if (grew || !(meas < meas_u)) {
-      k_copy<float><<<nblocks_, kThreads, 0, s>>>(g_.total, A.q, A.s, sc_);
+      k_copy<float><<<nblocks_, kThreads, 0, s>>>(g_, ws_.order_fwd, A.q, A.s, sc_);
       cudaMemsetAsync(&sc_->beta, 0, sizeof(double), s);
       launches_ += 1;
     }
@@ -2537,14 +2562,14 @@ int PcgSolver::time_kernels(int reps, double* ms) {
   k_init<double><<<nblocks_, kThreads, 0, s>>>(g_, rhs_, 1.0, active_, d64_.r, d64_.p, partials_,
                                                sc_);
   cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
-  k_copy<double><<<grid, kThreads, 0, s>>>(g_.total, d64_.r, d64_.s, sc_);
+  k_copy<double><<<grid, kThreads, 0, s>>>(g_, ws_.order_fwd, d64_.r, d64_.s, sc_);
   // The mixed solver iterates in FP32: time its FP32 kernels (the pivot sweep
   // is FP64 in both).
   const bool f32 = opt_.precision == PREC_MIXED && have_f32_;
   if (f32) {
     k_init<float><<<nblocks_, kThreads, 0, s>>>(g_, rhs_, 1.0, active_, d32_.r, d32_.p, partials_, sc_);
     cudaMemcpyAsync(sc_, &init, sizeof(PcgScalars), cudaMemcpyHostToDevice, s);
-    k_copy<float><<<grid, kThreads, 0, s>>>(g_.total, d32_.r, d32_.s, sc_);
+    k_copy<float><<<grid, kThreads, 0, s>>>(g_, ws_.order_fwd, d32_.r, d32_.s, sc_);
   }
   auto kernel = [&](auto& A, int which) {
     using T = std::remove_reference_t<decltype(*A.r)>;
@@ -2562,10 +2587,10 @@ int PcgSolver::time_kernels(int reps, double* ms) {
         launch_spmv<T>(A, s, 0);
         break;
       case 4:
-        k_axpy<T><<<nblocks_, kThreads, 0, s>>>(g_.total, active_, A.s, A.Az, A.p, A.r, partials_, sc_);
+        k_axpy<T><<<nblocks_, kThreads, 0, s>>>(g_, ws_.order_fwd, A.s, A.Az, A.p, A.r, partials_, sc_);
         break;
       case 5:
-        k_sa<T><<<nblocks_, kThreads, 0, s>>>(g_.total, active_, A.z, A.s, partials_, sc_);
+        k_sa<T><<<nblocks_, kThreads, 0, s>>>(g_, ws_.order_fwd, A.z, A.s, partials_, sc_);
         break;
       case 6:
         if constexpr (sizeof(T) == 4)

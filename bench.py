@@ -582,6 +582,7 @@ def flip_leg(args, dev, ctx, dist, rank, world):
     split = {}
     iters = []
     launches = 0
+    unconverged, flags = 0, 0
     e0.record(stream)
     for _ in range(args.flip_steps):
         st = one()
@@ -590,6 +591,8 @@ def flip_leg(args, dev, ctx, dist, rank, world):
                 split[k[3:]] = split.get(k[3:], 0.0) + v
         iters.append(st["pcg_iterations"])
         launches += st["kernel_launches"]
+        unconverged += st["pcg_status"] != 1
+        flags |= st["pcg_flags"]
     e1.record(stream)
     torch.cuda.synchronize()
     from simcraft_b200.replicas import Replicas
@@ -602,6 +605,7 @@ def flip_leg(args, dev, ctx, dist, rank, world):
            "steps_per_s": world * K / (ms * 1e-3), "ms_per_step": ms / K,
            "split_ms_per_step": {k: v / K for k, v in split.items()},
            "pcg_inner_iterations_mean": float(np.mean(iters)), "gpu_launches": int(launches),
+           "pcg_solves_not_converged": int(unconverged), "pcg_device_flags": int(flags),
            "steps_note": (f"{K} of the configuration's 100 substeps are timed (--flip-steps 100 times all of "
                           f"them): each substep takes about a second, and the default run keeps the timed work "
                           f"near a minute; the timed substeps follow the warm-up ones from the same initial "

@@ -356,6 +356,8 @@ typedef struct {
   double ms_advect, ms_sort_sdf, ms_p2g, ms_build, ms_solve, ms_project_g2p;
   double ms_total;       /* device time, CUDA events, summed over substeps */
   int64_t kernel_launches;
+  int pcg_status;        /* last substep's solve: SC_DONE_* */
+  unsigned pcg_flags;    /* device_flags of the solves, OR-ed over the substeps */
 } sc_fluid_stats;
 
 typedef struct sc_fluid sc_fluid;

@@ -40,7 +40,8 @@ class sc_fluid_stats(ctypes.Structure):
     _fields_ = [("substeps", c_int), ("pcg_iterations", c_int), ("pcg_outer", c_int),
                 ("pcg_residual", c_double), ("ms_advect", c_double), ("ms_sort_sdf", c_double),
                 ("ms_p2g", c_double), ("ms_build", c_double), ("ms_solve", c_double),
-                ("ms_project_g2p", c_double), ("ms_total", c_double), ("kernel_launches", c_int64)]
+                ("ms_project_g2p", c_double), ("ms_total", c_double), ("kernel_launches", c_int64),
+                ("pcg_status", c_int), ("pcg_flags", ctypes.c_uint)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

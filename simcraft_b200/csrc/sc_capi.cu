@@ -812,6 +812,8 @@ static void stats_out(const sc::StepStats& s, sc_fluid_stats* o) {
   o->ms_project_g2p = s.ms_project_g2p;
   o->ms_total = s.ms_total;
   o->kernel_launches = s.kernel_launches;
+  o->pcg_status = s.pcg_status;
+  o->pcg_flags = s.pcg_flags;
 }
 
 int sc_fluid_substep(sc_fluid* sim, double dt, sc_fluid_stats* stats) {

@@ -653,6 +653,7 @@ DiffSim::DiffSim(Context* ctx, const DiffConfig& cfg) : ctx_(ctx), c_(cfg) {
   ok &= (rho_ = (double*)alloc(sizeof(double) * N_)) != nullptr;
   ok &= (target_ = (double*)alloc(sizeof(double) * N_)) != nullptr;
   ok &= (red_ = (double*)alloc(sizeof(double) * 4)) != nullptr;
+  ok &= (p2g_scr_ = alloc(p2g_scratch_bytes(Geo{c_.nx, c_.ny, c_.nz}, rs_))) != nullptr;
   if (ok && cudaMallocHost(&host_red_, sizeof(double) * 4) != cudaSuccess) ok = false;
   scur_ck_.assign(nck_, 0);
   svcur_ck_.assign(nck_, 0);
@@ -786,16 +787,9 @@ int DiffSim::step_t(int t, int mode, const void* in, void* out) {
   } else {
     k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, c_.recon_factor * h, start_, cnt_, S.px, S.py, S.pz,
                                              sdf_[scur_], sdfv_[svcur_]);
-    for (int k = 0; k < c_.sdf_extrap_iters; k++) {
-      k_extrap_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_], sdfv_[svcur_], sdfv_[1 - svcur_]);
-      scur_ = 1 - scur_;
-      svcur_ = 1 - svcur_;
-    }
-    for (int k = 0; k < c_.smooth_iters; k++) {
-      k_smooth_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_]);
-      scur_ = 1 - scur_;
-    }
-    launches_ += 1 + c_.sdf_extrap_iters + c_.smooth_iters;
+    launches_ += 1 + launch_iter_cells<ITER_SDF>(st, G, c_.sdf_extrap_iters, sdf_, sdfv_, scur_, svcur_);
+    int unused = 0;
+    launches_ += launch_iter_cells<ITER_SMOOTH>(st, G, c_.smooth_iters, sdf_, nullptr, scur_, unused);
     if (mode == TAPE_RECORD)
       cudaMemcpyAsync(tape_sdf_ + (size_t)t * N, sdf_[scur_], sizeof(double) * N, cudaMemcpyDeviceToDevice, st);
   }
@@ -803,23 +797,20 @@ int DiffSim::step_t(int t, int mode, const void* in, void* out) {
   const double* fluid = sdf_[scur_];
   // P2G, Dirichlet, extrapolation, gravity
   for (int a = 0; a < 3; a++) gstart_[a] = gcur_[a];
-  launches_ += launch_p2g<T>(st, G, h, start_, cnt_, S, (T*)g_[0][gcur_[0]], (T*)g_[1][gcur_[1]],
+  launches_ += launch_p2g<T>(st, G, h, start_, cnt_, S, p2g_scratch_at(p2g_scr_, G, rs_), (T*)g_[0][gcur_[0]],
+                             (T*)g_[1][gcur_[1]],
                              (T*)g_[2][gcur_[2]], (T*)W_[0], (T*)W_[1], (T*)W_[2], mask_[0], mask_[1], mask_[2],
                              (T*)last_[0], (T*)last_[1], (T*)last_[2], tb, sid_);
   k_dirichlet<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, (T*)g_[0][gcur_[0]], mask_[0]);
   k_dirichlet<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, (T*)g_[1][gcur_[1]], mask_[1]);
   k_dirichlet<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, (T*)g_[2][gcur_[2]], mask_[2]);
-  for (int k = 0; k < it; k++) {
-    k_extrap_face<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, (T*)g_[0][gcur_[0]], (T*)g_[0][1 - gcur_[0]],
-                                                        mask_[0] + (size_t)k * fsz_[0], mask_[0] + (size_t)(k + 1) * fsz_[0]);
-    k_extrap_face<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, (T*)g_[1][gcur_[1]], (T*)g_[1][1 - gcur_[1]],
-                                                        mask_[1] + (size_t)k * fsz_[1], mask_[1] + (size_t)(k + 1) * fsz_[1]);
-    k_extrap_face<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, (T*)g_[2][gcur_[2]], (T*)g_[2][1 - gcur_[2]],
-                                                        mask_[2] + (size_t)k * fsz_[2], mask_[2] + (size_t)(k + 1) * fsz_[2]);
-    for (int a = 0; a < 3; a++) gcur_[a] = 1 - gcur_[a];
+  // extrapolation, temporally blocked, each pass's flags kept for the adjoint
+  {
+    T* const fb[3][2] = {{(T*)g_[0][0], (T*)g_[0][1]}, {(T*)g_[1][0], (T*)g_[1][1]}, {(T*)g_[2][0], (T*)g_[2][1]}};
+    launches_ += launch_extrap_faces<T>(st, G, it, fb, nullptr, mask_, fsz_, gcur_);
   }
   k_force<T><<<nblk(fsz_[1]), kT, 0, st>>>(G, (T*)g_[1][gcur_[1]], mask_[1] + (size_t)it * fsz_[1], c_.gravity * dt);
-  launches_ += 4 + 3 * it;
+  launches_ += 4;
   // buildSystem, solve, project, walls
   SystemOut so;
   so.g = pcg_->geom();

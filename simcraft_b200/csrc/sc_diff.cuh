@@ -99,6 +99,7 @@ class DiffSim {
   int gcur_[3] = {0, 0, 0};
   int gstart_[3] = {0, 0, 0};            // buffer P2G wrote in the last substep
   void* W_[3] = {};                      // P2G weight sums
+  void* p2g_scr_ = nullptr;              // P2G tile slices (p2g_scratch_bytes)
   void* last_[3] = {};                   // P2G result (FLIP u_last)
   uint8_t* mask_[3] = {};                // extrapolation masks: (vel_extrap_iters + 1) per grid
   double* wt_[3] = {};                   // face weights of buildSystem

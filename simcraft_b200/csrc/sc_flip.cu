@@ -70,6 +70,7 @@ FluidSim::FluidSim(Context* ctx, const FluidConfig& cfg) : ctx_(ctx), c_(cfg) {
   ok &= (cursor_ = (int*)alloc(sizeof(int) * N)) != nullptr;
   ok &= (bsum_ = (int*)alloc(sizeof(int) * ((N + 1023) / 1024 + 1))) != nullptr;
   ok &= (redbuf_ = (double*)alloc(sizeof(double) * 4)) != nullptr;
+  ok &= (p2g_scr_ = alloc(p2g_scratch_bytes(Geo{nx, ny, nz}, rs_))) != nullptr;
   if (ok && cudaMallocHost(&host_red_, sizeof(double) * 4) != cudaSuccess) ok = false;
   if (!ok) {
     status_ = -3;
@@ -233,20 +234,17 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
   k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, c_.recon_factor * h, start_, cnt_, P.px, P.py, P.pz,
                                            sdf_[scur_], sdfv_[svcur_]);
   launches_ += 1;
-  for (int it = 0; it < c_.sdf_extrap_iters; it++) {
-    k_extrap_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_], sdfv_[svcur_], sdfv_[1 - svcur_]);
-    scur_ = 1 - scur_;
-    svcur_ = 1 - svcur_;
+  // extrapolateFluidSdf(10) and smoothFluidSurface(5), temporally blocked
+  launches_ += launch_iter_cells<ITER_SDF>(st, G, c_.sdf_extrap_iters, sdf_, sdfv_, scur_, svcur_);
+  {
+    int unused = 0;
+    launches_ += launch_iter_cells<ITER_SMOOTH>(st, G, c_.smooth_iters, sdf_, nullptr, scur_, unused);
   }
-  for (int it = 0; it < c_.smooth_iters; it++) {
-    k_smooth_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_]);
-    scur_ = 1 - scur_;
-  }
-  launches_ += c_.sdf_extrap_iters + c_.smooth_iters;
   const double* fluid = sdf_[scur_];
   cudaEventRecord(ev_[2], st);
   // P2G + Dirichlet walls + extrapolation + gravity (fluid-simulator.cc:155-164)
-  launches_ += launch_p2g<T>(st, G, h, start_, cnt_, P, G_(0), G_(1), G_(2), (T*)gw_[0], (T*)gw_[1],
+  launches_ += launch_p2g<T>(st, G, h, start_, cnt_, P, p2g_scratch_at(p2g_scr_, G, rs_), G_(0), G_(1), G_(2),
+                             (T*)gw_[0], (T*)gw_[1],
                              (T*)gw_[2], gv_[0][gcur_[0]], gv_[1][gcur_[1]], gv_[2][gcur_[2]],
                              c_.flip ? (T*)last_[0] : nullptr, c_.flip ? (T*)last_[1] : nullptr,
                              c_.flip ? (T*)last_[2] : nullptr);
@@ -254,23 +252,13 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
   k_dirichlet<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, G_(1), gv_[1][gcur_[1]]);
   k_dirichlet<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, G_(2), gv_[2][gcur_[2]]);
   launches_ += 3;
-  for (int it = 0; it < c_.vel_extrap_iters; it++) {
-    k_extrap_face<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, (T*)g_[0][gcur_[0]], (T*)g_[0][1 - gcur_[0]],
-                                                        gv_[0][gcur_[0]], gv_[0][1 - gcur_[0]]);
-    gcur_[0] = 1 - gcur_[0];
-  }
-  for (int it = 0; it < c_.vel_extrap_iters; it++) {
-    k_extrap_face<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, (T*)g_[1][gcur_[1]], (T*)g_[1][1 - gcur_[1]],
-                                                        gv_[1][gcur_[1]], gv_[1][1 - gcur_[1]]);
-    gcur_[1] = 1 - gcur_[1];
-  }
-  for (int it = 0; it < c_.vel_extrap_iters; it++) {
-    k_extrap_face<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, (T*)g_[2][gcur_[2]], (T*)g_[2][1 - gcur_[2]],
-                                                        gv_[2][gcur_[2]], gv_[2][1 - gcur_[2]]);
-    gcur_[2] = 1 - gcur_[2];
+  // extrapolate(.., 10) on the three face grids, temporally blocked
+  {
+    T* const fb[3][2] = {{(T*)g_[0][0], (T*)g_[0][1]}, {(T*)g_[1][0], (T*)g_[1][1]}, {(T*)g_[2][0], (T*)g_[2][1]}};
+    launches_ += launch_extrap_faces<T>(st, G, c_.vel_extrap_iters, fb, gv_, nullptr, fsz_, gcur_);
   }
   k_force<T><<<nblk(fsz_[1]), kT, 0, st>>>(G, G_(1), gv_[1][gcur_[1]], c_.gravity * dt);
-  launches_ += 3 * c_.vel_extrap_iters + 1;
+  launches_ += 1;
   cudaEventRecord(ev_[3], st);
   // buildSystem straight into the solver's tiled arrays (fluid-simulator.cc:166)
   SystemOut so;
@@ -301,9 +289,10 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
   k_collider<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, h, G_(0), collider_);
   k_collider<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, h, G_(1), collider_);
   k_collider<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, h, G_(2), collider_);
+  // the particles are still in the order of this substep's sort
   if (n > 0)
-    k_g2p<T><<<nblk(n), kT, 0, st>>>(n, P, G_(0), G_(1), G_(2), (T*)last_[0], (T*)last_[1],
-                                     (T*)last_[2], G, h, c_.flip ? c_.flip_alpha : -1.0);
+    launch_g2p_tiles<T>(st, G, h, c_.flip ? c_.flip_alpha : -1.0, start_, cnt_, P, G_(0), G_(1), G_(2),
+                        (T*)last_[0], (T*)last_[1], (T*)last_[2]);
   launches_ += 7;
   cudaEventRecord(ev_[6], st);
   cudaEventSynchronize(ev_[6]);
@@ -320,6 +309,8 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
     stt->pcg_iterations = ps.iterations;
     stt->pcg_outer = ps.outer;
     stt->pcg_residual = ps.residual;
+    stt->pcg_status = ps.status;
+    stt->pcg_flags |= ps.device_flags;
     stt->substeps += 1;
     stt->kernel_launches += launches_ - l0;
   }
@@ -509,19 +500,6 @@ int flip_sample(cudaStream_t st, int64_t n, const double* pts, int nx, int ny, i
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-int flip_g2p(cudaStream_t st, int64_t n, const double* pos, double* vel, int nx, int ny, int nz,
-             double h, const double* u, const double* v, const double* w, const double* ulast,
-             const double* vlast, const double* wlast, double alpha) {
-  StageParticles sp;
-  sp.st = st;
-  sp.n = n;
-  if (cudaMallocAsync(&sp.buf, sizeof(double) * 6 * (size_t)std::max<int64_t>(n, 1), st) != cudaSuccess) return -3;
-  k_aos_to_soa<double><<<nblk(n), kT, 0, st>>>(n, pos, vel, sp.P(), nullptr);
-  k_g2p<double><<<nblk(n), kT, 0, st>>>(n, sp.P(), u, v, w, ulast, vlast, wlast, Geo{nx, ny, nz}, h, alpha);
-  k_soa_to_aos<double><<<nblk(n), kT, 0, st>>>(n, sp.P(), nullptr, nullptr, vel);
-  return cudaGetLastError() == cudaSuccess ? 0 : -2;
-}
-
 int flip_advect(cudaStream_t st, int64_t n, double* pos, double* vel, int nx, int ny, int nz,
                 double h, const double* u, const double* v, const double* w,
                 const double* collider, double dt) {
@@ -591,8 +569,27 @@ int flip_p2g(cudaStream_t st, int64_t n, const double* pos, const double* vel, i
   cudaMemsetAsync(uw, 0, sizeof(double) * f0, st);
   cudaMemsetAsync(vw, 0, sizeof(double) * f1, st);
   cudaMemsetAsync(ww, 0, sizeof(double) * f2, st);
-  launch_p2g<double>(st, G, h, s.start, s.cnt, s.b.P(), u, v, w, uw, vw, ww, uvalid, vvalid, wvalid, ulast,
-                     vlast, wlast);
+  void* scr = nullptr;
+  if (cudaMallocAsync(&scr, p2g_scratch_bytes(G, sizeof(double)), st) != cudaSuccess) return -3;
+  launch_p2g<double>(st, G, h, s.start, s.cnt, s.b.P(), p2g_scratch_at(scr, G, sizeof(double)), u, v, w, uw, vw,
+                     ww, uvalid, vvalid, wvalid, ulast, vlast, wlast);
+  cudaFreeAsync(scr, st);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// solveG2P through the simulator's tile kernel: the particles are sorted by
+// cell first, and each velocity is written back at its particle's index.
+int flip_g2p(cudaStream_t st, int64_t n, const double* pos, double* vel, int nx, int ny, int nz,
+             double h, const double* u, const double* v, const double* w, const double* ulast,
+             const double* vlast, const double* wlast, double alpha) {
+  const Geo G{nx, ny, nz};
+  Sorted s;
+  int e = make_sorted(s, st, n, pos, vel, G, h);
+  if (e) return e;
+  if (n > 0) {
+    launch_g2p_tiles<double>(st, G, h, alpha, s.start, s.cnt, s.b.P(), u, v, w, ulast, vlast, wlast);
+    k_soa_to_aos<double><<<nblk(n), kT, 0, st>>>(n, s.b.P(), s.b.id, nullptr, vel);
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

@@ -32,6 +32,8 @@ struct StepStats {
   double ms_advect = 0, ms_sort_sdf = 0, ms_p2g = 0, ms_build = 0, ms_solve = 0, ms_project_g2p = 0;
   double ms_total = 0;
   int64_t kernel_launches = 0;
+  int pcg_status = 0;        // last substep's solve (DONE_*)
+  unsigned pcg_flags = 0;    // device flags of the solves, OR-ed
 };
 
 // Grids and particles in precision T.  The particle arrays are kept sorted by
@@ -82,6 +84,7 @@ class FluidSim {
   uint8_t* gv_[3][2] = {};
   int gcur_[3] = {0, 0, 0};
   void* gw_[3] = {};     // weight sums
+  void* p2g_scr_ = nullptr;  // P2G tile slices (p2g_scratch_bytes)
   void* last_[3] = {};   // FLIP u_last/v_last/w_last
   double* wt_[3] = {};   // FVM face weights
   double* sdf_[2] = {};

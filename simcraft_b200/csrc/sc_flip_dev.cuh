@@ -467,8 +467,11 @@ __global__ void __launch_bounds__(kT)
     const int x0 = max(0, (int)floor(rdiv(rsub(cx, r2), h))), x1 = min(G.nx - 1, (int)ceil(rdiv(radd(cx, r2), h)));
     const int y0 = max(0, (int)floor(rdiv(rsub(cy, r2), h))), y1 = min(G.ny - 1, (int)ceil(rdiv(radd(cy, r2), h)));
     const int z0 = max(0, (int)floor(rdiv(rsub(cz, r2), h))), z1 = min(G.nz - 1, (int)ceil(rdiv(radd(cz, r2), h)));
-    double best = 1e9;
-    uint8_t ok = 0;
+    // min over the candidates of |x - p| - r where |x - p| <= 2r: sqrt and the
+    // subtraction are monotone and correctly rounded, so that is sqrt of the
+    // least squared distance minus r, when its root passes the test (if the
+    // nearest particle fails it, all do): one square root per cell
+    double m2 = INFINITY;
     const double lim = r2 * r2 * (1.0 + 1e-9);
     // Distance from the cell centre to a bucket's cell box; boundary buckets
     // also hold the particles clamped into them, so their boxes are open.
@@ -491,13 +494,18 @@ __global__ void __launch_bounds__(kT)
           for (int l = s; l < s + m - 1; l++) {
             const double dx = rsub((double)px[l], cx), dy = rsub((double)py[l], cy),
                          dz = rsub((double)pz[l], cz);
-            const double dis = sqrt(radd(radd(rmul(dx, dx), rmul(dy, dy)), rmul(dz, dz)));
-            if (dis <= r2) {
-              best = fmin(best, rsub(dis, radius));
-              ok = 1;
-            }
+            m2 = fmin(m2, radd(radd(rmul(dx, dx), rmul(dy, dy)), rmul(dz, dz)));
           }
         }
+      }
+    }
+    double best = 1e9;
+    uint8_t ok = 0;
+    if (m2 < INFINITY) {
+      const double dis = sqrt(m2);
+      if (dis <= r2) {
+        best = rsub(dis, radius);
+        ok = 1;
       }
     }
     sdf[id] = best;
@@ -558,16 +566,309 @@ __global__ void __launch_bounds__(kT)
   }
 }
 
-// solveP2G (advect-solver.cc:188-271) as a tile splat.  A block owns an
-// 8x8x8 tile of cells, one thread per cell; each thread walks its cell's
-// particles (contiguous after the per-substep sort), evaluates the per-axis
-// kernel factors once per particle and adds the 64 weighted contributions per
-// face grid into shared-memory accumulators covering every node the tile's
-// particles can reach (nearest + {-1..2}: 12 nodes along a grid's own axis,
-// 13 along the others).  The block then adds its accumulators into the global
-// sums once.  Threads of a warp own distinct cells, so their shared-memory
-// atomics at one stencil offset hit distinct nodes.  Like the reference's
-// parallel FLIP splat, the floating-point summation order is not fixed.
+// ---- the iterated grid passes, temporally blocked ----
+// extrapolate(.., 10) per face grid (cpu/fluid-simulator.h:204-253),
+// extrapolateFluidSdf(10) (:123-166) and smoothFluidSurface(5)
+// (fluid-simulator.cc:39-74) are Jacobi-style passes over two buffers: pass k
+// reads buffer k mod 2 and writes buffer (k + 1) mod 2, and a cell a pass does
+// not write keeps that buffer's older value.  One launch runs up to kIterHalo
+// passes: a block loads its tile plus a halo of kIterHalo cells (both value
+// buffers and the source flags) into shared memory, runs the passes there
+// over a region that shrinks by one cell per pass, and writes its tile back:
+// both buffers and both flag arrays, or, for the differentiable step, each
+// pass's flags into their history.  The passes and their arithmetic are those
+// of k_extrap_face, k_extrap_sdf and k_smooth_sdf, so the results are the same
+// bit for bit.  A tile whose loaded region holds no valid flag is left as it is
+// (every pass would leave it so), but for the SDF flags, which the passes
+// rewrite with zeros.
+enum { ITER_FACE = 0, ITER_SDF = 1, ITER_SMOOTH = 2 };
+constexpr int kIterThreads = 512;
+constexpr int kIterHalo = 5;  // passes per launch at most
+template <class T>
+struct IterTile;
+template <>
+struct IterTile<float> {
+  static constexpr int X = 16, Y = 16, Z = 16;
+};
+template <>
+struct IterTile<double> {
+  static constexpr int X = 8, Y = 16, Z = 16;
+};
+template <class T>
+constexpr int iter_region() {
+  return (IterTile<T>::X + 2 * kIterHalo) * (IterTile<T>::Y + 2 * kIterHalo) * (IterTile<T>::Z + 2 * kIterHalo);
+}
+template <class T>
+constexpr size_t iter_smem_bytes() {
+  return (size_t)iter_region<T>() * (2 * sizeof(T) + 2);
+}
+template <class T>
+inline int iter_tiles(int dx, int dy, int dz) {
+  return ((dx + IterTile<T>::X - 1) / IterTile<T>::X) * ((dy + IterTile<T>::Y - 1) / IterTile<T>::Y) *
+         ((dz + IterTile<T>::Z - 1) / IterTile<T>::Z);
+}
+
+// One grid's buffers for a launch: values b[2], flags f[2] (ping-pong) or a
+// flag history (hist: pass k's flags at hist + k * hstride, f unused); cur:
+// the buffer pass 0 reads.
+template <class T>
+struct IterGrid {
+  int dx, dy, dz;
+  T* b[2];
+  uint8_t* f[2];
+  uint8_t* hist;
+  int64_t hstride;
+  int cur;
+};
+
+template <class T, int MODE>
+__device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char* smem) {
+  constexpr int TX = IterTile<T>::X, TY = IterTile<T>::Y, TZ = IterTile<T>::Z, H = kIterHalo;
+  constexpr int RX = TX + 2 * H, RY = TY + 2 * H, RZ = TZ + 2 * H, RN = RX * RY * RZ;
+  constexpr bool FLAGS = MODE != ITER_SMOOTH;
+  T* V = reinterpret_cast<T*>(smem);                        // [2][RN]: side 0 = buffer cur
+  uint8_t* F = reinterpret_cast<uint8_t*>(V + 2 * RN);     // [2][RN]
+  const int dx = G.dx, dy = G.dy, dz = G.dz;
+  const int ntz = (dz + TZ - 1) / TZ, nty = (dy + TY - 1) / TY;
+  const int tz = tile % ntz, ty = (tile / ntz) % nty, tx = tile / (ntz * nty);
+  const int x0 = tx * TX - H, y0 = ty * TY - H, z0 = tz * TZ - H;  // region origin
+  const T* bs = G.b[G.cur];
+  const T* bd = G.b[1 - G.cur];
+  const uint8_t* fs = G.hist ? G.hist : G.f[G.cur];
+  int any = 0;
+  for (int e = threadIdx.x; e < RN; e += blockDim.x) {
+    const int i = e / (RY * RZ), r = e - i * (RY * RZ), j = r / RZ, k = r - j * RZ;
+    const int gx = x0 + i, gy = y0 + j, gz = z0 + k;
+    const bool in = gx >= 0 && gx < dx && gy >= 0 && gy < dy && gz >= 0 && gz < dz;
+    const int64_t gi = in ? lin(gx, gy, gz, dy, dz) : 0;
+    V[e] = in ? bs[gi] : T(0);
+    V[RN + e] = in ? bd[gi] : T(0);
+    if (FLAGS) {
+      const uint8_t fv = in ? fs[gi] : 0;
+      F[e] = fv;
+      F[RN + e] = 0;  // out-of-domain cells are never written: they must read as invalid
+      any |= fv;
+    }
+  }
+  if (FLAGS && !__syncthreads_or(any)) {
+    // no valid cell within reach: the face passes would write zeros where the
+    // buffers hold zeros already; the SDF passes leave the values and write
+    // zero flags into the buffers they write
+    if (MODE == ITER_SDF && !G.hist)
+      for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
+        const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
+        const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
+        if (gx >= dx || gy >= dy || gz >= dz) continue;
+        const int64_t gi = lin(gx, gy, gz, dy, dz);
+        G.f[1 - G.cur][gi] = 0;
+        if (nit > 1) G.f[G.cur][gi] = 0;
+      }
+    return;
+  }
+  __syncthreads();
+  constexpr int sX = RY * RZ, sY = RZ;
+  for (int p = 0; p < nit; p++) {
+    const int src = p & 1;
+    const T* Vs = V + src * RN;
+    T* Vd = V + (1 - src) * RN;
+    const uint8_t* Fs = F + src * RN;
+    uint8_t* Fd = F + (1 - src) * RN;
+    // cells whose six neighbours still hold the data of p passes
+    constexpr int CX = RX - 2, CY = RY - 2, CZ = RZ - 2;
+    const int lo = p + 1, nxr = RX - 2 * (p + 1), nyr = RY - 2 * (p + 1), nzr = RZ - 2 * (p + 1);
+    (void)CX;
+    (void)CY;
+    (void)CZ;
+    for (int q = threadIdx.x; q < nxr * nyr * nzr; q += blockDim.x) {
+      const int a = q / (nyr * nzr), r = q - a * (nyr * nzr), b = r / nzr, c = r - b * nzr;
+      const int i = lo + a, j = lo + b, k = lo + c;
+      const int gx = x0 + i, gy = y0 + j, gz = z0 + k;
+      if (gx < 0 || gx >= dx || gy < 0 || gy >= dy || gz < 0 || gz >= dz) continue;
+      const int e = i * sX + j * sY + k;
+      if (MODE == ITER_SMOOTH) {
+        T sum = T(0);
+        int cnt = 0;
+        if (gx > 0) { sum = radd(sum, Vs[e - sX]); cnt++; }
+        if (gx < dx - 1) { sum = radd(sum, Vs[e + sX]); cnt++; }
+        if (gy > 0) { sum = radd(sum, Vs[e - sY]); cnt++; }
+        if (gy < dy - 1) { sum = radd(sum, Vs[e + sY]); cnt++; }
+        if (gz > 0) { sum = radd(sum, Vs[e - 1]); cnt++; }
+        if (gz < dz - 1) { sum = radd(sum, Vs[e + 1]); cnt++; }
+        T v = rdiv(sum, (T)cnt);
+        if (Vs[e] < v) v = Vs[e];
+        Vd[e] = v;
+      } else {
+        uint8_t fl;
+        if (Fs[e]) {
+          fl = 1;
+        } else {
+          // out-of-domain neighbours hold flag 0 and are never counted
+          T sum = T(0);
+          int cnt = 0;
+          if (Fs[e - sX]) { sum = radd(sum, Vs[e - sX]); cnt++; }
+          if (Fs[e + sX]) { sum = radd(sum, Vs[e + sX]); cnt++; }
+          if (Fs[e - sY]) { sum = radd(sum, Vs[e - sY]); cnt++; }
+          if (Fs[e + sY]) { sum = radd(sum, Vs[e + sY]); cnt++; }
+          if (Fs[e - 1]) { sum = radd(sum, Vs[e - 1]); cnt++; }
+          if (Fs[e + 1]) { sum = radd(sum, Vs[e + 1]); cnt++; }
+          if (cnt > 0) {
+            Vd[e] = rdiv(sum, (T)cnt);
+            fl = 1;
+          } else {
+            if (MODE == ITER_FACE) Vd[e] = T(0);
+            fl = 0;
+          }
+        }
+        Fd[e] = fl;
+        if (G.hist && i >= H && i < H + TX && j >= H && j < H + TY && k >= H && k < H + TZ)
+          G.hist[(int64_t)(p + 1) * G.hstride + lin(gx, gy, gz, dy, dz)] = fl;
+      }
+    }
+    __syncthreads();
+  }
+  // the tile: both buffers (side 0 is buffer cur) and both flag arrays
+  for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
+    const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
+    const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
+    if (gx >= dx || gy >= dy || gz >= dz) continue;
+    const int64_t gi = lin(gx, gy, gz, dy, dz);
+    const int le = (H + i) * sX + (H + j) * sY + (H + k);
+    G.b[G.cur][gi] = V[le];
+    G.b[1 - G.cur][gi] = V[RN + le];
+    if (FLAGS && !G.hist) {
+      G.f[G.cur][gi] = F[le];
+      G.f[1 - G.cur][gi] = F[RN + le];
+    }
+  }
+}
+
+// The three face grids in one launch (blocks of grid 0, then 1, then 2).
+template <class T>
+struct IterFaces {
+  IterGrid<T> g[3];
+  int t0, t1;  // tiles of grid 0, of grids 0 and 1
+};
+template <class T>
+__global__ void __launch_bounds__(kIterThreads) k_iter_faces(IterFaces<T> a, int nit) {
+  extern __shared__ __align__(16) unsigned char iter_dyn[];
+  const int b = blockIdx.x;
+  if (b < a.t0)
+    iter_tile<T, ITER_FACE>(a.g[0], b, nit, iter_dyn);
+  else if (b < a.t1)
+    iter_tile<T, ITER_FACE>(a.g[1], b - a.t0, nit, iter_dyn);
+  else
+    iter_tile<T, ITER_FACE>(a.g[2], b - a.t1, nit, iter_dyn);
+}
+template <int MODE>
+__global__ void __launch_bounds__(kIterThreads) k_iter_cells(IterGrid<double> g, int nit) {
+  extern __shared__ __align__(16) unsigned char iter_dyn[];
+  iter_tile<double, MODE>(g, blockIdx.x, nit, iter_dyn);
+}
+
+// `iters` passes of extrapolate() over the three face grids; cur[a] is the
+// buffer holding grid a's current values, flipped once per pass.  hist[a]:
+// the differentiable step's flag history (pass 0 reads hist[a]), or null for
+// the ping-pong flags f[a][2].
+template <class T>
+int launch_extrap_faces(cudaStream_t st, const Geo& G, int iters, T* const b[3][2], uint8_t* const f[3][2],
+                        uint8_t* const hist[3], const int64_t fsz[3], int cur[3]) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_iter_faces<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)iter_smem_bytes<T>());
+    attr = true;
+  }
+  int launches = 0;
+  for (int k0 = 0; k0 < iters; k0 += kIterHalo) {
+    const int nit = std::min(kIterHalo, iters - k0);
+    IterFaces<T> a;
+    int acc = 0;
+    for (int ax = 0; ax < 3; ax++) {
+      IterGrid<T>& g = a.g[ax];
+      g.dx = G.nx + (ax == 0);
+      g.dy = G.ny + (ax == 1);
+      g.dz = G.nz + (ax == 2);
+      g.b[0] = b[ax][0];
+      g.b[1] = b[ax][1];
+      g.f[0] = f ? f[ax][0] : nullptr;
+      g.f[1] = f ? f[ax][1] : nullptr;
+      g.hist = hist ? hist[ax] + (int64_t)k0 * fsz[ax] : nullptr;
+      g.hstride = fsz[ax];
+      g.cur = cur[ax];
+      acc += iter_tiles<T>(g.dx, g.dy, g.dz);
+      if (ax == 0) a.t0 = acc;
+      if (ax == 1) a.t1 = acc;
+    }
+    k_iter_faces<T><<<acc, kIterThreads, iter_smem_bytes<T>(), st>>>(a, nit);
+    launches++;
+    for (int ax = 0; ax < 3; ax++)
+      if (nit & 1) cur[ax] = 1 - cur[ax];
+  }
+  return launches;
+}
+// `iters` passes of extrapolateFluidSdf (MODE ITER_SDF, flags f[2]) or of
+// smoothFluidSurface (ITER_SMOOTH) over the cell grid; cur and fcur flip per pass.
+template <int MODE>
+int launch_iter_cells(cudaStream_t st, const Geo& G, int iters, double* const b[2], uint8_t* const f[2], int& cur,
+                      int& fcur) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_iter_cells<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)iter_smem_bytes<double>());
+    attr = true;
+  }
+  int launches = 0;
+  for (int k0 = 0; k0 < iters; k0 += kIterHalo) {
+    const int nit = std::min(kIterHalo, iters - k0);
+    IterGrid<double> g;
+    g.dx = G.nx;
+    g.dy = G.ny;
+    g.dz = G.nz;
+    g.b[0] = b[0];
+    g.b[1] = b[1];
+    // the value and flag buffers flip together, but need not start together:
+    // address the flags so that side 0 is the one pass 0 reads
+    g.cur = cur;
+    g.f[0] = f ? (fcur == cur ? f[0] : f[1]) : nullptr;
+    g.f[1] = f ? (fcur == cur ? f[1] : f[0]) : nullptr;
+    g.hist = nullptr;
+    g.hstride = 0;
+    k_iter_cells<MODE><<<iter_tiles<double>(G.nx, G.ny, G.nz), kIterThreads, iter_smem_bytes<double>(), st>>>(g, nit);
+    launches++;
+    if (nit & 1) {
+      cur = 1 - cur;
+      if (f) fcur = 1 - fcur;
+    }
+  }
+  return launches;
+}
+
+// ---- solveP2G (advect-solver.cc:188-271) ----
+// Two kernels, no global atomics and a summation order fixed by the data, so
+// the sums are the same bit for bit on every run:
+//  k_p2g_tiles:  a block owns an 8x8x8 tile of cells, one thread per cell, and
+//                sums its particles' contributions over the nodes they reach
+//                (the tile's "region") into shared memory, then writes the
+//                region to the tile's slice of a scratch buffer;
+//  k_p2g_gather: each face node adds the slices of the tiles whose regions
+//                hold it (at most 2 per axis), in tile order, and normalises.
+// Within a tile the accumulation is a fixed sequence too.  The weights of a
+// particle for face grid AX are the same per-axis factors as the reference's
+// (offset 0 along AX, 1/2 along the others).  Along AX the particle's stencil
+// starts at its cell - 1 or at its cell (nearest node below or above its
+// centre); along the other axes at cell - 1, rounding aside.  So the nodes of
+// one cell's particles lie in a 5 x 4 x 4 window.  The tile walks that window
+// in 5 passes, one node plane along AX at a time: in a pass each thread sums
+// its particles (in bucket order) into 16 registers per quantity for the 4 x 4
+// nodes of the plane, stages them, and after a barrier each region node adds
+// the staged values of the (up to 16) cells that reach it, in a fixed order.
+// Particles whose stencil starts elsewhere (rounding of the half-offset
+// nearest-node test, particles outside the grid box, or recorded bases of the
+// differentiable step) are added one thread after another, in thread order,
+// straight into the region; the region spans cell - 2 .. cell + 3 across AX
+// and cell - 1 .. cell + 3 along it, which holds every in-grid node of any
+// such particle.  Only a node beyond it (a recorded base far from the
+// particle's cell) goes to the global sums with an atomic add, raising the
+// spill flag that makes the gather read them.
 constexpr int kPT = 8;                        // cells per tile edge
 constexpr int kPThreads = kPT * kPT * kPT;    // one thread per cell
 template <int AX, int D>
@@ -579,88 +880,252 @@ template <int AX>
 constexpr int p2g_region() {
   return P2GRegion<AX, 0>::n * P2GRegion<AX, 1>::n * P2GRegion<AX, 2>::n;
 }
+constexpr int kP2GRegion = p2g_region<0>();  // the same for all three grids
+static_assert(p2g_region<1>() == kP2GRegion && p2g_region<2>() == kP2GRegion, "region sizes");
 template <class T>
 constexpr size_t p2g_smem_bytes() {
-  return sizeof(T) * 2 * (size_t)(p2g_region<0>() + p2g_region<1>() + p2g_region<2>());
+  // 2 x 16 staged values per thread, the region (sum and weight), outlier list
+  return sizeof(T) * (2 * 16 * (size_t)kPThreads + 2 * (size_t)kP2GRegion) + sizeof(int) * (kPThreads + 32);
+}
+
+// Device scratch of the two kernels: per tile the three grids' regions (sum
+// and weight), per tile a flag (the tile held particles), the spill flag.
+struct P2GScratch {
+  void* slices = nullptr;
+  int* occ = nullptr;
+  int* spill = nullptr;
+};
+inline int64_t p2g_ntiles(const Geo& G) {
+  return (int64_t)((G.nx + kPT - 1) / kPT) * ((G.ny + kPT - 1) / kPT) * ((G.nz + kPT - 1) / kPT);
+}
+inline size_t p2g_scratch_bytes(const Geo& G, size_t elem) {
+  const int64_t nt = p2g_ntiles(G);
+  const size_t a = (elem * 6 * (size_t)kP2GRegion * nt + 255) & ~(size_t)255;
+  return a + ((sizeof(int) * (size_t)(nt + 1) + 255) & ~(size_t)255);
+}
+inline P2GScratch p2g_scratch_at(void* base, const Geo& G, size_t elem) {
+  const int64_t nt = p2g_ntiles(G);
+  const size_t a = (elem * 6 * (size_t)kP2GRegion * nt + 255) & ~(size_t)255;
+  P2GScratch s;
+  s.slices = base;
+  s.occ = (int*)((char*)base + a);
+  s.spill = s.occ + nt;
+  return s;
+}
+
+// Spacing of the P2G kernels: a division by h is a multiplication by 1/h,
+// exactly, when h is a power of two (the usual 1/2^k grids); otherwise divide.
+template <class T>
+struct P2GSpacing {
+  T h, inv;
+  bool pow2;
+  __device__ __forceinline__ T over(T x) const { return pow2 ? rmul(x, inv) : rdiv(x, h); }
+};
+// Nearest-node base along axis D for face grid AX (TGrid::nearest, as
+// nearest1 computes it); tb: recorded bases, or null.
+template <class T, int AX, int D>
+__device__ __forceinline__ int p2g_base(T p, const P2GSpacing<T>& sp, const int16_t* tb) {
+  constexpr int o = D == AX ? 0 : 1;
+  if (tb) return (int)tb[D * 2 + o];
+  return (int)radd(sp.over(rsub(rsub(p, T(0)), rmul(o ? T(0.5) : T(0), sp.h))), T(0.5)) - 1;
+}
+// The per-axis factor N(|p - x_node| / h) of the cubic B-spline (bspline),
+// with the 1/6 of its outer piece as a multiplication: within an ulp of the
+// reference's factor, which divides.
+template <class T, int AX, int D>
+__device__ __forceinline__ T p2g_factor(T p, int node, const P2GSpacing<T>& sp) {
+  constexpr T off = D == AX ? T(0) : T(0.5);
+  const T r = sp.over(fabs(rsub(p, coord1(node, off, sp.h))));
+  if (r < T(1)) return radd(rsub(T(2.0 / 3.0), rmul(r, r)), rmul(rmul(rmul(T(0.5), r), r), r));
+  if (r < T(2)) {
+    const T t = rsub(T(2), r);
+    return rmul(rmul(rmul(t, t), t), T(1.0 / 6.0));
+  }
+  return T(0);
+}
+// The reference's product order: (w_x w_y) w_z.
+template <class T>
+__device__ __forceinline__ T p2g_weight(T w0, T w1, T w2) {
+  return rmul(rmul(w0, w1), w2);
 }
 
 template <class T, int AX>
-__device__ __forceinline__ void p2g_splat_one(const Stencil<T>& S, T val, T* __restrict__ acc,
-                                              int x0, int y0, int z0, const Geo& G, T* gsum,
-                                              T* gwt) {
-  constexpr int o0 = AX == 0 ? 0 : 1, o1 = AX == 1 ? 0 : 1, o2 = AX == 2 ? 0 : 1;
+__device__ void p2g_tile_grid(const Geo& G, const P2GSpacing<T>& h, int x0, int y0, int z0, int cx, int cy, int cz, int s0, int m,
+                              const PartsT<T>& P, const T* __restrict__ vel, const int16_t* tape,
+                              const int64_t* ids, T* stage, T* Rs, int* olist, T* slice, T* gsum, T* gwt,
+                              int* spill) {
+  constexpr int D1 = AX == 0 ? 1 : 0, D2 = AX == 2 ? 1 : 2;  // the two axes across AX
   constexpr int n0 = P2GRegion<AX, 0>::n, n1 = P2GRegion<AX, 1>::n, n2 = P2GRegion<AX, 2>::n;
-  constexpr int R = n0 * n1 * n2;
-  const int b0 = S.base[0][o0], b1 = S.base[1][o1], b2 = S.base[2][o2];
-  const int l0 = b0 - (x0 - P2GRegion<AX, 0>::lo), l1 = b1 - (y0 - P2GRegion<AX, 1>::lo),
-            l2 = b2 - (z0 - P2GRegion<AX, 2>::lo);
-  if (l0 >= 0 && l0 + 3 < n0 && l1 >= 0 && l1 + 3 < n1 && l2 >= 0 && l2 + 3 < n2) {
+  constexpr int lo0 = P2GRegion<AX, 0>::lo, lo1 = P2GRegion<AX, 1>::lo, lo2 = P2GRegion<AX, 2>::lo;
+  T* Rw = Rs + kP2GRegion;
+  const int tid = threadIdx.x;
+  const int c[3] = {cx, cy, cz};
+  const int t0[3] = {x0, y0, z0};
+  for (int e = tid; e < 2 * kP2GRegion; e += kPThreads) Rs[e] = T(0);
+  int nout = 0;
+  // region strides along AX and across it
+  constexpr int stA = AX == 0 ? n1 * n2 : (AX == 1 ? n2 : 1);
+  constexpr int st1 = D1 == 0 ? n1 * n2 : (D1 == 1 ? n2 : 1);
+  constexpr int st2 = D2 == 0 ? n1 * n2 : (D2 == 1 ? n2 : 1);
+  for (int ip = 0; ip < 5; ip++) {
+    T as[16], aw[16];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int q = 0; q < 16; q++) {
+      as[q] = T(0);
+      aw[q] = T(0);
+    }
+    for (int l = s0; l < s0 + m; l++) {
+      const T p[3] = {P.px[l], P.py[l], P.pz[l]};
+      const int16_t* tb = tape ? tape + 6 * ids[l] : nullptr;
+      const int bA = p2g_base<T, AX, AX>(p[AX], h, tb);
+      const int b1 = p2g_base<T, AX, D1>(p[D1], h, tb), b2 = p2g_base<T, AX, D2>(p[D2], h, tb);
+      const int sh = bA - (c[AX] - 1);
+      if (sh < 0 || sh > 1 || b1 != c[D1] - 1 || b2 != c[D2] - 1) {
+        if (ip == 0) nout++;
+        continue;
+      }
+      const int t = ip - sh;
+      if (t < 0 || t > 3) continue;
+      const T wA = p2g_factor<T, AX, AX>(p[AX], bA + t, h);
+      T w1[4], w2[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        const T wxy = rmul(S.w[0][o0][i], S.w[1][o1][j]);
-        T* row = acc + ((l0 + i) * n1 + (l1 + j)) * n2 + l2;
+        w1[j] = p2g_factor<T, AX, D1>(p[D1], b1 + j, h);
+        w2[j] = p2g_factor<T, AX, D2>(p[D2], b2 + j, h);
+      }
+      const T v = vel[l];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-          const T wt = rmul(wxy, S.w[2][o2][k]);
-          atomicAdd(row + k, rmul(val, wt));
-          atomicAdd(row + k + R, wt);
+          // factors in axis order x, y, z
+          T f[3];
+          f[AX] = wA;
+          f[D1] = w1[j];
+          f[D2] = w2[k];
+          const T wt = p2g_weight(f[0], f[1], f[2]);
+          as[j * 4 + k] = radd(as[j * 4 + k], rmul(v, wt));
+          aw[j * 4 + k] = radd(aw[j * 4 + k], wt);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      stage[q * kPThreads + tid] = as[q];
+      stage[(16 + q) * kPThreads + tid] = aw[q];
+    }
+    __syncthreads();
+    // region nodes of this pass: along AX the plane of cell + ip - 1 of each
+    // cell of the tile (region index cell + ip), across AX the nodes reached
+    // from the tile's cells at their typical bases (region indices 1..11)
+    constexpr int NA = kPT, NB = kPT + 3;
+    for (int e = tid; e < NA * NB * NB; e += kPThreads) {
+      const int a = e / (NB * NB), r = e - a * (NB * NB);
+      const int b = r / NB, cc = r - b * NB;
+      const int rb = b + 1, rc = cc + 1;  // region indices across AX
+      T S = T(0), W = T(0);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int q1 = rb - 1 - j;  // the cell along D1 whose window index j is this node
+        if (q1 < 0 || q1 >= kPT) continue;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const int q2 = rc - 1 - k;
+          if (q2 < 0 || q2 >= kPT) continue;
+          int lc[3];
+          lc[AX] = a;
+          lc[D1] = q1;
+          lc[D2] = q2;
+          const int src = (lc[0] * kPT + lc[1]) * kPT + lc[2];
+          S = radd(S, stage[(j * 4 + k) * kPThreads + src]);
+          W = radd(W, stage[(16 + j * 4 + k) * kPThreads + src]);
         }
       }
-    return;
+      const int ridx = (a + ip) * stA + rb * st1 + rc * st2;
+      Rs[ridx] = radd(Rs[ridx], S);
+      Rw[ridx] = radd(Rw[ridx], W);
+    }
+    __syncthreads();
   }
-  // a particle outside the domain box: straight to the global sums
-  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
-  for (int i = 0; i < 4; i++) {
-    const int a = b0 + i;
-    if (a < 0 || a >= fx) continue;
-    for (int j = 0; j < 4; j++) {
-      const int b = b1 + j;
-      if (b < 0 || b >= fy) continue;
-      const T wxy = rmul(S.w[0][o0][i], S.w[1][o1][j]);
-      for (int k = 0; k < 4; k++) {
-        const int c = b2 + k;
-        if (c < 0 || c >= fz) continue;
-        const T wt = rmul(wxy, S.w[2][o2][k]);
-        atomicAdd(gsum + lin(a, b, c, fy, fz), rmul(val, wt));
-        atomicAdd(gwt + lin(a, b, c, fy, fz), wt);
+  // the particles outside the typical windows, thread after thread
+  if (__syncthreads_or(nout > 0)) {
+    const int lane = tid & 31, warp = tid >> 5;
+    int* wcnt = olist + kPThreads;
+    const unsigned bal = __ballot_sync(0xffffffffu, nout > 0);
+    if (lane == 0) wcnt[warp] = __popc(bal);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < kPThreads / 32; w++) {
+      if (w < warp) before += wcnt[w];
+      total += wcnt[w];
+    }
+    if (nout > 0) olist[before + __popc(bal & ((1u << lane) - 1u))] = tid;
+    __syncthreads();
+    for (int qi = 0; qi < total; qi++) {
+      if (olist[qi] == tid) {
+        const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+        for (int l = s0; l < s0 + m; l++) {
+          const T p[3] = {P.px[l], P.py[l], P.pz[l]};
+          const int16_t* tb = tape ? tape + 6 * ids[l] : nullptr;
+          int b[3];
+          b[AX] = p2g_base<T, AX, AX>(p[AX], h, tb);
+          b[D1] = p2g_base<T, AX, D1>(p[D1], h, tb);
+          b[D2] = p2g_base<T, AX, D2>(p[D2], h, tb);
+          const int sh = b[AX] - (c[AX] - 1);
+          if (!(sh < 0 || sh > 1 || b[D1] != c[D1] - 1 || b[D2] != c[D2] - 1)) continue;
+          const T v = vel[l];
+          T w[3][4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            w[0][i] = p2g_factor<T, AX, 0>(p[0], b[0] + i, h);
+            w[1][i] = p2g_factor<T, AX, 1>(p[1], b[1] + i, h);
+            w[2][i] = p2g_factor<T, AX, 2>(p[2], b[2] + i, h);
+          }
+          for (int i = 0; i < 4; i++) {
+            const int ga = b[0] + i;
+            if (ga < 0 || ga >= fx) continue;
+            for (int j = 0; j < 4; j++) {
+              const int gb = b[1] + j;
+              if (gb < 0 || gb >= fy) continue;
+              for (int k = 0; k < 4; k++) {
+                const int gc = b[2] + k;
+                if (gc < 0 || gc >= fz) continue;
+                const T wt = p2g_weight(w[0][i], w[1][j], w[2][k]);
+                const int la = ga - (t0[0] - lo0), lb = gb - (t0[1] - lo1), lcc = gc - (t0[2] - lo2);
+                if (la >= 0 && la < n0 && lb >= 0 && lb < n1 && lcc >= 0 && lcc < n2) {
+                  const int ridx = (la * n1 + lb) * n2 + lcc;
+                  Rs[ridx] = radd(Rs[ridx], rmul(v, wt));
+                  Rw[ridx] = radd(Rw[ridx], wt);
+                } else {
+                  const int64_t gi = lin(ga, gb, gc, fy, fz);
+                  atomicAdd(gsum + gi, rmul(v, wt));
+                  atomicAdd(gwt + gi, wt);
+                  *spill = 1;
+                }
+              }
+            }
+          }
+        }
       }
+      __syncthreads();
     }
   }
+  for (int e = tid; e < 2 * kP2GRegion; e += kPThreads) slice[e] = Rs[e];
+  __syncthreads();
 }
 
-template <class T, int AX>
-__device__ __forceinline__ void p2g_merge(const T* __restrict__ acc, int x0, int y0, int z0,
-                                          const Geo& G, T* gsum, T* gwt) {
-  constexpr int n1 = P2GRegion<AX, 1>::n, n2 = P2GRegion<AX, 2>::n;
-  constexpr int R = p2g_region<AX>();
-  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
-  for (int e = threadIdx.x; e < R; e += blockDim.x) {
-    const T w = acc[R + e];
-    if (w == T(0)) continue;
-    const int k = e % n2, j = (e / n2) % n1, i = e / (n1 * n2);
-    const int a = x0 - P2GRegion<AX, 0>::lo + i, b = y0 - P2GRegion<AX, 1>::lo + j,
-              c = z0 - P2GRegion<AX, 2>::lo + k;
-    if (a < 0 || a >= fx || b < 0 || b >= fy || c < 0 || c >= fz) continue;  // outside the grid
-    const int64_t id = lin(a, b, c, fy, fz);
-    atomicAdd(gsum + id, acc[e]);
-    atomicAdd(gwt + id, w);
-  }
-}
-
-// Accumulates sum(v w) and sum(w) of all particles into gsum/gwt (zeroed by
-// the caller); k_p2g_normalize finishes solveP2G.
 template <class T>
 __global__ void __launch_bounds__(kPThreads)
-    k_p2g_splat(Geo G, double hd, const int* __restrict__ start, const int* __restrict__ cnt,
-                PartsT<T> P, T* su, T* sv, T* sw, T* wu, T* wv, T* ww, const int16_t* tape,
+    k_p2g_tiles(Geo G, double hd, int pow2, const int* __restrict__ start, const int* __restrict__ cnt, PartsT<T> P,
+                T* slices, int* occ, T* su, T* sv, T* sw, T* wu, T* wv, T* ww, int* spill, const int16_t* tape,
                 const int64_t* ids) {
   extern __shared__ __align__(16) unsigned char p2g_dyn[];
-  T* acc0 = reinterpret_cast<T*>(p2g_dyn);
-  T* acc1 = acc0 + 2 * p2g_region<0>();
-  T* acc2 = acc1 + 2 * p2g_region<1>();
-  const T h = (T)hd;
+  T* stage = reinterpret_cast<T*>(p2g_dyn);
+  T* Rs = stage + 32 * kPThreads;
+  int* olist = reinterpret_cast<int*>(Rs + 2 * kP2GRegion);
+  P2GSpacing<T> h;
+  h.h = (T)hd;
+  h.inv = (T)(1.0 / hd);
+  h.pow2 = pow2 != 0;
   const int ntz = (G.nz + kPT - 1) / kPT, nty = (G.ny + kPT - 1) / kPT;
   const int tz = blockIdx.x % ntz, ty = (blockIdx.x / ntz) % nty, tx = blockIdx.x / (ntz * nty);
   const int x0 = tx * kPT, y0 = ty * kPT, z0 = tz * kPT;
@@ -672,61 +1137,341 @@ __global__ void __launch_bounds__(kPThreads)
     m = cnt[cell];
     s0 = start[cell];
   }
-  if (!__syncthreads_or(m > 0)) return;  // no particle in this tile
-  constexpr int NACC = 2 * (p2g_region<0>() + p2g_region<1>() + p2g_region<2>());
-  for (int e = threadIdx.x; e < NACC; e += blockDim.x) acc0[e] = T(0);
-  __syncthreads();
-  for (int l = s0; l < s0 + m; l++) {
-    Stencil<T> S;
-    make_stencil_tb(S, P.px[l], P.py[l], P.pz[l], h, tape ? tape + 6 * ids[l] : nullptr);
-    p2g_splat_one<T, 0>(S, P.vx[l], acc0, x0, y0, z0, G, su, wu);
-    p2g_splat_one<T, 1>(S, P.vy[l], acc1, x0, y0, z0, G, sv, wv);
-    p2g_splat_one<T, 2>(S, P.vz[l], acc2, x0, y0, z0, G, sw, ww);
-  }
-  __syncthreads();
-  p2g_merge<T, 0>(acc0, x0, y0, z0, G, su, wu);
-  p2g_merge<T, 1>(acc1, x0, y0, z0, G, sv, wv);
-  p2g_merge<T, 2>(acc2, x0, y0, z0, G, sw, ww);
+  const bool any = __syncthreads_or(m > 0);
+  if (threadIdx.x == 0) occ[blockIdx.x] = any ? 1 : 0;
+  if (!any) return;  // no particle in this tile: its slices are never read
+  T* slice = slices + (int64_t)blockIdx.x * 6 * kP2GRegion;
+  p2g_tile_grid<T, 0>(G, h, x0, y0, z0, cx, cy, cz, s0, m, P, P.vx, tape, ids, stage, Rs, olist, slice, su, wu,
+                      spill);
+  p2g_tile_grid<T, 1>(G, h, x0, y0, z0, cx, cy, cz, s0, m, P, P.vy, tape, ids, stage, Rs, olist,
+                      slice + 2 * kP2GRegion, sv, wv, spill);
+  p2g_tile_grid<T, 2>(G, h, x0, y0, z0, cx, cy, cz, s0, m, P, P.vz, tape, ids, stage, Rs, olist,
+                      slice + 4 * kP2GRegion, sw, ww, spill);
 }
 
-// Normalisation of solveP2G (advect-solver.cc:238-267): g = sum / W where
-// W > 0 (valid), else 0; FLIP copies the result into `last` (:268-270).
+// Tiles along one axis whose regions hold node x: [lo, hi] (empty if lo > hi).
+__device__ __forceinline__ void p2g_tiles_of(int x, int rlo, int rn, int ntile, int& lo, int& hi) {
+  const int v = x + rlo - rn;  // >= -13
+  lo = max(0, (v + 16) / kPT - 16 / kPT + 1);
+  hi = min(ntile - 1, (x + rlo) / kPT);
+}
+
+// Sum of the tile slices holding each node (tile order), plus the spilled
+// global sums when the spill flag is set, then the normalisation of solveP2G
+// (advect-solver.cc:238-267): W > 0 -> g = sum / W, valid; else 0, invalid;
+// FLIP copies g into `last` (:268-270).  w keeps W.
+template <class T, int AX>
+__device__ __forceinline__ void p2g_gather_node(const Geo& G, int64_t id, const T* __restrict__ slices,
+                                                const int* __restrict__ occ, bool spilled, T* g, T* w,
+                                                uint8_t* valid, T* last) {
+  const int fy = G.fy(AX), fz = G.fz(AX);
+  int a, b, c;
+  decode3(id, fy, fz, a, b, c);
+  const int ntx = (G.nx + kPT - 1) / kPT, nty = (G.ny + kPT - 1) / kPT, ntz = (G.nz + kPT - 1) / kPT;
+  constexpr int lo0 = P2GRegion<AX, 0>::lo, lo1 = P2GRegion<AX, 1>::lo, lo2 = P2GRegion<AX, 2>::lo;
+  constexpr int n0 = P2GRegion<AX, 0>::n, n1 = P2GRegion<AX, 1>::n, n2 = P2GRegion<AX, 2>::n;
+  int xa, xb, ya, yb, za, zb;
+  p2g_tiles_of(a, lo0, n0, ntx, xa, xb);
+  p2g_tiles_of(b, lo1, n1, nty, ya, yb);
+  p2g_tiles_of(c, lo2, n2, ntz, za, zb);
+  T S = T(0), W = T(0);
+  for (int tx = xa; tx <= xb; tx++)
+    for (int ty = ya; ty <= yb; ty++)
+      for (int tz = za; tz <= zb; tz++) {
+        const int64_t tile = ((int64_t)tx * nty + ty) * ntz + tz;
+        if (!occ[tile]) continue;
+        const int la = a - (tx * kPT - lo0), lb = b - (ty * kPT - lo1), lc = c - (tz * kPT - lo2);
+        const T* sl = slices + (tile * 6 + 2 * AX) * kP2GRegion + (la * n1 + lb) * n2 + lc;
+        S = radd(S, __ldg(sl));
+        W = radd(W, __ldg(sl + kP2GRegion));
+      }
+  if (spilled) {
+    S = radd(S, g[id]);
+    W = radd(W, w[id]);
+  }
+  const bool ok = W > T(0);
+  const T out = ok ? rdiv(S, W) : T(0);
+  g[id] = out;
+  w[id] = W;
+  valid[id] = ok ? 1 : 0;
+  if (last) last[id] = out;
+}
 template <class T>
 __global__ void __launch_bounds__(kT)
-    k_p2g_normalize(int64_t n, T* __restrict__ g, const T* __restrict__ wsum,
-                    uint8_t* __restrict__ valid, T* __restrict__ last) {
-  GRID_LOOP(i, n) {
-    const T w = wsum[i];
-    const bool ok = w > T(0);
-    const T out = ok ? rdiv(g[i], w) : T(0);
-    g[i] = out;
-    valid[i] = ok ? 1 : 0;
-    if (last) last[i] = out;
+    k_p2g_gather(Geo G, const T* __restrict__ slices, const int* __restrict__ occ, const int* __restrict__ spill,
+                 T* gu, T* gv, T* gw, T* wu, T* wv, T* ww, uint8_t* vu, uint8_t* vv, uint8_t* vw, T* lu, T* lv,
+                 T* lw) {
+  const int64_t f0 = (int64_t)(G.nx + 1) * G.ny * G.nz, f1 = (int64_t)G.nx * (G.ny + 1) * G.nz,
+                f2 = (int64_t)G.nx * G.ny * (G.nz + 1);
+  const bool spilled = *spill != 0;
+  GRID_LOOP(i, f0 + f1 + f2) {
+    if (i < f0)
+      p2g_gather_node<T, 0>(G, i, slices, occ, spilled, gu, wu, vu, lu);
+    else if (i < f0 + f1)
+      p2g_gather_node<T, 1>(G, i - f0, slices, occ, spilled, gv, wv, vv, lv);
+    else
+      p2g_gather_node<T, 2>(G, i - f0 - f1, slices, occ, spilled, gw, ww, vw, lw);
   }
 }
 
-// Launches the splat over all cell tiles and normalises the three grids; g*
-// and w* must hold zeros.
+// solveP2G: the tile sums, then the gather.  g* and w* must hold zeros (the
+// spill path adds into them); `scratch` holds p2g_scratch_bytes(G, sizeof(T)).
 template <class T>
-int launch_p2g(cudaStream_t st, const Geo& G, double h, const int* start, const int* cnt,
-               PartsT<T> P, T* gu, T* gv, T* gw, T* wu, T* wv, T* ww, uint8_t* vu, uint8_t* vv,
-               uint8_t* vw, T* lu, T* lv, T* lw, const int16_t* tape = nullptr,
-               const int64_t* ids = nullptr) {
+int launch_p2g(cudaStream_t st, const Geo& G, double h, const int* start, const int* cnt, PartsT<T> P,
+               const P2GScratch& scr, T* gu, T* gv, T* gw, T* wu, T* wv, T* ww, uint8_t* vu, uint8_t* vv,
+               uint8_t* vw, T* lu, T* lv, T* lw, const int16_t* tape = nullptr, const int64_t* ids = nullptr) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_p2g_splat<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)p2g_smem_bytes<T>());
+    cudaFuncSetAttribute(k_p2g_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes<T>());
     attr = true;
   }
-  const int tiles = ((G.nx + kPT - 1) / kPT) * ((G.ny + kPT - 1) / kPT) * ((G.nz + kPT - 1) / kPT);
-  k_p2g_splat<T><<<tiles, kPThreads, p2g_smem_bytes<T>(), st>>>(G, h, start, cnt, P, gu, gv, gw, wu, wv,
-                                                                 ww, tape, ids);
-  const int64_t f0 = (int64_t)(G.nx + 1) * G.ny * G.nz, f1 = (int64_t)G.nx * (G.ny + 1) * G.nz,
-                f2 = (int64_t)G.nx * G.ny * (G.nz + 1);
-  k_p2g_normalize<T><<<nblk(f0), kT, 0, st>>>(f0, gu, wu, vu, lu);
-  k_p2g_normalize<T><<<nblk(f1), kT, 0, st>>>(f1, gv, wv, vv, lv);
-  k_p2g_normalize<T><<<nblk(f2), kT, 0, st>>>(f2, gw, ww, vw, lw);
-  return 4;
+  const int64_t tiles = p2g_ntiles(G);
+  cudaMemsetAsync(scr.spill, 0, sizeof(int), st);
+  int ex = 0;
+  const int pow2 = std::frexp(h, &ex) == 0.5 ? 1 : 0;
+  k_p2g_tiles<T><<<(unsigned)tiles, kPThreads, p2g_smem_bytes<T>(), st>>>(G, h, pow2, start, cnt, P, (T*)scr.slices,
+                                                                          scr.occ, gu, gv, gw, wu, wv, ww,
+                                                                          scr.spill, tape, ids);
+  const int64_t nf = (int64_t)(G.nx + 1) * G.ny * G.nz + (int64_t)G.nx * (G.ny + 1) * G.nz +
+                     (int64_t)G.nx * G.ny * (G.nz + 1);
+  k_p2g_gather<T><<<nblk(nf), kT, 0, st>>>(G, (const T*)scr.slices, scr.occ, scr.spill, gu, gv, gw, wu, wv, ww,
+                                          vu, vv, vw, lu, lv, lw);
+  return 2;
+}
+
+// ---- solveG2P over cell tiles (advect-solver.cc:157-169, util.cc:40-85) ----
+// A block takes the same 8x8x8 cell tiles as the P2G kernels and first copies
+// the P2G region of each face grid it samples (u, v, w and, for FLIP, their
+// last values) into shared memory, row by row; the tile's particles then read
+// their 4x4x4 stencil nodes from there.  The particles of a column of the tile
+// (8 cells along z) are contiguous after the sort, so each warp walks whole
+// columns.  The nodes, their order and the arithmetic are those of
+// sampleVelocity (gather), so the velocities are the same bit for bit; a
+// particle whose stencil leaves the region (outside the grid box, recorded
+// bases) samples the grids in global memory instead.
+constexpr int kG2PThreads = 256;
+template <class T, int AX>
+__device__ __forceinline__ void g2p_stage(T* __restrict__ R, const T* __restrict__ g, const Geo& G, int x0, int y0,
+                                          int z0) {
+  constexpr int n1 = P2GRegion<AX, 1>::n, n2 = P2GRegion<AX, 2>::n;
+  constexpr int lo0 = P2GRegion<AX, 0>::lo, lo1 = P2GRegion<AX, 1>::lo, lo2 = P2GRegion<AX, 2>::lo;
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+  for (int e = threadIdx.x; e < kP2GRegion; e += blockDim.x) {
+    const int i0 = e / (n1 * n2), r = e - i0 * (n1 * n2);
+    const int i1 = r / n2, i2 = r - i1 * n2;
+    const int a = x0 - lo0 + i0, b = y0 - lo1 + i1, c = z0 - lo2 + i2;
+    R[e] = (a >= 0 && a < fx && b >= 0 && b < fy && c >= 0 && c < fz) ? __ldg(g + lin(a, b, c, fy, fz)) : T(0);
+  }
+}
+template <class T, int AX>
+__device__ __forceinline__ bool g2p_in_region(const Stencil<T>& S, int x0, int y0, int z0) {
+  constexpr int ox = AX == 0 ? 0 : 1, oy = AX == 1 ? 0 : 1, oz = AX == 2 ? 0 : 1;
+  const int r0 = S.base[0][ox] - (x0 - P2GRegion<AX, 0>::lo), r1 = S.base[1][oy] - (y0 - P2GRegion<AX, 1>::lo),
+            r2 = S.base[2][oz] - (z0 - P2GRegion<AX, 2>::lo);
+  return r0 >= 0 && r0 + 3 < P2GRegion<AX, 0>::n && r1 >= 0 && r1 + 3 < P2GRegion<AX, 1>::n && r2 >= 0 &&
+         r2 + 3 < P2GRegion<AX, 2>::n;
+}
+// gather<T, AX> on the staged region: the same nodes, order and arithmetic.
+template <class T, int AX>
+__device__ __forceinline__ T g2p_gather_tile(const T* __restrict__ R, const Stencil<T>& S, const Geo& G, int x0,
+                                             int y0, int z0) {
+  constexpr int ox = AX == 0 ? 0 : 1, oy = AX == 1 ? 0 : 1, oz = AX == 2 ? 0 : 1;
+  constexpr int n1 = P2GRegion<AX, 1>::n, n2 = P2GRegion<AX, 2>::n;
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+  const int r0 = S.base[0][ox] - (x0 - P2GRegion<AX, 0>::lo), r1 = S.base[1][oy] - (y0 - P2GRegion<AX, 1>::lo),
+            r2 = S.base[2][oz] - (z0 - P2GRegion<AX, 2>::lo);
+  T s = T(0), ws = T(0);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int a = S.base[0][ox] + i;
+    if (a < 0 || a >= fx) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int b = S.base[1][oy] + j;
+      if (b < 0 || b >= fy) continue;
+      const T wxy = rmul(S.w[0][ox][i], S.w[1][oy][j]);
+      const T* row = R + ((r0 + i) * n1 + (r1 + j)) * n2 + r2;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int c = S.base[2][oz] + k;
+        if (c < 0 || c >= fz) continue;
+        const T wt = rmul(wxy, S.w[2][oz][k]);
+        s = radd(s, rmul(row[k], wt));
+        ws = radd(ws, wt);
+      }
+    }
+  }
+  return ws > T(0) ? rdiv(s, ws) : T(0);
+}
+// All three (or six) staged gathers of a particle whose stencils lie inside
+// the grid: no node is skipped, so the loops are branch-free and the chains
+// of the grids interleave; each grid's sum keeps gather's order.
+template <class T, int NG>
+__device__ __forceinline__ void g2p_gather_tile_inner(const T* __restrict__ R, const Stencil<T>& S, int x0, int y0,
+                                                      int z0, T* out) {
+  const T* row0[NG];
+  T s[NG], ws[NG];
+#pragma unroll
+  for (int q = 0; q < NG; q++) {
+    s[q] = T(0);
+    ws[q] = T(0);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+#pragma unroll
+      for (int q = 0; q < NG; q++) {
+        const int ax = q % 3;
+        const int ox = ax == 0 ? 0 : 1, oy = ax == 1 ? 0 : 1, oz = ax == 2 ? 0 : 1;
+        const int n1 = ax == 1 ? kPT + 4 : kPT + 5, n2 = ax == 2 ? kPT + 4 : kPT + 5;
+        const int lo0 = ax == 0 ? 1 : 2, lo1 = ax == 1 ? 1 : 2, lo2 = ax == 2 ? 1 : 2;
+        const int r0 = S.base[0][ox] - (x0 - lo0), r1 = S.base[1][oy] - (y0 - lo1), r2 = S.base[2][oz] - (z0 - lo2);
+        row0[q] = R + q * kP2GRegion + ((r0 + i) * n1 + (r1 + j)) * n2 + r2;
+        const T wxy = rmul(S.w[0][ox][i], S.w[1][oy][j]);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const T wt = rmul(wxy, S.w[2][oz][k]);
+          s[q] = radd(s[q], rmul(row0[q][k], wt));
+          ws[q] = radd(ws[q], wt);
+        }
+      }
+    }
+#pragma unroll
+  for (int q = 0; q < NG; q++) out[q] = ws[q] > T(0) ? rdiv(s[q], ws[q]) : T(0);
+}
+template <class T>
+__device__ __forceinline__ bool g2p_inner(const Stencil<T>& S, const Geo& G) {
+  // every stencil node of the three grids inside the grid
+  bool ok = true;
+#pragma unroll
+  for (int ax = 0; ax < 3; ax++) {
+    const int f[3] = {G.nx + (ax == 0), G.ny + (ax == 1), G.nz + (ax == 2)};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const int b = S.base[d][d == ax ? 0 : 1];
+      ok = ok && b >= 0 && b + 3 < f[d];
+    }
+  }
+  return ok;
+}
+template <class T>
+constexpr size_t g2p_smem_bytes(bool flip) {
+  return sizeof(T) * (size_t)(flip ? 6 : 3) * kP2GRegion;
+}
+template <class T>
+__global__ void __launch_bounds__(kG2PThreads)
+    k_g2p_tiles(Geo G, double hd, double alphad, const int* __restrict__ start, const int* __restrict__ cnt,
+                PartsT<T> P, const T* u, const T* v, const T* w, const T* ul, const T* vl, const T* wl) {
+  extern __shared__ __align__(16) unsigned char g2p_dyn[];
+  T* R = reinterpret_cast<T*>(g2p_dyn);  // [grid][region]: u, v, w, then u, v, w last
+  __shared__ int rbeg[kPT * kPT], rend[kPT * kPT];
+  const T h = (T)hd;
+  const bool flip = alphad >= 0.0;
+  const int ntz = (G.nz + kPT - 1) / kPT, nty = (G.ny + kPT - 1) / kPT;
+  const int tz = blockIdx.x % ntz, ty = (blockIdx.x / ntz) % nty, tx = blockIdx.x / (ntz * nty);
+  const int x0 = tx * kPT, y0 = ty * kPT, z0 = tz * kPT;
+  bool mine = false;
+  if (threadIdx.x < kPT * kPT) {
+    // the particle run of column (x0 + lx, y0 + ly): cells z0 .. z0 + 7
+    const int lx = threadIdx.x / kPT, ly = threadIdx.x % kPT;
+    const int x = x0 + lx, y = y0 + ly, zl = min(z0 + kPT, G.nz) - 1;
+    int b = 0, e = 0;
+    if (x < G.nx && y < G.ny) {
+      const int c0 = (int)lin(x, y, z0, G.ny, G.nz), c1 = (int)lin(x, y, zl, G.ny, G.nz);
+      b = start[c0];
+      e = start[c1] + cnt[c1];
+    }
+    rbeg[threadIdx.x] = b;
+    rend[threadIdx.x] = e;
+    mine = e > b;
+  }
+  if (!__syncthreads_or(mine)) return;  // no particle in this tile
+  g2p_stage<T, 0>(R, u, G, x0, y0, z0);
+  g2p_stage<T, 1>(R + kP2GRegion, v, G, x0, y0, z0);
+  g2p_stage<T, 2>(R + 2 * kP2GRegion, w, G, x0, y0, z0);
+  if (flip) {
+    g2p_stage<T, 0>(R + 3 * kP2GRegion, ul, G, x0, y0, z0);
+    g2p_stage<T, 1>(R + 4 * kP2GRegion, vl, G, x0, y0, z0);
+    g2p_stage<T, 2>(R + 5 * kP2GRegion, wl, G, x0, y0, z0);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int col = warp; col < kPT * kPT; col += kG2PThreads / 32) {
+    const int e = rend[col];
+    for (int i = rbeg[col] + lane; i < e; i += 32) {
+      const T px = P.px[i], py = P.py[i], pz = P.pz[i];
+      Stencil<T> S;
+      make_stencil(S, px, py, pz, h);
+      const bool in = g2p_in_region<T, 0>(S, x0, y0, z0) && g2p_in_region<T, 1>(S, x0, y0, z0) &&
+                      g2p_in_region<T, 2>(S, x0, y0, z0);
+      if (in && g2p_inner(S, G)) {
+        // the common case: all nodes staged and inside the grid
+        if (!flip) {
+          T o[3];
+          g2p_gather_tile_inner<T, 3>(R, S, x0, y0, z0, o);
+          P.vx[i] = o[0];
+          P.vy[i] = o[1];
+          P.vz[i] = o[2];
+        } else {
+          T o[6];
+          g2p_gather_tile_inner<T, 6>(R, S, x0, y0, z0, o);
+          const T al = (T)alphad, bl = rsub(T(1), al);
+          const T fx = rsub(radd(P.vx[i], o[0]), o[3]), fy = rsub(radd(P.vy[i], o[1]), o[4]),
+                  fz = rsub(radd(P.vz[i], o[2]), o[5]);
+          P.vx[i] = radd(rmul(al, fx), rmul(bl, o[0]));
+          P.vy[i] = radd(rmul(al, fy), rmul(bl, o[1]));
+          P.vz[i] = radd(rmul(al, fz), rmul(bl, o[2]));
+        }
+        continue;
+      }
+      T pu, pv, pw;
+      if (in) {
+        pu = g2p_gather_tile<T, 0>(R, S, G, x0, y0, z0);
+        pv = g2p_gather_tile<T, 1>(R + kP2GRegion, S, G, x0, y0, z0);
+        pw = g2p_gather_tile<T, 2>(R + 2 * kP2GRegion, S, G, x0, y0, z0);
+      } else {
+        pu = gather<T, 0>(u, S, G);
+        pv = gather<T, 1>(v, S, G);
+        pw = gather<T, 2>(w, S, G);
+      }
+      if (!flip) {
+        P.vx[i] = pu;
+        P.vy[i] = pv;
+        P.vz[i] = pw;
+        continue;
+      }
+      T lu, lv, lw;
+      if (in) {
+        lu = g2p_gather_tile<T, 0>(R + 3 * kP2GRegion, S, G, x0, y0, z0);
+        lv = g2p_gather_tile<T, 1>(R + 4 * kP2GRegion, S, G, x0, y0, z0);
+        lw = g2p_gather_tile<T, 2>(R + 5 * kP2GRegion, S, G, x0, y0, z0);
+      } else {
+        lu = gather<T, 0>(ul, S, G);
+        lv = gather<T, 1>(vl, S, G);
+        lw = gather<T, 2>(wl, S, G);
+      }
+      const T al = (T)alphad, bl = rsub(T(1), al);
+      const T fx = rsub(radd(P.vx[i], pu), lu), fy = rsub(radd(P.vy[i], pv), lv), fz = rsub(radd(P.vz[i], pw), lw);
+      P.vx[i] = radd(rmul(al, fx), rmul(bl, pu));
+      P.vy[i] = radd(rmul(al, fy), rmul(bl, pv));
+      P.vz[i] = radd(rmul(al, fz), rmul(bl, pw));
+    }
+  }
+}
+// G2P of cell-sorted particles (start/cnt of the sort that ordered P).
+template <class T>
+int launch_g2p_tiles(cudaStream_t st, const Geo& G, double h, double alpha, const int* start, const int* cnt,
+                     PartsT<T> P, const T* u, const T* v, const T* w, const T* ul, const T* vl, const T* wl) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_g2p_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes<T>(true));
+    attr = true;
+  }
+  const bool flip = alpha >= 0.0;
+  k_g2p_tiles<T><<<(unsigned)p2g_ntiles(G), kG2PThreads, g2p_smem_bytes<T>(flip), st>>>(G, h, alpha, start, cnt, P, u,
+                                                                                      v, w, ul, vl, wl);
+  return 1;
 }
 
 // applyDirichletBoundary for one face grid (fluid-simulator.cc:113-138).

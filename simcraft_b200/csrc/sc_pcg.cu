@@ -36,6 +36,10 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kRing = 32;     // boundary ring entries per wavefront CTA
+// 1: the iterations sweep only the tiles holding an active cell; 0: every tile
+#ifndef SC_SKIP_EMPTY_TILES
+#define SC_SKIP_EMPTY_TILES 1
+#endif
 #ifndef SC_WAVE_STAGE_MAX
 #define SC_WAVE_STAGE_MAX 8
 #endif
@@ -1056,11 +1060,14 @@ __device__ __forceinline__ void wave_abort(const WaveArgs& a, WaveShared<T, TY>&
   sh.availY = NS;
 }
 
+// A wait ends early only when another wait of the sweep gave up (the timeout
+// bit): the other status bits (a breakdown, a non-finite dot product) belong
+// to the iteration, and a sweep run after one of them still completes.
 __device__ __forceinline__ bool wave_should_stop(const WaveArgs& a, int& spins,
                                                  volatile int* s_abort, int limit) {
   if (*s_abort) return true;
   ++spins;
-  if ((spins & 63) == 0 && ld_relaxed_gpu_u32(&a.sc->err)) return true;
+  if ((spins & 63) == 0 && (ld_relaxed_gpu_u32(&a.sc->err) & DEV_ERR_TIMEOUT)) return true;
   return spins > limit;
 }
 
@@ -2106,7 +2113,11 @@ int PcgSolver::ensure_pivots() {
 void PcgSolver::select_active_tiles() {
   cudaStream_t st = ctx_->stream;
   const int ntiles = g_.ntiles();
+#if SC_SKIP_EMPTY_TILES
   k_tile_activity<<<ntiles, kThreads, 0, st>>>(g_, active_, tile_act_);
+#else
+  cudaMemsetAsync(tile_act_, 1, (size_t)ntiles, st);  // every tile swept
+#endif
   k_compact_order<<<1, 1024, 0, st>>>(g_.ntx, g_.nty, 0, tile_act_, ws_.order_all, ntiles, ws_.order_fwd,
                                       tile_partials_);
   launches_ += 2;
@@ -2124,10 +2135,13 @@ void PcgSolver::select_active_tiles() {
 
 template <class T>
 void PcgSolver::launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip) {
-  // slot runs per tile: about 1024 work items in all, runs of at least 16 slots
+  // slot runs per tile: about 16 work items per SM (4 resident blocks x 4),
+  // runs of at least 16 slots; whole tiles as items left a partial last wave
+  // at 512^3 (1024 tiles over 592 block slots)
   const int ntiles = g_.ntiles();
-  const int chunks = std::max(1, std::min((1024 + ntiles - 1) / ntiles, g_.nz / 16));
-  const int grid = std::min(nblocks_, ntiles * chunks);
+  const int want = 16 * ctx_->sm_count;
+  const int chunks = std::max(1, std::min((want + ntiles - 1) / ntiles, g_.nz / 16));
+  const int grid = std::min(4 * ctx_->sm_count, ntiles * chunks);
   k_spmv_stream<T><<<grid, kThreads, 0, st>>>(g_, ws_.order_fwd, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az, partials_, sc_,
                                               use_skip, chunks);
 }
@@ -2311,7 +2325,7 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
   const bool abs_crit = opt_.criterion == CRIT_ABS_LINF;
   const double bnorm = sqrt(sc_host_->rn2);
   double meas = abs_crit ? sc_host_->rinf : (bnorm > 0 ? 1.0 : 0.0);
-  int updates = 0, status = DONE_RUNNING, iters = 0;
+  int updates = 0, status = DONE_RUNNING, iters = 0, restarts = 0;
   unsigned flags = 0;
   if (meas < opt_.tol) status = DONE_CONVERGED;
   const double scale = bnorm;
@@ -2375,8 +2389,21 @@ int PcgSolver::solve_mixed_reliable(PcgStats* st) {
     if (u.err & DEV_ERR_TIMEOUT) return recover_after_timeout();
     if (meas < opt_.tol) {
       status = DONE_CONVERGED;
-    } else if (u.done == DONE_BREAKDOWN) {
+    } else if (u.done == DONE_BREAKDOWN && (!(u.err & DEV_ERR_BREAKDOWN) || (u.err & DEV_ERR_NONFINITE) ||
+                                            restarts >= 4 || updates >= opt_.max_outer)) {
       status = DONE_BREAKDOWN;
+    } else if (u.done == DONE_BREAKDOWN) {
+      // s.w == 0: the FP32 recursion lost its search direction before the FP64
+      // residual met the test; restart it from the replaced residual (s = rh)
+      const int running = DONE_RUNNING;
+      const unsigned keep = u.err & ~(unsigned)DEV_ERR_BREAKDOWN;
+      cudaMemcpyAsync(&sc_->done, &running, sizeof(int), cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(&sc_->err, &keep, sizeof(unsigned), cudaMemcpyHostToDevice, s);
+      k_copy<float><<<nblocks_, kThreads, 0, s>>>(g_, ws_.order_fwd, A.q, A.s, sc_);
+      cudaMemsetAsync(&sc_->beta, 0, sizeof(double), s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) return check_dev_error("mixed restart");
+      launches_ += 1;
+      restarts++;
     } else if (u.done == DONE_MAXITER || launched >= max_chunks || updates >= opt_.max_outer) {
       status = DONE_MAXITER;
     } else if (grew || !(meas < meas_u)) {

@@ -120,6 +120,39 @@ def test_p2g_matches_oracle(oracle, torch_mod, n):
         np.testing.assert_array_equal(got[g + "last"], got[g])
 
 
+def _p2g_box_inputs(dims, h, seed, ppc=3):
+    """Jittered particles in every cell of a non-cubic grid, plus particles on
+    cell faces and centres (where the nearest-node tests round) and outside."""
+    rng = np.random.default_rng(seed)
+    ext = np.array(dims) * h
+    n = int(np.prod(dims)) * ppc
+    pos = rng.uniform(0, 1, (n, 3)) * ext
+    faces = rng.integers(0, 2 * min(dims) + 1, (300, 3)) * (h / 2)
+    outside = rng.uniform(-1.5 * h, ext + 1.5 * h, (60, 3))
+    pos = np.concatenate([pos, faces, outside])
+    return pos, rng.normal(size=pos.shape)
+
+
+@pytest.mark.parametrize("dims", [(40, 24, 33), (9, 17, 8)])
+def test_p2g_non_cubic_matches_oracle_and_repeats_bit_for_bit(oracle, torch_mod, dims):
+    """Several 8^3 tiles with partial tiles at the far faces; the sums are the
+    same bit for bit on every run (no atomics on the regular path)."""
+    from simcraft_b200 import fluid
+    t = torch_mod
+    h = 1.0 / max(dims)
+    pos, vel = _p2g_box_inputs(dims, h, 31)
+    ref = oracle.p2g(pos, vel, dims, h, flip=True)
+    runs = [{k: a.cpu().numpy() for k, a in fluid.p2g(_dev(t, pos), _dev(t, vel), dims, h, flip=True).items()}
+            for _ in range(3)]
+    for g in "uvw":
+        np.testing.assert_array_equal(runs[0][g + "valid"], ref[g + "valid"])
+        np.testing.assert_allclose(runs[0][g + "w"], ref[g + "w"], rtol=1e-13, atol=1e-15)
+        np.testing.assert_allclose(runs[0][g], ref[g], rtol=1e-12, atol=1e-13)
+    for r in runs[1:]:
+        for k in runs[0]:
+            np.testing.assert_array_equal(r[k], runs[0][k])
+
+
 def test_p2g_empty_and_permutation_invariant(oracle, torch_mod):
     from simcraft_b200 import fluid
     t = torch_mod

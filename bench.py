@@ -551,8 +551,10 @@ def surface_leg(dev, ctx, sim, h, cpu):
     return out
 
 
-def flip_leg(args, dev, ctx, dist, rank, world):
-    """FLIP substeps/s on the 256^3 FP32 dam break (device-resident particles)."""
+def flip_run(args, dev, ctx, dist, rank, world, steps, tau):
+    """`steps` FLIP substeps timed after args.warmup untimed ones on the 256^3
+    FP32 dam break (device-resident particles), MIC(0) tau = `tau`; returns
+    the result dict and the simulator."""
     import torch
 
     from simcraft_b200 import scenes
@@ -563,7 +565,7 @@ def flip_leg(args, dev, ctx, dist, rank, world):
     pos, vel, h = scenes.dam_break(n, seed=4)
     sim = FluidSimulator(len(pos), (1.0, 1.0, 1.0), (n, n, n), context=ctx, precision="f32",
                          flip_alpha=0.95, cfl_factor=1.0, pcg_tol=TOL, pcg_max_iter=5000,
-                         pcg_criterion=CRIT_REL_L2, pcg_precision=PREC_MIXED)
+                         pcg_criterion=CRIT_REL_L2, pcg_precision=PREC_MIXED, pcg_mic_tau=tau)
     sim.set_initial_fluid(pos, vel)
     n_particles = len(pos)
     del pos, vel
@@ -584,7 +586,7 @@ def flip_leg(args, dev, ctx, dist, rank, world):
     launches = 0
     unconverged, flags = 0, 0
     e0.record(stream)
-    for _ in range(args.flip_steps):
+    for _ in range(steps):
         st = one()
         for k, v in st.items():
             if k.startswith("ms_"):
@@ -598,24 +600,44 @@ def flip_leg(args, dev, ctx, dist, rank, world):
     from simcraft_b200.replicas import Replicas
 
     ms = Replicas(rank, world, dist, dev).max(e0.elapsed_time(e1))
-    K = args.flip_steps
+    K = steps
     out = {"workload": f"FLIP dam break {n}^3, block x<0.5 y<0.5, 8 particles/cell, FP32 particles and grids, "
-                       f"CFL factor 1, FLIP 0.95, mixed MIC(0)-PCG to {TOL:g}",
+                       f"CFL factor 1, FLIP 0.95, mixed MIC(0)-PCG (tau {tau:g}, sigma 0.25) to {TOL:g}",
            "particles": n_particles, "steps": K, "warmup": args.warmup,
            "steps_per_s": world * K / (ms * 1e-3), "ms_per_step": ms / K,
            "split_ms_per_step": {k: v / K for k, v in split.items()},
            "pcg_inner_iterations_mean": float(np.mean(iters)), "gpu_launches": int(launches),
-           "pcg_solves_not_converged": int(unconverged), "pcg_device_flags": int(flags),
-           "steps_note": (f"{K} of the configuration's 100 substeps are timed (--flip-steps 100 times all of "
-                          f"them): each substep takes about a second, and the default run keeps the timed work "
-                          f"near a minute; the timed substeps follow the warm-up ones from the same initial "
-                          f"block, where the flow and the iteration counts are still developing")}
+           "pcg_solves_not_converged": int(unconverged), "pcg_device_flags": int(flags)}
+    return out, sim, h
+
+
+def flip_leg(args, dev, ctx, dist, rank, world):
+    """FLIP substeps/s on the 256^3 FP32 dam break with the reference's MIC(0)
+    constants, and the configuration's 100 substeps with tau = 0."""
+    import torch
+
+    K = args.flip_steps
+    out, sim, h = flip_run(args, dev, ctx, dist, rank, world, K, 0.97)
+    out["steps_note"] = (
+        f"{K} substeps timed after {args.warmup} warm-up ones (substeps {args.warmup}-{args.warmup + K - 1} from the "
+        f"initial block). The configuration's 100 substeps are not reachable with the reference's MIC(0) constants "
+        f"(tau 0.97, sigma 0.25): on this scene the preconditioner stalls from substep ~15 (5000 iterations short of "
+        f"the tolerance, FP64 and mixed alike; its tau terms divide by E^2) and by substep ~18 the unprojected "
+        f"velocities make the system non-finite. flip_100 is the same run over 100 substeps with tau = 0 (IC(0), "
+        f"the same preconditioner code)")
     if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = flip_cpu_sample(sim, n, h)
+        out["cpu_baseline"] = flip_cpu_sample(sim, sim.dims[0], h)
     if args.surface:
         out["surface"] = surface_leg(dev, ctx, sim, h, rank == 0 and world == 1 and not args.no_cpu)
     del sim
     torch.cuda.empty_cache()
+    if args.flip100 > 0:
+        o100, sim, _ = flip_run(args, dev, ctx, dist, rank, world, args.flip100, 0.0)
+        o100["steps_note"] = (f"the configuration's {args.flip100} substeps, timed after {args.warmup} warm-up "
+                              f"ones, with MIC(0) tau = 0 (IC(0)): every solve reaches the tolerance")
+        out["flip_100"] = o100
+        del sim
+        torch.cuda.empty_cache()
     return out
 
 
@@ -739,6 +761,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--flip-steps", type=int, default=10, help="timed FLIP substeps (0 skips the FLIP leg)")
     ap.add_argument("--flip-n", type=int, default=FLIP_N, help="FLIP dam-break grid size (profiling runs)")
+    ap.add_argument("--flip100", type=int, default=100,
+                    help="substeps of the tau = 0 FLIP run (the configuration's 100; 0 skips it)")
     ap.add_argument("--skip-solve", action="store_true",
                     help="run only the FLIP leg (profiling runs; prints the FLIP object)")
     ap.add_argument("--solve-n", type=int, default=N_GRID, help="standalone solve grid size")

@@ -124,7 +124,8 @@ typedef struct {
   double true_linf;      /* ||b - A p||_inf recomputed in FP64 */
   double ms;             /* device time of the solve */
   double sym_err;        /* max asymmetry found when check_symmetry is set */
-  unsigned device_flags; /* device-side error bits: 1 wait timeout, 2 non-finite, 4 breakdown */
+  unsigned device_flags; /* device-side error bits: 1 wait timeout, 2 non-finite, 4 breakdown;
+                            8: a mixed solve whose FP32 iteration left the FP32 range, solved again in FP64 */
   int64_t kernel_launches; /* kernels this call launched (CUDA-graph nodes counted) */
 } sc_pcg_stats;
 

@@ -16,6 +16,7 @@ enum : unsigned {
   DEV_ERR_TIMEOUT = 1u,     // a bounded spin-wait gave up
   DEV_ERR_NONFINITE = 2u,   // NaN/Inf in a reduction
   DEV_ERR_BREAKDOWN = 4u,   // PCG breakdown (s.As == 0)
+  DEV_FLAG_FP64_RERUN = 8u, // (host) the mixed solve left the FP32 range and was solved again in FP64
 };
 
 constexpr int kWarp = 32;

@@ -788,8 +788,11 @@ int DiffSim::step_t(int t, int mode, const void* in, void* out) {
     k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, c_.recon_factor * h, start_, cnt_, S.px, S.py, S.pz,
                                              sdf_[scur_], sdfv_[svcur_]);
     launches_ += 1 + launch_iter_cells<ITER_SDF>(st, G, c_.sdf_extrap_iters, sdf_, sdfv_, scur_, svcur_);
-    int unused = 0;
-    launches_ += launch_iter_cells<ITER_SMOOTH>(st, G, c_.smooth_iters, sdf_, nullptr, scur_, unused);
+    for (int k = 0; k < c_.smooth_iters; k++) {
+      k_smooth_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_]);
+      scur_ = 1 - scur_;
+    }
+    launches_ += c_.smooth_iters;
     if (mode == TAPE_RECORD)
       cudaMemcpyAsync(tape_sdf_ + (size_t)t * N, sdf_[scur_], sizeof(double) * N, cudaMemcpyDeviceToDevice, st);
   }

@@ -234,12 +234,15 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
   k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, c_.recon_factor * h, start_, cnt_, P.px, P.py, P.pz,
                                            sdf_[scur_], sdfv_[svcur_]);
   launches_ += 1;
-  // extrapolateFluidSdf(10) and smoothFluidSurface(5), temporally blocked
+  // extrapolateFluidSdf(10), temporally blocked
   launches_ += launch_iter_cells<ITER_SDF>(st, G, c_.sdf_extrap_iters, sdf_, sdfv_, scur_, svcur_);
-  {
-    int unused = 0;
-    launches_ += launch_iter_cells<ITER_SMOOTH>(st, G, c_.smooth_iters, sdf_, nullptr, scur_, unused);
+  // smoothFluidSurface(5): one launch per pass (all cells change each pass,
+  // so a blocked version has nothing to skip and measured slower)
+  for (int it = 0; it < c_.smooth_iters; it++) {
+    k_smooth_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_]);
+    scur_ = 1 - scur_;
   }
+  launches_ += c_.smooth_iters;
   const double* fluid = sdf_[scur_];
   cudaEventRecord(ev_[2], st);
   // P2G + Dirichlet walls + extrapolation + gravity (fluid-simulator.cc:155-164)

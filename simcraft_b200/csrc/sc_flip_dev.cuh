@@ -95,6 +95,25 @@ __device__ __forceinline__ void make_stencil(Stencil<T>& S, T px, T py, T pz, T 
     }
 }
 
+// make_stencil with every division by h done as a multiplication by 1/h when
+// h is a power of two, where the two are the same operation (the bases and
+// factors equal make_stencil's bit for bit); pow2 false divides.
+template <class T>
+__device__ __forceinline__ void make_stencil_pow2(Stencil<T>& S, T px, T py, T pz, T h, T inv, bool pow2) {
+  const T p[3] = {px, py, pz};
+  auto over = [&](T x) { return pow2 ? rmul(x, inv) : rdiv(x, h); };
+#pragma unroll
+  for (int ax = 0; ax < 3; ax++)
+#pragma unroll
+    for (int o = 0; o < 2; o++) {
+      const T off = o ? T(0.5) : T(0);
+      const int b = (int)radd(over(rsub(rsub(p[ax], T(0)), rmul(off, h))), T(0.5)) - 1;
+      S.base[ax][o] = b;
+#pragma unroll
+      for (int i = 0; i < 4; i++) S.w[ax][o][i] = bspline(over(fabs(rsub(p[ax], coord1(b + i, off, h)))));
+    }
+}
+
 // The same stencil with its nearest-node bases taken from a record of an
 // earlier run (tb: 6 int16 per particle, [axis][offset]); tb == nullptr
 // computes them.  The differentiable step replays recorded bases so that the
@@ -567,9 +586,8 @@ __global__ void __launch_bounds__(kT)
 }
 
 // ---- the iterated grid passes, temporally blocked ----
-// extrapolate(.., 10) per face grid (cpu/fluid-simulator.h:204-253),
-// extrapolateFluidSdf(10) (:123-166) and smoothFluidSurface(5)
-// (fluid-simulator.cc:39-74) are Jacobi-style passes over two buffers: pass k
+// extrapolate(.., 10) per face grid (cpu/fluid-simulator.h:204-253) and
+// extrapolateFluidSdf(10) (:123-166) are Jacobi-style passes over two buffers: pass k
 // reads buffer k mod 2 and writes buffer (k + 1) mod 2, and a cell a pass does
 // not write keeps that buffer's older value.  One launch runs up to kIterHalo
 // passes: a block loads its tile plus a halo of kIterHalo cells (both value
@@ -577,11 +595,13 @@ __global__ void __launch_bounds__(kT)
 // over a region that shrinks by one cell per pass, and writes its tile back:
 // both buffers and both flag arrays, or, for the differentiable step, each
 // pass's flags into their history.  The passes and their arithmetic are those
-// of k_extrap_face, k_extrap_sdf and k_smooth_sdf, so the results are the same
-// bit for bit.  A tile whose loaded region holds no valid flag is left as it is
-// (every pass would leave it so), but for the SDF flags, which the passes
-// rewrite with zeros.
-enum { ITER_FACE = 0, ITER_SDF = 1, ITER_SMOOTH = 2 };
+// of k_extrap_face and k_extrap_sdf, so the results are the same bit for bit.
+// Two kinds of tile need no values: one whose loaded region holds no valid
+// flag (the face passes would write zeros where the buffers hold zeros
+// already; the SDF passes would leave the values and write zero flags), and
+// one whose cells are all valid (the passes leave the values and set the
+// flags).  Only the tiles along the front of the valid region run the passes.
+enum { ITER_FACE = 0, ITER_SDF = 1 };
 constexpr int kIterThreads = 512;
 constexpr int kIterHalo = 5;  // passes per launch at most
 template <class T>
@@ -625,7 +645,6 @@ template <class T, int MODE>
 __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char* smem) {
   constexpr int TX = IterTile<T>::X, TY = IterTile<T>::Y, TZ = IterTile<T>::Z, H = kIterHalo;
   constexpr int RX = TX + 2 * H, RY = TY + 2 * H, RZ = TZ + 2 * H, RN = RX * RY * RZ;
-  constexpr bool FLAGS = MODE != ITER_SMOOTH;
   T* V = reinterpret_cast<T*>(smem);                        // [2][RN]: side 0 = buffer cur
   uint8_t* F = reinterpret_cast<uint8_t*>(V + 2 * RN);     // [2][RN]
   const int dx = G.dx, dy = G.dy, dz = G.dz;
@@ -635,35 +654,87 @@ __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char
   const T* bs = G.b[G.cur];
   const T* bd = G.b[1 - G.cur];
   const uint8_t* fs = G.hist ? G.hist : G.f[G.cur];
-  int any = 0;
-  for (int e = threadIdx.x; e < RN; e += blockDim.x) {
+  // region cell e -> global index (or -1 outside the grid)
+  auto gidx = [&](int e) -> int64_t {
     const int i = e / (RY * RZ), r = e - i * (RY * RZ), j = r / RZ, k = r - j * RZ;
     const int gx = x0 + i, gy = y0 + j, gz = z0 + k;
     const bool in = gx >= 0 && gx < dx && gy >= 0 && gy < dy && gz >= 0 && gz < dz;
-    const int64_t gi = in ? lin(gx, gy, gz, dy, dz) : 0;
-    V[e] = in ? bs[gi] : T(0);
-    V[RN + e] = in ? bd[gi] : T(0);
-    if (FLAGS) {
-      const uint8_t fv = in ? fs[gi] : 0;
-      F[e] = fv;
-      F[RN + e] = 0;  // out-of-domain cells are never written: they must read as invalid
-      any |= fv;
+    return in ? lin(gx, gy, gz, dy, dz) : -1;
+  };
+  constexpr int NB = 8;  // loads in flight per thread
+  {
+    // the flags first: a tile with no valid flag within reach needs no values
+    int any = 0, all = 1;  // a valid cell within reach; every in-grid tile cell valid
+    for (int e0 = threadIdx.x; e0 < RN; e0 += NB * blockDim.x) {
+      uint8_t fv[NB];
+      int64_t gv[NB];
+#pragma unroll
+      for (int u = 0; u < NB; u++) {
+        const int e = e0 + u * (int)blockDim.x;
+        gv[u] = e < RN ? gidx(e) : -1;
+        fv[u] = gv[u] >= 0 ? fs[gv[u]] : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < NB; u++) {
+        const int e = e0 + u * (int)blockDim.x;
+        if (e < RN) {
+          F[e] = fv[u];
+          F[RN + e] = 0;  // cells no pass writes (outside the grid) read as invalid
+          any |= fv[u];
+          const int i = e / (RY * RZ), r = e - i * (RY * RZ), j = r / RZ, k = r - j * RZ;
+          if (gv[u] >= 0 && i >= H && i < H + TX && j >= H && j < H + TY && k >= H && k < H + TZ) all &= fv[u];
+        }
+      }
     }
-  }
-  if (FLAGS && !__syncthreads_or(any)) {
-    // no valid cell within reach: the face passes would write zeros where the
-    // buffers hold zeros already; the SDF passes leave the values and write
-    // zero flags into the buffers they write
-    if (MODE == ITER_SDF && !G.hist)
+    if (__syncthreads_and(all)) {
+      // every tile cell valid: each pass leaves the values and sets the flags
       for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
         const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
         const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
         if (gx >= dx || gy >= dy || gz >= dz) continue;
         const int64_t gi = lin(gx, gy, gz, dy, dz);
-        G.f[1 - G.cur][gi] = 0;
-        if (nit > 1) G.f[G.cur][gi] = 0;
+        if (G.hist) {
+          for (int p = 1; p <= nit; p++) G.hist[(int64_t)p * G.hstride + gi] = 1;
+        } else {
+          G.f[0][gi] = 1;
+          G.f[1][gi] = 1;
+        }
       }
-    return;
+      return;
+    }
+    if (!__syncthreads_or(any)) {
+      // no valid cell within reach: the face passes would write zeros where the
+      // buffers hold zeros already; the SDF passes leave the values and write
+      // zero flags into the buffers they write
+      if (MODE == ITER_SDF && !G.hist)
+        for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
+          const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
+          const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
+          if (gx >= dx || gy >= dy || gz >= dz) continue;
+          const int64_t gi = lin(gx, gy, gz, dy, dz);
+          G.f[1 - G.cur][gi] = 0;
+          if (nit > 1) G.f[G.cur][gi] = 0;
+        }
+      return;
+    }
+  }
+  for (int e0 = threadIdx.x; e0 < RN; e0 += NB * blockDim.x) {
+    T va[NB], vb[NB];
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+      const int e = e0 + u * (int)blockDim.x;
+      const int64_t gi = e < RN ? gidx(e) : -1;
+      va[u] = gi >= 0 ? bs[gi] : T(0);
+      vb[u] = gi >= 0 ? bd[gi] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+      const int e = e0 + u * (int)blockDim.x;
+      if (e < RN) {
+        V[e] = va[u];
+        V[RN + e] = vb[u];
+      }
+    }
   }
   __syncthreads();
   constexpr int sX = RY * RZ, sY = RZ;
@@ -674,30 +745,13 @@ __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char
     const uint8_t* Fs = F + src * RN;
     uint8_t* Fd = F + (1 - src) * RN;
     // cells whose six neighbours still hold the data of p passes
-    constexpr int CX = RX - 2, CY = RY - 2, CZ = RZ - 2;
-    const int lo = p + 1, nxr = RX - 2 * (p + 1), nyr = RY - 2 * (p + 1), nzr = RZ - 2 * (p + 1);
-    (void)CX;
-    (void)CY;
-    (void)CZ;
-    for (int q = threadIdx.x; q < nxr * nyr * nzr; q += blockDim.x) {
-      const int a = q / (nyr * nzr), r = q - a * (nyr * nzr), b = r / nzr, c = r - b * nzr;
-      const int i = lo + a, j = lo + b, k = lo + c;
+    const int lo = p + 1;
+    for (int e = threadIdx.x; e < RN; e += blockDim.x) {
+      const int i = e / sX, r = e - i * sX, j = r / sY, k = r - j * sY;
+      if (i < lo || i >= RX - lo || j < lo || j >= RY - lo || k < lo || k >= RZ - lo) continue;
       const int gx = x0 + i, gy = y0 + j, gz = z0 + k;
       if (gx < 0 || gx >= dx || gy < 0 || gy >= dy || gz < 0 || gz >= dz) continue;
-      const int e = i * sX + j * sY + k;
-      if (MODE == ITER_SMOOTH) {
-        T sum = T(0);
-        int cnt = 0;
-        if (gx > 0) { sum = radd(sum, Vs[e - sX]); cnt++; }
-        if (gx < dx - 1) { sum = radd(sum, Vs[e + sX]); cnt++; }
-        if (gy > 0) { sum = radd(sum, Vs[e - sY]); cnt++; }
-        if (gy < dy - 1) { sum = radd(sum, Vs[e + sY]); cnt++; }
-        if (gz > 0) { sum = radd(sum, Vs[e - 1]); cnt++; }
-        if (gz < dz - 1) { sum = radd(sum, Vs[e + 1]); cnt++; }
-        T v = rdiv(sum, (T)cnt);
-        if (Vs[e] < v) v = Vs[e];
-        Vd[e] = v;
-      } else {
+      {
         uint8_t fl;
         if (Fs[e]) {
           fl = 1;
@@ -735,7 +789,7 @@ __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char
     const int le = (H + i) * sX + (H + j) * sY + (H + k);
     G.b[G.cur][gi] = V[le];
     G.b[1 - G.cur][gi] = V[RN + le];
-    if (FLAGS && !G.hist) {
+    if (!G.hist) {
       G.f[G.cur][gi] = F[le];
       G.f[1 - G.cur][gi] = F[RN + le];
     }
@@ -805,8 +859,8 @@ int launch_extrap_faces(cudaStream_t st, const Geo& G, int iters, T* const b[3][
   }
   return launches;
 }
-// `iters` passes of extrapolateFluidSdf (MODE ITER_SDF, flags f[2]) or of
-// smoothFluidSurface (ITER_SMOOTH) over the cell grid; cur and fcur flip per pass.
+// `iters` passes of extrapolateFluidSdf over the cell grid (flags f[2]); cur
+// and fcur flip per pass.
 template <int MODE>
 int launch_iter_cells(cudaStream_t st, const Geo& G, int iters, double* const b[2], uint8_t* const f[2], int& cur,
                       int& fcur) {
@@ -1361,12 +1415,13 @@ constexpr size_t g2p_smem_bytes(bool flip) {
 }
 template <class T>
 __global__ void __launch_bounds__(kG2PThreads)
-    k_g2p_tiles(Geo G, double hd, double alphad, const int* __restrict__ start, const int* __restrict__ cnt,
-                PartsT<T> P, const T* u, const T* v, const T* w, const T* ul, const T* vl, const T* wl) {
+    k_g2p_tiles(Geo G, double hd, double alphad, int pow2, const int* __restrict__ start,
+                const int* __restrict__ cnt, PartsT<T> P, const T* u, const T* v, const T* w, const T* ul,
+                const T* vl, const T* wl) {
   extern __shared__ __align__(16) unsigned char g2p_dyn[];
   T* R = reinterpret_cast<T*>(g2p_dyn);  // [grid][region]: u, v, w, then u, v, w last
   __shared__ int rbeg[kPT * kPT], rend[kPT * kPT];
-  const T h = (T)hd;
+  const T h = (T)hd, hinv = (T)(1.0 / hd);
   const bool flip = alphad >= 0.0;
   const int ntz = (G.nz + kPT - 1) / kPT, nty = (G.ny + kPT - 1) / kPT;
   const int tz = blockIdx.x % ntz, ty = (blockIdx.x / ntz) % nty, tx = blockIdx.x / (ntz * nty);
@@ -1402,7 +1457,7 @@ __global__ void __launch_bounds__(kG2PThreads)
     for (int i = rbeg[col] + lane; i < e; i += 32) {
       const T px = P.px[i], py = P.py[i], pz = P.pz[i];
       Stencil<T> S;
-      make_stencil(S, px, py, pz, h);
+      make_stencil_pow2(S, px, py, pz, h, hinv, pow2 != 0);
       const bool in = g2p_in_region<T, 0>(S, x0, y0, z0) && g2p_in_region<T, 1>(S, x0, y0, z0) &&
                       g2p_in_region<T, 2>(S, x0, y0, z0);
       if (in && g2p_inner(S, G)) {
@@ -1469,8 +1524,10 @@ int launch_g2p_tiles(cudaStream_t st, const Geo& G, double h, double alpha, cons
     attr = true;
   }
   const bool flip = alpha >= 0.0;
-  k_g2p_tiles<T><<<(unsigned)p2g_ntiles(G), kG2PThreads, g2p_smem_bytes<T>(flip), st>>>(G, h, alpha, start, cnt, P, u,
-                                                                                      v, w, ul, vl, wl);
+  int ex = 0;
+  const int pow2 = std::frexp(h, &ex) == 0.5 ? 1 : 0;
+  k_g2p_tiles<T><<<(unsigned)p2g_ntiles(G), kG2PThreads, g2p_smem_bytes<T>(flip), st>>>(G, h, alpha, pow2, start, cnt,
+                                                                                      P, u, v, w, ul, vl, wl);
   return 1;
 }
 

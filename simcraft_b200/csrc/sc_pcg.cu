@@ -36,6 +36,11 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kRing = 32;     // boundary ring entries per wavefront CTA
+// Nanoseconds a mailbox loader sleeps between two polls that found nothing
+// (0: it polls back to back).
+#ifndef SC_WAVE_POLL_NS
+#define SC_WAVE_POLL_NS 0
+#endif
 // 1: the iterations sweep only the tiles holding an active cell; 0: every tile
 #ifndef SC_SKIP_EMPTY_TILES
 #define SC_SKIP_EMPTY_TILES 1
@@ -452,7 +457,7 @@ __global__ void __launch_bounds__(kThreads)
 // The sum is the same as apply_row_pcg's, term for term.  A work item is the
 // TY row warps of one tile over a run of consecutive slots.
 template <class T>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 3)
     k_spmv_stream(Tiled g, const int2* __restrict__ tiles, const T* __restrict__ adiag, const T* __restrict__ al,
                   const T* __restrict__ ad, const T* __restrict__ ab, const uint8_t* __restrict__ act,
                   const T* __restrict__ x, T* __restrict__ y, double* partials, PcgScalars* sc, int use_skip,
@@ -487,24 +492,46 @@ __global__ void __launch_bounds__(kThreads, 4)
       x_p = __ldg(x + row + (int64_t)sp * RS);
     T al_c = __ldg(al + row + (int64_t)s0 * RS), al_p = __ldg(al + row + (int64_t)sp * RS);
     T ab_c = __ldg(ab + row + (int64_t)s0 * RS), ab_p = __ldg(ab + row + (int64_t)sp * RS);
+    // the other loads of a slot are issued one slot ahead too (slot sp is a
+    // valid slot index at the end of the run as well, so they stay in bounds)
+    const bool ex0 = tx == 0 && hx, ex31 = tx == 31 && px;
+    T d_n = __ldg(adiag + row + (int64_t)s0 * RS), adc_n = __ldg(ad + row + (int64_t)s0 * RS);
+    uint8_t a_n = __ldg(act + row + (int64_t)s0 * RS);
+    T ym_n = hy ? __ldg(x + rym + (int64_t)s0 * RS) : T(0), yp_n = py ? __ldg(x + ryp + (int64_t)s0 * RS) : T(0),
+      adp_n = py ? __ldg(ad + ryp + (int64_t)s0 * RS) : T(0);
+    T xme_n = ex0 ? __ldg(x + rxm + (int64_t)s31 * RS) : T(0), xpe_n = ex31 ? __ldg(x + rxp + (int64_t)sm31 * RS) : T(0),
+      alpe_n = ex31 ? __ldg(al + rxp + (int64_t)sm31 * RS) : T(0);
     for (int s = s0; s < s1; s++) {
       const int64_t e = row + (int64_t)s * RS;
       const int s2 = wrap(sp + 1);
-      // next window entries first: their latency overlaps this slot's work
+      const T d = d_n, adc = adc_n, ymv = ym_n, ypv = yp_n, adp = adp_n, xme = xme_n, xpe = xpe_n, alpe = alpe_n;
+      const bool a = inside && a_n;
+      // next window entries and the next slot's loads first: their latency
+      // overlaps this slot's work
       const T x_n = __ldg(x + row + (int64_t)s2 * RS), al_n = __ldg(al + row + (int64_t)s2 * RS),
               ab_n = __ldg(ab + row + (int64_t)s2 * RS);
-      const T d = __ldg(adiag + e), adc = __ldg(ad + e);
-      const bool a = inside && __ldg(act + e);
+      {
+        const int64_t en = row + (int64_t)sp * RS;
+        const int s31n = wrap(s31 + 1), sm31n = wrap(sm31 + 1);
+        d_n = __ldg(adiag + en);
+        adc_n = __ldg(ad + en);
+        a_n = __ldg(act + en);
+        ym_n = hy ? __ldg(x + rym + (int64_t)sp * RS) : T(0);
+        yp_n = py ? __ldg(x + ryp + (int64_t)sp * RS) : T(0);
+        adp_n = py ? __ldg(ad + ryp + (int64_t)sp * RS) : T(0);
+        xme_n = ex0 ? __ldg(x + rxm + (int64_t)s31n * RS) : T(0);
+        xpe_n = ex31 ? __ldg(x + rxp + (int64_t)sm31n * RS) : T(0);
+        alpe_n = ex31 ? __ldg(al + rxp + (int64_t)sm31n * RS) : T(0);
+      }
       const bool hz = z > 0, pz = z < nz - 1;
-      const T ym = hy ? __ldg(x + rym + (int64_t)s * RS) : x_c;
-      const T yp = py ? __ldg(x + ryp + (int64_t)s * RS) : x_c;
-      const T adp = py ? __ldg(ad + ryp + (int64_t)s * RS) : T(0);
+      const T ym = hy ? ymv : x_c;
+      const T yp = py ? ypv : x_c;
       T xm = __shfl_up_sync(kFull, x_m, 1), xp = __shfl_down_sync(kFull, x_p, 1),
         alp = __shfl_down_sync(kFull, al_p, 1);
-      if (tx == 0) xm = hx ? __ldg(x + rxm + (int64_t)s31 * RS) : x_c;
+      if (tx == 0) xm = hx ? xme : x_c;
       if (tx == 31) {
-        xp = px ? __ldg(x + rxp + (int64_t)sm31 * RS) : x_c;
-        alp = px ? __ldg(al + rxp + (int64_t)sm31 * RS) : T(0);
+        xp = px ? xpe : x_c;
+        alp = px ? alpe : T(0);
       }
       if (!hx) xm = x_c;
       if (!px) xp = x_c;
@@ -1066,6 +1093,9 @@ __device__ __forceinline__ void wave_abort(const WaveArgs& a, WaveShared<T, TY>&
 __device__ __forceinline__ bool wave_should_stop(const WaveArgs& a, int& spins,
                                                  volatile int* s_abort, int limit) {
   if (*s_abort) return true;
+#if SC_WAVE_POLL_NS > 0
+  __nanosleep(SC_WAVE_POLL_NS);  // back off between polls of a mailbox loader
+#endif
   ++spins;
   if ((spins & 63) == 0 && (ld_relaxed_gpu_u32(&a.sc->err) & DEV_ERR_TIMEOUT)) return true;
   return spins > limit;
@@ -2135,13 +2165,13 @@ void PcgSolver::select_active_tiles() {
 
 template <class T>
 void PcgSolver::launch_spmv(SysArrays<T>& A, cudaStream_t st, int use_skip) {
-  // slot runs per tile: about 16 work items per SM (4 resident blocks x 4),
+  // slot runs per tile: about 12 work items per SM (3 resident blocks x 4),
   // runs of at least 16 slots; whole tiles as items left a partial last wave
   // at 512^3 (1024 tiles over 592 block slots)
   const int ntiles = g_.ntiles();
-  const int want = 16 * ctx_->sm_count;
+  const int want = 12 * ctx_->sm_count;
   const int chunks = std::max(1, std::min((want + ntiles - 1) / ntiles, g_.nz / 16));
-  const int grid = std::min(4 * ctx_->sm_count, ntiles * chunks);
+  const int grid = std::min(3 * ctx_->sm_count, ntiles * chunks);
   k_spmv_stream<T><<<grid, kThreads, 0, st>>>(g_, ws_.order_fwd, A.adiag, A.al, A.ad, A.ab, active_, A.s, A.Az, partials_, sc_,
                                               use_skip, chunks);
 }
@@ -2520,6 +2550,18 @@ int PcgSolver::solve(PcgStats* st) {
   cudaEventRecord(evt0_, ctx_->stream);
   int e = opt_.precision == PREC_MIXED ? solve_mixed(st) : solve_fp64(st);
   if (e) return e;
+  if (opt_.precision == PREC_MIXED && st->status == DONE_BREAKDOWN && (st->device_flags & DEV_ERR_NONFINITE)) {
+    // The FP32 recursion left the FP32 range (a preconditioner with very large
+    // eigenvalues: the reference's tau terms at some dt/h) while the system is
+    // finite: solve it again with the FP64 iteration.
+    PcgStats f{};
+    e = solve_fp64(&f);
+    if (e) return e;
+    st->iterations += f.iterations;
+    st->status = f.status;
+    st->residual = f.residual;
+    st->device_flags |= f.device_flags | DEV_FLAG_FP64_RERUN;
+  }
   cudaEventRecord(evt1_, ctx_->stream);
   cudaEventSynchronize(evt1_);
   float ms = 0;

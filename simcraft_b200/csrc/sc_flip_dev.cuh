@@ -997,6 +997,20 @@ __device__ __forceinline__ T p2g_factor(T p, int node, const P2GSpacing<T>& sp) 
   }
   return T(0);
 }
+// The same factor from q = p / h and the node's index plus offset c = b + i +
+// off: |q - c| is (p - c h) / h rounded once, which on a power-of-two grid is
+// the reference's rounding of p - c h scaled exactly, so the factor is the
+// same bit for bit; otherwise q carries one more rounding.
+template <class T>
+__device__ __forceinline__ T p2g_factor_q(T q, T c) {
+  const T r = fabs(rsub(q, c));
+  if (r < T(1)) return radd(rsub(T(2.0 / 3.0), rmul(r, r)), rmul(rmul(rmul(T(0.5), r), r), r));
+  if (r < T(2)) {
+    const T t = rsub(T(2), r);
+    return rmul(rmul(rmul(t, t), t), T(1.0 / 6.0));
+  }
+  return T(0);
+}
 // The reference's product order: (w_x w_y) w_z.
 template <class T>
 __device__ __forceinline__ T p2g_weight(T w0, T w1, T w2) {
@@ -1040,12 +1054,15 @@ __device__ void p2g_tile_grid(const Geo& G, const P2GSpacing<T>& h, int x0, int 
       }
       const int t = ip - sh;
       if (t < 0 || t > 3) continue;
-      const T wA = p2g_factor<T, AX, AX>(p[AX], bA + t, h);
+      // own axis: offset 0, across: 1/2
+      const T wA = p2g_factor_q(h.over(p[AX]), (T)(bA + t));
+      const T q1 = h.over(p[D1]), q2 = h.over(p[D2]);
+      const T c1 = radd((T)b1, T(0.5)), c2 = radd((T)b2, T(0.5));
       T w1[4], w2[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        w1[j] = p2g_factor<T, AX, D1>(p[D1], b1 + j, h);
-        w2[j] = p2g_factor<T, AX, D2>(p[D2], b2 + j, h);
+        w1[j] = p2g_factor_q(q1, radd(c1, (T)j));
+        w2[j] = p2g_factor_q(q2, radd(c2, (T)j));
       }
       const T v = vel[l];
 #pragma unroll

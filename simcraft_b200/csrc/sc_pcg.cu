@@ -36,11 +36,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kRing = 32;     // boundary ring entries per wavefront CTA
-// Nanoseconds a mailbox loader sleeps between two polls that found nothing
-// (0: it polls back to back).
-#ifndef SC_WAVE_POLL_NS
-#define SC_WAVE_POLL_NS 0
-#endif
 // 1: the iterations sweep only the tiles holding an active cell; 0: every tile
 #ifndef SC_SKIP_EMPTY_TILES
 #define SC_SKIP_EMPTY_TILES 1
@@ -1093,9 +1088,6 @@ __device__ __forceinline__ void wave_abort(const WaveArgs& a, WaveShared<T, TY>&
 __device__ __forceinline__ bool wave_should_stop(const WaveArgs& a, int& spins,
                                                  volatile int* s_abort, int limit) {
   if (*s_abort) return true;
-#if SC_WAVE_POLL_NS > 0
-  __nanosleep(SC_WAVE_POLL_NS);  // back off between polls of a mailbox loader
-#endif
   ++spins;
   if ((spins & 63) == 0 && (ld_relaxed_gpu_u32(&a.sc->err) & DEV_ERR_TIMEOUT)) return true;
   return spins > limit;

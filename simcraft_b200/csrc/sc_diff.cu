@@ -785,8 +785,9 @@ int DiffSim::step_t(int t, int mode, const void* in, void* out) {
     const double* src = mode == TAPE_REPLAY ? tape_sdf_ + (size_t)t * N : seg_sdf_in_;
     cudaMemcpyAsync(sdf_[scur_], src, sizeof(double) * N, cudaMemcpyDeviceToDevice, st);
   } else {
-    k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, c_.recon_factor * h, start_, cnt_, S.px, S.py, S.pz,
-                                             sdf_[scur_], sdfv_[svcur_]);
+    if (launch_reconstruct<T>(st, G, h, c_.recon_factor * h, start_, cnt_, S.px, S.py, S.pz, sdf_[scur_],
+                              sdfv_[svcur_]))
+      return ctx_->set_error(-1, "reconstruct: radius reaches past 6 cells");
     launches_ += 1 + launch_iter_cells<ITER_SDF>(st, G, c_.sdf_extrap_iters, sdf_, sdfv_, scur_, svcur_);
     for (int k = 0; k < c_.smooth_iters; k++) {
       k_smooth_sdf<<<nblk(N), kT, 0, st>>>(G, sdf_[scur_], sdf_[1 - scur_]);

@@ -231,8 +231,9 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
     cudaMemsetAsync(cnt_, 0, sizeof(int) * N, st);
     cudaMemsetAsync(start_, 0, sizeof(int) * N, st);
   }
-  k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, c_.recon_factor * h, start_, cnt_, P.px, P.py, P.pz,
-                                           sdf_[scur_], sdfv_[svcur_]);
+  if (launch_reconstruct<T>(st, G, h, c_.recon_factor * h, start_, cnt_, P.px, P.py, P.pz, sdf_[scur_],
+                            sdfv_[svcur_]))
+    return ctx_->set_error(-1, "reconstruct: radius reaches past 6 cells");
   launches_ += 1;
   // extrapolateFluidSdf(10), temporally blocked
   launches_ += launch_iter_cells<ITER_SDF>(st, G, c_.sdf_extrap_iters, sdf_, sdfv_, scur_, svcur_);
@@ -352,8 +353,8 @@ int FluidSim::reconstruct_t(double radius) {
     cudaMemsetAsync(cnt_, 0, sizeof(int) * N, st);
     cudaMemsetAsync(start_, 0, sizeof(int) * N, st);
   }
-  k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, radius, start_, cnt_, P.px, P.py, P.pz, sdf_[scur_],
-                                           sdfv_[svcur_]);
+  if (launch_reconstruct<T>(st, G, h, radius, start_, cnt_, P.px, P.py, P.pz, sdf_[scur_], sdfv_[svcur_]))
+    return ctx_->set_error(-1, "reconstruct: radius reaches past 6 cells");
   launches_ += 1;
   return err("reconstruct");
 }
@@ -602,9 +603,8 @@ int flip_reconstruct(cudaStream_t st, int64_t n, const double* pos, int nx, int 
   Sorted s;
   int e = make_sorted(s, st, n, pos, nullptr, G, h);
   if (e) return e;
-  const int64_t N = (int64_t)nx * ny * nz;
   PartsT<double> P = s.b.P();
-  k_reconstruct<double><<<nblk(N), kT, 0, st>>>(G, h, radius, s.start, s.cnt, P.px, P.py, P.pz, sdf, valid);
+  if (launch_reconstruct<double>(st, G, h, radius, s.start, s.cnt, P.px, P.py, P.pz, sdf, valid)) return -1;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

@@ -470,11 +470,36 @@ __global__ void __launch_bounds__(kT)
 // cell-centred SDF = min over particles within 2r of (|x - p| - r).  Each
 // bucket's last particle is skipped, as the reference's forNeighbours loop
 // stops one short of its inclusive end index (ns-util.h:76-77, 103).
+// The buckets the reference's loop can visit around a cell, as offsets from
+// the cell (packed dx + 8 | dy + 8 << 8 | dz + 8 << 16): every offset whose
+// bucket box comes within 2r of the cell centre (box distance, in units of h,
+// with a margin), the same set for every cell (a boundary bucket's open side
+// faces away from the cells that reach it).  A superset of the buckets the
+// loop keeps is harmless: only the nearest particle decides the result.
+struct ReconOffsets {
+  int n;
+  int d[1024];
+};
+inline bool recon_offsets(double h, double radius, ReconOffsets& o) {
+  const double R = 2.0 * radius / h;
+  const int D = (int)std::ceil(R + 0.5) + 1;
+  o.n = 0;
+  auto gap = [](int d) { return d == 0 ? 0.0 : std::abs(d) - 0.5; };
+  for (int dx = -D; dx <= D; dx++)
+    for (int dy = -D; dy <= D; dy++)
+      for (int dz = -D; dz <= D; dz++) {
+        const double g2 = gap(dx) * gap(dx) + gap(dy) * gap(dy) + gap(dz) * gap(dz);
+        if (g2 > R * R * (1.0 + 1e-6) + 1e-12) continue;
+        if (o.n >= 1024 || D > 7) return false;
+        o.d[o.n++] = (dx + 8) | ((dy + 8) << 8) | ((dz + 8) << 16);
+      }
+  return true;
+}
 template <class T>
 __global__ void __launch_bounds__(kT)
     k_reconstruct(Geo G, double h, double radius, const int* start, const int* cnt,
                   const T* __restrict__ px, const T* __restrict__ py, const T* __restrict__ pz,
-                  double* sdf, uint8_t* valid) {
+                  double* sdf, uint8_t* valid, const ReconOffsets off) {
   const int64_t N = (int64_t)G.nx * G.ny * G.nz;
   const double r2 = 2 * radius;
   GRID_LOOP(id, N) {
@@ -483,39 +508,24 @@ __global__ void __launch_bounds__(kT)
     const double cx = radd(rmul(radd((double)i, 0.5), h), 0.0);
     const double cy = radd(rmul(radd((double)j, 0.5), h), 0.0);
     const double cz = radd(rmul(radd((double)k, 0.5), h), 0.0);
-    const int x0 = max(0, (int)floor(rdiv(rsub(cx, r2), h))), x1 = min(G.nx - 1, (int)ceil(rdiv(radd(cx, r2), h)));
-    const int y0 = max(0, (int)floor(rdiv(rsub(cy, r2), h))), y1 = min(G.ny - 1, (int)ceil(rdiv(radd(cy, r2), h)));
-    const int z0 = max(0, (int)floor(rdiv(rsub(cz, r2), h))), z1 = min(G.nz - 1, (int)ceil(rdiv(radd(cz, r2), h)));
     // min over the candidates of |x - p| - r where |x - p| <= 2r: sqrt and the
     // subtraction are monotone and correctly rounded, so that is sqrt of the
     // least squared distance minus r, when its root passes the test (if the
     // nearest particle fails it, all do): one square root per cell
     double m2 = INFINITY;
-    const double lim = r2 * r2 * (1.0 + 1e-9);
-    // Distance from the cell centre to a bucket's cell box; boundary buckets
-    // also hold the particles clamped into them, so their boxes are open.
-    auto gap = [&](int a, int n, double c) {
-      const double lo = a > 0 ? a * h - c : -1e300, hi = a < n - 1 ? c - (a + 1) * h : -1e300;
-      return fmax(0.0, fmax(lo, hi));
-    };
-    for (int a = x0; a <= x1; a++) {
-      const double ex = gap(a, G.nx, cx);
-      for (int b = y0; b <= y1; b++) {
-        const double ey = gap(b, G.ny, cy);
-        if (ex * ex + ey * ey > lim) continue;
-        for (int c = z0; c <= z1; c++) {
-          const double ez = gap(c, G.nz, cz);
-          if (ex * ex + ey * ey + ez * ez > lim) continue;  // no particle of the bucket can be within 2r
-          const int cell = (int)lin(a, b, c, G.ny, G.nz);
-          const int m = cnt[cell];
-          if (m < 2) continue;
-          const int s = start[cell];
-          for (int l = s; l < s + m - 1; l++) {
-            const double dx = rsub((double)px[l], cx), dy = rsub((double)py[l], cy),
-                         dz = rsub((double)pz[l], cz);
-            m2 = fmin(m2, radd(radd(rmul(dx, dx), rmul(dy, dy)), rmul(dz, dz)));
-          }
-        }
+    for (int q = 0; q < off.n; q++) {
+      const int w = off.d[q];
+      const int a = i + (w & 255) - 8, b = j + ((w >> 8) & 255) - 8, c = k + ((w >> 16) & 255) - 8;
+      if (a < 0 || a >= G.nx || b < 0 || b >= G.ny || c < 0 || c >= G.nz) continue;
+      const int cell = (int)lin(a, b, c, G.ny, G.nz);
+      const int m = __ldg(cnt + cell);
+      if (m < 2) continue;
+      const int s = __ldg(start + cell);
+      // each bucket's last particle is skipped (the reference's forNeighbours
+      // loop stops one short of its inclusive end index)
+      for (int l = s; l < s + m - 1; l++) {
+        const double dx = rsub((double)px[l], cx), dy = rsub((double)py[l], cy), dz = rsub((double)pz[l], cz);
+        m2 = fmin(m2, radd(radd(rmul(dx, dx), rmul(dy, dy)), rmul(dz, dz)));
       }
     }
     double best = 1e9;
@@ -530,6 +540,17 @@ __global__ void __launch_bounds__(kT)
     sdf[id] = best;
     valid[id] = ok;
   }
+}
+// NaiveReconstructor::reconstruct over the sorted buckets; -1 when the radius
+// reaches past the offsets the kernel takes (over ~6 cells).
+template <class T>
+int launch_reconstruct(cudaStream_t st, const Geo& G, double h, double radius, const int* start, const int* cnt,
+                       const T* px, const T* py, const T* pz, double* sdf, uint8_t* valid) {
+  ReconOffsets off;
+  if (!recon_offsets(h, radius, off)) return -1;
+  const int64_t N = (int64_t)G.nx * G.ny * G.nz;
+  k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, radius, start, cnt, px, py, pz, sdf, valid, off);
+  return 0;
 }
 
 // extrapolateFluidSdf iteration (cpu/fluid-simulator.h:123-166): valid cells
@@ -1374,6 +1395,12 @@ __device__ __forceinline__ T g2p_gather_tile(const T* __restrict__ R, const Sten
   }
   return ws > T(0) ? rdiv(s, ws) : T(0);
 }
+// Unroll factor of the outer stencil loop of the branch-free G2P gathers.
+#ifndef SC_G2P_UNROLL_I
+#define SC_G2P_UNROLL_I 4
+#endif
+#define SC_STR(x) #x
+#define SC_UNROLL(n) _Pragma(SC_STR(unroll n))
 // All three (or six) staged gathers of a particle whose stencils lie inside
 // the grid: no node is skipped, so the loops are branch-free and the chains
 // of the grids interleave; each grid's sum keeps gather's order.
@@ -1387,7 +1414,7 @@ __device__ __forceinline__ void g2p_gather_tile_inner(const T* __restrict__ R, c
     s[q] = T(0);
     ws[q] = T(0);
   }
-#pragma unroll
+  SC_UNROLL(SC_G2P_UNROLL_I)
   for (int i = 0; i < 4; i++)
 #pragma unroll
     for (int j = 0; j < 4; j++) {

@@ -436,14 +436,57 @@ __global__ void __launch_bounds__(kT)
   }
 }
 
-// Order each cell's bucket by original particle index (insertion sort); the
-// reference's bucket order is then pinned (ns-util.h:65-69 uses std::sort).
+// Order each cell's bucket by original particle index; the reference's
+// bucket order is then pinned (ns-util.h:65-69 uses std::sort).  A bucket of
+// up to kSortSmall particles is permuted through shared memory (each index's
+// rank among the bucket's indices, then one read and one write per array
+// element); larger ones take an insertion sort in place.
+constexpr int kSortSmall = 16;
+__device__ __forceinline__ int64_t to_bits(float v) { return (int64_t)__float_as_uint(v); }
+__device__ __forceinline__ int64_t to_bits(double v) { return __double_as_longlong(v); }
+template <class T>
+__device__ __forceinline__ T from_bits(int64_t b);
+template <>
+__device__ __forceinline__ float from_bits<float>(int64_t b) { return __uint_as_float((unsigned)b); }
+template <>
+__device__ __forceinline__ double from_bits<double>(int64_t b) { return __longlong_as_double(b); }
 template <class T>
 __global__ void __launch_bounds__(kT)
     k_sort_cells(int64_t ncell, const int* start, const int* cnt, PartsT<T> P, int64_t* id) {
+  __shared__ int64_t buf[kSortSmall * kT];      // [slot][thread]
+  __shared__ unsigned char perm[kSortSmall * kT];  // destination slot -> source slot
+  const int t = threadIdx.x;
   GRID_LOOP(c, ncell) {
     const int64_t b = start[c];
     const int m = cnt[c];
+    if (m < 2) continue;
+    if (m <= kSortSmall) {
+      for (int l = 0; l < m; l++) buf[l * kT + t] = id[b + l];
+      for (int l = 0; l < m; l++) {
+        // rank by index, ties (none in a valid bucket) by slot: a permutation
+        const int64_t v = buf[l * kT + t];
+        int r = 0;
+        for (int k = 0; k < m; k++) {
+          const int64_t o = buf[k * kT + t];
+          r += o < v || (o == v && k < l);
+        }
+        perm[r * kT + t] = (unsigned char)l;
+      }
+      for (int r = 0; r < m; r++) id[b + r] = buf[perm[r * kT + t] * kT + t];
+      // values go through the same int64 buffer as their bit patterns (one
+      // type for every access: no aliasing between the id and value passes)
+      auto permute = [&](T* a) {
+        for (int l = 0; l < m; l++) buf[l * kT + t] = to_bits(a[b + l]);
+        for (int r = 0; r < m; r++) a[b + r] = from_bits<T>(buf[perm[r * kT + t] * kT + t]);
+      };
+      permute(P.px);
+      permute(P.py);
+      permute(P.pz);
+      permute(P.vx);
+      permute(P.vy);
+      permute(P.vz);
+      continue;
+    }
     for (int i = 1; i < m; i++) {
       int j = i;
       while (j > 0 && id[b + j - 1] > id[b + j]) {
@@ -1096,7 +1139,9 @@ __device__ void p2g_tile_grid(const Geo& G, const P2GSpacing<T>& h, int x0, int 
           f[D1] = w1[j];
           f[D2] = w2[k];
           const T wt = p2g_weight(f[0], f[1], f[2]);
-          as[j * 4 + k] = radd(as[j * 4 + k], rmul(v, wt));
+          // one fused multiply-add (the sums' order is not the reference's
+          // anyway, which adds from a parallel loop)
+          as[j * 4 + k] = fma(v, wt, as[j * 4 + k]);
           aw[j * 4 + k] = radd(aw[j * 4 + k], wt);
         }
     }
@@ -1395,12 +1440,6 @@ __device__ __forceinline__ T g2p_gather_tile(const T* __restrict__ R, const Sten
   }
   return ws > T(0) ? rdiv(s, ws) : T(0);
 }
-// Unroll factor of the outer stencil loop of the branch-free G2P gathers.
-#ifndef SC_G2P_UNROLL_I
-#define SC_G2P_UNROLL_I 4
-#endif
-#define SC_STR(x) #x
-#define SC_UNROLL(n) _Pragma(SC_STR(unroll n))
 // All three (or six) staged gathers of a particle whose stencils lie inside
 // the grid: no node is skipped, so the loops are branch-free and the chains
 // of the grids interleave; each grid's sum keeps gather's order.
@@ -1414,7 +1453,9 @@ __device__ __forceinline__ void g2p_gather_tile_inner(const T* __restrict__ R, c
     s[q] = T(0);
     ws[q] = T(0);
   }
-  SC_UNROLL(SC_G2P_UNROLL_I)
+  // fully unrolled: with the outer loop rolled (or "unroll 4") the kernel
+  // measured 5x slower, its warps stalled on instruction fetch
+#pragma unroll
   for (int i = 0; i < 4; i++)
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -1457,7 +1498,7 @@ template <class T>
 constexpr size_t g2p_smem_bytes(bool flip) {
   return sizeof(T) * (size_t)(flip ? 6 : 3) * kP2GRegion;
 }
-template <class T>
+template <class T, bool FLIP>
 __global__ void __launch_bounds__(kG2PThreads)
     k_g2p_tiles(Geo G, double hd, double alphad, int pow2, const int* __restrict__ start,
                 const int* __restrict__ cnt, PartsT<T> P, const T* u, const T* v, const T* w, const T* ul,
@@ -1466,7 +1507,7 @@ __global__ void __launch_bounds__(kG2PThreads)
   T* R = reinterpret_cast<T*>(g2p_dyn);  // [grid][region]: u, v, w, then u, v, w last
   __shared__ int rbeg[kPT * kPT], rend[kPT * kPT];
   const T h = (T)hd, hinv = (T)(1.0 / hd);
-  const bool flip = alphad >= 0.0;
+  constexpr bool flip = FLIP;
   const int ntz = (G.nz + kPT - 1) / kPT, nty = (G.ny + kPT - 1) / kPT;
   const int tz = blockIdx.x % ntz, ty = (blockIdx.x / ntz) % nty, tx = blockIdx.x / (ntz * nty);
   const int x0 = tx * kPT, y0 = ty * kPT, z0 = tz * kPT;
@@ -1564,14 +1605,22 @@ int launch_g2p_tiles(cudaStream_t st, const Geo& G, double h, double alpha, cons
                      PartsT<T> P, const T* u, const T* v, const T* w, const T* ul, const T* vl, const T* wl) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_g2p_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g2p_smem_bytes<T>(true));
+    cudaFuncSetAttribute(k_g2p_tiles<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)g2p_smem_bytes<T>(true));
+    cudaFuncSetAttribute(k_g2p_tiles<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)g2p_smem_bytes<T>(false));
     attr = true;
   }
   const bool flip = alpha >= 0.0;
   int ex = 0;
   const int pow2 = std::frexp(h, &ex) == 0.5 ? 1 : 0;
-  k_g2p_tiles<T><<<(unsigned)p2g_ntiles(G), kG2PThreads, g2p_smem_bytes<T>(flip), st>>>(G, h, alpha, pow2, start, cnt,
-                                                                                      P, u, v, w, ul, vl, wl);
+  const unsigned nt = (unsigned)p2g_ntiles(G);
+  if (flip)
+    k_g2p_tiles<T, true><<<nt, kG2PThreads, g2p_smem_bytes<T>(true), st>>>(G, h, alpha, pow2, start, cnt, P, u, v,
+                                                                           w, ul, vl, wl);
+  else
+    k_g2p_tiles<T, false><<<nt, kG2PThreads, g2p_smem_bytes<T>(false), st>>>(G, h, alpha, pow2, start, cnt, P, u, v,
+                                                                            w, ul, vl, wl);
   return 1;
 }
 

@@ -1498,8 +1498,16 @@ template <class T>
 constexpr size_t g2p_smem_bytes(bool flip) {
   return sizeof(T) * (size_t)(flip ? 6 : 3) * kP2GRegion;
 }
+// Four FP32 blocks of 256 threads per SM (64 registers a thread, no spills)
+// measured 25% faster than the register count the compiler picks on its own
+// (9.9 -> 7.4 ms for project + G2P of 33.5M particles); the FP64 kernel keeps
+// its registers, since its staged regions allow two blocks per SM anyway.
+template <class T>
+constexpr int g2p_min_blocks() {
+  return sizeof(T) == 4 ? 4 : 1;
+}
 template <class T, bool FLIP>
-__global__ void __launch_bounds__(kG2PThreads)
+__global__ void __launch_bounds__(kG2PThreads, g2p_min_blocks<T>())
     k_g2p_tiles(Geo G, double hd, double alphad, int pow2, const int* __restrict__ start,
                 const int* __restrict__ cnt, PartsT<T> P, const T* u, const T* v, const T* w, const T* ul,
                 const T* vl, const T* wl) {

@@ -649,6 +649,135 @@ __global__ void __launch_bounds__(kT)
   }
 }
 
+// ---- smoothFluidSurface, plane-pipelined ----
+// The smoothing passes (fluid-simulator.cc:39-74) write every cell, so there
+// is nothing to skip; instead of one launch per pass, one launch runs up to
+// kSmH passes.  A block owns a (y, z) tile of kSmTY x kSmTZ columns and a run
+// of x planes, and walks along x: each step loads the next input plane (with
+// a halo of kSmH cells in y and z) into a ring of three planes, then pass l
+// computes its plane x - l from pass l - 1's planes x - l - 1 .. x - l + 1,
+// over a rectangle that shrinks by one cell per pass.  The last pass and the
+// one before it are written out, as the per-pass launches leave them in the
+// two buffers.  The arithmetic is that of k_smooth_sdf, so the values are
+// the same bit for bit.
+constexpr int kSmH = 5, kSmTY = 16, kSmTZ = 32;
+constexpr int kSmRY = kSmTY + 2 * kSmH, kSmRZ = kSmTZ + 2 * kSmH, kSmRP = kSmRY * kSmRZ;
+constexpr int kSmThreads = 512;
+constexpr int kSmPer = (kSmRP + kSmThreads - 1) / kSmThreads;  // plane cells per thread
+constexpr size_t smooth_smem_bytes() { return sizeof(double) * (size_t)kSmH * 3 * kSmRP; }
+// src: the values before the passes; outN / outN1: where the last pass and
+// the one before it go (outN1 unused for one pass); nl <= kSmH passes; each
+// block takes lx planes.
+__global__ void __launch_bounds__(kSmThreads)
+    k_smooth_planes(Geo G, const double* __restrict__ src, double* __restrict__ outN, double* __restrict__ outN1,
+                    int nl, int lx) {
+  extern __shared__ __align__(16) unsigned char sm_dyn[];
+  double* ring = reinterpret_cast<double*>(sm_dyn);  // [pass 0 .. nl - 1][x mod 3][kSmRP]
+  const int nx = G.nx, ny = G.ny, nz = G.nz;
+  const int ntz = (nz + kSmTZ - 1) / kSmTZ, nty = (ny + kSmTY - 1) / kSmTY;
+  const int tz = blockIdx.x % ntz, ty = (blockIdx.x / ntz) % nty, tx = blockIdx.x / (ntz * nty);
+  const int y0 = ty * kSmTY - kSmH, z0 = tz * kSmTZ - kSmH;  // region origin
+  const int xa = tx * lx, xb = min(nx, xa + lx);
+  const int64_t sx = (int64_t)ny * nz;
+  // this thread's plane cells: region offset, global (y, z) offset, in-domain
+  int off[kSmPer], ry[kSmPer], rz[kSmPer];
+  bool dom[kSmPer];
+#pragma unroll
+  for (int u = 0; u < kSmPer; u++) {
+    const int e = threadIdx.x + u * kSmThreads;
+    off[u] = e;
+    ry[u] = e / kSmRZ;
+    rz[u] = e - ry[u] * kSmRZ;
+    const int y = y0 + ry[u], z = z0 + rz[u];
+    dom[u] = e < kSmRP && y >= 0 && y < ny && z >= 0 && z < nz;
+  }
+  auto load = [&](int x, double* v) {
+#pragma unroll
+    for (int u = 0; u < kSmPer; u++)
+      v[u] = (dom[u] && x >= 0 && x < nx) ? __ldg(src + x * sx + (int64_t)(y0 + ry[u]) * nz + (z0 + rz[u])) : 0.0;
+  };
+  const int s0 = max(0, xa - nl), s1 = min(nx, xb + nl);  // input planes
+  double nxt[kSmPer];
+  load(s0, nxt);
+  for (int s = s0; s < xb + nl; s++) {
+    // input plane s into the ring of pass 0; prefetch plane s + 1
+    if (s < s1) {
+      double* R0 = ring + (s % 3) * kSmRP;
+#pragma unroll
+      for (int u = 0; u < kSmPer; u++)
+        if (off[u] < kSmRP) R0[off[u]] = nxt[u];
+      if (s + 1 < s1) load(s + 1, nxt);
+    }
+    __syncthreads();
+    for (int l = 1; l <= nl; l++) {
+      const int x = s - l;
+      // pass l is needed on planes [xa - (nl - l), xb + (nl - l)) of the grid
+      if (x >= max(0, xa - (nl - l)) && x < min(nx, xb + (nl - l))) {
+        const double* P = ring + (size_t)(l - 1) * 3 * kSmRP;
+        const double* Pm = P + ((x + 2) % 3) * kSmRP;  // plane x - 1
+        const double* P0 = P + (x % 3) * kSmRP;
+        const double* Pp = P + ((x + 1) % 3) * kSmRP;  // plane x + 1
+        double* D = l < nl ? ring + (size_t)l * 3 * kSmRP + (x % 3) * kSmRP : nullptr;
+#pragma unroll
+        for (int u = 0; u < kSmPer; u++) {
+          if (!dom[u] || ry[u] < l || ry[u] >= kSmRY - l || rz[u] < l || rz[u] >= kSmRZ - l) continue;
+          const int e = off[u], y = y0 + ry[u], z = z0 + rz[u];
+          double sum = 0.0;
+          int cnt = 0;
+          if (x > 0) { sum = radd(sum, Pm[e]); cnt++; }
+          if (x < nx - 1) { sum = radd(sum, Pp[e]); cnt++; }
+          if (y > 0) { sum = radd(sum, P0[e - kSmRZ]); cnt++; }
+          if (y < ny - 1) { sum = radd(sum, P0[e + kSmRZ]); cnt++; }
+          if (z > 0) { sum = radd(sum, P0[e - 1]); cnt++; }
+          if (z < nz - 1) { sum = radd(sum, P0[e + 1]); cnt++; }
+          double v = rdiv(sum, (double)cnt);
+          if (P0[e] < v) v = P0[e];
+          if (D) D[e] = v;
+          const bool tile = ry[u] >= kSmH && ry[u] < kSmH + kSmTY && rz[u] >= kSmH && rz[u] < kSmH + kSmTZ;
+          if (tile && x >= xa && x < xb) {
+            const int64_t g = x * sx + (int64_t)y * nz + z;
+            if (l == nl) outN[g] = v;
+            if (l == nl - 1) outN1[g] = v;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+// `iters` smoothing passes over sdf[cur], kSmH per launch.  Each launch reads
+// sdf[cur] and leaves its last pass and the one before it where the per-pass
+// launches would (buffers (cur + n) mod 2 and (cur + n - 1) mod 2); the one
+// of them that is sdf[cur] itself is written to the spare buffer instead,
+// which then takes sdf[cur]'s place.  Returns the launches.
+inline int launch_smooth(cudaStream_t st, const Geo& G, int iters, double* sdf[2], double*& spare, int& cur) {
+  static bool attr = false;
+  static int sms = 0;
+  if (!attr) {
+    cudaFuncSetAttribute(k_smooth_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem_bytes());
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    attr = true;
+  }
+  const int64_t cols = (int64_t)((G.ny + kSmTY - 1) / kSmTY) * ((G.nz + kSmTZ - 1) / kSmTZ);
+  // runs of x planes: at least 16 planes, and about three blocks per SM
+  int lx = G.nx;
+  while (lx > 16 && cols * ((G.nx + lx - 1) / lx) < 3 * (int64_t)sms) lx = (lx + 1) / 2;
+  const unsigned nb = (unsigned)(cols * ((G.nx + lx - 1) / lx));
+  int launches = 0;
+  for (int k0 = 0; k0 < iters; k0 += kSmH) {
+    const int nl = std::min(kSmH, iters - k0);
+    double* dN = (nl & 1) ? sdf[1 - cur] : spare;
+    double* dN1 = nl >= 2 ? ((nl & 1) ? spare : sdf[1 - cur]) : nullptr;
+    k_smooth_planes<<<nb, kSmThreads, smooth_smem_bytes(), st>>>(G, sdf[cur], dN, dN1, nl, lx);
+    launches++;
+    if (nl >= 2) std::swap(sdf[cur], spare);
+    cur = (cur + nl) & 1;
+  }
+  return launches;
+}
+
 // ---- the iterated grid passes, temporally blocked ----
 // extrapolate(.., 10) per face grid (cpu/fluid-simulator.h:204-253) and
 // extrapolateFluidSdf(10) (:123-166) are Jacobi-style passes over two buffers: pass k
@@ -1065,15 +1194,15 @@ __device__ __forceinline__ T p2g_factor(T p, int node, const P2GSpacing<T>& sp) 
 // off: |q - c| is (p - c h) / h rounded once, which on a power-of-two grid is
 // the reference's rounding of p - c h scaled exactly, so the factor is the
 // same bit for bit; otherwise q carries one more rounding.
+// Both pieces are evaluated and one is selected: the lanes of a warp fall in
+// different pieces, and the selection keeps them on one path.
 template <class T>
 __device__ __forceinline__ T p2g_factor_q(T q, T c) {
   const T r = fabs(rsub(q, c));
-  if (r < T(1)) return radd(rsub(T(2.0 / 3.0), rmul(r, r)), rmul(rmul(rmul(T(0.5), r), r), r));
-  if (r < T(2)) {
-    const T t = rsub(T(2), r);
-    return rmul(rmul(rmul(t, t), t), T(1.0 / 6.0));
-  }
-  return T(0);
+  const T inner = radd(rsub(T(2.0 / 3.0), rmul(r, r)), rmul(rmul(rmul(T(0.5), r), r), r));
+  const T t = rsub(T(2), r);
+  const T outer = rmul(rmul(rmul(t, t), t), T(1.0 / 6.0));
+  return r < T(1) ? inner : (r < T(2) ? outer : T(0));
 }
 // The reference's product order: (w_x w_y) w_z.
 template <class T>
@@ -1154,10 +1283,23 @@ __device__ void p2g_tile_grid(const Geo& G, const P2GSpacing<T>& h, int x0, int 
     // region nodes of this pass: along AX the plane of cell + ip - 1 of each
     // cell of the tile (region index cell + ip), across AX the nodes reached
     // from the tile's cells at their typical bases (region indices 1..11)
+    // (the index that runs fastest over the threads is the one along z, in the
+    // staged values and in the region alike: consecutive threads read
+    // consecutive words)
     constexpr int NA = kPT, NB = kPT + 3;
     for (int e = tid; e < NA * NB * NB; e += kPThreads) {
-      const int a = e / (NB * NB), r = e - a * (NB * NB);
-      const int b = r / NB, cc = r - b * NB;
+      int a, b, cc;
+      if (AX == 2) {
+        a = e % NA;
+        const int r = e / NA;
+        b = r / NB;
+        cc = r - b * NB;
+      } else {
+        a = e / (NB * NB);
+        const int r = e - a * (NB * NB);
+        b = r / NB;
+        cc = r - b * NB;
+      }
       const int rb = b + 1, rc = cc + 1;  // region indices across AX
       T S = T(0), W = T(0);
 #pragma unroll
@@ -1381,11 +1523,13 @@ int launch_p2g(cudaStream_t st, const Geo& G, double h, const int* start, const 
 // the P2G region of each face grid it samples (u, v, w and, for FLIP, their
 // last values) into shared memory, row by row; the tile's particles then read
 // their 4x4x4 stencil nodes from there.  The particles of a column of the tile
-// (8 cells along z) are contiguous after the sort, so each warp walks whole
-// columns.  The nodes, their order and the arithmetic are those of
-// sampleVelocity (gather), so the velocities are the same bit for bit; a
-// particle whose stencil leaves the region (outside the grid box, recorded
-// bases) samples the grids in global memory instead.
+// (8 cells along z) are contiguous after the sort; the block numbers the
+// tile's particles column after column and gives consecutive particles to
+// consecutive threads, so no lane waits on a short column.  The nodes, their
+// order and the arithmetic are those of sampleVelocity (gather), so the
+// velocities are the same bit for bit; a particle whose stencil leaves the
+// region (far outside the grid box, or outside its sorted cell) samples the
+// grids in global memory instead.
 constexpr int kG2PThreads = 256;
 template <class T, int AX>
 __device__ __forceinline__ void g2p_stage(T* __restrict__ R, const T* __restrict__ g, const Geo& G, int x0, int y0,
@@ -1408,91 +1552,74 @@ __device__ __forceinline__ bool g2p_in_region(const Stencil<T>& S, int x0, int y
   return r0 >= 0 && r0 + 3 < P2GRegion<AX, 0>::n && r1 >= 0 && r1 + 3 < P2GRegion<AX, 1>::n && r2 >= 0 &&
          r2 + 3 < P2GRegion<AX, 2>::n;
 }
-// gather<T, AX> on the staged region: the same nodes, order and arithmetic.
-template <class T, int AX>
-__device__ __forceinline__ T g2p_gather_tile(const T* __restrict__ R, const Stencil<T>& S, const Geo& G, int x0,
-                                             int y0, int z0) {
-  constexpr int ox = AX == 0 ? 0 : 1, oy = AX == 1 ? 0 : 1, oz = AX == 2 ? 0 : 1;
-  constexpr int n1 = P2GRegion<AX, 1>::n, n2 = P2GRegion<AX, 2>::n;
-  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
-  const int r0 = S.base[0][ox] - (x0 - P2GRegion<AX, 0>::lo), r1 = S.base[1][oy] - (y0 - P2GRegion<AX, 1>::lo),
-            r2 = S.base[2][oz] - (z0 - P2GRegion<AX, 2>::lo);
-  T s = T(0), ws = T(0);
+// Nodes outside the grid get weight zero: the staged region holds zeros
+// there, so such a node adds +0 to the value sum and nothing to the weight
+// sum, which is what gather's skip of it gives (up to the sign of a zero
+// sum, which compares equal).  Along axis d the grid with offset 0 (the face
+// grid of axis d) has n_d + 1 nodes, the grids with offset 1/2 have n_d.
+template <class T>
+__device__ __forceinline__ void g2p_mask_outside(Stencil<T>& S, const Geo& G) {
+  const int n[3] = {G.nx, G.ny, G.nz};
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int a = S.base[0][ox] + i;
-    if (a < 0 || a >= fx) continue;
+  for (int d = 0; d < 3; d++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int b = S.base[1][oy] + j;
-      if (b < 0 || b >= fy) continue;
-      const T wxy = rmul(S.w[0][ox][i], S.w[1][oy][j]);
-      const T* row = R + ((r0 + i) * n1 + (r1 + j)) * n2 + r2;
+    for (int o = 0; o < 2; o++) {
+      const int ext = n[d] + (o == 0 ? 1 : 0);
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const int c = S.base[2][oz] + k;
-        if (c < 0 || c >= fz) continue;
-        const T wt = rmul(wxy, S.w[2][oz][k]);
-        s = radd(s, rmul(row[k], wt));
-        ws = radd(ws, wt);
+      for (int i = 0; i < 4; i++) {
+        const int b = S.base[d][o] + i;
+        if (b < 0 || b >= ext) S.w[d][o][i] = T(0);
       }
     }
-  }
-  return ws > T(0) ? rdiv(s, ws) : T(0);
 }
-// All three (or six) staged gathers of a particle whose stencils lie inside
-// the grid: no node is skipped, so the loops are branch-free and the chains
-// of the grids interleave; each grid's sum keeps gather's order.
-template <class T, int NG>
-__device__ __forceinline__ void g2p_gather_tile_inner(const T* __restrict__ R, const Stencil<T>& S, int x0, int y0,
-                                                      int z0, T* out) {
-  const T* row0[NG];
-  T s[NG], ws[NG];
+// The staged gathers of a particle whose stencils lie inside the region, the
+// weights of nodes outside the grid masked: no node is skipped, so the loops
+// are branch-free; each grid's sum keeps gather's order.  One grid (and its
+// last values) at a time, in a loop over the axes that is not unrolled: with
+// all six grids unrolled together the kernel's warps stalled on instruction
+// fetch (project + G2P of 33.5M particles 4.3 ms, against 4.1 ms so).
+template <class T, bool FLIP>
+__device__ __forceinline__ void g2p_gather_axes(const T* __restrict__ R, const Stencil<T>& S, int x0, int y0, int z0,
+                                                const PartsT<T>& P, int64_t p, T al, T bl) {
+#pragma unroll 1
+  for (int ax = 0; ax < 3; ax++) {
+    T wx[4], wy[4], wz[4];
 #pragma unroll
-  for (int q = 0; q < NG; q++) {
-    s[q] = T(0);
-    ws[q] = T(0);
-  }
-  // fully unrolled: with the outer loop rolled (or "unroll 4") the kernel
-  // measured 5x slower, its warps stalled on instruction fetch
+    for (int q = 0; q < 4; q++) {
+      wx[q] = ax == 0 ? S.w[0][0][q] : S.w[0][1][q];
+      wy[q] = ax == 1 ? S.w[1][0][q] : S.w[1][1][q];
+      wz[q] = ax == 2 ? S.w[2][0][q] : S.w[2][1][q];
+    }
+    const int bx = ax == 0 ? S.base[0][0] - (x0 - 1) : S.base[0][1] - (x0 - 2);
+    const int by = ax == 1 ? S.base[1][0] - (y0 - 1) : S.base[1][1] - (y0 - 2);
+    const int bz = ax == 2 ? S.base[2][0] - (z0 - 1) : S.base[2][1] - (z0 - 2);
+    const int n1 = ax == 1 ? kPT + 4 : kPT + 5, n2 = ax == 2 ? kPT + 4 : kPT + 5;
+    const T* g = R + ax * kP2GRegion + (bx * n1 + by) * n2 + bz;
+    T s = T(0), sl = T(0), ws = T(0);
 #pragma unroll
-  for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-#pragma unroll
-      for (int q = 0; q < NG; q++) {
-        const int ax = q % 3;
-        const int ox = ax == 0 ? 0 : 1, oy = ax == 1 ? 0 : 1, oz = ax == 2 ? 0 : 1;
-        const int n1 = ax == 1 ? kPT + 4 : kPT + 5, n2 = ax == 2 ? kPT + 4 : kPT + 5;
-        const int lo0 = ax == 0 ? 1 : 2, lo1 = ax == 1 ? 1 : 2, lo2 = ax == 2 ? 1 : 2;
-        const int r0 = S.base[0][ox] - (x0 - lo0), r1 = S.base[1][oy] - (y0 - lo1), r2 = S.base[2][oz] - (z0 - lo2);
-        row0[q] = R + q * kP2GRegion + ((r0 + i) * n1 + (r1 + j)) * n2 + r2;
-        const T wxy = rmul(S.w[0][ox][i], S.w[1][oy][j]);
+      for (int j = 0; j < 4; j++) {
+        const T wxy = rmul(wx[i], wy[j]);
+        const T* row = g + (i * n1 + j) * n2;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-          const T wt = rmul(wxy, S.w[2][oz][k]);
-          s[q] = radd(s[q], rmul(row0[q][k], wt));
-          ws[q] = radd(ws[q], wt);
+          const T wt = rmul(wxy, wz[k]);
+          s = radd(s, rmul(row[k], wt));
+          if (FLIP) sl = radd(sl, rmul(row[3 * kP2GRegion + k], wt));
+          ws = radd(ws, wt);
         }
       }
-    }
-#pragma unroll
-  for (int q = 0; q < NG; q++) out[q] = ws[q] > T(0) ? rdiv(s[q], ws[q]) : T(0);
-}
-template <class T>
-__device__ __forceinline__ bool g2p_inner(const Stencil<T>& S, const Geo& G) {
-  // every stencil node of the three grids inside the grid
-  bool ok = true;
-#pragma unroll
-  for (int ax = 0; ax < 3; ax++) {
-    const int f[3] = {G.nx + (ax == 0), G.ny + (ax == 1), G.nz + (ax == 2)};
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const int b = S.base[d][d == ax ? 0 : 1];
-      ok = ok && b >= 0 && b + 3 < f[d];
+    T* vp = ax == 0 ? P.vx : (ax == 1 ? P.vy : P.vz);
+    const T pic = ws > T(0) ? rdiv(s, ws) : T(0);
+    if (!FLIP) {
+      vp[p] = pic;
+    } else {
+      const T last = ws > T(0) ? rdiv(sl, ws) : T(0);
+      const T f = rsub(radd(vp[p], pic), last);
+      vp[p] = radd(rmul(al, f), rmul(bl, pic));
     }
   }
-  return ok;
 }
 template <class T>
 constexpr size_t g2p_smem_bytes(bool flip) {
@@ -1513,28 +1640,44 @@ __global__ void __launch_bounds__(kG2PThreads, g2p_min_blocks<T>())
                 const T* vl, const T* wl) {
   extern __shared__ __align__(16) unsigned char g2p_dyn[];
   T* R = reinterpret_cast<T*>(g2p_dyn);  // [grid][region]: u, v, w, then u, v, w last
-  __shared__ int rbeg[kPT * kPT], rend[kPT * kPT];
+  __shared__ int cbeg[kPT * kPT], pre[kPT * kPT + 1];
   const T h = (T)hd, hinv = (T)(1.0 / hd);
   constexpr bool flip = FLIP;
   const int ntz = (G.nz + kPT - 1) / kPT, nty = (G.ny + kPT - 1) / kPT;
   const int tz = blockIdx.x % ntz, ty = (blockIdx.x / ntz) % nty, tx = blockIdx.x / (ntz * nty);
   const int x0 = tx * kPT, y0 = ty * kPT, z0 = tz * kPT;
-  bool mine = false;
-  if (threadIdx.x < kPT * kPT) {
-    // the particle run of column (x0 + lx, y0 + ly): cells z0 .. z0 + 7
-    const int lx = threadIdx.x / kPT, ly = threadIdx.x % kPT;
-    const int x = x0 + lx, y = y0 + ly, zl = min(z0 + kPT, G.nz) - 1;
-    int b = 0, e = 0;
-    if (x < G.nx && y < G.ny) {
-      const int c0 = (int)lin(x, y, z0, G.ny, G.nz), c1 = (int)lin(x, y, zl, G.ny, G.nz);
-      b = start[c0];
-      e = start[c1] + cnt[c1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) {
+    // the particle runs of columns 2 lane and 2 lane + 1 (cells z0 .. z0 + 7
+    // of column (x0 + col / 8, y0 + col % 8)), and their exclusive prefix
+    int c2[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int col = 2 * lane + q;
+      const int x = x0 + col / kPT, y = y0 + col % kPT, zl = min(z0 + kPT, G.nz) - 1;
+      int b = 0, e = 0;
+      if (x < G.nx && y < G.ny) {
+        const int e0 = (int)lin(x, y, z0, G.ny, G.nz), e1 = (int)lin(x, y, zl, G.ny, G.nz);
+        b = start[e0];
+        e = start[e1] + cnt[e1];
+      }
+      cbeg[col] = b;
+      c2[q] = e - b;
     }
-    rbeg[threadIdx.x] = b;
-    rend[threadIdx.x] = e;
-    mine = e > b;
+    int inc = c2[0] + c2[1];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, d);
+      if (lane >= d) inc += t;
+    }
+    const int ex = inc - c2[0] - c2[1];
+    pre[2 * lane] = ex;
+    pre[2 * lane + 1] = ex + c2[0];
+    if (lane == 31) pre[kPT * kPT] = inc;
   }
-  if (!__syncthreads_or(mine)) return;  // no particle in this tile
+  __syncthreads();
+  const int total = pre[kPT * kPT];
+  if (total == 0) return;  // no particle in this tile
   g2p_stage<T, 0>(R, u, G, x0, y0, z0);
   g2p_stage<T, 1>(R + kP2GRegion, v, G, x0, y0, z0);
   g2p_stage<T, 2>(R + 2 * kP2GRegion, w, G, x0, y0, z0);
@@ -1544,67 +1687,40 @@ __global__ void __launch_bounds__(kG2PThreads, g2p_min_blocks<T>())
     g2p_stage<T, 2>(R + 5 * kP2GRegion, wl, G, x0, y0, z0);
   }
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int col = warp; col < kPT * kPT; col += kG2PThreads / 32) {
-    const int e = rend[col];
-    for (int i = rbeg[col] + lane; i < e; i += 32) {
-      const T px = P.px[i], py = P.py[i], pz = P.pz[i];
-      Stencil<T> S;
-      make_stencil_pow2(S, px, py, pz, h, hinv, pow2 != 0);
-      const bool in = g2p_in_region<T, 0>(S, x0, y0, z0) && g2p_in_region<T, 1>(S, x0, y0, z0) &&
-                      g2p_in_region<T, 2>(S, x0, y0, z0);
-      if (in && g2p_inner(S, G)) {
-        // the common case: all nodes staged and inside the grid
-        if (!flip) {
-          T o[3];
-          g2p_gather_tile_inner<T, 3>(R, S, x0, y0, z0, o);
-          P.vx[i] = o[0];
-          P.vy[i] = o[1];
-          P.vz[i] = o[2];
-        } else {
-          T o[6];
-          g2p_gather_tile_inner<T, 6>(R, S, x0, y0, z0, o);
-          const T al = (T)alphad, bl = rsub(T(1), al);
-          const T fx = rsub(radd(P.vx[i], o[0]), o[3]), fy = rsub(radd(P.vy[i], o[1]), o[4]),
-                  fz = rsub(radd(P.vz[i], o[2]), o[5]);
-          P.vx[i] = radd(rmul(al, fx), rmul(bl, o[0]));
-          P.vy[i] = radd(rmul(al, fy), rmul(bl, o[1]));
-          P.vz[i] = radd(rmul(al, fz), rmul(bl, o[2]));
-        }
-        continue;
-      }
-      T pu, pv, pw;
-      if (in) {
-        pu = g2p_gather_tile<T, 0>(R, S, G, x0, y0, z0);
-        pv = g2p_gather_tile<T, 1>(R + kP2GRegion, S, G, x0, y0, z0);
-        pw = g2p_gather_tile<T, 2>(R + 2 * kP2GRegion, S, G, x0, y0, z0);
-      } else {
-        pu = gather<T, 0>(u, S, G);
-        pv = gather<T, 1>(v, S, G);
-        pw = gather<T, 2>(w, S, G);
-      }
-      if (!flip) {
-        P.vx[i] = pu;
-        P.vy[i] = pv;
-        P.vz[i] = pw;
-        continue;
-      }
-      T lu, lv, lw;
-      if (in) {
-        lu = g2p_gather_tile<T, 0>(R + 3 * kP2GRegion, S, G, x0, y0, z0);
-        lv = g2p_gather_tile<T, 1>(R + 4 * kP2GRegion, S, G, x0, y0, z0);
-        lw = g2p_gather_tile<T, 2>(R + 5 * kP2GRegion, S, G, x0, y0, z0);
-      } else {
-        lu = gather<T, 0>(ul, S, G);
-        lv = gather<T, 1>(vl, S, G);
-        lw = gather<T, 2>(wl, S, G);
-      }
-      const T al = (T)alphad, bl = rsub(T(1), al);
-      const T fx = rsub(radd(P.vx[i], pu), lu), fy = rsub(radd(P.vy[i], pv), lv), fz = rsub(radd(P.vz[i], pw), lw);
-      P.vx[i] = radd(rmul(al, fx), rmul(bl, pu));
-      P.vy[i] = radd(rmul(al, fy), rmul(bl, pv));
-      P.vz[i] = radd(rmul(al, fz), rmul(bl, pw));
+  const T al = (T)alphad, bl = rsub(T(1), al);
+  // the tile's particles in order, column after column: particle k lies in
+  // the last column whose prefix is <= k
+  for (int k = threadIdx.x; k < total; k += kG2PThreads) {
+    int col = 0;
+#pragma unroll
+    for (int s = 32; s >= 1; s >>= 1)
+      if (pre[col + s] <= k) col += s;
+    const int64_t i = (int64_t)cbeg[col] + (k - pre[col]);
+    const T px = P.px[i], py = P.py[i], pz = P.pz[i];
+    Stencil<T> S;
+    make_stencil_pow2(S, px, py, pz, h, hinv, pow2 != 0);
+    const bool in = g2p_in_region<T, 0>(S, x0, y0, z0) && g2p_in_region<T, 1>(S, x0, y0, z0) &&
+                    g2p_in_region<T, 2>(S, x0, y0, z0);
+    if (in) {
+      // the common case: every node staged
+      g2p_mask_outside(S, G);
+      g2p_gather_axes<T, FLIP>(R, S, x0, y0, z0, P, i, al, bl);
+      continue;
     }
+    // a stencil beyond the staged region: sampleVelocity on the grids in
+    // global memory
+    const T pu = gather<T, 0>(u, S, G), pv = gather<T, 1>(v, S, G), pw = gather<T, 2>(w, S, G);
+    if (!flip) {
+      P.vx[i] = pu;
+      P.vy[i] = pv;
+      P.vz[i] = pw;
+      continue;
+    }
+    const T lu = gather<T, 0>(ul, S, G), lv = gather<T, 1>(vl, S, G), lw = gather<T, 2>(wl, S, G);
+    const T fx = rsub(radd(P.vx[i], pu), lu), fy = rsub(radd(P.vy[i], pv), lv), fz = rsub(radd(P.vz[i], pw), lw);
+    P.vx[i] = radd(rmul(al, fx), rmul(bl, pu));
+    P.vy[i] = radd(rmul(al, fy), rmul(bl, pv));
+    P.vz[i] = radd(rmul(al, fz), rmul(bl, pw));
   }
 }
 // G2P of cell-sorted particles (start/cnt of the sort that ordered P).

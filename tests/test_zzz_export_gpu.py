@@ -61,3 +61,34 @@ def test_export_collider_surface(gpu):
     assert np.array_equal(sim.export_collider_surface(), C)
     sim.set_collider(None)
     assert (sim.export_collider_surface() == 1e9).all()
+
+
+@pytest.mark.parametrize("passes", [(7, 2), (1, 4, 3)])
+def test_smoothing_pass_counts_follow_the_oracle(oracle, gpu, passes):
+    """smoothFluidSurface with pass counts that are not one launch of five:
+    a launch takes at most five passes and leaves the last pass and the one
+    before it in the two buffers the per-pass flips would, so the next
+    substep's SDF extrapolation, which keeps the older buffer's values in
+    valid cells, still follows the oracle.  24 x 20 x 36 cells: several
+    column tiles and runs of x planes per launch."""
+    from simcraft_b200 import scenes
+    from simcraft_b200.fluid import FluidSimulator
+
+    dims = (24, 20, 36)
+    pos, vel, h = scenes.dam_break(24, seed=4)  # the block x, y < 1/2, z < 1
+    cfg = oracle.default_config(*dims, h, flip_alpha=0.95, pcg_tol=1e-8, pcg_criterion=1)
+    ref = oracle.Sim(**cfg)
+    ref.set_particles(pos, vel)
+    ext = tuple(d * h for d in dims)
+    sim = FluidSimulator(len(pos), ext, dims, flip_alpha=0.95, pcg_tol=1e-8, pcg_criterion=1)
+    sim.set_initial_fluid(pos, vel)
+    ref.step(1.0 / 120)
+    sim.step(1.0 / 120)
+    for k in passes:
+        ref.smooth_fluid_surface(k)
+        sim.smooth_fluid_surface(k)
+        np.testing.assert_allclose(sim.export_fluid_surface(), ref.fluid_sdf(), rtol=0, atol=1e-9 * h)
+    ref.step(1.0 / 120)
+    sim.step(1.0 / 120)
+    assert np.abs(sim.positions() - ref.particles()[0]).max() < 1e-4 * h
+    np.testing.assert_allclose(sim.export_fluid_surface(), ref.fluid_sdf(), rtol=0, atol=1e-6 * h)

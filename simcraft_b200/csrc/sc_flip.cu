@@ -65,7 +65,6 @@ FluidSim::FluidSim(Context* ctx, const FluidConfig& cfg) : ctx_(ctx), c_(cfg) {
     ok &= (sdf_[b] = (double*)alloc(sizeof(double) * N)) != nullptr;
     ok &= (sdfv_[b] = (uint8_t*)alloc(N)) != nullptr;
   }
-  ok &= (sdf_spare_ = (double*)alloc(sizeof(double) * N)) != nullptr;
   ok &= (cnt_ = (int*)alloc(sizeof(int) * N)) != nullptr;
   ok &= (start_ = (int*)alloc(sizeof(int) * N)) != nullptr;
   ok &= (cursor_ = (int*)alloc(sizeof(int) * N)) != nullptr;
@@ -238,8 +237,8 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
   launches_ += 1;
   // extrapolateFluidSdf(10), temporally blocked
   launches_ += launch_iter_cells<ITER_SDF>(st, G, c_.sdf_extrap_iters, sdf_, sdfv_, scur_, svcur_);
-  // smoothFluidSurface(5), plane-pipelined
-  launches_ += launch_smooth(st, G, c_.smooth_iters, sdf_, sdf_spare_, scur_);
+  // smoothFluidSurface(5)
+  launches_ += launch_smooth(st, G, c_.smooth_iters, sdf_, scur_);
   const double* fluid = sdf_[scur_];
   cudaEventRecord(ev_[2], st);
   // P2G + Dirichlet walls + extrapolation + gravity (fluid-simulator.cc:155-164)
@@ -360,11 +359,11 @@ int FluidSim::reconstruct(double radius) {
 }
 
 // smoothFluidSurface (fluid-simulator.cc:39-74) on the simulator's surface
-// buffers, leaving them as one flip per pass would.
+// buffers, flipping them once per pass as the substep does.
 int FluidSim::smooth_fluid_surface(int iters) {
   cudaStream_t st = ctx_->stream;
   const Geo G{c_.nx, c_.ny, c_.nz};
-  launches_ += launch_smooth(st, G, iters, sdf_, sdf_spare_, scur_);
+  launches_ += launch_smooth(st, G, iters, sdf_, scur_);
   return err("smooth_fluid_surface");
 }
 

@@ -88,7 +88,6 @@ class FluidSim {
   void* last_[3] = {};   // FLIP u_last/v_last/w_last
   double* wt_[3] = {};   // FVM face weights
   double* sdf_[2] = {};
-  double* sdf_spare_ = nullptr;  // takes a buffer's place in the plane-pipelined smoothing
   uint8_t* sdfv_[2] = {};
   int scur_ = 0, svcur_ = 0;
   double* collider_ = nullptr;  // null: empty-mesh collider

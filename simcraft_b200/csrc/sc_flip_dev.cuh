@@ -643,157 +643,62 @@ __global__ void __launch_bounds__(kT)
     if (j < G.ny - 1) { sum = radd(sum, src[id + sy]); cnt++; }
     if (k > 0) { sum = radd(sum, src[id - 1]); cnt++; }
     if (k < G.nz - 1) { sum = radd(sum, src[id + 1]); cnt++; }
-    double v = rdiv(sum, (double)cnt);
-    if (src[id] < v) v = src[id];
+    // min(own, sum / cnt): when own * cnt < sum exactly (the sign of one fused
+    // multiply-add), own is below the rounded quotient or equal to it, so the
+    // minimum is own and the division is not needed
+    const double own = src[id], cd = (double)cnt;
+    double v;
+    if (fma(own, cd, -sum) < 0.0) {
+      v = own;
+    } else {
+      v = rdiv(sum, cd);
+      if (own < v) v = own;
+    }
     dst[id] = v;
   }
 }
 
-// ---- smoothFluidSurface, plane-pipelined ----
-// The smoothing passes (fluid-simulator.cc:39-74) write every cell, so there
-// is nothing to skip; instead of one launch per pass, one launch runs up to
-// kSmH passes.  A block owns a (y, z) tile of kSmTY x kSmTZ columns and a run
-// of x planes, and walks along x: each step loads the next input plane (with
-// a halo of kSmH cells in y and z) into a ring of three planes, then pass l
-// computes its plane x - l from pass l - 1's planes x - l - 1 .. x - l + 1,
-// over a rectangle that shrinks by one cell per pass.  The last pass and the
-// one before it are written out, as the per-pass launches leave them in the
-// two buffers.  The arithmetic is that of k_smooth_sdf, so the values are
-// the same bit for bit.
-constexpr int kSmH = 5, kSmTY = 16, kSmTZ = 32;
-constexpr int kSmRY = kSmTY + 2 * kSmH, kSmRZ = kSmTZ + 2 * kSmH, kSmRP = kSmRY * kSmRZ;
-constexpr int kSmThreads = 512;
-constexpr int kSmPer = (kSmRP + kSmThreads - 1) / kSmThreads;  // plane cells per thread
-constexpr size_t smooth_smem_bytes() { return sizeof(double) * (size_t)kSmH * 3 * kSmRP; }
-// src: the values before the passes; outN / outN1: where the last pass and
-// the one before it go (outN1 unused for one pass); nl <= kSmH passes; each
-// block takes lx planes.
-__global__ void __launch_bounds__(kSmThreads)
-    k_smooth_planes(Geo G, const double* __restrict__ src, double* __restrict__ outN, double* __restrict__ outN1,
-                    int nl, int lx) {
-  extern __shared__ __align__(16) unsigned char sm_dyn[];
-  double* ring = reinterpret_cast<double*>(sm_dyn);  // [pass 0 .. nl - 1][x mod 3][kSmRP]
-  const int nx = G.nx, ny = G.ny, nz = G.nz;
-  const int ntz = (nz + kSmTZ - 1) / kSmTZ, nty = (ny + kSmTY - 1) / kSmTY;
-  const int tz = blockIdx.x % ntz, ty = (blockIdx.x / ntz) % nty, tx = blockIdx.x / (ntz * nty);
-  const int y0 = ty * kSmTY - kSmH, z0 = tz * kSmTZ - kSmH;  // region origin
-  const int xa = tx * lx, xb = min(nx, xa + lx);
-  const int64_t sx = (int64_t)ny * nz;
-  // this thread's plane cells: region offset, global (y, z) offset, in-domain
-  int off[kSmPer], ry[kSmPer], rz[kSmPer];
-  bool dom[kSmPer];
-#pragma unroll
-  for (int u = 0; u < kSmPer; u++) {
-    const int e = threadIdx.x + u * kSmThreads;
-    off[u] = e;
-    ry[u] = e / kSmRZ;
-    rz[u] = e - ry[u] * kSmRZ;
-    const int y = y0 + ry[u], z = z0 + rz[u];
-    dom[u] = e < kSmRP && y >= 0 && y < ny && z >= 0 && z < nz;
+// `iters` smoothing passes (fluid-simulator.cc:39-74), one launch each: every
+// cell changes in every pass, so a tile has nothing to skip, and a
+// plane-pipelined kernel running five passes per launch (a ring of planes per
+// pass in shared memory) measured slower than five launches of this streaming
+// one (256^3: 1.07 ms against 0.60 ms).
+inline int launch_smooth(cudaStream_t st, const Geo& G, int iters, double* const sdf[2], int& cur) {
+  const int64_t N = (int64_t)G.nx * G.ny * G.nz;
+  for (int it = 0; it < iters; it++) {
+    k_smooth_sdf<<<nblk(N), kT, 0, st>>>(G, sdf[cur], sdf[1 - cur]);
+    cur = 1 - cur;
   }
-  auto load = [&](int x, double* v) {
-#pragma unroll
-    for (int u = 0; u < kSmPer; u++)
-      v[u] = (dom[u] && x >= 0 && x < nx) ? __ldg(src + x * sx + (int64_t)(y0 + ry[u]) * nz + (z0 + rz[u])) : 0.0;
-  };
-  const int s0 = max(0, xa - nl), s1 = min(nx, xb + nl);  // input planes
-  double nxt[kSmPer];
-  load(s0, nxt);
-  for (int s = s0; s < xb + nl; s++) {
-    // input plane s into the ring of pass 0; prefetch plane s + 1
-    if (s < s1) {
-      double* R0 = ring + (s % 3) * kSmRP;
-#pragma unroll
-      for (int u = 0; u < kSmPer; u++)
-        if (off[u] < kSmRP) R0[off[u]] = nxt[u];
-      if (s + 1 < s1) load(s + 1, nxt);
-    }
-    __syncthreads();
-    for (int l = 1; l <= nl; l++) {
-      const int x = s - l;
-      // pass l is needed on planes [xa - (nl - l), xb + (nl - l)) of the grid
-      if (x >= max(0, xa - (nl - l)) && x < min(nx, xb + (nl - l))) {
-        const double* P = ring + (size_t)(l - 1) * 3 * kSmRP;
-        const double* Pm = P + ((x + 2) % 3) * kSmRP;  // plane x - 1
-        const double* P0 = P + (x % 3) * kSmRP;
-        const double* Pp = P + ((x + 1) % 3) * kSmRP;  // plane x + 1
-        double* D = l < nl ? ring + (size_t)l * 3 * kSmRP + (x % 3) * kSmRP : nullptr;
-#pragma unroll
-        for (int u = 0; u < kSmPer; u++) {
-          if (!dom[u] || ry[u] < l || ry[u] >= kSmRY - l || rz[u] < l || rz[u] >= kSmRZ - l) continue;
-          const int e = off[u], y = y0 + ry[u], z = z0 + rz[u];
-          double sum = 0.0;
-          int cnt = 0;
-          if (x > 0) { sum = radd(sum, Pm[e]); cnt++; }
-          if (x < nx - 1) { sum = radd(sum, Pp[e]); cnt++; }
-          if (y > 0) { sum = radd(sum, P0[e - kSmRZ]); cnt++; }
-          if (y < ny - 1) { sum = radd(sum, P0[e + kSmRZ]); cnt++; }
-          if (z > 0) { sum = radd(sum, P0[e - 1]); cnt++; }
-          if (z < nz - 1) { sum = radd(sum, P0[e + 1]); cnt++; }
-          double v = rdiv(sum, (double)cnt);
-          if (P0[e] < v) v = P0[e];
-          if (D) D[e] = v;
-          const bool tile = ry[u] >= kSmH && ry[u] < kSmH + kSmTY && rz[u] >= kSmH && rz[u] < kSmH + kSmTZ;
-          if (tile && x >= xa && x < xb) {
-            const int64_t g = x * sx + (int64_t)y * nz + z;
-            if (l == nl) outN[g] = v;
-            if (l == nl - 1) outN1[g] = v;
-          }
-        }
-      }
-      __syncthreads();
-    }
-  }
-}
-// `iters` smoothing passes over sdf[cur], kSmH per launch.  Each launch reads
-// sdf[cur] and leaves its last pass and the one before it where the per-pass
-// launches would (buffers (cur + n) mod 2 and (cur + n - 1) mod 2); the one
-// of them that is sdf[cur] itself is written to the spare buffer instead,
-// which then takes sdf[cur]'s place.  Returns the launches.
-inline int launch_smooth(cudaStream_t st, const Geo& G, int iters, double* sdf[2], double*& spare, int& cur) {
-  static bool attr = false;
-  static int sms = 0;
-  if (!attr) {
-    cudaFuncSetAttribute(k_smooth_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem_bytes());
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    attr = true;
-  }
-  const int64_t cols = (int64_t)((G.ny + kSmTY - 1) / kSmTY) * ((G.nz + kSmTZ - 1) / kSmTZ);
-  // runs of x planes: at least 16 planes, and about three blocks per SM
-  int lx = G.nx;
-  while (lx > 16 && cols * ((G.nx + lx - 1) / lx) < 3 * (int64_t)sms) lx = (lx + 1) / 2;
-  const unsigned nb = (unsigned)(cols * ((G.nx + lx - 1) / lx));
-  int launches = 0;
-  for (int k0 = 0; k0 < iters; k0 += kSmH) {
-    const int nl = std::min(kSmH, iters - k0);
-    double* dN = (nl & 1) ? sdf[1 - cur] : spare;
-    double* dN1 = nl >= 2 ? ((nl & 1) ? spare : sdf[1 - cur]) : nullptr;
-    k_smooth_planes<<<nb, kSmThreads, smooth_smem_bytes(), st>>>(G, sdf[cur], dN, dN1, nl, lx);
-    launches++;
-    if (nl >= 2) std::swap(sdf[cur], spare);
-    cur = (cur + nl) & 1;
-  }
-  return launches;
+  return iters;
 }
 
 // ---- the iterated grid passes, temporally blocked ----
 // extrapolate(.., 10) per face grid (cpu/fluid-simulator.h:204-253) and
-// extrapolateFluidSdf(10) (:123-166) are Jacobi-style passes over two buffers: pass k
-// reads buffer k mod 2 and writes buffer (k + 1) mod 2, and a cell a pass does
-// not write keeps that buffer's older value.  One launch runs up to kIterHalo
-// passes: a block loads its tile plus a halo of kIterHalo cells (both value
-// buffers and the source flags) into shared memory, runs the passes there
-// over a region that shrinks by one cell per pass, and writes its tile back:
-// both buffers and both flag arrays, or, for the differentiable step, each
-// pass's flags into their history.  The passes and their arithmetic are those
-// of k_extrap_face and k_extrap_sdf, so the results are the same bit for bit.
-// Two kinds of tile need no values: one whose loaded region holds no valid
-// flag (the face passes would write zeros where the buffers hold zeros
-// already; the SDF passes would leave the values and write zero flags), and
-// one whose cells are all valid (the passes leave the values and set the
-// flags).  Only the tiles along the front of the valid region run the passes.
+// extrapolateFluidSdf(10) (:123-166) are Jacobi-style passes over two buffers:
+// pass k reads buffer k mod 2 and writes buffer (k + 1) mod 2, and a cell a
+// pass does not write keeps that buffer's older value.  A pass makes valid
+// exactly the invalid cells with a valid neighbour, so the cells pass p makes
+// valid are those at (6-neighbour) distance p from the cells valid before the
+// first pass, and their valid neighbours are all at distance p - 1: made
+// valid by pass p - 1, which wrote their values into the very buffer pass p
+// reads (or valid from the start, in buffer 0).  So each cell's value is
+// computed once, from values computed once, and one value per cell is enough:
+// a block loads its tile plus a halo of kIterHalo cells (the values of the
+// buffer pass 0 reads, and from the flags the pass that makes each cell valid,
+// 0 or not yet) into shared memory, runs up to kIterHalo passes there over a
+// region that shrinks by one cell per pass, and writes back, for its tile,
+// each new value into the buffer its pass wrote and the last two passes'
+// flags (or, for the differentiable step, each pass's flags into their
+// history).  Nothing else changes: in the SDF passes a cell without a valid
+// neighbour keeps its values; in the face passes it is given zero, which is
+// what both face buffers hold there (cleared before P2G, which writes zero
+// where it writes no value).  The neighbour order and the arithmetic are
+// those of k_extrap_face and k_extrap_sdf, so the results are the same bit
+// for bit.  Two kinds of tile need no values: one whose loaded region holds
+// no valid flag (the passes change no value; the SDF passes write zero
+// flags), and one whose cells are all valid (the passes leave the values and
+// set the flags).  Only the tiles along the front of the valid region run the
+// passes.
 enum { ITER_FACE = 0, ITER_SDF = 1 };
 constexpr int kIterThreads = 512;
 constexpr int kIterHalo = 5;  // passes per launch at most
@@ -813,8 +718,10 @@ constexpr int iter_region() {
 }
 template <class T>
 constexpr size_t iter_smem_bytes() {
-  return (size_t)iter_region<T>() * (2 * sizeof(T) + 2);
+  return (size_t)iter_region<T>() * (sizeof(T) + 1);
 }
+// The pass that makes a cell valid, for cells not valid yet or outside the grid.
+constexpr uint8_t kIterNotYet = 255, kIterOutside = 254;
 template <class T>
 inline int iter_tiles(int dx, int dy, int dz) {
   return ((dx + IterTile<T>::X - 1) / IterTile<T>::X) * ((dy + IterTile<T>::Y - 1) / IterTile<T>::Y) *
@@ -838,8 +745,8 @@ template <class T, int MODE>
 __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char* smem) {
   constexpr int TX = IterTile<T>::X, TY = IterTile<T>::Y, TZ = IterTile<T>::Z, H = kIterHalo;
   constexpr int RX = TX + 2 * H, RY = TY + 2 * H, RZ = TZ + 2 * H, RN = RX * RY * RZ;
-  T* V = reinterpret_cast<T*>(smem);                        // [2][RN]: side 0 = buffer cur
-  uint8_t* F = reinterpret_cast<uint8_t*>(V + 2 * RN);     // [2][RN]
+  T* V = reinterpret_cast<T*>(smem);                  // [RN]: buffer cur, then each cell's new value
+  uint8_t* D = reinterpret_cast<uint8_t*>(V + RN);    // [RN]: the pass that makes the cell valid
   const int dx = G.dx, dy = G.dy, dz = G.dz;
   const int ntz = (dz + TZ - 1) / TZ, nty = (dy + TY - 1) / TY;
   const int tz = tile % ntz, ty = (tile / ntz) % nty, tx = tile / (ntz * nty);
@@ -871,8 +778,7 @@ __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char
       for (int u = 0; u < NB; u++) {
         const int e = e0 + u * (int)blockDim.x;
         if (e < RN) {
-          F[e] = fv[u];
-          F[RN + e] = 0;  // cells no pass writes (outside the grid) read as invalid
+          D[e] = fv[u] ? 0 : (gv[u] >= 0 ? kIterNotYet : kIterOutside);
           any |= fv[u];
           const int i = e / (RY * RZ), r = e - i * (RY * RZ), j = r / RZ, k = r - j * RZ;
           if (gv[u] >= 0 && i >= H && i < H + TX && j >= H && j < H + TY && k >= H && k < H + TZ) all &= fv[u];
@@ -912,79 +818,74 @@ __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char
     }
   }
   for (int e0 = threadIdx.x; e0 < RN; e0 += NB * blockDim.x) {
-    T va[NB], vb[NB];
+    T va[NB];
 #pragma unroll
     for (int u = 0; u < NB; u++) {
       const int e = e0 + u * (int)blockDim.x;
       const int64_t gi = e < RN ? gidx(e) : -1;
       va[u] = gi >= 0 ? bs[gi] : T(0);
-      vb[u] = gi >= 0 ? bd[gi] : T(0);
     }
 #pragma unroll
     for (int u = 0; u < NB; u++) {
       const int e = e0 + u * (int)blockDim.x;
-      if (e < RN) {
-        V[e] = va[u];
-        V[RN + e] = vb[u];
-      }
+      if (e < RN) V[e] = va[u];
     }
   }
   __syncthreads();
   constexpr int sX = RY * RZ, sY = RZ;
-  for (int p = 0; p < nit; p++) {
-    const int src = p & 1;
-    const T* Vs = V + src * RN;
-    T* Vd = V + (1 - src) * RN;
-    const uint8_t* Fs = F + src * RN;
-    uint8_t* Fd = F + (1 - src) * RN;
-    // cells whose six neighbours still hold the data of p passes
-    const int lo = p + 1;
-    for (int e = threadIdx.x; e < RN; e += blockDim.x) {
-      const int i = e / sX, r = e - i * sX, j = r / sY, k = r - j * sY;
-      if (i < lo || i >= RX - lo || j < lo || j >= RY - lo || k < lo || k >= RZ - lo) continue;
-      const int gx = x0 + i, gy = y0 + j, gz = z0 + k;
-      if (gx < 0 || gx >= dx || gy < 0 || gy >= dy || gz < 0 || gz >= dz) continue;
-      {
-        uint8_t fl;
-        if (Fs[e]) {
-          fl = 1;
-        } else {
-          // out-of-domain neighbours hold flag 0 and are never counted
-          T sum = T(0);
-          int cnt = 0;
-          if (Fs[e - sX]) { sum = radd(sum, Vs[e - sX]); cnt++; }
-          if (Fs[e + sX]) { sum = radd(sum, Vs[e + sX]); cnt++; }
-          if (Fs[e - sY]) { sum = radd(sum, Vs[e - sY]); cnt++; }
-          if (Fs[e + sY]) { sum = radd(sum, Vs[e + sY]); cnt++; }
-          if (Fs[e - 1]) { sum = radd(sum, Vs[e - 1]); cnt++; }
-          if (Fs[e + 1]) { sum = radd(sum, Vs[e + 1]); cnt++; }
-          if (cnt > 0) {
-            Vd[e] = rdiv(sum, (T)cnt);
-            fl = 1;
-          } else {
-            if (MODE == ITER_FACE) Vd[e] = T(0);
-            fl = 0;
-          }
+  constexpr int CL = 8;  // cells of an x run
+  for (int p = 1; p <= nit; p++) {
+    // the cells whose six neighbours hold the data of p - 1 passes: the box
+    // [p, R - p) in each axis, as runs of up to CL cells along x, one run a
+    // thread (consecutive threads take consecutive z)
+    const int wy = RY - 2 * p, wz = RZ - 2 * p, ncol = wy * wz;
+    const int nrun = ncol * ((RX - 2 * p + CL - 1) / CL);
+    const int ia = max(p, -x0), ib = min(RX - p, dx - x0);  // in the box and the grid
+    const int q = p - 1;  // valid before pass p: D <= q
+    for (int it = threadIdx.x; it < nrun; it += blockDim.x) {
+      const int ch = it / ncol, col = it - ch * ncol;
+      const int jj = col / wz;
+      const int j = p + jj, k = p + (col - jj * wz);
+      const int gy = y0 + j, gz = z0 + k;
+      if (gy < 0 || gy >= dy || gz < 0 || gz >= dz) continue;
+      const int i0 = max(ia, p + ch * CL), i1 = min(ib, p + ch * CL + CL);
+      for (int i = i0; i < i1; i++) {
+        const int e = i * sX + j * sY + k;
+        if (D[e] != kIterNotYet) continue;
+        // out-of-domain neighbours are never valid and never counted
+        T sum = T(0);
+        int cnt = 0;
+        if (D[e - sX] <= q) { sum = radd(sum, V[e - sX]); cnt++; }
+        if (D[e + sX] <= q) { sum = radd(sum, V[e + sX]); cnt++; }
+        if (D[e - sY] <= q) { sum = radd(sum, V[e - sY]); cnt++; }
+        if (D[e + sY] <= q) { sum = radd(sum, V[e + sY]); cnt++; }
+        if (D[e - 1] <= q) { sum = radd(sum, V[e - 1]); cnt++; }
+        if (D[e + 1] <= q) { sum = radd(sum, V[e + 1]); cnt++; }
+        if (cnt > 0) {
+          V[e] = rdiv(sum, (T)cnt);
+          D[e] = (uint8_t)p;
         }
-        Fd[e] = fl;
-        if (G.hist && i >= H && i < H + TX && j >= H && j < H + TY && k >= H && k < H + TZ)
-          G.hist[(int64_t)(p + 1) * G.hstride + lin(gx, gy, gz, dy, dz)] = fl;
       }
     }
     __syncthreads();
   }
-  // the tile: both buffers (side 0 is buffer cur) and both flag arrays
+  // the tile: a cell made valid by pass d has its value in the buffer that
+  // pass wrote, side d mod 2 (the other side keeps what it held: zero in the
+  // face grids, which cells without a valid neighbour are given anyway);
+  // the last two passes' flags (or every pass's, into the history)
   for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
     const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
     const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
     if (gx >= dx || gy >= dy || gz >= dz) continue;
     const int64_t gi = lin(gx, gy, gz, dy, dz);
     const int le = (H + i) * sX + (H + j) * sY + (H + k);
-    G.b[G.cur][gi] = V[le];
-    G.b[1 - G.cur][gi] = V[RN + le];
-    if (!G.hist) {
-      G.f[G.cur][gi] = F[le];
-      G.f[1 - G.cur][gi] = F[RN + le];
+    const int d = D[le];
+    if (d >= 1 && d <= nit) G.b[G.cur ^ (d & 1)][gi] = V[le];
+    if (G.hist) {
+      for (int p = 1; p <= nit; p++) G.hist[(int64_t)p * G.hstride + gi] = d <= p ? 1 : 0;
+    } else {
+      G.f[G.cur ^ (nit & 1)][gi] = d <= nit ? 1 : 0;
+      G.f[G.cur ^ ((nit - 1) & 1)][gi] = d <= nit - 1 ? 1 : 0;
     }
   }
 }

@@ -65,12 +65,11 @@ def test_export_collider_surface(gpu):
 
 @pytest.mark.parametrize("passes", [(7, 2), (1, 4, 3)])
 def test_smoothing_pass_counts_follow_the_oracle(oracle, gpu, passes):
-    """smoothFluidSurface with pass counts that are not one launch of five:
-    a launch takes at most five passes and leaves the last pass and the one
-    before it in the two buffers the per-pass flips would, so the next
-    substep's SDF extrapolation, which keeps the older buffer's values in
-    valid cells, still follows the oracle.  24 x 20 x 36 cells: several
-    column tiles and runs of x planes per launch."""
+    """smoothFluidSurface with pass counts other than five, odd and even, on a
+    non-cubic grid: the surface after each call, and the next substep, whose
+    SDF extrapolation keeps the older buffer's values in valid cells, so the
+    buffer the pass before the last one wrote must hold what the oracle's
+    holds."""
     from simcraft_b200 import scenes
     from simcraft_b200.fluid import FluidSimulator
 

@@ -212,7 +212,10 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
     cudaMemsetAsync(gw_[a], 0, rs_ * fsz_[a], st);
   }
   // advect on the just-cleared grids (fluid-simulator.cc:143)
-  if (n > 0) k_advect_still<T><<<nblk(n), kT, 0, st>>>(n, P, G, h, collider_, dt);
+  if (n > 0 && collider_)
+    k_advect_still<T, true><<<nblk(n), kT, 0, st>>>(n, P, G, h, collider_, dt);
+  else if (n > 0)
+    k_advect_still<T, false><<<nblk(n), kT, 0, st>>>(n, P, G, h, nullptr, dt);
   launches_ += 1;
   cudaEventRecord(ev_[1], st);
   // sort by cell, then reconstruct (fluid-simulator.cc:146-148)

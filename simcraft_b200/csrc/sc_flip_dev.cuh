@@ -212,7 +212,7 @@ __device__ void sdf_grad(const double* S, const Geo& G, double h, double px, dou
 
 // HybridAdvectionSolver3D::handleCollision (advect-solver.cc:100-137).
 template <class T>
-__device__ void handle_collision(const double* col, const Geo& G, double h, T& px, T& py, T& pz,
+__device__ __forceinline__ void handle_collision(const double* col, const Geo& G, double h, T& px, T& py, T& pz,
                                  T& vx, T& vy, T& vz) {
   if (col) {
     const double d = sdf_eval(col, G.nx, G.ny, G.nz, h, (double)px, (double)py, (double)pz);
@@ -309,8 +309,10 @@ __global__ void __launch_bounds__(kT)
 // zeroed the grids advect samples, so both RK3 samples are exactly +0 (a
 // weighted average of zeros, or 0 where no node is in range) and the update
 // reduces to the same rounded sums with zero k2, k3.  Bit-identical to
-// k_advect on zero grids.
-template <class T>
+// k_advect on zero grids.  COL: a collider SDF is given; without one the
+// kernel is a stream of loads and stores, compiled apart from the collider's
+// FP64 sampling so that it needs a fifth of the registers (full occupancy).
+template <class T, bool COL>
 __global__ void __launch_bounds__(kT)
     k_advect_still(int64_t n, PartsT<T> P, Geo G, double hd, const double* col, double dtd) {
   const T dt = (T)dtd;
@@ -323,7 +325,7 @@ __global__ void __launch_bounds__(kT)
     py = radd(radd(radd(py, rmul(c1, k1y)), rmul(c2, zero)), rmul(c3, zero));
     pz = radd(radd(radd(pz, rmul(c1, k1z)), rmul(c2, zero)), rmul(c3, zero));
     T vx = k1x, vy = k1y, vz = k1z;
-    handle_collision(col, G, hd, px, py, pz, vx, vy, vz);
+    handle_collision(COL ? col : nullptr, G, hd, px, py, pz, vx, vy, vz);
     P.px[i] = px;
     P.py[i] = py;
     P.pz[i] = pz;
@@ -519,23 +521,50 @@ __global__ void __launch_bounds__(kT)
 // with a margin), the same set for every cell (a boundary bucket's open side
 // faces away from the cells that reach it).  A superset of the buckets the
 // loop keeps is harmless: only the nearest particle decides the result.
+// The buckets (cell offsets) a cell's reconstruction visits, nearest first,
+// each with a lower bound on the squared distance from the cell centre to any
+// particle of that bucket: the box distance of the bucket's cell, less a
+// margin for the rounding of the particle's cell key (one ulp of the grid
+// size in the particle type, times h) and for the rounding of the squared
+// distance.  Particles the sort clamped into boundary buckets lie beyond the
+// bucket's box, on the side away from every cell centre, so the bound holds
+// for them too.
 struct ReconOffsets {
   int n;
-  int d[1024];
+  int d[512];
+  double g2[512];
 };
-inline bool recon_offsets(double h, double radius, ReconOffsets& o) {
+inline bool recon_offsets(double h, double radius, double key_ulp, ReconOffsets& o) {
   const double R = 2.0 * radius / h;
   const int D = (int)std::ceil(R + 0.5) + 1;
-  o.n = 0;
   auto gap = [](int d) { return d == 0 ? 0.0 : std::abs(d) - 0.5; };
+  struct Off {
+    double g2;
+    int d;
+  };
+  Off all[15 * 15 * 15];
+  int n = 0;
+  if (D > 7) return false;
   for (int dx = -D; dx <= D; dx++)
     for (int dy = -D; dy <= D; dy++)
       for (int dz = -D; dz <= D; dz++) {
-        const double g2 = gap(dx) * gap(dx) + gap(dy) * gap(dy) + gap(dz) * gap(dz);
-        if (g2 > R * R * (1.0 + 1e-6) + 1e-12) continue;
-        if (o.n >= 1024 || D > 7) return false;
-        o.d[o.n++] = (dx + 8) | ((dy + 8) << 8) | ((dz + 8) << 16);
+        const double g = gap(dx) * gap(dx) + gap(dy) * gap(dy) + gap(dz) * gap(dz);
+        if (g > R * R * (1.0 + 1e-6) + 1e-12) continue;
+        double b = 0.0;
+        for (int e : {dx, dy, dz}) {
+          const double t = std::max(0.0, gap(e) * h - key_ulp * h);
+          b += t * t;
+        }
+        all[n++] = Off{b * (1.0 - 1e-12), (dx + 8) | ((dy + 8) << 8) | ((dz + 8) << 16)};
       }
+  if (n > 512) return false;
+  // ascending bounds, so that the first bound above the least distance ends the search
+  std::stable_sort(all, all + n, [](const Off& a, const Off& b) { return a.g2 < b.g2; });
+  o.n = n;
+  for (int q = 0; q < n; q++) {
+    o.d[q] = all[q].d;
+    o.g2[q] = all[q].g2;
+  }
   return true;
 }
 template <class T>
@@ -554,9 +583,13 @@ __global__ void __launch_bounds__(kT)
     // min over the candidates of |x - p| - r where |x - p| <= 2r: sqrt and the
     // subtraction are monotone and correctly rounded, so that is sqrt of the
     // least squared distance minus r, when its root passes the test (if the
-    // nearest particle fails it, all do): one square root per cell
+    // nearest particle fails it, all do): one square root per cell.  The
+    // buckets come nearest first; once a bucket's bound exceeds the least
+    // squared distance found, no particle of it or of any later bucket can
+    // be nearer, and the minimum is exact.
     double m2 = INFINITY;
     for (int q = 0; q < off.n; q++) {
+      if (m2 < off.g2[q]) break;
       const int w = off.d[q];
       const int a = i + (w & 255) - 8, b = j + ((w >> 8) & 255) - 8, c = k + ((w >> 16) & 255) - 8;
       if (a < 0 || a >= G.nx || b < 0 || b >= G.ny || c < 0 || c >= G.nz) continue;
@@ -590,7 +623,10 @@ template <class T>
 int launch_reconstruct(cudaStream_t st, const Geo& G, double h, double radius, const int* start, const int* cnt,
                        const T* px, const T* py, const T* pz, double* sdf, uint8_t* valid) {
   ReconOffsets off;
-  if (!recon_offsets(h, radius, off)) return -1;
+  // one ulp of the largest cell index in T: the cell key's rounding, in cells
+  const int nmax = std::max(G.nx, std::max(G.ny, G.nz));
+  const double key_ulp = std::ldexp(1.0, std::ilogb((double)nmax) + 1 - (sizeof(T) == 4 ? 24 : 53));
+  if (!recon_offsets(h, radius, key_ulp, off)) return -1;
   const int64_t N = (int64_t)G.nx * G.ny * G.nz;
   k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, radius, start, cnt, px, py, pz, sdf, valid, off);
   return 0;
@@ -1125,6 +1161,24 @@ __device__ void p2g_tile_grid(const Geo& G, const P2GSpacing<T>& h, int x0, int 
   const int t0[3] = {x0, y0, z0};
   for (int e = tid; e < 2 * kP2GRegion; e += kPThreads) Rs[e] = T(0);
   int nout = 0;
+  // the stencil class of the cell's first 32 particles, computed once: bit l
+  // of `outm` marks a particle whose stencil starts elsewhere, of `shm` one
+  // whose stencil starts at its cell along AX (else at cell - 1)
+  unsigned shm = 0u, outm = 0u;
+  for (int l = s0; l < s0 + min(m, 32); l++) {
+    const T p[3] = {P.px[l], P.py[l], P.pz[l]};
+    const int16_t* tb = tape ? tape + 6 * ids[l] : nullptr;
+    const int bA = p2g_base<T, AX, AX>(p[AX], h, tb);
+    const int b1 = p2g_base<T, AX, D1>(p[D1], h, tb), b2 = p2g_base<T, AX, D2>(p[D2], h, tb);
+    const int sh = bA - (c[AX] - 1);
+    const unsigned bit = 1u << (l - s0);
+    if (sh < 0 || sh > 1 || b1 != c[D1] - 1 || b2 != c[D2] - 1) {
+      outm |= bit;
+      nout++;
+    } else if (sh) {
+      shm |= bit;
+    }
+  }
   // region strides along AX and across it
   constexpr int stA = AX == 0 ? n1 * n2 : (AX == 1 ? n2 : 1);
   constexpr int st1 = D1 == 0 ? n1 * n2 : (D1 == 1 ? n2 : 1);
@@ -1137,17 +1191,26 @@ __device__ void p2g_tile_grid(const Geo& G, const P2GSpacing<T>& h, int x0, int 
       aw[q] = T(0);
     }
     for (int l = s0; l < s0 + m; l++) {
-      const T p[3] = {P.px[l], P.py[l], P.pz[l]};
-      const int16_t* tb = tape ? tape + 6 * ids[l] : nullptr;
-      const int bA = p2g_base<T, AX, AX>(p[AX], h, tb);
-      const int b1 = p2g_base<T, AX, D1>(p[D1], h, tb), b2 = p2g_base<T, AX, D2>(p[D2], h, tb);
-      const int sh = bA - (c[AX] - 1);
-      if (sh < 0 || sh > 1 || b1 != c[D1] - 1 || b2 != c[D2] - 1) {
-        if (ip == 0) nout++;
-        continue;
+      int sh;
+      if (l - s0 < 32) {
+        const unsigned bit = 1u << (l - s0);
+        if (outm & bit) continue;
+        sh = (shm & bit) ? 1 : 0;
+      } else {
+        const T p[3] = {P.px[l], P.py[l], P.pz[l]};
+        const int16_t* tb = tape ? tape + 6 * ids[l] : nullptr;
+        const int bA = p2g_base<T, AX, AX>(p[AX], h, tb);
+        const int b1 = p2g_base<T, AX, D1>(p[D1], h, tb), b2 = p2g_base<T, AX, D2>(p[D2], h, tb);
+        sh = bA - (c[AX] - 1);
+        if (sh < 0 || sh > 1 || b1 != c[D1] - 1 || b2 != c[D2] - 1) {
+          if (ip == 0) nout++;
+          continue;
+        }
       }
       const int t = ip - sh;
       if (t < 0 || t > 3) continue;
+      const T p[3] = {P.px[l], P.py[l], P.pz[l]};
+      const int bA = c[AX] - 1 + sh, b1 = c[D1] - 1, b2 = c[D2] - 1;
       // own axis: offset 0, across: 1/2
       const T wA = p2g_factor_q(h.over(p[AX]), (T)(bA + t));
       const T q1 = h.over(p[D1]), q2 = h.over(p[D2]);

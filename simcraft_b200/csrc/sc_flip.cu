@@ -71,6 +71,10 @@ FluidSim::FluidSim(Context* ctx, const FluidConfig& cfg) : ctx_(ctx), c_(cfg) {
   ok &= (bsum_ = (int*)alloc(sizeof(int) * ((N + 1023) / 1024 + 1))) != nullptr;
   ok &= (redbuf_ = (double*)alloc(sizeof(double) * 4)) != nullptr;
   ok &= (p2g_scr_ = alloc(p2g_scratch_bytes(Geo{nx, ny, nz}, rs_))) != nullptr;
+  for (int k = 0; k < 2; k++)
+    for (int a = 0; a < 3; a++)  // the FP64 tiles are the smaller ones: enough for either
+      ok &= (cls_[k][a] = (uint8_t*)alloc((size_t)iter_tiles<double>(nx + (a == 0), ny + (a == 1), nz + (a == 2)))) !=
+            nullptr;
   if (ok && cudaMallocHost(&host_red_, sizeof(double) * 4) != cudaSuccess) ok = false;
   if (!ok) {
     status_ = -3;
@@ -250,14 +254,16 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
                              (T*)gw_[2], gv_[0][gcur_[0]], gv_[1][gcur_[1]], gv_[2][gcur_[2]],
                              c_.flip ? (T*)last_[0] : nullptr, c_.flip ? (T*)last_[1] : nullptr,
                              c_.flip ? (T*)last_[2] : nullptr);
-  k_dirichlet<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, G_(0), gv_[0][gcur_[0]]);
-  k_dirichlet<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, G_(1), gv_[1][gcur_[1]]);
-  k_dirichlet<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, G_(2), gv_[2][gcur_[2]]);
-  launches_ += 3;
+  // Dirichlet walls, with the extrapolation tiles' classes
+  {
+    T* const gg[3] = {G_(0), G_(1), G_(2)};
+    uint8_t* const ff[3] = {gv_[0][gcur_[0]], gv_[1][gcur_[1]], gv_[2][gcur_[2]]};
+    launches_ += launch_dirichlet_tiles<T>(st, G, gg, ff, cls_[0]);
+  }
   // extrapolate(.., 10) on the three face grids, temporally blocked
   {
     T* const fb[3][2] = {{(T*)g_[0][0], (T*)g_[0][1]}, {(T*)g_[1][0], (T*)g_[1][1]}, {(T*)g_[2][0], (T*)g_[2][1]}};
-    launches_ += launch_extrap_faces<T>(st, G, c_.vel_extrap_iters, fb, gv_, nullptr, fsz_, gcur_);
+    launches_ += launch_extrap_faces<T>(st, G, c_.vel_extrap_iters, fb, gv_, nullptr, fsz_, gcur_, cls_);
   }
   k_force<T><<<nblk(fsz_[1]), kT, 0, st>>>(G, G_(1), gv_[1][gcur_[1]], c_.gravity * dt);
   launches_ += 1;

@@ -85,6 +85,7 @@ class FluidSim {
   int gcur_[3] = {0, 0, 0};
   void* gw_[3] = {};     // weight sums
   void* p2g_scr_ = nullptr;  // P2G tile slices (p2g_scratch_bytes)
+  uint8_t* cls_[2][3] = {};  // extrapolation tile classes, per face grid (two launches' worth)
   void* last_[3] = {};   // FLIP u_last/v_last/w_last
   double* wt_[3] = {};   // FVM face weights
   double* sdf_[2] = {};

@@ -775,7 +775,13 @@ struct IterGrid {
   uint8_t* hist;
   int64_t hstride;
   int cur;
+  // tile classes (kClsAny: a valid cell in the tile, kClsAll: every in-grid
+  // cell of the tile valid) before the launch, and after it; null: the block
+  // scans its region's flags instead
+  const uint8_t* cin;
+  uint8_t* cout;
 };
+constexpr uint8_t kClsAny = 1, kClsAll = 2;
 
 template <class T, int MODE>
 __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char* smem) {
@@ -797,6 +803,58 @@ __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char
     const bool in = gx >= 0 && gx < dx && gy >= 0 && gy < dy && gz >= 0 && gz < dz;
     return in ? lin(gx, gy, gz, dy, dz) : -1;
   };
+  const int ntx = (dx + TX - 1) / TX;
+  // every tile cell valid: each pass leaves the values and sets the flags
+  auto all_valid = [&]() {
+    for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
+      const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
+      const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
+      if (gx >= dx || gy >= dy || gz >= dz) continue;
+      const int64_t gi = lin(gx, gy, gz, dy, dz);
+      if (G.hist) {
+        for (int p = 1; p <= nit; p++) G.hist[(int64_t)p * G.hstride + gi] = 1;
+      } else {
+        G.f[0][gi] = 1;
+        G.f[1][gi] = 1;
+      }
+    }
+    if (G.cout && threadIdx.x == 0) G.cout[tile] = kClsAny | kClsAll;
+  };
+  // no valid cell within reach: the face passes would write zeros where the
+  // buffers hold zeros already; the SDF passes leave the values and write zero
+  // flags into the buffers they write
+  auto none_valid = [&]() {
+    if (MODE == ITER_SDF && !G.hist)
+      for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
+        const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
+        const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
+        if (gx >= dx || gy >= dy || gz >= dz) continue;
+        const int64_t gi = lin(gx, gy, gz, dy, dz);
+        G.f[1 - G.cur][gi] = 0;
+        if (nit > 1) G.f[G.cur][gi] = 0;
+      }
+    if (G.cout && threadIdx.x == 0) G.cout[tile] = 0;
+  };
+  if (G.cin) {
+    // the classes say which tiles are on the front: the halo is shorter than
+    // a tile, so a valid cell within reach lies in one of the 27 tiles around
+    int nb = 0;
+    if (threadIdx.x < 27) {
+      const int ax = tx + (int)threadIdx.x % 3 - 1, ay = ty + ((int)threadIdx.x / 3) % 3 - 1,
+                az = tz + (int)threadIdx.x / 9 - 1;
+      if (ax >= 0 && ax < ntx && ay >= 0 && ay < nty && az >= 0 && az < ntz)
+        nb = G.cin[((int64_t)ax * nty + ay) * ntz + az] & kClsAny;
+    }
+    const bool near = __syncthreads_or(nb);
+    if (G.cin[tile] & kClsAll) {
+      all_valid();
+      return;
+    }
+    if (!near) {
+      none_valid();
+      return;
+    }
+  }
   constexpr int NB = 8;  // loads in flight per thread
   {
     // the flags first: a tile with no valid flag within reach needs no values
@@ -822,34 +880,11 @@ __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char
       }
     }
     if (__syncthreads_and(all)) {
-      // every tile cell valid: each pass leaves the values and sets the flags
-      for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
-        const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
-        const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
-        if (gx >= dx || gy >= dy || gz >= dz) continue;
-        const int64_t gi = lin(gx, gy, gz, dy, dz);
-        if (G.hist) {
-          for (int p = 1; p <= nit; p++) G.hist[(int64_t)p * G.hstride + gi] = 1;
-        } else {
-          G.f[0][gi] = 1;
-          G.f[1][gi] = 1;
-        }
-      }
+      all_valid();
       return;
     }
     if (!__syncthreads_or(any)) {
-      // no valid cell within reach: the face passes would write zeros where the
-      // buffers hold zeros already; the SDF passes leave the values and write
-      // zero flags into the buffers they write
-      if (MODE == ITER_SDF && !G.hist)
-        for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
-          const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
-          const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
-          if (gx >= dx || gy >= dy || gz >= dz) continue;
-          const int64_t gi = lin(gx, gy, gz, dy, dz);
-          G.f[1 - G.cur][gi] = 0;
-          if (nit > 1) G.f[G.cur][gi] = 0;
-        }
+      none_valid();
       return;
     }
   }
@@ -909,6 +944,7 @@ __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char
   // pass wrote, side d mod 2 (the other side keeps what it held: zero in the
   // face grids, which cells without a valid neighbour are given anyway);
   // the last two passes' flags (or every pass's, into the history)
+  int any = 0, all = 1;  // the tile's class after the passes
   for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
     const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
     const int gx = x0 + H + i, gy = y0 + H + j, gz = z0 + H + k;
@@ -923,6 +959,13 @@ __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char
       G.f[G.cur ^ (nit & 1)][gi] = d <= nit ? 1 : 0;
       G.f[G.cur ^ ((nit - 1) & 1)][gi] = d <= nit - 1 ? 1 : 0;
     }
+    any |= d <= nit;
+    all &= d <= nit;
+  }
+  if (G.cout) {
+    any = __syncthreads_or(any);
+    all = __syncthreads_and(all);
+    if (threadIdx.x == 0) G.cout[tile] = (any ? kClsAny : 0) | (all ? kClsAll : 0);
   }
 }
 
@@ -955,7 +998,8 @@ __global__ void __launch_bounds__(kIterThreads) k_iter_cells(IterGrid<double> g,
 // the ping-pong flags f[a][2].
 template <class T>
 int launch_extrap_faces(cudaStream_t st, const Geo& G, int iters, T* const b[3][2], uint8_t* const f[3][2],
-                        uint8_t* const hist[3], const int64_t fsz[3], int cur[3]) {
+                        uint8_t* const hist[3], const int64_t fsz[3], int cur[3],
+                        uint8_t* const cls[2][3] = nullptr) {
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_iter_faces<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)iter_smem_bytes<T>());
@@ -978,6 +1022,11 @@ int launch_extrap_faces(cudaStream_t st, const Geo& G, int iters, T* const b[3][
       g.hist = hist ? hist[ax] + (int64_t)k0 * fsz[ax] : nullptr;
       g.hstride = fsz[ax];
       g.cur = cur[ax];
+      // launch k reads the classes launch k - 1 wrote (the first, those of
+      // k_dirichlet_tiles) and writes the other array
+      const int kl = k0 / kIterHalo;
+      g.cin = cls ? cls[kl & 1][ax] : nullptr;
+      g.cout = cls ? cls[(kl + 1) & 1][ax] : nullptr;
       acc += iter_tiles<T>(g.dx, g.dy, g.dz);
       if (ax == 0) a.t0 = acc;
       if (ax == 1) a.t1 = acc;
@@ -1016,6 +1065,8 @@ int launch_iter_cells(cudaStream_t st, const Geo& G, int iters, double* const b[
     g.f[1] = f ? (fcur == cur ? f[1] : f[0]) : nullptr;
     g.hist = nullptr;
     g.hstride = 0;
+    g.cin = nullptr;
+    g.cout = nullptr;
     k_iter_cells<MODE><<<iter_tiles<double>(G.nx, G.ny, G.nz), kIterThreads, iter_smem_bytes<double>(), st>>>(g, nit);
     launches++;
     if (nit & 1) {
@@ -1726,6 +1777,69 @@ __global__ void __launch_bounds__(kT) k_dirichlet(Geo G, T* g, uint8_t* valid) {
       valid[id] = 1;
     }
   }
+}
+
+// applyDirichletBoundary for the three face grids in one launch, a block per
+// extrapolation tile (the tiles of k_iter_faces), which also records each
+// tile's class (kClsAny, kClsAll) from its flags after the walls are set: the
+// first extrapolation launch reads the classes instead of scanning every
+// tile's region.
+template <class T>
+struct DirTiles {
+  T* g[3];
+  uint8_t* f[3];
+  uint8_t* cls[3];
+  int t0, t1;  // tiles of grid 0, of grids 0 and 1
+};
+constexpr int kDirThreads = 512;
+template <class T>
+__global__ void __launch_bounds__(kDirThreads) k_dirichlet_tiles(Geo G, DirTiles<T> a) {
+  constexpr int TX = IterTile<T>::X, TY = IterTile<T>::Y, TZ = IterTile<T>::Z;
+  const int b = blockIdx.x;
+  const int ax = b < a.t0 ? 0 : (b < a.t1 ? 1 : 2);
+  const int tile = b - (ax == 0 ? 0 : (ax == 1 ? a.t0 : a.t1));
+  const int dx = G.fx(ax), dy = G.fy(ax), dz = G.fz(ax);
+  const int ntz = (dz + TZ - 1) / TZ, nty = (dy + TY - 1) / TY;
+  const int tz = tile % ntz, ty = (tile / ntz) % nty, tx = tile / (ntz * nty);
+  T* g = a.g[ax];
+  uint8_t* f = a.f[ax];
+  const int qm = (ax == 0 ? dx : (ax == 1 ? dy : dz)) - 1;
+  int any = 0, all = 1;
+  for (int e = threadIdx.x; e < TX * TY * TZ; e += blockDim.x) {
+    const int i = e / (TY * TZ), r = e - i * (TY * TZ), j = r / TZ, k = r - j * TZ;
+    const int gx = tx * TX + i, gy = ty * TY + j, gz = tz * TZ + k;
+    if (gx >= dx || gy >= dy || gz >= dz) continue;
+    const int64_t gi = lin(gx, gy, gz, dy, dz);
+    const int q = ax == 0 ? gx : (ax == 1 ? gy : gz);
+    int v;
+    if (q == 0 || q == qm) {
+      g[gi] = T(0);
+      f[gi] = 1;
+      v = 1;
+    } else {
+      v = f[gi] ? 1 : 0;
+    }
+    any |= v;
+    all &= v;
+  }
+  any = __syncthreads_or(any);
+  all = __syncthreads_and(all);
+  if (threadIdx.x == 0) a.cls[ax][tile] = (any ? kClsAny : 0) | (all ? kClsAll : 0);
+}
+template <class T>
+int launch_dirichlet_tiles(cudaStream_t st, const Geo& G, T* const g[3], uint8_t* const f[3], uint8_t* const cls[3]) {
+  DirTiles<T> a;
+  int acc = 0;
+  for (int ax = 0; ax < 3; ax++) {
+    a.g[ax] = g[ax];
+    a.f[ax] = f[ax];
+    a.cls[ax] = cls[ax];
+    acc += iter_tiles<T>(G.nx + (ax == 0), G.ny + (ax == 1), G.nz + (ax == 2));
+    if (ax == 0) a.t0 = acc;
+    if (ax == 1) a.t1 = acc;
+  }
+  k_dirichlet_tiles<T><<<acc, kDirThreads, 0, st>>>(G, a);
+  return 1;
 }
 
 // extrapolate iteration for one face grid (cpu/fluid-simulator.h:204-253):

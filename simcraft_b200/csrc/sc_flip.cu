@@ -71,6 +71,7 @@ FluidSim::FluidSim(Context* ctx, const FluidConfig& cfg) : ctx_(ctx), c_(cfg) {
   ok &= (bsum_ = (int*)alloc(sizeof(int) * ((N + 1023) / 1024 + 1))) != nullptr;
   ok &= (redbuf_ = (double*)alloc(sizeof(double) * 4)) != nullptr;
   ok &= (p2g_scr_ = alloc(p2g_scratch_bytes(Geo{nx, ny, nz}, rs_))) != nullptr;
+  for (int k = 0; k < 2; k++) ok &= (clsS_[k] = (uint8_t*)alloc((size_t)iter_tiles<double>(nx, ny, nz))) != nullptr;
   for (int k = 0; k < 2; k++)
     for (int a = 0; a < 3; a++)  // the FP64 tiles are the smaller ones: enough for either
       ok &= (cls_[k][a] = (uint8_t*)alloc((size_t)iter_tiles<double>(nx + (a == 0), ny + (a == 1), nz + (a == 2)))) !=
@@ -239,11 +240,11 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
     cudaMemsetAsync(start_, 0, sizeof(int) * N, st);
   }
   if (launch_reconstruct<T>(st, G, h, c_.recon_factor * h, start_, cnt_, P.px, P.py, P.pz, sdf_[scur_],
-                            sdfv_[svcur_]))
+                            sdfv_[svcur_], clsS_[0]))
     return ctx_->set_error(-1, "reconstruct: radius reaches past 6 cells");
   launches_ += 1;
   // extrapolateFluidSdf(10), temporally blocked
-  launches_ += launch_iter_cells<ITER_SDF>(st, G, c_.sdf_extrap_iters, sdf_, sdfv_, scur_, svcur_);
+  launches_ += launch_iter_cells<ITER_SDF>(st, G, c_.sdf_extrap_iters, sdf_, sdfv_, scur_, svcur_, clsS_);
   // smoothFluidSurface(5)
   launches_ += launch_smooth(st, G, c_.smooth_iters, sdf_, scur_);
   const double* fluid = sdf_[scur_];

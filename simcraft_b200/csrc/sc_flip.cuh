@@ -86,6 +86,7 @@ class FluidSim {
   void* gw_[3] = {};     // weight sums
   void* p2g_scr_ = nullptr;  // P2G tile slices (p2g_scratch_bytes)
   uint8_t* cls_[2][3] = {};  // extrapolation tile classes, per face grid (two launches' worth)
+  uint8_t* clsS_[2] = {};    // the same for the fluid SDF's extrapolation
   void* last_[3] = {};   // FLIP u_last/v_last/w_last
   double* wt_[3] = {};   // FVM face weights
   double* sdf_[2] = {};

@@ -567,16 +567,27 @@ inline bool recon_offsets(double h, double radius, double key_ulp, ReconOffsets&
   }
   return true;
 }
+// A block takes one tile of the FP64 extrapolation (8 x 16 x 16 cells) and,
+// given `cls`, records the tile's class (a valid cell; all valid), which the
+// SDF extrapolation reads instead of scanning every tile's region.
+constexpr int kRecTX = 8, kRecTY = 16, kRecTZ = 16;
+inline int recon_tiles(const Geo& G) {
+  return ((G.nx + kRecTX - 1) / kRecTX) * ((G.ny + kRecTY - 1) / kRecTY) * ((G.nz + kRecTZ - 1) / kRecTZ);
+}
 template <class T>
 __global__ void __launch_bounds__(kT)
     k_reconstruct(Geo G, double h, double radius, const int* start, const int* cnt,
                   const T* __restrict__ px, const T* __restrict__ py, const T* __restrict__ pz,
-                  double* sdf, uint8_t* valid, const ReconOffsets off) {
-  const int64_t N = (int64_t)G.nx * G.ny * G.nz;
+                  double* sdf, uint8_t* valid, const ReconOffsets off, uint8_t* cls) {
   const double r2 = 2 * radius;
-  GRID_LOOP(id, N) {
-    int i, j, k;
-    decode3(id, G.ny, G.nz, i, j, k);
+  const int ntz = (G.nz + kRecTZ - 1) / kRecTZ, nty = (G.ny + kRecTY - 1) / kRecTY;
+  const int tz = blockIdx.x % ntz, ty = (blockIdx.x / ntz) % nty, tx = blockIdx.x / (ntz * nty);
+  int any = 0, all = 1;
+  for (int e = threadIdx.x; e < kRecTX * kRecTY * kRecTZ; e += blockDim.x) {
+    const int i = tx * kRecTX + e / (kRecTY * kRecTZ), j = ty * kRecTY + (e / kRecTZ) % kRecTY,
+              k = tz * kRecTZ + e % kRecTZ;
+    if (i >= G.nx || j >= G.ny || k >= G.nz) continue;
+    const int64_t id = lin(i, j, k, G.ny, G.nz);
     const double cx = radd(rmul(radd((double)i, 0.5), h), 0.0);
     const double cy = radd(rmul(radd((double)j, 0.5), h), 0.0);
     const double cz = radd(rmul(radd((double)k, 0.5), h), 0.0);
@@ -615,20 +626,26 @@ __global__ void __launch_bounds__(kT)
     }
     sdf[id] = best;
     valid[id] = ok;
+    any |= ok;
+    all &= ok;
+  }
+  if (cls) {
+    any = __syncthreads_or(any);
+    all = __syncthreads_and(all);
+    if (threadIdx.x == 0) cls[blockIdx.x] = (any ? 1 : 0) | (all ? 2 : 0);
   }
 }
 // NaiveReconstructor::reconstruct over the sorted buckets; -1 when the radius
 // reaches past the offsets the kernel takes (over ~6 cells).
 template <class T>
 int launch_reconstruct(cudaStream_t st, const Geo& G, double h, double radius, const int* start, const int* cnt,
-                       const T* px, const T* py, const T* pz, double* sdf, uint8_t* valid) {
+                       const T* px, const T* py, const T* pz, double* sdf, uint8_t* valid, uint8_t* cls = nullptr) {
   ReconOffsets off;
   // one ulp of the largest cell index in T: the cell key's rounding, in cells
   const int nmax = std::max(G.nx, std::max(G.ny, G.nz));
   const double key_ulp = std::ldexp(1.0, std::ilogb((double)nmax) + 1 - (sizeof(T) == 4 ? 24 : 53));
   if (!recon_offsets(h, radius, key_ulp, off)) return -1;
-  const int64_t N = (int64_t)G.nx * G.ny * G.nz;
-  k_reconstruct<T><<<nblk(N), kT, 0, st>>>(G, h, radius, start, cnt, px, py, pz, sdf, valid, off);
+  k_reconstruct<T><<<recon_tiles(G), kT, 0, st>>>(G, h, radius, start, cnt, px, py, pz, sdf, valid, off, cls);
   return 0;
 }
 
@@ -782,6 +799,8 @@ struct IterGrid {
   uint8_t* cout;
 };
 constexpr uint8_t kClsAny = 1, kClsAll = 2;
+static_assert(IterTile<double>::X == kRecTX && IterTile<double>::Y == kRecTY && IterTile<double>::Z == kRecTZ,
+              "the reconstruction's tiles are the FP64 extrapolation's");
 
 template <class T, int MODE>
 __device__ void iter_tile(const IterGrid<T>& G, int tile, int nit, unsigned char* smem) {
@@ -1042,7 +1061,7 @@ int launch_extrap_faces(cudaStream_t st, const Geo& G, int iters, T* const b[3][
 // and fcur flip per pass.
 template <int MODE>
 int launch_iter_cells(cudaStream_t st, const Geo& G, int iters, double* const b[2], uint8_t* const f[2], int& cur,
-                      int& fcur) {
+                      int& fcur, uint8_t* const cls[2] = nullptr) {
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_iter_cells<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1065,8 +1084,10 @@ int launch_iter_cells(cudaStream_t st, const Geo& G, int iters, double* const b[
     g.f[1] = f ? (fcur == cur ? f[1] : f[0]) : nullptr;
     g.hist = nullptr;
     g.hstride = 0;
-    g.cin = nullptr;
-    g.cout = nullptr;
+    // launch k reads the classes launch k - 1 wrote (the first, the
+    // reconstruction's) and writes the other array
+    g.cin = cls ? cls[(k0 / kIterHalo) & 1] : nullptr;
+    g.cout = cls ? cls[(k0 / kIterHalo + 1) & 1] : nullptr;
     k_iter_cells<MODE><<<iter_tiles<double>(G.nx, G.ny, G.nz), kIterThreads, iter_smem_bytes<double>(), st>>>(g, nit);
     launches++;
     if (nit & 1) {

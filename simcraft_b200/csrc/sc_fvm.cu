@@ -71,24 +71,22 @@ __global__ void __launch_bounds__(kT)
 }
 
 // Matrix row, rhs and active flag of one cell (project-solver.cc:129-226).
+struct CellRow {
+  double ad, aL, aR, aU, aD, aF, aB, r;
+  uint8_t act;
+};
 template <class T>
-__global__ void __launch_bounds__(kT)
-    k_build_cells(int nx, int ny, int nz, double h, double dt, const T* __restrict__ u,
-                  const T* __restrict__ v, const T* __restrict__ w,
-                  const double* __restrict__ F, const double* __restrict__ uw,
-                  const double* __restrict__ vw, const double* __restrict__ ww, SystemOut out) {
-  const int64_t n = (int64_t)nx * ny * nz;
-  const int64_t su = (int64_t)ny * nz;  // u grid x-stride
-  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n;
-       id += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(id % nz);
-    const int j = (int)((id / nz) % ny);
-    const int i = (int)(id / ((int64_t)ny * nz));
+__device__ __forceinline__ CellRow build_cell(int nx, int ny, int nz, double h, double dt, int i, int j, int k,
+                                              const T* __restrict__ u, const T* __restrict__ v,
+                                              const T* __restrict__ w, const double* __restrict__ F,
+                                              const double* __restrict__ uw, const double* __restrict__ vw,
+                                              const double* __restrict__ ww) {
+  const int64_t id = lin(i, j, k, ny, nz);
+  {
     // face indices of this cell
     const int64_t uL = lin(i, j, k, ny, nz), uR = lin(i + 1, j, k, ny, nz);
     const int64_t vD = lin(i, j, k, ny + 1, nz), vU = lin(i, j + 1, k, ny + 1, nz);
     const int64_t wB = lin(i, j, k, ny, nz + 1), wF = lin(i, j, k + 1, ny, nz + 1);
-    (void)su;
     double ad = 0.0, aL = 0.0, aR = 0.0, aU = 0.0, aD = 0.0, aF = 0.0, aB = 0.0, r = 0.0;
     uint8_t act = 0;
     const bool any = !(uw[uL] == 0.0 && uw[uR] == 0.0 && vw[vD] == 0.0 && vw[vU] == 0.0 &&
@@ -166,24 +164,64 @@ __global__ void __launch_bounds__(kT)
         r -= ww[wF] * (double)w[wF];
       }
     }
-    if (out.adiag) out.adiag[id] = ad;
-    if (out.an[0]) out.an[0][id] = aL;
-    if (out.an[1]) out.an[1][id] = aR;
-    if (out.an[2]) out.an[2][id] = aU;
-    if (out.an[3]) out.an[3][id] = aD;
-    if (out.an[4]) out.an[4][id] = aF;
-    if (out.an[5]) out.an[5][id] = aB;
-    if (out.rhs) out.rhs[id] = r;
-    if (out.active) out.active[id] = act;
-    if (out.t_adiag) {
-      const int64_t e = out.g.off(i, j, k);
-      out.t_adiag[e] = ad;
-      out.t_al[e] = aL;
-      out.t_ad[e] = aD;
-      out.t_ab[e] = aB;
-      out.t_rhs[e] = act ? r : 0.0;
-      out.t_active[e] = act;
-    }
+    return CellRow{ad, aL, aR, aU, aD, aF, aB, r, act};
+  }
+}
+__device__ __forceinline__ void store_row_linear(const SystemOut& out, int64_t id, const CellRow& c) {
+  if (out.adiag) out.adiag[id] = c.ad;
+  if (out.an[0]) out.an[0][id] = c.aL;
+  if (out.an[1]) out.an[1][id] = c.aR;
+  if (out.an[2]) out.an[2][id] = c.aU;
+  if (out.an[3]) out.an[3][id] = c.aD;
+  if (out.an[4]) out.an[4][id] = c.aF;
+  if (out.an[5]) out.an[5][id] = c.aB;
+  if (out.rhs) out.rhs[id] = c.r;
+  if (out.active) out.active[id] = c.act;
+}
+__device__ __forceinline__ void store_row_tiled(const SystemOut& out, int64_t e, const CellRow& c) {
+  out.t_adiag[e] = c.ad;
+  out.t_al[e] = c.aL;
+  out.t_ad[e] = c.aD;
+  out.t_ab[e] = c.aB;
+  out.t_rhs[e] = c.act ? c.r : 0.0;
+  out.t_active[e] = c.act;
+}
+// Cells in the reference's order: the rows in the reference layout.
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_build_cells(int nx, int ny, int nz, double h, double dt, const T* __restrict__ u,
+                  const T* __restrict__ v, const T* __restrict__ w,
+                  const double* __restrict__ F, const double* __restrict__ uw,
+                  const double* __restrict__ vw, const double* __restrict__ ww, SystemOut out) {
+  const int64_t n = (int64_t)nx * ny * nz;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < n;
+       id += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(id % nz);
+    const int j = (int)((id / nz) % ny);
+    const int i = (int)(id / ((int64_t)ny * nz));
+    const CellRow c = build_cell<T>(nx, ny, nz, h, dt, i, j, k, u, v, w, F, uw, vw, ww);
+    store_row_linear(out, id, c);
+    if (out.t_adiag) store_row_tiled(out, out.g.off(i, j, k), c);
+  }
+}
+// Cells in the solver's tiled order, a block per row block (tile, slot), so
+// that the tiled rows are written in whole 256-element runs (in the
+// reference's order consecutive cells lie a tile row apart there).
+template <class T>
+__global__ void __launch_bounds__(kT)
+    k_build_cells_tiled(int nx, int ny, int nz, double h, double dt, const T* __restrict__ u,
+                        const T* __restrict__ v, const T* __restrict__ w,
+                        const double* __restrict__ F, const double* __restrict__ uw,
+                        const double* __restrict__ vw, const double* __restrict__ ww, SystemOut out) {
+  static_assert(Tiled::TY * 32 == kT, "one thread per element of a row block");
+  const int64_t nrb = (int64_t)out.g.ntiles() * out.g.nz;
+  for (int64_t rb = blockIdx.x; rb < nrb; rb += gridDim.x) {
+    Cell cl;
+    cl.init(out.g, (int)rb, threadIdx.x);
+    if (!cl.inside) continue;
+    const CellRow c = build_cell<T>(nx, ny, nz, h, dt, cl.x, cl.y, cl.z, u, v, w, F, uw, vw, ww);
+    store_row_linear(out, lin(cl.x, cl.y, cl.z, ny, nz), c);
+    store_row_tiled(out, cl.e, c);
   }
 }
 
@@ -237,8 +275,11 @@ int fvm_build_system(cudaStream_t st, int nx, int ny, int nz, double h, double d
   k_face_weights<1><<<blocks_for(fv), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, collider, vwt);
   k_face_weights<2><<<blocks_for(fw), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, collider, wwt);
   const int64_t n = (int64_t)nx * ny * nz;
-  k_build_cells<T><<<blocks_for(n), kT, 0, st>>>(nx, ny, nz, h, dt, u, v, w, fluid_sdf, uwt, vwt,
-                                                 wwt, out);
+  if (out.t_adiag)
+    k_build_cells_tiled<T><<<blocks_for((int64_t)out.g.ntiles() * out.g.nz * kT), kT, 0, st>>>(
+        nx, ny, nz, h, dt, u, v, w, fluid_sdf, uwt, vwt, wwt, out);
+  else
+    k_build_cells<T><<<blocks_for(n), kT, 0, st>>>(nx, ny, nz, h, dt, u, v, w, fluid_sdf, uwt, vwt, wwt, out);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

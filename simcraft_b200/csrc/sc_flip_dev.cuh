@@ -64,6 +64,14 @@ __device__ __forceinline__ T bspline(T r) {
   }
   return T(0);
 }
+// The same factor with both pieces evaluated and one selected (no branch).
+template <class T>
+__device__ __forceinline__ T bspline_sel(T r) {
+  const T inner = radd(rsub(T(2.0 / 3.0), rmul(r, r)), rmul(rmul(rmul(T(0.5), r), r), r));
+  const T t = rsub(T(2), r);
+  const T outer = rdiv(rmul(rmul(t, t), t), T(6));
+  return r < T(1) ? inner : (r < T(2) ? outer : T(0));
+}
 template <class T>
 __device__ __forceinline__ T kweight(T h, T dx, T dy, T dz) {
   return rmul(rmul(bspline(rdiv(fabs(dx), h)), bspline(rdiv(fabs(dy), h))),
@@ -110,7 +118,13 @@ __device__ __forceinline__ void make_stencil_pow2(Stencil<T>& S, T px, T py, T p
       const int b = (int)radd(over(rsub(rsub(p[ax], T(0)), rmul(off, h))), T(0.5)) - 1;
       S.base[ax][o] = b;
 #pragma unroll
-      for (int i = 0; i < 4; i++) S.w[ax][o][i] = bspline(over(fabs(rsub(p[ax], coord1(b + i, off, h)))));
+      for (int i = 0; i < 4; i++) {
+#if SC_G2P_SELECT
+        S.w[ax][o][i] = bspline_sel(over(fabs(rsub(p[ax], coord1(b + i, off, h)))));
+#else
+        S.w[ax][o][i] = bspline(over(fabs(rsub(p[ax], coord1(b + i, off, h)))));
+#endif
+      }
     }
 }
 

@@ -529,20 +529,19 @@ __global__ void __launch_bounds__(kT)
 // cell-centred SDF = min over particles within 2r of (|x - p| - r).  Each
 // bucket's last particle is skipped, as the reference's forNeighbours loop
 // stops one short of its inclusive end index (ns-util.h:76-77, 103).
-// The buckets the reference's loop can visit around a cell, as offsets from
-// the cell (packed dx + 8 | dy + 8 << 8 | dz + 8 << 16): every offset whose
-// bucket box comes within 2r of the cell centre (box distance, in units of h,
-// with a margin), the same set for every cell (a boundary bucket's open side
-// faces away from the cells that reach it).  A superset of the buckets the
-// loop keeps is harmless: only the nearest particle decides the result.
-// The buckets (cell offsets) a cell's reconstruction visits, nearest first,
-// each with a lower bound on the squared distance from the cell centre to any
-// particle of that bucket: the box distance of the bucket's cell, less a
-// margin for the rounding of the particle's cell key (one ulp of the grid
-// size in the particle type, times h) and for the rounding of the squared
-// distance.  Particles the sort clamped into boundary buckets lie beyond the
-// bucket's box, on the side away from every cell centre, so the bound holds
-// for them too.
+// The buckets a cell's reconstruction visits, as offsets from the cell
+// (packed dx + 8 | dy + 8 << 8 | dz + 8 << 16): every offset whose bucket box
+// comes within 2r of the cell centre (box distance, in units of h, with a
+// margin), the same set for every cell (a boundary bucket's open side faces
+// away from the cells that reach it).  A superset of the buckets the
+// reference's loop keeps is harmless: only the nearest particle decides the
+// result.  They come nearest first, each with a lower bound on the squared
+// distance from the cell centre to any particle of that bucket: the box
+// distance of the bucket's cell, less a margin for the rounding of the
+// particle's cell key (one ulp of the grid size in the particle type, times
+// h) and for the rounding of the squared distance.  Particles the sort
+// clamped into boundary buckets lie beyond the bucket's box, on the side away
+// from every cell centre, so the bound holds for them too.
 struct ReconOffsets {
   int n;
   int d[512];

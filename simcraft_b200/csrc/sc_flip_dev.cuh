@@ -64,7 +64,10 @@ __device__ __forceinline__ T bspline(T r) {
   }
   return T(0);
 }
-// The same factor with both pieces evaluated and one selected (no branch).
+// The same factor with both pieces evaluated and one selected: the lanes of a
+// warp fall in different pieces, and without the branch the G2P tile kernel
+// measured 3% faster (project + G2P of 33.5M particles 4.11 -> 3.97 ms); the
+// values are the same bit for bit.
 template <class T>
 __device__ __forceinline__ T bspline_sel(T r) {
   const T inner = radd(rsub(T(2.0 / 3.0), rmul(r, r)), rmul(rmul(rmul(T(0.5), r), r), r));
@@ -118,13 +121,7 @@ __device__ __forceinline__ void make_stencil_pow2(Stencil<T>& S, T px, T py, T p
       const int b = (int)radd(over(rsub(rsub(p[ax], T(0)), rmul(off, h))), T(0.5)) - 1;
       S.base[ax][o] = b;
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-#if SC_G2P_SELECT
-        S.w[ax][o][i] = bspline_sel(over(fabs(rsub(p[ax], coord1(b + i, off, h)))));
-#else
-        S.w[ax][o][i] = bspline(over(fabs(rsub(p[ax], coord1(b + i, off, h)))));
-#endif
-      }
+      for (int i = 0; i < 4; i++) S.w[ax][o][i] = bspline_sel(over(fabs(rsub(p[ax], coord1(b + i, off, h)))));
     }
 }
 

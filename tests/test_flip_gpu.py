@@ -186,6 +186,28 @@ def test_reconstruct_bit_exact(oracle, torch_mod, n, radius_factor):
     assert v_ref.any() and not v_ref.all()
 
 
+def test_reconstruct_dense_buckets_bit_exact(oracle, torch_mod):
+    """Buckets far fuller than the dam breaks' (about 20 to 25 particles, past
+    the 16 that are ordered through shared memory, so the sort's in-place
+    path): the bucket order, which fixes the particle the reference's loop
+    skips, and so the SDF, bit for bit."""
+    from simcraft_b200 import fluid
+    n = 16
+    h = 1.0 / n
+    rng = np.random.default_rng(16)
+    # cells (0, 0..7, 0..15): ~2600 particles
+    a = rng.uniform(0, 1, (2600, 3)) * np.array([h, 8 * h, 16 * h])
+    # cells (5, 8..15, 0..15): ~1500 particles, ~23 a bucket
+    b = rng.uniform(0, 1, (1500, 3)) * np.array([h, 8 * h, 16 * h]) + np.array([5 * h, 8 * h, 0.0])
+    pos, _, _ = scenes.dam_break(n, frac_x=0.5, frac_y=0.5, ppc=3, seed=17)
+    pos = rng.permutation(np.concatenate([pos, a, b]))
+    dims = (n, n, n)
+    s_ref, v_ref = oracle.reconstruct(pos, dims, h, 0.8 * h)
+    s, v = fluid.reconstruct(_dev(torch_mod, pos), dims, h, 0.8 * h)
+    np.testing.assert_array_equal(v.cpu().numpy(), v_ref)
+    np.testing.assert_array_equal(s.cpu().numpy(), s_ref)
+
+
 def _config1_sim(oracle, n=32, steps=10, precision="f64", advection="flip", collider=None, seed=1):
     """The 32^3 dam break: block x<0.5, y<0.5, 8 jittered particles per cell,
     frame dt 1/120, FLIP blend 0.95, MIC(0)-PCG to 1e-6 relative, max 200."""

@@ -839,9 +839,7 @@ int DiffSim::step_t(int t, int mode, const void* in, void* out) {
   if (fvm_project<T>(st, c_.nx, c_.ny, c_.nz, h, dt, gu, gv, gw, pcg_->pressure64(), &tg, fluid, wt_[0], wt_[1],
                      wt_[2]))
     return err("project");
-  k_collider<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, h, gu, nullptr);
-  k_collider<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, h, gv, nullptr);
-  k_collider<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, h, gw, nullptr);
+  launch_collider<T>(st, G, h, gu, gv, gw, nullptr);
   // G2P into out
   cudaMemcpyAsync(out, xa_, rs_ * 6 * (size_t)n, cudaMemcpyDeviceToDevice, st);
   k_g2p<T><<<nblk(n), kT, 0, st>>>(n, O, gu, gv, gw, (T*)last_[0], (T*)last_[1], (T*)last_[2], G, h,

@@ -295,9 +295,7 @@ int FluidSim::substep_t(double dt, StepStats* stt) {
   e = fvm_project<T>(st, nx, ny, nz, h, dt, G_(0), G_(1), G_(2), pcg_->pressure64(), &tg, fluid,
                      wt_[0], wt_[1], wt_[2]);
   if (e) return err("project");
-  k_collider<T, 0><<<nblk(fsz_[0]), kT, 0, st>>>(G, h, G_(0), collider_);
-  k_collider<T, 1><<<nblk(fsz_[1]), kT, 0, st>>>(G, h, G_(1), collider_);
-  k_collider<T, 2><<<nblk(fsz_[2]), kT, 0, st>>>(G, h, G_(2), collider_);
+  launch_collider<T>(st, G, h, G_(0), G_(1), G_(2), collider_);
   // the particles are still in the order of this substep's sort
   if (n > 0)
     launch_g2p_tiles<T>(st, G, h, c_.flip ? c_.flip_alpha : -1.0, start_, cnt_, P, G_(0), G_(1), G_(2),

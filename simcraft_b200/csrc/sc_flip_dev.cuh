@@ -1952,6 +1952,41 @@ __global__ void __launch_bounds__(kT) k_collider(Geo G, double h, T* g, const do
   }
 }
 
+// applyCollider without a collider mesh: only the walls along AX change (to
+// zero), so the launch covers the two wall planes alone instead of the grid.
+template <class T, int AX>
+__global__ void __launch_bounds__(kT) k_collider_walls(Geo G, T* g) {
+  const int fx = G.fx(AX), fy = G.fy(AX), fz = G.fz(AX);
+  const int nu = AX == 0 ? fy : fx, nv = AX == 2 ? fy : fz;  // the plane across AX
+  const int qm = (AX == 0 ? fx : (AX == 1 ? fy : fz)) - 1;
+  const int64_t np = (int64_t)nu * nv;
+  GRID_LOOP(t, 2 * np) {
+    const int side = t >= np ? 1 : 0;
+    const int64_t r = t - side * np;
+    const int u = (int)(r / nv), v = (int)(r - (int64_t)u * nv);
+    const int q = side ? qm : 0;
+    const int a = AX == 0 ? q : u, b = AX == 0 ? u : (AX == 1 ? q : v), c = AX == 2 ? q : v;
+    g[lin(a, b, c, fy, fz)] = T(0);
+  }
+}
+// applyCollider on the three face grids (col: the collider SDF, or null for
+// the empty-mesh collider); returns the launches.
+template <class T>
+inline int launch_collider(cudaStream_t st, const Geo& G, double h, T* gu, T* gv, T* gw, const double* col) {
+  const int64_t fu = (int64_t)(G.nx + 1) * G.ny * G.nz, fv = (int64_t)G.nx * (G.ny + 1) * G.nz,
+                fw = (int64_t)G.nx * G.ny * (G.nz + 1);
+  if (col) {
+    k_collider<T, 0><<<nblk(fu), kT, 0, st>>>(G, h, gu, col);
+    k_collider<T, 1><<<nblk(fv), kT, 0, st>>>(G, h, gv, col);
+    k_collider<T, 2><<<nblk(fw), kT, 0, st>>>(G, h, gw, col);
+  } else {
+    k_collider_walls<T, 0><<<nblk(2 * (int64_t)G.ny * G.nz), kT, 0, st>>>(G, gu);
+    k_collider_walls<T, 1><<<nblk(2 * (int64_t)G.nx * G.nz), kT, 0, st>>>(G, gv);
+    k_collider_walls<T, 2><<<nblk(2 * (int64_t)G.nx * G.ny), kT, 0, st>>>(G, gw);
+  }
+  return 3;
+}
+
 // max |u| over a face grid (for CFL, fluid-simulator.cc:184-203).
 template <class T>
 __global__ void __launch_bounds__(kT) k_maxabs(int64_t n, const T* g, double* out) {

@@ -19,7 +19,9 @@ inline int blocks_for(int64_t n) {
 
 // Face weights (project-solver.cc:77-127): 1 - fractionInside(collider at the
 // four face corners); walls 0; faces between two air cells are left at 0.
-template <int AX>
+// COL: a collider SDF is given (without one the kernel is compiled apart from
+// the collider's sampling, a quarter of the registers).
+template <int AX, bool COL>
 __global__ void __launch_bounds__(kT)
     k_face_weights(int nx, int ny, int nz, double h, const double* __restrict__ fluid,
                    const double* __restrict__ collider, double* __restrict__ wt) {
@@ -38,7 +40,7 @@ __global__ void __launch_bounds__(kT)
       const int64_t hi = lin(i, j, k, ny, nz);
       if (fluid[lo] > 0.0 && fluid[hi] > 0.0) {
         out = 0.0;  // untouched by the reference: stays at its fill value 0
-      } else if (!collider) {
+      } else if (!COL || !collider) {
         out = 1.0 - 0.0;  // empty-mesh collider: all corners positive, fraction 0
       } else {
         // face centre (indexToCoord with the face offset), corners at +-h/2
@@ -271,9 +273,15 @@ int fvm_build_system(cudaStream_t st, int nx, int ny, int nz, double h, double d
                      double* uwt, double* vwt, double* wwt, const SystemOut& out) {
   const int64_t fu = (int64_t)(nx + 1) * ny * nz, fv = (int64_t)nx * (ny + 1) * nz,
                 fw = (int64_t)nx * ny * (nz + 1);
-  k_face_weights<0><<<blocks_for(fu), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, collider, uwt);
-  k_face_weights<1><<<blocks_for(fv), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, collider, vwt);
-  k_face_weights<2><<<blocks_for(fw), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, collider, wwt);
+  if (collider) {
+    k_face_weights<0, true><<<blocks_for(fu), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, collider, uwt);
+    k_face_weights<1, true><<<blocks_for(fv), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, collider, vwt);
+    k_face_weights<2, true><<<blocks_for(fw), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, collider, wwt);
+  } else {
+    k_face_weights<0, false><<<blocks_for(fu), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, nullptr, uwt);
+    k_face_weights<1, false><<<blocks_for(fv), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, nullptr, vwt);
+    k_face_weights<2, false><<<blocks_for(fw), kT, 0, st>>>(nx, ny, nz, h, fluid_sdf, nullptr, wwt);
+  }
   const int64_t n = (int64_t)nx * ny * nz;
   if (out.t_adiag)
     k_build_cells_tiled<T><<<blocks_for((int64_t)out.g.ntiles() * out.g.nz * kT), kT, 0, st>>>(

@@ -179,11 +179,14 @@ int FluidSim::set_collider(const double* sdf, bool device) {
 double FluidSim::cfl() {
   cudaStream_t st = ctx_->stream;
   cudaMemsetAsync(redbuf_, 0, sizeof(double), st);
+  // a few blocks per SM, each looping over the grid: one atomic per block (a
+  // block per 256 nodes queued ~65k atomics on the one word at 256^3)
   for (int a = 0; a < 3; a++) {
+    const int nb = std::min(nblk(fsz_[a]), 2048);
     if (c_.f32)
-      k_maxabs<float><<<nblk(fsz_[a]), kT, 0, st>>>(fsz_[a], (const float*)g_[a][gcur_[a]], redbuf_);
+      k_maxabs<float><<<nb, kT, 0, st>>>(fsz_[a], (const float*)g_[a][gcur_[a]], redbuf_);
     else
-      k_maxabs<double><<<nblk(fsz_[a]), kT, 0, st>>>(fsz_[a], (const double*)g_[a][gcur_[a]], redbuf_);
+      k_maxabs<double><<<nb, kT, 0, st>>>(fsz_[a], (const double*)g_[a][gcur_[a]], redbuf_);
   }
   launches_ += 3;
   cudaMemcpyAsync(host_red_, redbuf_, sizeof(double), cudaMemcpyDeviceToHost, st);
